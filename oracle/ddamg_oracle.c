@@ -1,0 +1,889 @@
+/*
+ * ddamg_oracle.c — CPU restatement of the reference DD-alphaAMG solve path.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker; see ddamg_oracle.h).  Every function
+ * cites the reference file:line it restates.  Arithmetic is written in the
+ * reference's order (loop nesting, accumulation order, complex operations) so
+ * that the restatement agrees with the reference to rounding; the fixtures in
+ * tests/golden/ pin that agreement.
+ *
+ * Layout: no halos (the reference's one-site halo is an MPI artefact); the
+ * periodic wrap that its halo exchange performs on one rank is index
+ * arithmetic here.
+ */
+#include "ddamg_oracle.h"
+
+#include <complex.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef double complex cplx;
+
+typedef struct {
+    int Nx, Nt, colors, dof, sites;
+    int ntest;          /* test vectors of this level (level < max) */
+    int agg_x, agg_t;   /* aggregation block counts */
+    int el_x, el_t;     /* sites per aggregate */
+    int sap_x, sap_t;   /* SAP block counts */
+    int sel_x, sel_t;   /* sites per SAP block */
+    cplx *G1, *G2, *G3; /* reference link layout, include/level.h:349-365 */
+    cplx* tvec;         /* [ntest][sites*dof] */
+} olevel;
+
+struct orc_mg {
+    int levels, maxLevel;
+    double m0;
+    int Nx, Nt;
+    cplx* U; /* [site][mu] */
+    olevel lv[ORC_MAX_LEVELS];
+    orc_constants k;
+};
+
+void orc_default_constants(orc_constants* c) {
+    /* src/variables.cpp:100-134 */
+    c->sap_gmres_m = 5;
+    c->sap_gmres_restarts = 5;
+    c->sap_gmres_tol = 1e-3;
+    c->sap_tv_iters = 4;
+    c->coarse_m = 400;
+    c->coarse_restarts = 10;
+    c->coarse_tol = 0.1;
+    c->nu1 = 0;
+    c->nu2 = 2;
+    c->kc_m = 5;
+    c->kc_restarts = 2;
+    c->kc_tol = 0.1;
+    c->smoother_tol = 1e-10;
+}
+
+static inline int mod(int a, int b) {
+    int r = a % b;
+    return r < 0 ? r + b : r;
+}
+static inline int G1i(const olevel* L, int n, int alf, int bet, int c, int b) {
+    int C = L->colors;
+    return (((n * 2 + alf) * 2 + bet) * C + c) * C + b;
+}
+static inline int G23i(const olevel* L, int n, int alf, int bet, int c, int b, int mu) {
+    int C = L->colors;
+    return ((((n * 2 + alf) * 2 + bet) * C + c) * C + b) * 2 + mu;
+}
+/* (x,t) + mu_hat, periodic; Level::rpb_l (include/level.h:411-422) after the halo wrap */
+static inline int nbr_fwd(int Nx, int Nt, int x, int t, int mu) {
+    return mu == 0 ? x * Nt + mod(t + 1, Nt) : mod(x + 1, Nx) * Nt + t;
+}
+static inline int nbr_bwd(int Nx, int Nt, int x, int t, int mu) {
+    return mu == 0 ? x * Nt + mod(t - 1, Nt) : mod(x - 1, Nx) * Nt + t;
+}
+/* antiperiodic t: Level::rsign_l / lsign_l (include/level.h:438-450) */
+static inline cplx rsign(int Nt, int t, int mu) { return (mu == 0 && t == Nt - 1) ? -1.0 : 1.0; }
+static inline cplx lsign(int t, int mu) { return (mu == 0 && t == 0) ? -1.0 : 1.0; }
+
+/* ------------------------------------------------------------------ RNG / inputs */
+static inline uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+uint64_t orc_rng(uint64_t seed, uint64_t stream, uint64_t counter) {
+    return mix64(mix64(seed ^ mix64(stream)) + counter);
+}
+static inline double u01(uint64_t r) { return (double)(r >> 11) * 0x1.0p-53; }
+
+#define PI_D 3.14159265358979323846
+static double plaq_angle(int Nx, int Nt, const double* th, int x, int t) {
+    /* theta_P(x,t) = th0(x,t) + th1(x,t+1) - th0(x+1,t) - th1(x,t) */
+    int n = x * Nt + t;
+    int ntp = x * Nt + mod(t + 1, Nt);
+    int nxp = mod(x + 1, Nx) * Nt + t;
+    return th[2 * n] + th[2 * ntp + 1] - th[2 * nxp] - th[2 * n + 1];
+}
+double orc_plaquette(int Nx, int Nt, const double* th) {
+    double s = 0;
+    for (int x = 0; x < Nx; x++)
+        for (int t = 0; t < Nt; t++) s += cos(plaq_angle(Nx, Nt, th, x, t));
+    return s / ((double)Nx * Nt);
+}
+/* Metropolis sweep order: 4 sub-sweeps (mu=0, x even / x odd; mu=1, t even / t odd); within a
+ * sub-sweep no two updated links share a plaquette, so the order inside it is immaterial and the
+ * GPU kernel that updates a whole sub-sweep at once produces the same chain. */
+double orc_metropolis(int Nx, int Nt, double beta, int sweeps, uint64_t seed, double delta, double* th) {
+    long V = (long)Nx * Nt;
+    for (long i = 0; i < 2 * V; i++) th[i] = -PI_D + 2.0 * PI_D * u01(orc_rng(seed, 0xC0FFEEull, (uint64_t)i));
+    double acc_rate = 0;
+    for (int sw = 0; sw < sweeps; sw++) {
+        long acc = 0;
+        for (int sub = 0; sub < 4; sub++) {
+            int mu = sub >> 1, par = sub & 1;
+            uint64_t sprop = ((uint64_t)sw * 4 + sub) * 2 + 1, sacc = sprop + 1;
+            for (int x = 0; x < Nx; x++)
+                for (int t = 0; t < Nt; t++) {
+                    if (((mu == 0) ? x : t) % 2 != par) continue;
+                    long n = (long)x * Nt + t;
+                    long li = 2 * n + mu;
+                    double d = delta * (2.0 * u01(orc_rng(seed, sprop, (uint64_t)li)) - 1.0);
+                    double p1, p2; /* the two plaquettes that contain the link */
+                    double s1, s2; /* orientation of the link in them */
+                    if (mu == 0) {
+                        p1 = plaq_angle(Nx, Nt, th, x, t);
+                        s1 = 1.0;
+                        p2 = plaq_angle(Nx, Nt, th, mod(x - 1, Nx), t);
+                        s2 = -1.0;
+                    } else {
+                        p1 = plaq_angle(Nx, Nt, th, x, t);
+                        s1 = -1.0;
+                        p2 = plaq_angle(Nx, Nt, th, x, mod(t - 1, Nt));
+                        s2 = 1.0;
+                    }
+                    double dS = -beta * (cos(p1 + s1 * d) + cos(p2 + s2 * d) - cos(p1) - cos(p2));
+                    double u = u01(orc_rng(seed, sacc, (uint64_t)li));
+                    if (dS <= 0.0 || u < exp(-dS)) {
+                        double v = th[li] + d;
+                        if (v >= PI_D) v -= 2.0 * PI_D;
+                        if (v < -PI_D) v += 2.0 * PI_D;
+                        th[li] = v;
+                        acc++;
+                    }
+                }
+        }
+        acc_rate = (double)acc / (2.0 * V);
+    }
+    return acc_rate;
+}
+void orc_gaussian(long n, uint64_t seed, double* out) {
+    for (long i = 0; i < n; i++) {
+        double u1 = u01(orc_rng(seed, 0x6A55ull, (uint64_t)(2 * i)));
+        double u2 = u01(orc_rng(seed, 0x6A55ull, (uint64_t)(2 * i + 1)));
+        double r = sqrt(-log(1.0 - u1)); /* E r^2 = 1 */
+        out[2 * i] = r * cos(2.0 * PI_D * u2);
+        out[2 * i + 1] = r * sin(2.0 * PI_D * u2);
+    }
+}
+void orc_uniform(long n, uint64_t seed, double* out) {
+    for (long i = 0; i < 2 * n; i++) out[i] = -1.0 + 2.0 * u01(orc_rng(seed, 0x7E57ull, (uint64_t)i));
+}
+/* src/io.cpp:32-44: per site (x slowest, then t) and mu: int32 x, t, mu, f64 re, im */
+int orc_write_binary(const char* path, int Nx, int Nt, const double* f) {
+    FILE* fp = fopen(path, "wb");
+    if (!fp) return -1;
+    for (int x = 0; x < Nx; x++)
+        for (int t = 0; t < Nt; t++)
+            for (int mu = 0; mu < 2; mu++) {
+                int32_t h[3] = {x, t, mu};
+                long i = ((long)x * Nt + t) * 2 + mu;
+                fwrite(h, 4, 3, fp);
+                fwrite(&f[2 * i], 8, 2, fp);
+            }
+    fclose(fp);
+    return 0;
+}
+int orc_read_binary(const char* path, int Nx, int Nt, double* f) {
+    FILE* fp = fopen(path, "rb");
+    if (!fp) return -1;
+    for (long i = 0; i < (long)Nx * Nt * 2; i++) {
+        int32_t h[3];
+        if (fread(h, 4, 3, fp) != 3 || fread(&f[2 * i], 8, 2, fp) != 2) {
+            fclose(fp);
+            return -2;
+        }
+    }
+    fclose(fp);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ hierarchy */
+static void make_dirac(orc_mg* mg) {
+    /* Level::makeDirac, src/level.cpp:286-331 */
+    olevel* L = &mg->lv[0];
+    cplx P[2][2][2], M[2][2][2];
+    P[0][0][0] = 1.0; P[0][0][1] = 1.0; P[0][1][0] = 1.0; P[0][1][1] = 1.0;
+    P[1][0][0] = 1.0; P[1][0][1] = -I;  P[1][1][0] = I;   P[1][1][1] = 1.0;
+    M[0][0][0] = 1.0; M[0][0][1] = -1.0; M[0][1][0] = -1.0; M[0][1][1] = 1.0;
+    M[1][0][0] = 1.0; M[1][0][1] = I;    M[1][1][0] = -I;   M[1][1][1] = 1.0;
+    for (int x = 0; x < L->Nx; x++)
+        for (int t = 0; t < L->Nt; t++) {
+            int n = x * L->Nt + t;
+            for (int alf = 0; alf < 2; alf++)
+                for (int bet = 0; bet < 2; bet++) {
+                    L->G1[G1i(L, n, alf, bet, 0, 0)] = 0;
+                    for (int mu = 0; mu < 2; mu++) {
+                        int nb = nbr_bwd(L->Nx, L->Nt, x, t, mu);
+                        L->G2[G23i(L, n, alf, bet, 0, 0, mu)] = 0.5 * M[mu][alf][bet] * mg->U[2 * n + mu];
+                        L->G3[G23i(L, n, alf, bet, 0, 0, mu)] = 0.5 * P[mu][alf][bet] * conj(mg->U[2 * nb + mu]);
+                    }
+                }
+        }
+}
+
+orc_mg* orc_create(int levels, double m0, int Nx, int Nt, const int* rows, const double* U, const orc_constants* c) {
+    if (levels < 2 || levels > ORC_MAX_LEVELS) return NULL;
+    orc_mg* mg = (orc_mg*)calloc(1, sizeof(orc_mg));
+    mg->levels = levels;
+    mg->maxLevel = levels - 1;
+    mg->m0 = m0;
+    mg->Nx = Nx;
+    mg->Nt = Nt;
+    if (c) mg->k = *c;
+    else orc_default_constants(&mg->k);
+    mg->U = (cplx*)malloc(sizeof(cplx) * 2 * Nx * Nt);
+    memcpy(mg->U, U, sizeof(cplx) * 2 * Nx * Nt);
+    /* include/params.h:34-69 */
+    for (int l = 0; l < levels; l++) {
+        olevel* L = &mg->lv[l];
+        if (l == 0) {
+            L->Nx = Nx; L->Nt = Nt; L->colors = 1;
+        } else {
+            const int* pr = rows + 6 * (l - 1);
+            L->Nx = pr[1]; L->Nt = pr[2]; L->colors = pr[3];
+        }
+        L->dof = 2 * L->colors;
+        L->sites = L->Nx * L->Nt;
+        if (l < levels - 1) {
+            const int* r = rows + 6 * l;
+            L->agg_x = r[1]; L->agg_t = r[2]; L->ntest = r[3]; L->sap_x = r[4]; L->sap_t = r[5];
+            L->el_x = L->Nx / L->agg_x; L->el_t = L->Nt / L->agg_t;
+            L->sel_x = L->Nx / L->sap_x; L->sel_t = L->Nt / L->sap_t;
+            L->tvec = (cplx*)calloc((size_t)L->ntest * L->sites * L->dof, sizeof(cplx));
+        } else {
+            L->ntest = 1;
+        }
+        size_t nl = (size_t)L->sites * 4 * L->colors * L->colors;
+        L->G1 = (cplx*)calloc(nl, sizeof(cplx));
+        L->G2 = (cplx*)calloc(2 * nl, sizeof(cplx));
+        L->G3 = (cplx*)calloc(2 * nl, sizeof(cplx));
+    }
+    make_dirac(mg);
+    return mg;
+}
+void orc_destroy(orc_mg* mg) {
+    if (!mg) return;
+    for (int l = 0; l < mg->levels; l++) {
+        free(mg->lv[l].G1); free(mg->lv[l].G2); free(mg->lv[l].G3); free(mg->lv[l].tvec);
+    }
+    free(mg->U);
+    free(mg);
+}
+int orc_level_sites(const orc_mg* mg, int l) { return mg->lv[l].sites; }
+int orc_level_dof(const orc_mg* mg, int l) { return mg->lv[l].dof; }
+int orc_level_ntest(const orc_mg* mg, int l) { return mg->lv[l].ntest; }
+
+/* ------------------------------------------------------------------ operators */
+/* D_phi / D_dagger_phi, src/dirac_operator.cpp:24-85 */
+void orc_dirac(const orc_mg* mg, int dagger, const double* inp, double* outp) {
+    const cplx* phi = (const cplx*)inp;
+    cplx* out = (cplx*)outp;
+    const cplx* U = mg->U;
+    int Nx = mg->Nx, Nt = mg->Nt;
+    double m0 = mg->m0;
+    for (int x = 0; x < Nx; x++)
+        for (int t = 0; t < Nt; t++) {
+            int n = x * Nt + t;
+            int r0 = nbr_fwd(Nx, Nt, x, t, 0), r1 = nbr_fwd(Nx, Nt, x, t, 1);
+            int l0 = nbr_bwd(Nx, Nt, x, t, 0), l1 = nbr_bwd(Nx, Nt, x, t, 1);
+            cplx rs0 = rsign(Nt, t, 0), ls0 = lsign(t, 0), rs1 = 1.0, ls1 = 1.0;
+            if (!dagger) {
+                out[2 * n] = (m0 + 2) * phi[2 * n] -
+                             0.5 * (U[2 * n] * rs0 * (phi[2 * r0] - phi[2 * r0 + 1]) +
+                                    U[2 * n + 1] * rs1 * (phi[2 * r1] + I * phi[2 * r1 + 1]) +
+                                    conj(U[2 * l0]) * ls0 * (phi[2 * l0] + phi[2 * l0 + 1]) +
+                                    conj(U[2 * l1 + 1]) * ls1 * (phi[2 * l1] - I * phi[2 * l1 + 1]));
+                out[2 * n + 1] = (m0 + 2) * phi[2 * n + 1] -
+                                 0.5 * (U[2 * n] * rs0 * (-phi[2 * r0] + phi[2 * r0 + 1]) +
+                                        U[2 * n + 1] * rs1 * (-I * phi[2 * r1] + phi[2 * r1 + 1]) +
+                                        conj(U[2 * l0]) * ls0 * (phi[2 * l0] + phi[2 * l0 + 1]) +
+                                        conj(U[2 * l1 + 1]) * ls1 * (I * phi[2 * l1] + phi[2 * l1 + 1]));
+            } else {
+                out[2 * n] = (m0 + 2) * phi[2 * n] -
+                             0.5 * (conj(U[2 * l0]) * ls0 * (phi[2 * l0] - phi[2 * l0 + 1]) +
+                                    conj(U[2 * l1 + 1]) * ls1 * (phi[2 * l1] + I * phi[2 * l1 + 1]) +
+                                    U[2 * n] * rs0 * (phi[2 * r0] + phi[2 * r0 + 1]) +
+                                    U[2 * n + 1] * rs1 * (phi[2 * r1] - I * phi[2 * r1 + 1]));
+                out[2 * n + 1] = (m0 + 2) * phi[2 * n + 1] -
+                                 0.5 * (conj(U[2 * l0]) * ls0 * (-phi[2 * l0] + phi[2 * l0 + 1]) +
+                                        conj(U[2 * l1 + 1]) * ls1 * (-I * phi[2 * l1] + phi[2 * l1 + 1]) +
+                                        U[2 * n] * rs0 * (phi[2 * r0] + phi[2 * r0 + 1]) +
+                                        U[2 * n + 1] * rs1 * (I * phi[2 * r1] + phi[2 * r1 + 1]));
+            }
+        }
+}
+
+/* Level::D_operator, src/level.cpp:394-426 */
+static void level_op(const orc_mg* mg, int l, const cplx* v, cplx* out) {
+    const olevel* L = &mg->lv[l];
+    int C = L->colors, Nx = L->Nx, Nt = L->Nt;
+    for (int x = 0; x < Nx; x++)
+        for (int t = 0; t < Nt; t++) {
+            int n = x * Nt + t;
+            int rp[2] = {nbr_fwd(Nx, Nt, x, t, 0), nbr_fwd(Nx, Nt, x, t, 1)};
+            int lp[2] = {nbr_bwd(Nx, Nt, x, t, 0), nbr_bwd(Nx, Nt, x, t, 1)};
+            for (int alf = 0; alf < 2; alf++)
+                for (int c = 0; c < C; c++) {
+                    int i = n * C * 2 + c * 2 + alf;
+                    out[i] = (mg->m0 + 2) * v[i];
+                    for (int bet = 0; bet < 2; bet++)
+                        for (int b = 0; b < C; b++) {
+                            out[i] -= L->G1[G1i(L, n, alf, bet, c, b)] * v[n * C * 2 + b * 2 + bet];
+                            for (int mu = 0; mu < 2; mu++) {
+                                out[i] -= (L->G2[G23i(L, n, alf, bet, c, b, mu)] * rsign(Nt, t, mu) *
+                                               v[rp[mu] * C * 2 + b * 2 + bet] +
+                                           L->G3[G23i(L, n, alf, bet, c, b, mu)] * lsign(t, mu) *
+                                               v[lp[mu] * C * 2 + b * 2 + bet]);
+                            }
+                        }
+                }
+        }
+}
+void orc_level_op(const orc_mg* mg, int l, const double* in, double* out) {
+    level_op(mg, l, (const cplx*)in, (cplx*)out);
+}
+
+/* Level::P_vc, src/level.cpp:92-141 */
+static void prolong(const orc_mg* mg, int l, const cplx* vc, cplx* out) {
+    const olevel* L = &mg->lv[l];
+    int C = L->colors, Nt = L->Nt, Ntest = L->ntest, BT = L->agg_t;
+    memset(out, 0, sizeof(cplx) * L->sites * L->dof);
+    for (int b = 0; b < L->agg_x * L->agg_t; b++) {
+        int bx = b / BT, bt = b % BT;
+        for (int cc = 0; cc < Ntest; cc++)
+            for (int x = bx * L->el_x; x < (bx + 1) * L->el_x; x++)
+                for (int t = bt * L->el_t; t < (bt + 1) * L->el_t; t++)
+                    for (int c = 0; c < C; c++)
+                        for (int s = 0; s < 2; s++) {
+                            int io = (x * Nt + t) * C * 2 + c * 2 + s;
+                            out[io] += L->tvec[(size_t)cc * L->sites * L->dof + io] * vc[b * Ntest * 2 + cc * 2 + s];
+                        }
+    }
+}
+void orc_prolong(const orc_mg* mg, int l, const double* in, double* out) {
+    prolong(mg, l, (const cplx*)in, (cplx*)out);
+}
+
+/* Level::Pdagg_v, src/level.cpp:145-189 */
+static void restrict_(const orc_mg* mg, int l, const cplx* v, cplx* out) {
+    const olevel* L = &mg->lv[l];
+    int C = L->colors, Nt = L->Nt, Ntest = L->ntest, BT = L->agg_t;
+    int nb = L->agg_x * L->agg_t;
+    memset(out, 0, sizeof(cplx) * nb * Ntest * 2);
+    for (int b = 0; b < nb; b++) {
+        int bx = b / BT, bt = b % BT;
+        for (int cc = 0; cc < Ntest; cc++)
+            for (int x = bx * L->el_x; x < (bx + 1) * L->el_x; x++)
+                for (int t = bt * L->el_t; t < (bt + 1) * L->el_t; t++)
+                    for (int c = 0; c < C; c++)
+                        for (int s = 0; s < 2; s++) {
+                            int iv = (x * Nt + t) * C * 2 + c * 2 + s;
+                            out[b * Ntest * 2 + cc * 2 + s] +=
+                                conj(L->tvec[(size_t)cc * L->sites * L->dof + iv]) * v[iv];
+                        }
+    }
+}
+void orc_restrict(const orc_mg* mg, int l, const double* in, double* out) {
+    restrict_(mg, l, (const cplx*)in, (cplx*)out);
+}
+
+void orc_set_tvec(orc_mg* mg, int l, const double* tv) {
+    olevel* L = &mg->lv[l];
+    memcpy(L->tvec, tv, sizeof(cplx) * L->ntest * L->sites * L->dof);
+}
+void orc_get_tvec(const orc_mg* mg, int l, double* tv) {
+    const olevel* L = &mg->lv[l];
+    memcpy(tv, L->tvec, sizeof(cplx) * L->ntest * L->sites * L->dof);
+}
+
+/* Level::orthonormalize, src/level.cpp:193-284 (per aggregate = block x spin, modified Gram-Schmidt) */
+void orc_orthonormalize(orc_mg* mg, int l) {
+    olevel* L = &mg->lv[l];
+    int C = L->colors, Nt = L->Nt, BT = L->agg_t;
+    size_t vs = (size_t)L->sites * L->dof;
+    for (int b = 0; b < L->agg_x * L->agg_t; b++) {
+        int bx = b / BT, bt = b % BT;
+        int x0 = bx * L->el_x, x1 = x0 + L->el_x, t0 = bt * L->el_t, t1 = t0 + L->el_t;
+        for (int s = 0; s < 2; s++)
+            for (int nt = 0; nt < L->ntest; nt++) {
+                cplx* w = L->tvec + nt * vs;
+                for (int ntt = 0; ntt < nt; ntt++) {
+                    const cplx* u = L->tvec + ntt * vs;
+                    cplx proj = 0;
+                    for (int x = x0; x < x1; x++)
+                        for (int t = t0; t < t1; t++)
+                            for (int c = 0; c < C; c++) {
+                                int i = (x * Nt + t) * C * 2 + c * 2 + s;
+                                proj += w[i] * conj(u[i]);
+                            }
+                    for (int x = x0; x < x1; x++)
+                        for (int t = t0; t < t1; t++)
+                            for (int c = 0; c < C; c++) {
+                                int i = (x * Nt + t) * C * 2 + c * 2 + s;
+                                w[i] -= proj * u[i];
+                            }
+                }
+                cplx nrm = 0;
+                for (int x = x0; x < x1; x++)
+                    for (int t = t0; t < t1; t++)
+                        for (int c = 0; c < C; c++) {
+                            int i = (x * Nt + t) * C * 2 + c * 2 + s;
+                            nrm += w[i] * conj(w[i]);
+                        }
+                double nr = sqrt(creal(nrm));
+                if (fabs(nr) > 1e-8)
+                    for (int x = x0; x < x1; x++)
+                        for (int t = t0; t < t1; t++)
+                            for (int c = 0; c < C; c++) {
+                                int i = (x * Nt + t) * C * 2 + c * 2 + s;
+                                w[i] = CMPLX(creal(w[i]) / nr, cimag(w[i]) / nr);
+                            }
+            }
+    }
+}
+
+/* Level::makeCoarseLinks, src/level.cpp:431-542.
+ * A hop n -> n +/- mu that leaves the aggregate (by local coordinate) feeds B_mu / C_mu, as the
+ * reference's getLatticeBlock test does for aggregates of >= 2 sites per direction (with one site
+ * per direction the reference drops the C links of the first block row: src/level.cpp getLatticeBlock
+ * computes block -1 for the halo, include/level.h:389-408). */
+void orc_make_coarse_links(orc_mg* mg, int l) {
+    olevel* L = &mg->lv[l];
+    olevel* N = &mg->lv[l + 1];
+    int C = L->colors, Nt = L->Nt, Nx = L->Nx, Ntest = L->ntest, BT = L->agg_t;
+    size_t vs = (size_t)L->sites * L->dof;
+    const cplx* w = L->tvec;
+    for (int blk = 0; blk < L->agg_x * L->agg_t; blk++) {
+        int bx = blk / BT, bt = blk % BT;
+        int x0 = bx * L->el_x, x1 = x0 + L->el_x, t0 = bt * L->el_t, t1 = t0 + L->el_t;
+        for (int alf = 0; alf < 2; alf++)
+            for (int bet = 0; bet < 2; bet++)
+                for (int p = 0; p < Ntest; p++)
+                    for (int s = 0; s < Ntest; s++) {
+                        int iA = G1i(N, blk, alf, bet, p, s);
+                        int iB0 = G23i(N, blk, alf, bet, p, s, 0), iB1 = G23i(N, blk, alf, bet, p, s, 1);
+                        cplx A = 0, B[2] = {0, 0}, Cc[2] = {0, 0};
+                        for (int x = x0; x < x1; x++)
+                            for (int t = t0; t < t1; t++) {
+                                int n = x * Nt + t;
+                                for (int c = 0; c < C; c++)
+                                    for (int b = 0; b < C; b++) {
+                                        int idx = n * C * 2 + c * 2 + alf;
+                                        A += conj(w[p * vs + idx]) * L->G1[G1i(L, n, alf, bet, c, b)] *
+                                             w[s * vs + n * C * 2 + b * 2 + bet];
+                                        for (int mu = 0; mu < 2; mu++) {
+                                            int rn = nbr_fwd(Nx, Nt, x, t, mu), ln = nbr_bwd(Nx, Nt, x, t, mu);
+                                            int rin = (mu == 0) ? (t + 1 < t1) : (x + 1 < x1);
+                                            int lin = (mu == 0) ? (t - 1 >= t0) : (x - 1 >= x0);
+                                            cplx wG2 = conj(w[p * vs + idx]) * L->G2[G23i(L, n, alf, bet, c, b, mu)];
+                                            cplx wG3 = conj(w[p * vs + idx]) * L->G3[G23i(L, n, alf, bet, c, b, mu)];
+                                            if (rin) A += wG2 * w[s * vs + rn * C * 2 + b * 2 + bet];
+                                            else B[mu] += wG2 * w[s * vs + rn * C * 2 + b * 2 + bet];
+                                            if (lin) A += wG3 * w[s * vs + ln * C * 2 + b * 2 + bet];
+                                            else Cc[mu] += wG3 * w[s * vs + ln * C * 2 + b * 2 + bet];
+                                        }
+                                    }
+                            }
+                        N->G1[iA] = A;
+                        N->G2[iB0] = B[0];
+                        N->G2[iB1] = B[1];
+                        N->G3[iB0] = Cc[0];
+                        N->G3[iB1] = Cc[1];
+                    }
+    }
+}
+
+void orc_get_links(const orc_mg* mg, int l, int which, double* out) {
+    const olevel* L = &mg->lv[l];
+    size_t n = (size_t)L->sites * 4 * L->colors * L->colors;
+    if (which == 1) memcpy(out, L->G1, n * sizeof(cplx));
+    else memcpy(out, which == 2 ? L->G2 : L->G3, 2 * n * sizeof(cplx));
+}
+void orc_set_links(orc_mg* mg, int l, int which, const double* in) {
+    olevel* L = &mg->lv[l];
+    size_t n = (size_t)L->sites * 4 * L->colors * L->colors;
+    if (which == 1) memcpy(L->G1, in, n * sizeof(cplx));
+    else memcpy(which == 2 ? L->G2 : L->G3, in, 2 * n * sizeof(cplx));
+}
+
+/* ------------------------------------------------------------------ FGMRES */
+/* FGMRES::fgmres, src/fgmres.cpp:5-97, with rotation (:99-115) and
+ * solve_upper_triangular (:118-128).  Quirk kept: maxIt is not reset between restarts. */
+typedef void (*op_fn)(const void* ctx, const cplx* in, cplx* out);
+typedef void (*prec_fn)(const void* ctx, const cplx* in, cplx* out); /* out is in/out (stale Z_j) */
+
+static cplx vdot(const cplx* a, const cplx* b, long n) {
+    cplx z = 0;
+    for (long i = 0; i < n; i++) z += a[i] * conj(b[i]);
+    return z;
+}
+
+static int fgmres(long n, int m, int restarts, double tol, op_fn A, const void* actx, prec_fn Mp,
+                  const void* mctx, const cplx* phi, const cplx* x0, cplx* x) {
+    cplx* V = (cplx*)calloc((size_t)(m + 1) * n, sizeof(cplx));
+    cplx* Z = (cplx*)calloc((size_t)m * n, sizeof(cplx));
+    cplx* r = (cplx*)calloc(n, sizeof(cplx));
+    cplx* w = (cplx*)calloc(n, sizeof(cplx));
+    cplx* Dx = (cplx*)calloc(n, sizeof(cplx));
+    cplx* H = (cplx*)calloc((size_t)(m + 1) * m, sizeof(cplx));
+    cplx* gm = (cplx*)calloc(m + 1, sizeof(cplx));
+    cplx* sn = (cplx*)calloc(m, sizeof(cplx));
+    cplx* cn = (cplx*)calloc(m, sizeof(cplx));
+    cplx* eta = (cplx*)calloc(m, sizeof(cplx));
+#define HH(i, j) H[(size_t)(i) * m + (j)]
+    int k = 0, ret = restarts * m;
+    memcpy(x, x0, sizeof(cplx) * n);
+    A(actx, x, Dx);
+    for (long i = 0; i < n; i++) r[i] = phi[i] + Dx[i] * (cplx)(-1.0);
+    double norm_phi = sqrt(creal(vdot(phi, phi, n)));
+    double err = sqrt(creal(vdot(r, r, n)));
+    int maxIt = m;
+    while (k < restarts) {
+        cplx beta = err;
+        cplx ib = 1.0 / beta;
+        for (long i = 0; i < n; i++) V[i] = ib * r[i];
+        gm[0] = beta;
+        for (int j = 0; j < m; j++) {
+            if (Mp) Mp(mctx, V + (size_t)j * n, Z + (size_t)j * n);
+            else memcpy(Z + (size_t)j * n, V + (size_t)j * n, sizeof(cplx) * n);
+            A(actx, Z + (size_t)j * n, w);
+            for (int i = 0; i <= j; i++) {
+                HH(i, j) = vdot(w, V + (size_t)i * n, n);
+                const cplx* vi = V + (size_t)i * n;
+                cplx h = HH(i, j);
+                for (long q = 0; q < n; q++) w[q] -= h * vi[q];
+            }
+            HH(j + 1, j) = sqrt(creal(vdot(w, w, n)));
+            if (creal(HH(j + 1, j)) > 0) {
+                cplx ih = 1.0 / HH(j + 1, j);
+                cplx* vn = V + (size_t)(j + 1) * n;
+                for (long q = 0; q < n; q++) vn[q] = ih * w[q];
+            }
+            /* rotation(j) */
+            for (int i = 0; i < j; i++) {
+                cplx temp = conj(cn[i]) * HH(i, j) + conj(sn[i]) * HH(i + 1, j);
+                HH(i + 1, j) = -sn[i] * HH(i, j) + cn[i] * HH(i + 1, j);
+                HH(i, j) = temp;
+            }
+            cplx den = sqrt(creal(conj(HH(j, j)) * HH(j, j) + conj(HH(j + 1, j)) * HH(j + 1, j)));
+            sn[j] = HH(j + 1, j) / den;
+            cn[j] = HH(j, j) / den;
+            HH(j, j) = conj(cn[j]) * HH(j, j) + conj(sn[j]) * HH(j + 1, j);
+            HH(j + 1, j) = 0.0;
+            gm[j + 1] = -sn[j] * gm[j];
+            gm[j] = conj(cn[j]) * gm[j];
+            if (cabs(gm[j + 1]) < tol * norm_phi) {
+                maxIt = j + 1;
+                break;
+            }
+        }
+        for (int i = maxIt - 1; i >= 0; i--) {
+            eta[i] = gm[i];
+            for (int j = i + 1; j < maxIt; j++) eta[i] -= HH(i, j) * eta[j];
+            eta[i] /= HH(i, i);
+        }
+        for (long q = 0; q < n; q++)
+            for (int j = 0; j < maxIt; j++) x[q] = x[q] + eta[j] * Z[(size_t)j * n + q];
+        A(actx, x, Dx);
+        for (long i = 0; i < n; i++) r[i] = phi[i] + Dx[i] * (cplx)(-1.0);
+        err = sqrt(creal(vdot(r, r, n)));
+        if (err < tol * norm_phi) {
+            ret = k * m + maxIt;
+            break;
+        }
+        k++;
+    }
+#undef HH
+    free(V); free(Z); free(r); free(w); free(Dx); free(H); free(gm); free(sn); free(cn); free(eta);
+    return ret;
+}
+
+/* ------------------------------------------------------------------ SAP */
+typedef struct {
+    const orc_mg* mg;
+    int l, block;
+} blkctx;
+
+/* Level::SAP_level_l::D_local, src/level.cpp:607-653: the level operator restricted to one SAP
+ * block, neighbours outside the block read as zero, no boundary sign. Block vectors are
+ * [local site][dof], local site = lx*sel_t + lt. */
+static void d_local(const void* vctx, const cplx* in, cplx* out) {
+    const blkctx* bc = (const blkctx*)vctx;
+    const orc_mg* mg = bc->mg;
+    const olevel* L = &mg->lv[bc->l];
+    int C = L->colors, ex = L->sel_x, et = L->sel_t;
+    int bx = bc->block / L->sap_t, bt = bc->block % L->sap_t;
+    for (int mx = 0; mx < ex; mx++)
+        for (int mt = 0; mt < et; mt++) {
+            int m = mx * et + mt;
+            int n = (bx * ex + mx) * L->Nt + (bt * et + mt);
+            int rp[2] = {(mt + 1 < et) ? mx * et + mt + 1 : -1, (mx + 1 < ex) ? (mx + 1) * et + mt : -1};
+            int lp[2] = {(mt - 1 >= 0) ? mx * et + mt - 1 : -1, (mx - 1 >= 0) ? (mx - 1) * et + mt : -1};
+            for (int alf = 0; alf < 2; alf++)
+                for (int c = 0; c < C; c++) {
+                    int i = m * C * 2 + c * 2 + alf;
+                    out[i] = (mg->m0 + 2) * in[i];
+                    for (int bet = 0; bet < 2; bet++)
+                        for (int b = 0; b < C; b++) {
+                            out[i] -= L->G1[G1i(L, n, alf, bet, c, b)] * in[m * C * 2 + b * 2 + bet];
+                            for (int mu = 0; mu < 2; mu++) {
+                                cplx vr = rp[mu] >= 0 ? in[rp[mu] * C * 2 + b * 2 + bet] : 0;
+                                cplx vl = lp[mu] >= 0 ? in[lp[mu] * C * 2 + b * 2 + bet] : 0;
+                                out[i] -= (L->G2[G23i(L, n, alf, bet, c, b, mu)] * vr +
+                                           L->G3[G23i(L, n, alf, bet, c, b, mu)] * vl);
+                            }
+                        }
+                }
+        }
+}
+
+static void op_level(const void* vctx, const cplx* in, cplx* out) {
+    const blkctx* bc = (const blkctx*)vctx;
+    level_op(bc->mg, bc->l, in, out);
+}
+
+/* red iff (bx + bt) even: SAP_C::SchwarzBlocks, src/sap.cpp:27-38 */
+static int block_is_red(const olevel* L, int block) {
+    int bx = block / L->sap_t, bt = block % L->sap_t;
+    return ((bx + bt) % 2) == 0;
+}
+
+/* one colour sweep: x += I_B D_B^-1 I_B^T r over the blocks of that colour (src/sap.cpp:48-77,104-139) */
+static void sap_colour(const orc_mg* mg, int l, int red, const cplx* r, cplx* x) {
+    const olevel* L = &mg->lv[l];
+    int nb = L->sap_x * L->sap_t;
+    int ex = L->sel_x, et = L->sel_t, dof = L->dof;
+    long nv = (long)ex * et * dof;
+    cplx* rb = (cplx*)malloc(sizeof(cplx) * nv);
+    cplx* eb = (cplx*)malloc(sizeof(cplx) * nv);
+    for (int blk = 0; blk < nb; blk++) {
+        int is_red = block_is_red(L, blk);
+        if (nb == 1) is_red = 1; /* single block: RedBlocks = BlackBlocks = {0} (src/sap.cpp:329,342-343) */
+        if (nb > 1 && is_red != red) continue;
+        int bx = blk / L->sap_t, bt = blk % L->sap_t;
+        for (int mx = 0; mx < ex; mx++)
+            for (int mt = 0; mt < et; mt++)
+                for (int d = 0; d < dof; d++)
+                    rb[(mx * et + mt) * dof + d] = r[((bx * ex + mx) * L->Nt + bt * et + mt) * dof + d];
+        blkctx bc = {mg, l, blk};
+        fgmres(nv, mg->k.sap_gmres_m, mg->k.sap_gmres_restarts, mg->k.sap_gmres_tol, d_local, &bc, NULL, NULL, rb,
+               rb, eb);
+        for (int mx = 0; mx < ex; mx++)
+            for (int mt = 0; mt < et; mt++)
+                for (int d = 0; d < dof; d++)
+                    x[((bx * ex + mx) * L->Nt + bt * et + mt) * dof + d] += eb[(mx * et + mt) * dof + d];
+    }
+    free(rb);
+    free(eb);
+}
+
+/* SAP_C::SAP, src/sap.cpp:81-165 */
+static int sap(const orc_mg* mg, int l, const cplx* v, cplx* x, int nu, double tol) {
+    const olevel* L = &mg->lv[l];
+    long n = (long)L->sites * L->dof;
+    cplx* r = (cplx*)malloc(sizeof(cplx) * n);
+    cplx* Dx = (cplx*)malloc(sizeof(cplx) * n);
+    double v_norm = sqrt(creal(vdot(v, v, n)));
+    int ret = nu;
+    level_op(mg, l, x, Dx);
+    for (long i = 0; i < n; i++) r[i] = v[i] - Dx[i];
+    for (int it = 0; it < nu; it++) {
+        sap_colour(mg, l, 1, r, x);
+        level_op(mg, l, x, Dx);
+        for (long i = 0; i < n; i++) r[i] = v[i] - Dx[i];
+        sap_colour(mg, l, 0, r, x);
+        level_op(mg, l, x, Dx);
+        for (long i = 0; i < n; i++) r[i] = v[i] - Dx[i];
+        double err = sqrt(creal(vdot(r, r, n)));
+        if (err < tol * v_norm) {
+            ret = it;
+            break;
+        }
+    }
+    free(r);
+    free(Dx);
+    return ret;
+}
+int orc_sap(const orc_mg* mg, int l, const double* v, double* x, int nu, double tol) {
+    return sap(mg, l, (const cplx*)v, (cplx*)x, nu, tol);
+}
+
+/* ------------------------------------------------------------------ cycles */
+/* coarsest solve: Level::GMRES_level_l (include/level.h:70-140), x0 = rhs (src/amg.cpp:69) */
+static int coarse_gmres(const orc_mg* mg, const cplx* b, cplx* x) {
+    const olevel* L = &mg->lv[mg->maxLevel];
+    blkctx bc = {mg, mg->maxLevel, 0};
+    return fgmres((long)L->sites * L->dof, mg->k.coarse_m, mg->k.coarse_restarts, mg->k.coarse_tol, op_level, &bc,
+                  NULL, NULL, b, b, x);
+}
+int orc_coarse_gmres(const orc_mg* mg, const double* b, double* x) {
+    return coarse_gmres(mg, (const cplx*)b, (cplx*)x);
+}
+
+static void vcycle(const orc_mg* mg, int l, const cplx* eta, cplx* psi);
+static void kcycle(const orc_mg* mg, int l, const cplx* eta, cplx* psi);
+
+/* AlgebraicMG::v_cycle, src/amg.cpp:64-116 */
+static void vcycle(const orc_mg* mg, int l, const cplx* eta, cplx* psi) {
+    if (l == mg->maxLevel) {
+        coarse_gmres(mg, eta, psi);
+        return;
+    }
+    const olevel* L = &mg->lv[l];
+    const olevel* N = &mg->lv[l + 1];
+    long n = (long)L->sites * L->dof, nc = (long)N->sites * N->dof;
+    cplx* Dpsi = (cplx*)calloc(n, sizeof(cplx));
+    cplx* r = (cplx*)calloc(n, sizeof(cplx));
+    cplx* e1 = (cplx*)calloc(nc, sizeof(cplx));
+    cplx* p1 = (cplx*)calloc(nc, sizeof(cplx));
+    if (mg->k.nu1 > 0) sap(mg, l, eta, psi, mg->k.nu1, mg->k.smoother_tol);
+    level_op(mg, l, psi, Dpsi);
+    for (long i = 0; i < n; i++) r[i] = eta[i] - Dpsi[i];
+    restrict_(mg, l, r, e1);
+    vcycle(mg, l + 1, e1, p1);
+    prolong(mg, l, p1, Dpsi);
+    for (long i = 0; i < n; i++) psi[i] += Dpsi[i];
+    if (mg->k.nu2 > 0) sap(mg, l, eta, psi, mg->k.nu2, mg->k.smoother_tol);
+    free(Dpsi); free(r); free(e1); free(p1);
+}
+
+typedef struct {
+    const orc_mg* mg;
+    int l;
+} kctx;
+static void kc_prec(const void* v, const cplx* in, cplx* out) {
+    const kctx* c = (const kctx*)v;
+    kcycle(c->mg, c->l, in, out);
+}
+
+/* AlgebraicMG::k_cycle, src/amg.cpp:119-174, with FGMRES_k_cycle (include/amg.h:16-94) */
+static void kcycle(const orc_mg* mg, int l, const cplx* eta, cplx* psi) {
+    if (l == mg->maxLevel) {
+        coarse_gmres(mg, eta, psi);
+        return;
+    }
+    const olevel* L = &mg->lv[l];
+    const olevel* N = &mg->lv[l + 1];
+    long n = (long)L->sites * L->dof, nc = (long)N->sites * N->dof;
+    cplx* Dpsi = (cplx*)calloc(n, sizeof(cplx));
+    cplx* r = (cplx*)calloc(n, sizeof(cplx));
+    cplx* e1 = (cplx*)calloc(nc, sizeof(cplx));
+    cplx* p1 = (cplx*)calloc(nc, sizeof(cplx));
+    if (mg->k.nu1 > 0) sap(mg, l, eta, psi, mg->k.nu1, mg->k.smoother_tol);
+    level_op(mg, l, psi, Dpsi);
+    for (long i = 0; i < n; i++) r[i] = eta[i] - Dpsi[i];
+    restrict_(mg, l, r, e1);
+    blkctx bc = {mg, l + 1, 0};
+    kctx kc = {mg, l + 1};
+    fgmres(nc, mg->k.kc_m, mg->k.kc_restarts, mg->k.kc_tol, op_level, &bc, kc_prec, &kc, e1, e1, p1);
+    prolong(mg, l, p1, Dpsi);
+    for (long i = 0; i < n; i++) psi[i] += Dpsi[i];
+    if (mg->k.nu2 > 0) sap(mg, l, eta, psi, mg->k.nu2, mg->k.smoother_tol);
+    free(Dpsi); free(r); free(e1); free(p1);
+}
+void orc_vcycle(const orc_mg* mg, const double* eta, double* psi) { vcycle(mg, 0, (const cplx*)eta, (cplx*)psi); }
+void orc_kcycle(const orc_mg* mg, const double* eta, double* psi) { kcycle(mg, 0, (const cplx*)eta, (cplx*)psi); }
+
+/* ------------------------------------------------------------------ setup */
+long orc_setup_random_count(const orc_mg* mg) {
+    long n = (long)mg->lv[0].ntest * mg->lv[0].sites * mg->lv[0].dof;
+    for (int l = 1; l < mg->levels - 1; l++) {
+        int extra = mg->lv[l].ntest - mg->lv[l - 1].ntest;
+        if (extra > 0) n += (long)extra * mg->lv[l].sites * mg->lv[l].dof;
+    }
+    return n;
+}
+/* AlgebraicMG::setUpPhase, src/amg.cpp:4-56, random draws taken from rnd in the same order */
+int orc_setup(orc_mg* mg, const double* rndp, long n_rnd) {
+    if (n_rnd < orc_setup_random_count(mg)) return -1;
+    const cplx* rnd = (const cplx*)rndp;
+    long pos = 0;
+    olevel* L0 = &mg->lv[0];
+    size_t vs0 = (size_t)L0->sites * L0->dof;
+    memcpy(L0->tvec, rnd, sizeof(cplx) * L0->ntest * vs0);
+    pos += L0->ntest * vs0;
+    for (int l = 1; l < mg->levels - 1; l++) {
+        olevel* L = &mg->lv[l];
+        olevel* P = &mg->lv[l - 1];
+        size_t vs = (size_t)L->sites * L->dof, vp = (size_t)P->sites * P->dof;
+        for (int cc = 0; cc < L->ntest; cc++) {
+            if (cc < P->ntest) restrict_(mg, l - 1, P->tvec + cc * vp, L->tvec + cc * vs);
+            else {
+                memcpy(L->tvec + cc * vs, rnd + pos, sizeof(cplx) * vs);
+                pos += vs;
+            }
+        }
+    }
+    for (int l = 0; l < mg->levels - 1; l++) {
+        olevel* L = &mg->lv[l];
+        size_t vs = (size_t)L->sites * L->dof;
+        cplx* zero = (cplx*)calloc(vs, sizeof(cplx));
+        for (int cc = 0; cc < L->ntest; cc++) sap(mg, l, zero, L->tvec + cc * vs, mg->k.sap_tv_iters, 1e-10);
+        free(zero);
+        orc_orthonormalize(mg, l);
+        orc_make_coarse_links(mg, l);
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ outer solve */
+typedef struct {
+    const orc_mg* mg;
+    int cycle;
+} octx;
+static void op_dirac(const void* v, const cplx* in, cplx* out) {
+    orc_dirac(((const octx*)v)->mg, 0, (const double*)in, (double*)out);
+}
+/* FGMRES_AMG_v_cycle / _k_cycle::preconditioner, include/amg.h:240-269: zero, then one cycle */
+static void outer_prec(const void* v, const cplx* in, cplx* out) {
+    const octx* c = (const octx*)v;
+    long n = (long)c->mg->lv[0].sites * 2;
+    memset(out, 0, sizeof(cplx) * n);
+    if (c->cycle == 0) vcycle(c->mg, 0, in, out);
+    else kcycle(c->mg, 0, in, out);
+}
+int orc_solve(const orc_mg* mg, int cycle, int m, int restarts, double tol, const double* b, double* x) {
+    long n = (long)mg->lv[0].sites * 2;
+    cplx* x0 = (cplx*)calloc(n, sizeof(cplx));
+    octx c = {mg, cycle};
+    int it = fgmres(n, m, restarts, tol, op_dirac, &c, outer_prec, &c, (const cplx*)b, x0, (cplx*)x);
+    free(x0);
+    return it;
+}
+int orc_gmres_plain(const orc_mg* mg, int m, int restarts, double tol, const double* b, double* x) {
+    long n = (long)mg->lv[0].sites * 2;
+    cplx* x0 = (cplx*)calloc(n, sizeof(cplx));
+    octx c = {mg, 0};
+    int it = fgmres(n, m, restarts, tol, op_dirac, &c, NULL, NULL, (const cplx*)b, x0, (cplx*)x);
+    free(x0);
+    return it;
+}
+
+/* ------------------------------------------------------------------ gradient (no reference counterpart) */
+/* dL/dtheta_mu(n) = -Re[ lam(n)^+ (-1/2)(1-sigma_mu)(i U_mu(n)) s psi(n+mu)
+ *                       + lam(n+mu)^+ (-1/2)(1+sigma_mu)(-i U*_mu(n)) s psi(n) ]
+ * from the hop terms of src/dirac_operator.cpp:37-48; s is the antiperiodic sign of the hop. */
+void orc_link_gradient(const orc_mg* mg, const double* psip, const double* lamp, double* out) {
+    const cplx* psi = (const cplx*)psip;
+    const cplx* lam = (const cplx*)lamp;
+    int Nx = mg->Nx, Nt = mg->Nt;
+    /* (1 -/+ sigma_mu) as 2x2 complex matrices, sigma_0 = sigma_x, sigma_1 = sigma_y */
+    const cplx Mm[2][2][2] = {{{1.0, -1.0}, {-1.0, 1.0}}, {{1.0, I}, {-I, 1.0}}};
+    const cplx Pp[2][2][2] = {{{1.0, 1.0}, {1.0, 1.0}}, {{1.0, -I}, {I, 1.0}}};
+    for (int x = 0; x < Nx; x++)
+        for (int t = 0; t < Nt; t++)
+            for (int mu = 0; mu < 2; mu++) {
+                int n = x * Nt + t;
+                int np = nbr_fwd(Nx, Nt, x, t, mu);
+                cplx s = rsign(Nt, t, mu);
+                cplx Uf = mg->U[2 * n + mu];
+                cplx acc = 0;
+                for (int a = 0; a < 2; a++) {
+                    cplx h1 = 0, h2 = 0;
+                    for (int b = 0; b < 2; b++) {
+                        h1 += Mm[mu][a][b] * psi[2 * np + b];
+                        h2 += Pp[mu][a][b] * psi[2 * n + b];
+                    }
+                    acc += conj(lam[2 * n + a]) * (-0.5) * (I * Uf) * s * h1;
+                    acc += conj(lam[2 * np + a]) * (-0.5) * (-I * conj(Uf)) * s * h2;
+                }
+                out[2 * n + mu] = -creal(acc);
+            }
+}

@@ -1,0 +1,131 @@
+"""Generate the golden fixtures in tests/golden/ from the reference's own code.
+
+Run in the development container (needs the reference sources; they are not
+present where the tests run):
+
+    python tests/golden/make_golden.py
+
+For each case it builds the reference harness for that lattice size
+(oracle/Makefile `ref`), generates seeded inputs with the oracle's input
+generators, runs the reference (oracle/_ref/ref_harness_<Nx>x<Nt>) and stores
+inputs + reference outputs in <case>.npz.  The tests compare the oracle
+restatement against these files (pinning it) and the CUDA library against the
+oracle.
+"""
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+import pyoracle  # noqa: E402
+
+# name, Nx, Nt, levels, m0, parameter rows, beta, sweeps, seed, fgmres m, which modes
+CASES = [
+    dict(name="ops_16x32_l3", Nx=16, Nt=32, levels=3, m0=-0.10,
+         rows=[[0, 4, 8, 4, 2, 4], [1, 2, 4, 6, 2, 2]], beta=2.0, sweeps=20, seed=11, m=20, modes=("ops", "solve")),
+    dict(name="ops_32x32_l2", Nx=32, Nt=32, levels=2, m0=-0.15,
+         rows=[[0, 8, 8, 6, 4, 4]], beta=2.0, sweeps=30, seed=12, m=20, modes=("ops", "solve")),
+    dict(name="ops_32x16_l3", Nx=32, Nt=16, levels=3, m0=-0.05,
+         rows=[[0, 8, 4, 4, 4, 2], [1, 4, 2, 4, 2, 2]], beta=3.0, sweeps=10, seed=13, m=20, modes=("ops",)),
+    # 64x64, 2 levels, SAP 4x4, Nv = 10, restart 20, beta = 2, 500 sweeps, m0 = -0.18
+    dict(name="solve_64x64_l2", Nx=64, Nt=64, levels=2, m0=-0.18,
+         rows=[[0, 16, 16, 10, 16, 16]], beta=2.0, sweeps=500, seed=2024, m=20, modes=("solve",)),
+]
+
+OPS_OUT = ["Dphi", "Ddagphi"]
+
+
+def run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"{cmd} failed:\n{r.stdout}\n{r.stderr}")
+    return r.stdout
+
+
+def rd(path):
+    return np.fromfile(path, dtype=np.complex128)
+
+
+def make_case(c, work):
+    Nx, Nt, L = c["Nx"], c["Nt"], c["levels"]
+    run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "ref", f"NX={Nx}", f"NT={Nt}", "-j8"])
+    harness = os.path.join(REPO, "oracle", "_ref", f"ref_harness_{Nx}x{Nt}")
+    theta, acc = pyoracle.metropolis(Nx, Nt, c["beta"], c["sweeps"], c["seed"])
+    U = pyoracle.links_from_theta(theta)
+    o = pyoracle.Oracle(Nx, Nt, L, c["m0"], c["rows"], U)
+    sizes = [o.size(l) for l in range(L)]
+    nrnd = o.setup_random_count()
+    rnd = pyoracle.uniform(nrnd, c["seed"] + 1)
+    probes = [pyoracle.gaussian(sizes[l], c["seed"] + 100 + l) for l in range(L)]
+    rhs = pyoracle.gaussian(Nx * Nt * 2, c["seed"] + 7)
+
+    pfile = os.path.join(work, "params")
+    with open(pfile, "w") as f:
+        for r in c["rows"]:
+            f.write(" ".join(str(v) for v in r) + "\n")
+    conf = os.path.join(work, "conf.bin")
+    pyoracle.write_binary(conf, Nx, Nt, U)
+    rhsf = os.path.join(work, "rhs.bin")
+    pyoracle.write_binary(rhsf, Nx, Nt, rhs)
+    tf = os.path.join(work, "tvec.bin")
+    rnd.tofile(tf)
+    pf = os.path.join(work, "probe.bin")
+    np.concatenate(probes).tofile(pf)
+
+    out = dict(Nx=Nx, Nt=Nt, levels=L, m0=c["m0"], rows=np.array(c["rows"], dtype=np.int32), theta=theta,
+               beta=c["beta"], sweeps=c["sweeps"], seed=c["seed"], rnd_count=nrnd, rhs=rhs, fgmres_m=c["m"],
+               acceptance=acc)
+    # the setup's random stream is pyoracle.uniform(rnd_count, seed + 1); it is regenerated, not stored
+    for l in range(L):
+        out[f"probe_{l}"] = probes[l]
+    if "ops" in c["modes"]:
+        od = os.path.join(work, "ops")
+        os.makedirs(od)
+        run([harness, "ops", str(L), repr(c["m0"]), pfile, conf, pf, tf, od])
+        for fn in sorted(os.listdir(od)):
+            key = "ref_" + fn.rsplit(".", 1)[0]
+            if fn.endswith(".bin"):
+                out[key] = rd(os.path.join(od, fn))
+            else:
+                out[key + "_iters"] = int(open(os.path.join(od, fn)).read().split()[0])
+    if "solve" in c["modes"]:
+        for cyc, tag in ((0, "V"), (1, "K")):
+            sd = os.path.join(work, f"solve{tag}")
+            os.makedirs(sd)
+            run([harness, "solve", str(L), repr(c["m0"]), pfile, conf, rhsf, tf, sd, str(cyc), str(c["m"]), "50",
+                 "1e-10"])
+            out[f"ref_x_{tag}"] = rd(os.path.join(sd, "x.bin"))
+            meta = dict(line.split() for line in open(os.path.join(sd, "solve.txt")))
+            out[f"ref_iters_{tag}"] = int(meta["iterations"])
+            out[f"ref_relres_{tag}"] = float(meta["relres"])
+        # the reference's own mt19937 setup (src/amg.cpp:6), for the iteration count only
+        sd = os.path.join(work, "solve_stock")
+        os.makedirs(sd)
+        run([harness, "solve", str(L), repr(c["m0"]), pfile, conf, rhsf, "-", sd, "0", str(c["m"]), "50", "1e-10"])
+        meta = dict(line.split() for line in open(os.path.join(sd, "solve.txt")))
+        out["ref_iters_V_stock"] = int(meta["iterations"])
+    return out
+
+
+def main():
+    pyoracle.build()
+    for c in CASES:
+        work = tempfile.mkdtemp(prefix="golden_")
+        try:
+            out = make_case(c, work)
+        finally:
+            shutil.rmtree(work, ignore_errors=True)
+        path = os.path.join(HERE, c["name"] + ".npz")
+        np.savez_compressed(path, **out)
+        print(f"{c['name']}: {os.path.getsize(path) / 1024:.0f} KiB, keys={len(out)}",
+              {k: int(v) for k, v in out.items() if k.endswith("_iters") or k.startswith("ref_iters")})
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,115 @@
+"""Pins the CPU restatement (oracle/ddamg_oracle.c) against outputs of the
+reference's own code (tests/golden/*.npz, made by tests/golden/make_golden.py
+from oracle/_ref).  Everything here runs on the CPU."""
+import numpy as np
+import pytest
+
+import pyoracle as po
+
+OPS = ["ops_16x32_l3", "ops_32x32_l2", "ops_32x16_l3"]
+# the restatement follows the reference's arithmetic order, so agreement is to a few ulps
+TOL = 1e-13
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def make_oracle(z):
+    Nx, Nt, L = int(z["Nx"]), int(z["Nt"]), int(z["levels"])
+    o = po.Oracle(Nx, Nt, L, float(z["m0"]), z["rows"], po.links_from_theta(z["theta"]))
+    o.setup(po.uniform(int(z["rnd_count"]), int(z["seed"]) + 1))
+    return o
+
+
+@pytest.fixture(scope="module", params=OPS)
+def case(request, golden):
+    z = golden(request.param)
+    return z, make_oracle(z)
+
+
+def test_inputs_regenerate(golden):
+    for name in OPS + ["solve_64x64_l2"]:
+        z = golden(name)
+        th, _ = po.metropolis(int(z["Nx"]), int(z["Nt"]), float(z["beta"]), int(z["sweeps"]), int(z["seed"]))
+        assert np.array_equal(th, z["theta"])
+        rhs = po.gaussian(int(z["Nx"]) * int(z["Nt"]) * 2, int(z["seed"]) + 7)
+        assert np.array_equal(rhs, z["rhs"])
+
+
+def test_dirac(case):
+    z, o = case
+    assert rel(o.dirac(z["probe_0"]), z["ref_Dphi"]) < TOL
+    assert rel(o.dirac(z["probe_0"], True), z["ref_Ddagphi"]) < TOL
+
+
+def test_level_ops_and_links(case):
+    z, o = case
+    L = int(z["levels"])
+    for l in range(L):
+        assert rel(o.level_op(l, z[f"probe_{l}"]), z[f"ref_Dop_{l}"]) < TOL
+        if l >= 1:
+            for w in (1, 2, 3):
+                assert rel(o.get_links(l, w), z[f"ref_G{w}_{l}"]) < TOL, (l, w)
+
+
+def test_transfers_and_tvec(case):
+    z, o = case
+    L = int(z["levels"])
+    for l in range(L - 1):
+        assert rel(o.get_tvec(l), z[f"ref_tvec_{l}"]) < TOL
+        assert rel(o.restrict(l, z[f"probe_{l}"]), z[f"ref_Pdagg_{l}"]) < TOL
+        assert rel(o.prolong(l, z[f"probe_{l + 1}"]), z[f"ref_P_{l}"]) < TOL
+
+
+def test_sap_and_coarse(case):
+    z, o = case
+    L = int(z["levels"])
+    for l in range(L - 1):
+        x, it = o.sap(l, z[f"probe_{l}"], nu=3)
+        assert it == int(z[f"ref_SAP_{l}_iters"])
+        assert rel(x, z[f"ref_SAP_{l}"]) < TOL
+    x, it = o.coarse_gmres(z[f"probe_{L - 1}"])
+    assert it == int(z["ref_coarse_gmres_iters"])
+    assert rel(x, z["ref_coarse_gmres"]) < 1e-12
+
+
+def test_cycles(case):
+    z, o = case
+    assert rel(o.vcycle(z["probe_0"]), z["ref_vcycle"]) < 1e-12
+    assert rel(o.kcycle(z["probe_0"]), z["ref_kcycle"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["ops_16x32_l3", "ops_32x32_l2", "solve_64x64_l2"])
+@pytest.mark.parametrize("cycle,tag", [(0, "V"), (1, "K")])
+def test_solve(golden, name, cycle, tag):
+    z = golden(name)
+    o = make_oracle(z)
+    x, it = o.solve(z["rhs"], cycle=cycle, m=int(z["fgmres_m"]))
+    assert it == int(z[f"ref_iters_{tag}"])
+    assert rel(x, z[f"ref_x_{tag}"]) < 1e-12
+    # the solve meets the reference's convergence test D x = b (src/methods.cpp:173-190)
+    r = o.dirac(x) - z["rhs"]
+    assert np.linalg.norm(r) / np.linalg.norm(z["rhs"]) < 1e-10
+
+
+def test_gamma5_hermiticity(golden):
+    """D^dagger = sigma_3 D sigma_3, the identity the adjoint solve relies on."""
+    z = golden("ops_16x32_l3")
+    o = make_oracle(z)
+    v = z["probe_0"].reshape(-1, 2)
+    s3 = np.array([1.0, -1.0])
+    lhs = o.dirac(v.reshape(-1), True)
+    rhs = (o.dirac((v * s3).reshape(-1)).reshape(-1, 2) * s3).reshape(-1)
+    assert rel(lhs, rhs) < 1e-14
+
+
+def test_galerkin_identity(golden):
+    """D_c = P^dagger D P at every level (amg.cpp:249-298)."""
+    z = golden("ops_16x32_l3")
+    o = make_oracle(z)
+    for l in range(int(z["levels"]) - 1):
+        vc = z[f"probe_{l + 1}"]
+        lhs = o.level_op(l + 1, vc)
+        rhs = o.restrict(l, o.level_op(l, o.prolong(l, vc)))
+        assert rel(lhs, rhs) < 1e-12
