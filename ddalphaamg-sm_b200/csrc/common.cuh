@@ -1,0 +1,166 @@
+// Shared device/host helpers for the DD-alphaAMG B200 library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstdio>
+#include <string>
+
+#include "ddamg.h"
+
+namespace ddamg {
+
+// ---------------------------------------------------------------- complex arithmetic
+// Complex numbers are CUDA's double2 / float2 (x = re, y = im); fields are arrays of them.
+template <typename R> struct CxT;
+template <> struct CxT<double> { typedef double2 V; };
+template <> struct CxT<float> { typedef float2 V; };
+template <typename V> struct RealOf;
+template <> struct RealOf<double2> { typedef double R; };
+template <> struct RealOf<float2> { typedef float R; };
+
+#define DDAMG_HD __host__ __device__ __forceinline__
+
+DDAMG_HD double2 mkc(double a, double b) { return make_double2(a, b); }
+DDAMG_HD float2 mkc(float a, float b) { return make_float2(a, b); }
+template <typename V> DDAMG_HD V czero() { return mkc(typename RealOf<V>::R(0), typename RealOf<V>::R(0)); }
+
+#define DDAMG_CX_OPS(V, R)                                                                        \
+    DDAMG_HD V operator+(V a, V b) { return mkc(a.x + b.x, a.y + b.y); }                          \
+    DDAMG_HD V operator-(V a, V b) { return mkc(a.x - b.x, a.y - b.y); }                          \
+    DDAMG_HD V operator-(V a) { return mkc(-a.x, -a.y); }                                         \
+    DDAMG_HD V operator*(R s, V a) { return mkc(s * a.x, s * a.y); }                              \
+    DDAMG_HD V& operator+=(V& a, V b) { a.x += b.x; a.y += b.y; return a; }                       \
+    DDAMG_HD V& operator-=(V& a, V b) { a.x -= b.x; a.y -= b.y; return a; }                       \
+    /* a * b */                                                                                   \
+    DDAMG_HD V cmul(V a, V b) { return mkc(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }      \
+    /* conj(a) * b */                                                                             \
+    DDAMG_HD V cmulc(V a, V b) { return mkc(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x); }     \
+    /* acc + a * b */                                                                             \
+    DDAMG_HD V cfma(V a, V b, V acc) {                                                            \
+        return mkc(fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y)));    \
+    }                                                                                             \
+    /* acc + conj(a) * b */                                                                       \
+    DDAMG_HD V cfmac(V a, V b, V acc) {                                                           \
+        return mkc(fma(a.x, b.x, fma(a.y, b.y, acc.x)), fma(a.x, b.y, fma(-a.y, b.x, acc.y)));    \
+    }                                                                                             \
+    DDAMG_HD V conjc(V a) { return mkc(a.x, -a.y); }                                              \
+    /* i * a */                                                                                   \
+    DDAMG_HD V imul(V a) { return mkc(-a.y, a.x); }                                               \
+    DDAMG_HD R cnorm2(V a) { return a.x * a.x + a.y * a.y; }
+
+DDAMG_CX_OPS(double2, double)
+DDAMG_CX_OPS(float2, float)
+
+DDAMG_HD double2 to_d(float2 a) { return make_double2(a.x, a.y); }
+DDAMG_HD double2 to_d(double2 a) { return a; }
+template <typename V> DDAMG_HD V from_d(double2 a);
+template <> DDAMG_HD double2 from_d<double2>(double2 a) { return a; }
+template <> DDAMG_HD float2 from_d<float2>(double2 a) { return make_float2((float)a.x, (float)a.y); }
+
+// complex division (Smith's algorithm), used for Givens rotations / back substitution
+DDAMG_HD double2 cdiv(double2 a, double2 b) {
+    if (fabs(b.x) >= fabs(b.y)) {
+        double r = b.y / b.x, den = b.x + b.y * r;
+        return make_double2((a.x + a.y * r) / den, (a.y - a.x * r) / den);
+    } else {
+        double r = b.x / b.y, den = b.x * r + b.y;
+        return make_double2((a.x * r + a.y) / den, (a.y * r - a.x) / den);
+    }
+}
+
+// ---------------------------------------------------------------- warp / block reductions
+__device__ __forceinline__ double2 warp_sum(double2 v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    return v;
+}
+__device__ __forceinline__ float2 warp_sum(float2 v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+// Sum over the whole CTA; every thread gets the result. `scratch` holds >= 33 V (shared).
+template <typename V>
+__device__ __forceinline__ V block_sum(V v, V* scratch) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();  // protect scratch from the previous use
+    if (lane == 0) scratch[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        V s = (lane < nw) ? scratch[lane] : V{};
+        s = warp_sum(s);
+        if (lane == 0) scratch[32] = s;
+    }
+    __syncthreads();
+    return scratch[32];
+}
+
+// ---------------------------------------------------------------- counter-based RNG
+// splitmix64 finaliser (Steele, Lea & Flood 2014), keyed by (seed, stream, counter);
+// identical to orc_rng in the CPU oracle so device draws match it bit for bit.
+DDAMG_HD uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+DDAMG_HD uint64_t rng64(uint64_t seed, uint64_t stream, uint64_t counter) {
+    return mix64(mix64(seed ^ mix64(stream)) + counter);
+}
+DDAMG_HD double u01(uint64_t r) { return (double)(r >> 11) * 0x1.0p-53; }
+constexpr uint64_t kStreamUniform = 0x7E57ull;   // test vectors, re/im ~ U(-1,1)
+constexpr uint64_t kStreamGauss = 0x6A55ull;     // Gaussian right-hand sides
+constexpr uint64_t kStreamHotStart = 0xC0FFEEull;  // Metropolis hot start
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+struct Status {
+    ddamg_status code = DDAMG_OK;
+};
+#define DDAMG_CUDA_TRY(expr)                                                                      \
+    do {                                                                                          \
+        cudaError_t e__ = (expr);                                                                 \
+        if (e__ != cudaSuccess) {                                                                 \
+            ::ddamg::set_error(std::string(#expr) + ": " + cudaGetErrorString(e__) + " (" +       \
+                               __FILE__ + ":" + std::to_string(__LINE__) + ")");                  \
+            throw ::ddamg::CudaFailure();                                                         \
+        }                                                                                         \
+    } while (0)
+struct CudaFailure {};
+struct ParamFailure {
+    std::string msg;
+};
+struct TimeoutFailure {};
+
+// launch bookkeeping: every kernel launch in the library goes through this counter
+extern long long g_launches;
+#define DDAMG_LAUNCH(kernel, grid, block, smem, stream, ...)                                      \
+    do {                                                                                          \
+        kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);                               \
+        ++::ddamg::g_launches;                                                                    \
+        DDAMG_CUDA_TRY(cudaGetLastError());                                                       \
+    } while (0)
+
+inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace ddamg

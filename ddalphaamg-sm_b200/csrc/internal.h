@@ -1,0 +1,119 @@
+// Kernel launchers and level geometry shared by the library's translation units.
+#pragma once
+
+#include "common.cuh"
+
+namespace ddamg {
+
+// Geometry of one multigrid level (include/params.h:34-69 derives the same numbers).
+struct Geom {
+    int level = 0;
+    int Nx = 0, Nt = 0, sites = 0;
+    int colors = 1, dof = 2;         // dof = 2 * colors
+    int ntest = 0;                   // test vectors = colours of level+1 (non-coarsest)
+    int agg_x = 0, agg_t = 0;        // aggregation block counts
+    int el_x = 0, el_t = 0;          // sites per aggregate and direction
+    int sap_x = 0, sap_t = 0;        // SAP block counts
+    int sel_x = 0, sel_t = 0;        // sites per SAP block and direction
+    __host__ __device__ long size() const { return (long)sites * dof; }
+};
+
+// Coarse links live as [site][d][j][i]: 5 dof x dof matrices per site, column j (input dof)
+// major and row i (output dof) fastest so a warp reads one column coalesced.
+// d = 0 self (G1 = A), 1 = +t (G2, mu=0), 2 = +x (G2, mu=1), 3 = -t (G3, mu=0), 4 = -x (G3, mu=1).
+// The level operator is out = (m0+2) v - sum_d s_d M_d v(nbr_d) with s_d the antiperiodic
+// sign of hops that cross t = Nt-1 <-> 0.
+
+// ------------------------------------------------------------ fine level (kernels_fine.cu)
+template <typename V>
+void launch_wilson(cudaStream_t s, const V* U, const V* in, V* out, const V* b, int Nx, int Nt, double m0,
+                   int dagger, int nrhs);
+void launch_link_derivative(cudaStream_t s, const double2* U, const double2* psi, const double2* lam, double* out,
+                            int Nx, int Nt);
+void launch_metropolis_init(cudaStream_t s, double* th, int Nx, int Nt, uint64_t seed);
+void launch_metropolis_sub(cudaStream_t s, double* th, int Nx, int Nt, double beta, double delta, uint64_t seed,
+                           int sweep, int sub, unsigned long long* acc);
+void launch_theta_to_links(cudaStream_t s, const double* th, double2* U, long n);
+void launch_fill_uniform(cudaStream_t s, double2* out, long n_complex, uint64_t seed, long offset_complex);
+template <typename A, typename B> void launch_convert(cudaStream_t s, const A* in, B* out, long n);
+
+// ------------------------------------------------------------ vector algebra (kernels_blas.cu)
+// Reductions use a fixed grid and a second pass, so results are deterministic.
+constexpr int kRedBlocks = 296;  // 2 x 148 SMs
+// out[r*k + i] = sum_e w_r[e] * conj(B_r,i[e]) for i < k; basis vector i of rhs r at B + r*bstride + i*ldb
+template <typename V>
+void launch_multidot(cudaStream_t s, const V* B, long ldb, long bstride, int k, const V* w, long wstride, long n,
+                     int nrhs, double2* partial, double2* out);
+// out[r] = sum_e |x_r[e]|^2
+template <typename V>
+void launch_norm2(cudaStream_t s, const V* x, long xstride, long n, int nrhs, double2* partial, double* out);
+// w_r -= sum_i coef[r*k+i] * B_r,i   (coef in FP64 on the device)
+template <typename V>
+void launch_multiaxpy(cudaStream_t s, const V* B, long ldb, long bstride, int k, const double2* coef, V* w,
+                      long wstride, long n, int nrhs, double sign);
+// y_r = alpha_r * x_r with alpha from the device
+template <typename V>
+void launch_scale(cudaStream_t s, const double2* alpha, const V* x, V* y, long n, int nrhs);
+// r = a - b
+template <typename V> void launch_sub(cudaStream_t s, const V* a, const V* b, V* r, long n);
+// y += x
+template <typename V> void launch_add(cudaStream_t s, const V* x, V* y, long n);
+// SAP convergence flags: done[r] = it + 1 the first time sqrt(rr[r]) < tol * sqrt(vv[r])
+void launch_flag_converged(cudaStream_t s, const double* rr, const double* vv, double tol, int nrhs, int it,
+                           int* done);
+// y = alpha x with alpha a host value
+template <typename V> void launch_scale_host(cudaStream_t s, double2 alpha, const V* x, V* y, long n);
+void launch_sigma3(cudaStream_t s, const double2* x, double2* y, long sites);
+size_t sap_smem_bytes(int m, int NE, bool fp64);
+
+// ------------------------------------------------------------ coarse levels (kernels_coarse.cu)
+template <typename V>
+void launch_coarse_op(cudaStream_t s, const V* links, const V* in, V* out, const V* b, int Nx, int Nt, int dof,
+                      double m0, int nrhs);
+// P^dagger: fine level g -> coarse; tv = [ntest][sites][dof]
+template <typename V>
+void launch_restrict(cudaStream_t s, const Geom& g, const V* tv, const V* in, V* out, int nrhs);
+// P (add = 0: out = P vc, add = 1: out += P vc)
+template <typename V>
+void launch_prolong(cudaStream_t s, const Geom& g, const V* tv, const V* vc, V* out, int add, int nrhs);
+void launch_orthonormalize(cudaStream_t s, const Geom& g, double2* tv);
+// next-level links from level g's operator (U for level 0, links otherwise) and test vectors
+void launch_build_coarse_links(cudaStream_t s, const Geom& g, const double2* U, const double2* links,
+                               const double2* tv, double2* next_links);
+
+// ------------------------------------------------------------ SAP (kernels_sap.cu)
+// One colour sweep of SAP_C::SAP: x_B += D_B^-1 r_B for every block of the colour, block
+// GMRES(m) x restarts to tol with x0 = r_B (src/sap.cpp:48-77).  blocks: device list.
+struct SapArgs {
+    int m, restarts;
+    double tol;
+    double m0;
+    const int* blocks;  // block indices of this colour
+    int nblocks;
+    const int* done;    // per-rhs skip flags (may be null)
+};
+template <typename V>
+void launch_sap_sweep_fine(cudaStream_t s, const Geom& g, const V* U, const V* r, V* x, const SapArgs& a,
+                           int nrhs);
+template <typename V>
+void launch_sap_sweep_coarse(cudaStream_t s, const Geom& g, const V* links, const V* r, V* x, const SapArgs& a,
+                             int nrhs);
+
+// ------------------------------------------------------------ coarsest GMRES (kernels_gmres.cu)
+struct CoarseGmresWork {
+    double2* V = nullptr;      // (m+1) x n
+    double2* w = nullptr;      // n
+    double2* r = nullptr;      // n
+    double2* partial = nullptr;  // grid x (m+2)
+    double2* H = nullptr;      // (m+1) x m (column major, ld m+1)
+    unsigned* bar = nullptr;   // barrier counter + generation
+    int* status = nullptr;     // [0] error flag, [1] iterations
+    int grid = 0;
+    int block = 256;
+};
+void coarse_gmres_prepare(CoarseGmresWork& w, int n, int m, int dof, int device);
+// x = GMRES(m) x restarts solution of D x = b from x0 = b; returns on the stream
+void launch_coarse_gmres(cudaStream_t s, const CoarseGmresWork& w, const double2* links, const double2* b,
+                         double2* x, int Nx, int Nt, int dof, double m0, int m, int restarts, double tol);
+
+}  // namespace ddamg

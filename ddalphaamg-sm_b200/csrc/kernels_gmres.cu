@@ -1,0 +1,365 @@
+// Coarsest-level solve (Level::GMRES_level_l, include/level.h:70-140: GMRES(m) x restarts with
+// the identity preconditioner, x0 = b) as ONE persistent cooperative kernel: every CTA owns a
+// slice of coarse sites, applies the level operator to it, and the CTAs meet at a bounded grid
+// barrier between phases.  Orthogonalisation is classical Gram-Schmidt with one
+// re-orthogonalisation pass (CGS2); the Hessenberg/Givens work is repeated by every CTA on
+// identical data so control flow stays uniform without broadcasts.
+#include "internal.h"
+
+#include <cooperative_groups.h>
+
+namespace ddamg {
+
+constexpr long long kSpinLimit = 1LL << 24;  // ~1-2 s of polling before a barrier gives up
+
+// Bounded grid barrier: arrive on bar[0], wait for the generation bar[1] to move.  On timeout
+// (or when another CTA already failed) it sets status[0] and returns false; callers return.
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status, unsigned nblocks) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = bar + 1;
+        volatile int* vst = status;
+        const unsigned gen = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(bar, 1u);
+        int good = 1;
+        if (arrived == nblocks - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long spins = 0;
+            while (*vgen == gen) {
+                if (*vst != 0) {
+                    good = 0;
+                    break;
+                }
+                if (++spins > kSpinLimit) {
+                    atomicExch(status, 1);
+                    good = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok = good && (*vst == 0);
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+struct GmresK {
+    const double2* links;
+    const double2* b;
+    double2* x;
+    double2* V;
+    double2* w;
+    double2* partial;  // 3 buffers of grid x P
+    double2* H;        // column j at H + j*(m+1)
+    unsigned* bar;
+    int* status;
+    int Nx, Nt, dof, m, restarts, P;
+    double m0, tol;
+};
+
+// out = [b -] D in on this CTA's sites (warp per site, lane per dof, NI = dof/32 rounded up)
+template <int NI>
+__device__ void apply_own(const GmresK& k, const double2* __restrict__ in, double2* __restrict__ out,
+                          const double2* __restrict__ bsub, int s0, int s1) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int dof = k.dof, Nt = k.Nt, Nx = k.Nx;
+    for (int n = s0 + wid; n < s1; n += nw) {
+        const int x = n / Nt, t = n - x * Nt;
+        int nb[5];
+        double sg[5];
+        nb[0] = n;
+        nb[1] = x * Nt + ((t + 1 == Nt) ? 0 : t + 1);
+        nb[2] = ((x + 1 == Nx) ? 0 : x + 1) * Nt + t;
+        nb[3] = x * Nt + ((t == 0) ? Nt - 1 : t - 1);
+        nb[4] = ((x == 0) ? Nx - 1 : x - 1) * Nt + t;
+        sg[0] = 1.0;
+        sg[1] = (t == Nt - 1) ? -1.0 : 1.0;
+        sg[2] = 1.0;
+        sg[3] = (t == 0) ? -1.0 : 1.0;
+        sg[4] = 1.0;
+        double2 acc[NI], self[NI];
+#pragma unroll
+        for (int q = 0; q < NI; q++) acc[q] = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int d = 0; d < 5; d++) {
+            double2 vd[NI];
+#pragma unroll
+            for (int q = 0; q < NI; q++) {
+                const int i = lane + 32 * q;
+                vd[q] = (i < dof) ? sg[d] * in[(long)nb[d] * dof + i] : make_double2(0.0, 0.0);
+                if (d == 0) self[q] = vd[q];
+            }
+            const double2* M = k.links + ((long)n * 5 + d) * dof * dof;
+#pragma unroll
+            for (int jq = 0; jq < NI; jq++) {
+                const int jn = min(32, dof - 32 * jq);
+                for (int jl = 0; jl < jn; jl++) {
+                    const double2 vj = make_double2(__shfl_sync(0xffffffffu, vd[jq].x, jl),
+                                                    __shfl_sync(0xffffffffu, vd[jq].y, jl));
+                    const double2* Mj = M + (long)(32 * jq + jl) * dof;
+#pragma unroll
+                    for (int q = 0; q < NI; q++) {
+                        const int i = lane + 32 * q;
+                        if (i < dof) acc[q] = cfma(__ldg(Mj + i), vj, acc[q]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NI; q++) {
+            const int i = lane + 32 * q;
+            if (i < dof) {
+                double2 o = (k.m0 + 2.0) * self[q] - acc[q];
+                if (bsub) o = bsub[(long)n * dof + i] - o;
+                out[(long)n * dof + i] = o;
+            }
+        }
+    }
+}
+
+// partial[blk*P + i] = sum_own w * conj(V_i), i < cnt (warp per i)
+__device__ void partial_dots(const GmresK& k, const double2* __restrict__ w, int cnt, double2* __restrict__ part,
+                             long e0, long e1, long n) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = wid; i < cnt; i += nw) {
+        const double2* vi = k.V + (long)i * n;
+        double2 s = make_double2(0.0, 0.0);
+        for (long e = e0 + lane; e < e1; e += 32) s = cfmac(vi[e], w[e], s);
+        s = warp_sum(s);
+        if (lane == 0) part[(long)blockIdx.x * k.P + i] = s;
+    }
+}
+// h[i] = sum_blk partial[blk*P + i], identical order in every CTA
+__device__ void reduce_partials(const GmresK& k, const double2* __restrict__ part, int cnt, double2* h) {
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int bk = 0; bk < (int)gridDim.x; bk++) s += part[(long)bk * k.P + i];
+        h[i] = s;
+    }
+    __syncthreads();
+}
+
+template <int NI>
+__global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
+    extern __shared__ double2 sh[];
+    const int m = k.m;
+    double2* h = sh;              // m+1
+    double2* h2 = h + (m + 1);    // m+1
+    double2* gm = h2 + (m + 1);   // m+1
+    double2* cn = gm + (m + 1);   // m
+    double2* sn = cn + m;         // m
+    double2* eta = sn + m;        // m
+    __shared__ int s_flag;
+    const unsigned G = gridDim.x;
+    const int sites = k.Nx * k.Nt;
+    const long n = (long)sites * k.dof;
+    const int spc = (sites + G - 1) / G;
+    const int s0 = min(sites, (int)blockIdx.x * spc), s1 = min(sites, s0 + spc);
+    const long e0 = (long)s0 * k.dof, e1 = (long)s1 * k.dof;
+    double2* pA = k.partial;
+    double2* pB = pA + (long)G * k.P;
+    double2* pC = pB + (long)G * k.P;
+
+    // x = x0 = b
+    for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) k.x[e] = k.b[e];
+    if (!grid_barrier(k.bar, k.status, G)) return;
+    apply_own<NI>(k, k.x, k.w, k.b, s0, s1);  // w = r = b - D x
+    __syncthreads();
+    {
+        double rr = 0.0, bb = 0.0;
+        for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+            rr += cnorm2(k.w[e]);
+            bb += cnorm2(k.b[e]);
+        }
+        __shared__ double2 red[33];
+        double2 t = block_sum(make_double2(rr, bb), red);
+        if (threadIdx.x == 0) pC[(long)blockIdx.x * k.P] = t;
+    }
+    if (!grid_barrier(k.bar, k.status, G)) return;
+    double err, norm_b;
+    {
+        double2 t = make_double2(0.0, 0.0);
+        for (unsigned bk = 0; bk < G; bk++) t += pC[(long)bk * k.P];
+        err = sqrt(t.x);
+        norm_b = sqrt(t.y);
+    }
+    int maxIt = m, iters = k.restarts * m;
+    bool converged = false;
+    for (int kk = 0; kk < k.restarts && !converged; kk++) {
+        const double inv = 1.0 / err;
+        for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) k.V[e] = inv * k.w[e];
+        if (threadIdx.x == 0) gm[0] = make_double2(err, 0.0);
+        if (!grid_barrier(k.bar, k.status, G)) return;
+        for (int j = 0; j < m; j++) {
+            const double2* vj = k.V + (long)j * n;
+            apply_own<NI>(k, vj, k.w, nullptr, s0, s1);
+            __syncthreads();
+            partial_dots(k, k.w, j + 1, pA, e0, e1, n);
+            if (!grid_barrier(k.bar, k.status, G)) return;
+            reduce_partials(k, pA, j + 1, h);
+            // w -= V h ; reorthogonalise
+            for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+                double2 a = k.w[e];
+                for (int i = 0; i <= j; i++) a = a - cmul(h[i], k.V[(long)i * n + e]);
+                k.w[e] = a;
+            }
+            __syncthreads();
+            partial_dots(k, k.w, j + 1, pB, e0, e1, n);
+            if (!grid_barrier(k.bar, k.status, G)) return;
+            reduce_partials(k, pB, j + 1, h2);
+            {
+                double ss = 0.0;
+                for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+                    double2 a = k.w[e];
+                    for (int i = 0; i <= j; i++) a = a - cmul(h2[i], k.V[(long)i * n + e]);
+                    k.w[e] = a;
+                    ss += cnorm2(a);
+                }
+                __shared__ double2 red2[33];
+                double2 t = block_sum(make_double2(ss, 0.0), red2);
+                if (threadIdx.x == 0) pC[(long)blockIdx.x * k.P] = t;
+            }
+            for (int i = threadIdx.x; i <= j; i += blockDim.x) h[i] = h[i] + h2[i];
+            if (!grid_barrier(k.bar, k.status, G)) return;
+            double hn;
+            {
+                double t = 0.0;
+                for (unsigned bk = 0; bk < G; bk++) t += pC[(long)bk * k.P].x;
+                hn = sqrt(t);
+            }
+            if (hn > 0) {
+                const double ih = 1.0 / hn;
+                double2* vn = k.V + (long)(j + 1) * n;
+                for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) vn[e] = ih * k.w[e];
+            }
+            if (threadIdx.x == 0) {  // FGMRES::rotation (src/fgmres.cpp:99-115) on column j
+                h[j + 1] = make_double2(hn, 0.0);
+                for (int i = 0; i < j; i++) {
+                    double2 tmp = cmulc(cn[i], h[i]) + cmulc(sn[i], h[i + 1]);
+                    h[i + 1] = cmul(cn[i], h[i + 1]) - cmul(sn[i], h[i]);
+                    h[i] = tmp;
+                }
+                const double den = sqrt(cnorm2(h[j]) + cnorm2(h[j + 1]));
+                sn[j] = make_double2(h[j + 1].x / den, h[j + 1].y / den);
+                cn[j] = make_double2(h[j].x / den, h[j].y / den);
+                h[j] = cmulc(cn[j], h[j]) + cmulc(sn[j], h[j + 1]);
+                h[j + 1] = make_double2(0.0, 0.0);
+                gm[j + 1] = -cmul(sn[j], gm[j]);
+                gm[j] = cmulc(cn[j], gm[j]);
+                s_flag = (sqrt(cnorm2(gm[j + 1])) < k.tol * norm_b) ? 1 : 0;
+            }
+            __syncthreads();
+            if (blockIdx.x == 0)
+                for (int i = threadIdx.x; i <= j; i += blockDim.x) k.H[(long)j * (m + 1) + i] = h[i];
+            const bool brk = s_flag != 0;
+            if (!grid_barrier(k.bar, k.status, G)) return;  // V_{j+1} and H column j visible
+            if (brk) {
+                maxIt = j + 1;
+                break;
+            }
+        }
+        // solve_upper_triangular (src/fgmres.cpp:118-128), column-oriented
+        for (int i = threadIdx.x; i < maxIt; i += blockDim.x) eta[i] = gm[i];
+        __syncthreads();
+        for (int i = maxIt - 1; i >= 0; i--) {
+            if (threadIdx.x == 0) eta[i] = cdiv(eta[i], k.H[(long)i * (m + 1) + i]);
+            __syncthreads();
+            for (int q = threadIdx.x; q < i; q += blockDim.x) eta[q] = eta[q] - cmul(k.H[(long)i * (m + 1) + q], eta[i]);
+            __syncthreads();
+        }
+        for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+            double2 a = k.x[e];
+            for (int jj = 0; jj < maxIt; jj++) a = cfma(eta[jj], k.V[(long)jj * n + e], a);
+            k.x[e] = a;
+        }
+        if (!grid_barrier(k.bar, k.status, G)) return;
+        apply_own<NI>(k, k.x, k.w, k.b, s0, s1);
+        __syncthreads();
+        {
+            double rr = 0.0;
+            for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) rr += cnorm2(k.w[e]);
+            __shared__ double2 red3[33];
+            double2 t = block_sum(make_double2(rr, 0.0), red3);
+            if (threadIdx.x == 0) pC[(long)blockIdx.x * k.P] = t;
+        }
+        if (!grid_barrier(k.bar, k.status, G)) return;
+        {
+            double t = 0.0;
+            for (unsigned bk = 0; bk < G; bk++) t += pC[(long)bk * k.P].x;
+            err = sqrt(t);
+        }
+        if (err < k.tol * norm_b) {
+            iters = kk * m + maxIt;
+            converged = true;
+        }
+        // pC is rewritten only after the next barrier, so no CTA can still be reading it then
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) k.status[1] = iters;
+}
+
+static int g_coop_grid_cache[2] = {0, 0};
+
+void coarse_gmres_prepare(CoarseGmresWork& w, int n, int m, int dof, int device) {
+    int sms = 0;
+    DDAMG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    size_t smem = sizeof(double2) * (size_t)(6 * (m + 1));
+    int per_sm = 0;
+    if (dof <= 32) {
+        DDAMG_CUDA_TRY(cudaFuncSetAttribute(coarse_gmres_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+        DDAMG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_gmres_kernel<1>, 256, smem));
+    } else {
+        DDAMG_CUDA_TRY(cudaFuncSetAttribute(coarse_gmres_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+        DDAMG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_gmres_kernel<2>, 256, smem));
+    }
+    if (per_sm < 1) throw ParamFailure{"coarsest GMRES kernel cannot be resident"};
+    const int sites = n / dof;
+    // one CTA per SM at most, and at least 8 sites per CTA so the phases have work
+    int grid = std::min(sms, std::max(1, sites / 8));
+    w.grid = grid;
+    w.block = 256;
+    (void)g_coop_grid_cache;
+}
+
+void launch_coarse_gmres(cudaStream_t s, const CoarseGmresWork& w, const double2* links, const double2* b,
+                         double2* x, int Nx, int Nt, int dof, double m0, int m, int restarts, double tol) {
+    GmresK k;
+    k.links = links;
+    k.b = b;
+    k.x = x;
+    k.V = w.V;
+    k.w = w.w;
+    k.partial = w.partial;
+    k.H = w.H;
+    k.bar = w.bar;
+    k.status = w.status;
+    k.Nx = Nx;
+    k.Nt = Nt;
+    k.dof = dof;
+    k.m = m;
+    k.restarts = restarts;
+    k.P = m + 2;
+    k.m0 = m0;
+    k.tol = tol;
+    DDAMG_CUDA_TRY(cudaMemsetAsync(w.bar, 0, 2 * sizeof(unsigned), s));
+    DDAMG_CUDA_TRY(cudaMemsetAsync(w.status, 0, 2 * sizeof(int), s));
+    size_t smem = sizeof(double2) * (size_t)(6 * (m + 1));
+    void* args[] = {&k};
+    if (dof <= 32)
+        DDAMG_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)coarse_gmres_kernel<1>, dim3(w.grid), dim3(w.block),
+                                                   args, smem, s));
+    else
+        DDAMG_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)coarse_gmres_kernel<2>, dim3(w.grid), dim3(w.block),
+                                                   args, smem, s));
+    ++g_launches;
+}
+
+}  // namespace ddamg

@@ -1,0 +1,1220 @@
+// Host side of the library: the multigrid hierarchy (Level / AlgebraicMG of the reference),
+// the SAP driver, V- and K-cycles, FGMRES, the adaptive setup, and the extern "C" API.
+// All device work is issued on the handle's stream; data-dependent branches that would
+// otherwise need a host round trip (SAP early exit) are device-side flags.
+#include <algorithm>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "internal.h"
+
+namespace ddamg {
+
+long long g_launches = 0;
+static thread_local std::string t_last_error;
+void set_error(const std::string& msg) { t_last_error = msg; }
+
+template <typename V> struct LevelBufs {
+    V* U = nullptr;      // level 0 links [site][mu]
+    V* links = nullptr;  // level >= 1: [site][5][dof][dof]
+    V* tv = nullptr;     // [ntest][size]
+    V* eta = nullptr;    // cycle input  (W x size)
+    V* psi = nullptr;    // cycle output (W x size)
+    V* xfer = nullptr;   // transfer buffer in the previous level's precision... (W x size)
+    V* r = nullptr;      // SAP / cycle residual (W x size)
+    V* t = nullptr;      // D x temporary (W x size)
+    // K-cycle FGMRES workspace (level >= 1)
+    V* kV = nullptr;
+    V* kZ = nullptr;
+    V* kw = nullptr;
+    V* kr = nullptr;
+    V* kx = nullptr;
+};
+
+struct LevelData {
+    Geom g;
+    bool fp32 = false;  // working precision of this level's smoother / operator
+    LevelBufs<double2> d;
+    LevelBufs<float2> f;
+    int* red = nullptr;
+    int* black = nullptr;
+    int nred = 0, nblack = 0;
+    int* done = nullptr;    // W flags
+    double* vv = nullptr;   // W norms
+    double* rr = nullptr;   // W norms
+};
+template <typename V> LevelBufs<V>& B(LevelData& L);
+template <> LevelBufs<double2>& B<double2>(LevelData& L) { return L.d; }
+template <> LevelBufs<float2>& B<float2>(LevelData& L) { return L.f; }
+
+}  // namespace ddamg
+
+struct ddamg_handle {
+    ddamg_params p;
+    int L = 0;          // levels
+    int W = 1;          // widest batch (max_rhs, test vectors)
+    cudaStream_t s = nullptr;
+    std::vector<ddamg::LevelData> lv;
+    std::vector<void*> allocs;
+    bool gauge = false, setup_done = false;
+    // outer FGMRES (FP64, fine level)
+    double2 *oV = nullptr, *oZ = nullptr, *ow = nullptr, *orr = nullptr, *ob = nullptr, *ox = nullptr;
+    double2* ohost_tmp = nullptr;
+    // scalars
+    double2* dpart = nullptr;  // reduction partials
+    double2* dh = nullptr;     // multidot results (2 x (max m + 1))
+    double2* dcoef = nullptr;  // coefficients for multiaxpy
+    double* dn = nullptr;      // norms
+    double2* hpin = nullptr;   // pinned host mirror
+    double2* grad = nullptr;   // gradient work: psi, lambda, sigma_3 eta (3 fine vectors)
+    ddamg::CoarseGmresWork cg;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_setup_s = 0;
+    long long launches_at_create = 0;
+};
+
+namespace ddamg {
+
+static void* dalloc(ddamg_handle* h, size_t bytes) {
+    void* p = nullptr;
+    if (bytes == 0) return nullptr;
+    DDAMG_CUDA_TRY(cudaMalloc(&p, bytes));
+    DDAMG_CUDA_TRY(cudaMemsetAsync(p, 0, bytes, h->s));
+    h->allocs.push_back(p);
+    return p;
+}
+template <typename V> static V* dalloc_t(ddamg_handle* h, size_t count) {
+    return static_cast<V*>(dalloc(h, count * sizeof(V)));
+}
+static void sync(ddamg_handle* h) { DDAMG_CUDA_TRY(cudaStreamSynchronize(h->s)); }
+static void bad(const std::string& m) { throw ParamFailure{m}; }
+
+// ------------------------------------------------------------------ geometry
+static void build_geometry(ddamg_handle* h) {
+    const ddamg_params& p = h->p;
+    if (p.levels < 2 || p.levels > DDAMG_MAX_LEVELS) bad("levels must be in [2, " + std::to_string(DDAMG_MAX_LEVELS) + "]");
+    if (p.Nx < 2 || p.Nt < 2) bad("lattice too small");
+    if (p.max_rhs < 1) bad("max_rhs must be >= 1");
+    h->L = p.levels;
+    h->lv.resize(p.levels);
+    for (int l = 0; l < p.levels; l++) {
+        Geom& g = h->lv[l].g;
+        g.level = l;
+        if (l == 0) {
+            g.Nx = p.Nx;
+            g.Nt = p.Nt;
+            g.colors = 1;
+        } else {
+            const int* r = p.rows[l - 1];
+            g.Nx = r[1];
+            g.Nt = r[2];
+            g.colors = r[3];
+        }
+        g.dof = 2 * g.colors;
+        g.sites = g.Nx * g.Nt;
+        if (l < p.levels - 1) {
+            const int* r = p.rows[l];
+            if (r[0] != l) bad("parameters row " + std::to_string(l) + " has level " + std::to_string(r[0]));
+            g.agg_x = r[1];
+            g.agg_t = r[2];
+            g.ntest = r[3];
+            g.sap_x = r[4];
+            g.sap_t = r[5];
+            if (g.agg_x <= 0 || g.agg_t <= 0 || g.Nx % g.agg_x || g.Nt % g.agg_t)
+                bad("level " + std::to_string(l) + ": aggregation blocks must divide the lattice");
+            if (g.sap_x <= 0 || g.sap_t <= 0 || g.Nx % g.sap_x || g.Nt % g.sap_t)
+                bad("level " + std::to_string(l) + ": SAP blocks must divide the lattice");
+            if (g.ntest < 1 || g.ntest > 16) bad("test vectors per level must be in [1, 16]");
+            g.el_x = g.Nx / g.agg_x;
+            g.el_t = g.Nt / g.agg_t;
+            g.sel_x = g.Nx / g.sap_x;
+            g.sel_t = g.Nt / g.sap_t;
+            const int nb = g.sap_x * g.sap_t;
+            // the reference fills RedBlocks[block/2] (src/sap.cpp:30-37): an odd count > 1 overruns it
+            if (nb > 1 && nb % 2) bad("level " + std::to_string(l) + ": the number of SAP blocks must be even");
+            const int NE = g.sel_x * g.sel_t * g.dof;
+            if (NE > 4096) bad("SAP block has more than 4096 unknowns");
+            const size_t sm = sap_smem_bytes(p.sap_gmres_restart_length, NE, true);
+            if (sm > 227 * 1024) bad("SAP block Krylov basis does not fit in shared memory");
+            const int dc = 2 * g.ntest;
+            const size_t bl = 16 * ((size_t)5 * dc * dc + 2 * (size_t)g.dof * g.ntest + (size_t)g.dof * dc);
+            if (bl > 227 * 1024) bad("coarse-link construction does not fit in shared memory");
+            const size_t on = 16 * (size_t)g.ntest * g.el_x * g.el_t * g.colors;
+            if (on > 227 * 1024) bad("aggregate too large for the orthonormalisation kernel");
+        }
+        if (l > 0 && g.dof > 64) bad("at most 32 test vectors");
+    }
+    for (int l = 1; l < p.levels; l++) {
+        const Geom& pg = h->lv[l - 1].g;
+        const Geom& g = h->lv[l].g;
+        if (g.Nx != pg.agg_x || g.Nt != pg.agg_t || g.colors != pg.ntest) bad("inconsistent level sizes");
+    }
+    if (p.sap_gmres_restart_length < 1 || p.sap_gmres_restarts < 1 || p.coarse_gmres_restart_length < 1 ||
+        p.coarse_gmres_restarts < 1 || p.kcycle_restart_length < 1 || p.kcycle_restarts < 1 ||
+        p.fgmres_restart_length < 1 || p.fgmres_restarts < 1)
+        bad("restart lengths and counts must be >= 1");
+    if (p.nu1 < 0 || p.nu2 < 0 || p.sap_test_vectors_iterations < 0) bad("smoothing counts must be >= 0");
+    if (p.cycle != DDAMG_CYCLE_V && p.cycle != DDAMG_CYCLE_K) bad("cycle must be 0 (V) or 1 (K)");
+    if (p.precision != DDAMG_PREC_DOUBLE && p.precision != DDAMG_PREC_MIXED) bad("precision must be 0 or 1");
+    int W = p.max_rhs;
+    for (int l = 0; l < p.levels - 1; l++) W = std::max(W, h->lv[l].g.ntest);
+    h->W = W;
+}
+
+static void allocate(ddamg_handle* h) {
+    const ddamg_params& p = h->p;
+    const int W = h->W, L = h->L;
+    const bool mixed = p.precision == DDAMG_PREC_MIXED;
+    for (int l = 0; l < L; l++) {
+        LevelData& D = h->lv[l];
+        const Geom& g = D.g;
+        D.fp32 = mixed && l < L - 1;
+        const long n = g.size();
+        if (l == 0) D.d.U = dalloc_t<double2>(h, 2L * g.sites);
+        else D.d.links = dalloc_t<double2>(h, (size_t)g.sites * 5 * g.dof * g.dof);
+        if (l < L - 1) D.d.tv = dalloc_t<double2>(h, (size_t)g.ntest * n);
+        D.d.eta = dalloc_t<double2>(h, (size_t)W * n);
+        D.d.psi = dalloc_t<double2>(h, (size_t)W * n);
+        D.d.r = dalloc_t<double2>(h, (size_t)W * n);
+        D.d.t = dalloc_t<double2>(h, (size_t)W * n);
+        if (D.fp32) {
+            if (l == 0) D.f.U = dalloc_t<float2>(h, 2L * g.sites);
+            else D.f.links = dalloc_t<float2>(h, (size_t)g.sites * 5 * g.dof * g.dof);
+            D.f.tv = dalloc_t<float2>(h, (size_t)g.ntest * n);
+            D.f.eta = dalloc_t<float2>(h, (size_t)W * n);
+            D.f.psi = dalloc_t<float2>(h, (size_t)W * n);
+            D.f.r = dalloc_t<float2>(h, (size_t)W * n);
+            D.f.t = dalloc_t<float2>(h, (size_t)W * n);
+        }
+        // transfer buffer in the previous level's precision when it differs from this level's
+        if (l > 0 && h->lv[l - 1].fp32 && !D.fp32) D.f.xfer = dalloc_t<float2>(h, (size_t)W * n);
+        if (l > 0 && p.cycle == DDAMG_CYCLE_K) {
+            const int km = p.kcycle_restart_length;
+            if (D.fp32) {
+                D.f.kV = dalloc_t<float2>(h, (size_t)(km + 1) * n);
+                D.f.kZ = dalloc_t<float2>(h, (size_t)km * n);
+                D.f.kw = dalloc_t<float2>(h, n);
+                D.f.kr = dalloc_t<float2>(h, n);
+                D.f.kx = dalloc_t<float2>(h, n);
+            } else {
+                D.d.kV = dalloc_t<double2>(h, (size_t)(km + 1) * n);
+                D.d.kZ = dalloc_t<double2>(h, (size_t)km * n);
+                D.d.kw = dalloc_t<double2>(h, n);
+                D.d.kr = dalloc_t<double2>(h, n);
+                D.d.kx = dalloc_t<double2>(h, n);
+            }
+        }
+        D.done = dalloc_t<int>(h, W);
+        D.vv = dalloc_t<double>(h, W);
+        D.rr = dalloc_t<double>(h, W);
+        if (l < L - 1) {
+            // red iff (bx + bt) even (src/sap.cpp:27-38); a single block is both colours
+            std::vector<int> red, black;
+            const int nb = g.sap_x * g.sap_t;
+            for (int b = 0; b < nb; b++) {
+                const int bx = b / g.sap_t, bt = b % g.sap_t;
+                if (nb == 1) {
+                    red.push_back(b);
+                    black.push_back(b);
+                } else if ((bx + bt) % 2 == 0) red.push_back(b);
+                else black.push_back(b);
+            }
+            D.red = dalloc_t<int>(h, red.size());
+            D.black = dalloc_t<int>(h, black.size());
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(D.red, red.data(), red.size() * sizeof(int), cudaMemcpyHostToDevice, h->s));
+            DDAMG_CUDA_TRY(
+                cudaMemcpyAsync(D.black, black.data(), black.size() * sizeof(int), cudaMemcpyHostToDevice, h->s));
+            D.nred = (int)red.size();
+            D.nblack = (int)black.size();
+            sync(h);
+        }
+    }
+    // outer FGMRES (one right-hand side at a time)
+    const long n0 = h->lv[0].g.size();
+    const int m = p.fgmres_restart_length;
+    h->oV = dalloc_t<double2>(h, (size_t)(m + 1) * n0);
+    h->oZ = dalloc_t<double2>(h, (size_t)m * n0);
+    h->ow = dalloc_t<double2>(h, n0);
+    h->orr = dalloc_t<double2>(h, n0);
+    h->ob = dalloc_t<double2>(h, (size_t)p.max_rhs * n0);
+    h->ox = dalloc_t<double2>(h, (size_t)p.max_rhs * n0);
+    const int mm = std::max(m, std::max(p.kcycle_restart_length, 1)) + 2;
+    h->dpart = dalloc_t<double2>(h, (size_t)kRedBlocks * std::max(2 * mm, 2 * W + 2));
+    h->dh = dalloc_t<double2>(h, 2 * mm + 2);
+    h->dcoef = dalloc_t<double2>(h, 2 * mm + 2);
+    h->dn = dalloc_t<double>(h, 2 * W + 4);
+    DDAMG_CUDA_TRY(cudaMallocHost(&h->hpin, sizeof(double2) * (4 * mm + 8)));
+    // coarsest GMRES
+    const Geom& gc = h->lv[L - 1].g;
+    const int cm = p.coarse_gmres_restart_length;
+    coarse_gmres_prepare(h->cg, (int)gc.size(), cm, gc.dof, p.device);
+    h->cg.V = dalloc_t<double2>(h, (size_t)(cm + 1) * gc.size());
+    h->cg.w = dalloc_t<double2>(h, gc.size());
+    h->cg.r = dalloc_t<double2>(h, gc.size());
+    h->cg.partial = dalloc_t<double2>(h, (size_t)3 * h->cg.grid * (cm + 2));
+    h->cg.H = dalloc_t<double2>(h, (size_t)(cm + 1) * cm);
+    h->cg.bar = dalloc_t<unsigned>(h, 2);
+    h->cg.status = dalloc_t<int>(h, 2);
+    sync(h);
+}
+
+// ------------------------------------------------------------------ operators
+template <typename V> static void level_op(ddamg_handle* h, int l, const V* in, V* out, const V* b, int nrhs) {
+    LevelData& D = h->lv[l];
+    const Geom& g = D.g;
+    if (l == 0) launch_wilson<V>(h->s, B<V>(D).U, in, out, b, g.Nx, g.Nt, h->p.m0, 0, nrhs);
+    else launch_coarse_op<V>(h->s, B<V>(D).links, in, out, b, g.Nx, g.Nt, g.dof, h->p.m0, nrhs);
+}
+
+// SAP_C::SAP (src/sap.cpp:81-165) on nrhs independent vectors; returns the reference's value
+// for rhs 0 when want_iters (one host sync), else nu.
+template <typename V>
+static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, bool x_zero, int nrhs, bool want_iters) {
+    LevelData& D = h->lv[l];
+    const Geom& g = D.g;
+    const long n = g.size();
+    V* r = B<V>(D).r;
+    DDAMG_CUDA_TRY(cudaMemsetAsync(D.done, 0, sizeof(int) * nrhs, h->s));
+    const bool check = tol > 0.0;
+    if (check) launch_norm2<V>(h->s, v, n, n, nrhs, h->dpart, D.vv);
+    if (x_zero) DDAMG_CUDA_TRY(cudaMemcpyAsync(r, v, sizeof(V) * n * nrhs, cudaMemcpyDeviceToDevice, h->s));
+    else level_op<V>(h, l, x, r, v, nrhs);  // r = v - D x
+    SapArgs a{h->p.sap_gmres_restart_length, h->p.sap_gmres_restarts, h->p.sap_gmres_tolerance, h->p.m0, nullptr, 0,
+              D.done};
+    for (int it = 0; it < nu; it++) {
+        for (int colour = 0; colour < 2; colour++) {
+            a.blocks = colour == 0 ? D.red : D.black;
+            a.nblocks = colour == 0 ? D.nred : D.nblack;
+            if (l == 0) launch_sap_sweep_fine<V>(h->s, g, B<V>(D).U, r, x, a, nrhs);
+            else launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs);
+            // the residual after the last black sweep only feeds the convergence test
+            const bool last = (colour == 1 && it == nu - 1);
+            if (!last || (check && want_iters)) level_op<V>(h, l, x, r, v, nrhs);
+        }
+        if (check && (it < nu - 1 || want_iters)) {
+            launch_norm2<V>(h->s, r, n, n, nrhs, h->dpart, D.rr);
+            launch_flag_converged(h->s, D.rr, D.vv, tol, nrhs, it, D.done);
+        }
+    }
+    if (!want_iters) return nu;
+    int done0 = 0;
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(&done0, D.done, sizeof(int), cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    return done0 ? done0 - 1 : nu;
+}
+
+static int coarse_solve(ddamg_handle* h, const double2* b, double2* x) {
+    LevelData& D = h->lv[h->L - 1];
+    const Geom& g = D.g;
+    launch_coarse_gmres(h->s, h->cg, D.d.links, b, x, g.Nx, g.Nt, g.dof, h->p.m0, h->p.coarse_gmres_restart_length,
+                        h->p.coarse_gmres_restarts, h->p.coarse_gmres_tolerance);
+    return 0;
+}
+static void check_coarse_status(ddamg_handle* h, int* iters) {
+    int st[2];
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(st, h->cg.status, sizeof(st), cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    if (st[0] != 0) throw TimeoutFailure();
+    if (iters) *iters = st[1];
+}
+
+// ------------------------------------------------------------------ FGMRES (host driven)
+// FGMRES::fgmres (src/fgmres.cpp:5-97) with CGS2 for the Arnoldi step; the Hessenberg matrix,
+// Givens rotations and back substitution run on the host in FP64 (one sync per step).
+// prec(in, out, restart): out = M in, out holds the previous restart's Z_j (src/amg.cpp:43-45).
+template <typename V> struct Krylov {
+    V* Vb;
+    V* Z;
+    V* w;
+    V* r;
+};
+template <typename V>
+static int fgmres_host(ddamg_handle* h, long n, int m, int restarts, double tol,
+                       const std::function<void(const V*, V*)>& A,
+                       const std::function<void(const V*, V*, int)>* M, const V* b, const V* x0, bool x0_zero, V* x,
+                       Krylov<V> K, double* final_rel) {
+    cudaStream_t s = h->s;
+    if (x0_zero) DDAMG_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(V) * n, s));
+    else if (x0 != x) DDAMG_CUDA_TRY(cudaMemcpyAsync(x, x0, sizeof(V) * n, cudaMemcpyDeviceToDevice, s));
+    DDAMG_CUDA_TRY(cudaMemsetAsync(K.Z, 0, sizeof(V) * n * m, s));  // setZeros (include/fgmres.h:119-143)
+    if (x0_zero) DDAMG_CUDA_TRY(cudaMemcpyAsync(K.r, b, sizeof(V) * n, cudaMemcpyDeviceToDevice, s));
+    else {
+        A(x, K.w);
+        launch_sub<V>(s, b, K.w, K.r, n);
+    }
+    launch_norm2<V>(s, b, n, n, 1, h->dpart, h->dn);
+    launch_norm2<V>(s, K.r, n, n, 1, h->dpart, h->dn + 1);
+    double nrm[2];
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(nrm, h->dn, sizeof(nrm), cudaMemcpyDeviceToHost, s));
+    sync(h);
+    const double norm_b = std::sqrt(nrm[0]);
+    double err = std::sqrt(nrm[1]);
+    if (!(err == err) || !(norm_b == norm_b)) throw ParamFailure{"NaN in the right-hand side"};
+    std::vector<double2> H((size_t)(m + 1) * m), gm(m + 1), cn(m), sn(m), eta(m);
+    auto Hij = [&](int i, int j) -> double2& { return H[(size_t)i * m + j]; };
+    int maxIt = m;
+    int ret = restarts * m;
+    for (int k = 0; k < restarts; k++) {
+        launch_scale_host<V>(s, make_double2(1.0 / err, 0.0), K.r, K.Vb, n);
+        gm[0] = make_double2(err, 0.0);
+        bool brk = false;
+        for (int j = 0; j < m; j++) {
+            const V* vj = K.Vb + (long)j * n;
+            V* zj = K.Z + (long)j * n;
+            if (M) (*M)(vj, zj, k);
+            else DDAMG_CUDA_TRY(cudaMemcpyAsync(zj, vj, sizeof(V) * n, cudaMemcpyDeviceToDevice, s));
+            A(zj, K.w);
+            launch_multidot<V>(s, K.Vb, n, 0, j + 1, K.w, 0, n, 1, h->dpart, h->dh);
+            launch_multiaxpy<V>(s, K.Vb, n, 0, j + 1, h->dh, K.w, 0, n, 1, -1.0);
+            launch_multidot<V>(s, K.Vb, n, 0, j + 1, K.w, 0, n, 1, h->dpart, h->dh + (j + 1));
+            launch_multiaxpy<V>(s, K.Vb, n, 0, j + 1, h->dh + (j + 1), K.w, 0, n, 1, -1.0);
+            launch_norm2<V>(s, K.w, n, n, 1, h->dpart, h->dn);
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(h->hpin, h->dh, sizeof(double2) * 2 * (j + 1), cudaMemcpyDeviceToHost, s));
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(h->hpin + 2 * (j + 1), h->dn, sizeof(double), cudaMemcpyDeviceToHost, s));
+            sync(h);
+            for (int i = 0; i <= j; i++) Hij(i, j) = h->hpin[i] + h->hpin[j + 1 + i];
+            const double hn = std::sqrt(reinterpret_cast<double*>(h->hpin + 2 * (j + 1))[0]);
+            if (!(hn == hn)) throw ParamFailure{"NaN in the Krylov basis"};
+            Hij(j + 1, j) = make_double2(hn, 0.0);
+            if (hn > 0) launch_scale_host<V>(s, make_double2(1.0 / hn, 0.0), K.w, K.Vb + (long)(j + 1) * n, n);
+            for (int i = 0; i < j; i++) {  // FGMRES::rotation (src/fgmres.cpp:99-115)
+                double2 tmp = cmulc(cn[i], Hij(i, j)) + cmulc(sn[i], Hij(i + 1, j));
+                Hij(i + 1, j) = cmul(cn[i], Hij(i + 1, j)) - cmul(sn[i], Hij(i, j));
+                Hij(i, j) = tmp;
+            }
+            const double den = std::sqrt(cnorm2(Hij(j, j)) + cnorm2(Hij(j + 1, j)));
+            sn[j] = make_double2(Hij(j + 1, j).x / den, Hij(j + 1, j).y / den);
+            cn[j] = make_double2(Hij(j, j).x / den, Hij(j, j).y / den);
+            Hij(j, j) = cmulc(cn[j], Hij(j, j)) + cmulc(sn[j], Hij(j + 1, j));
+            Hij(j + 1, j) = make_double2(0.0, 0.0);
+            gm[j + 1] = -cmul(sn[j], gm[j]);
+            gm[j] = cmulc(cn[j], gm[j]);
+            if (std::sqrt(cnorm2(gm[j + 1])) < tol * norm_b) {
+                maxIt = j + 1;  // not reset at the next restart (src/fgmres.cpp:14,56)
+                brk = true;
+                break;
+            }
+        }
+        (void)brk;
+        for (int i = maxIt - 1; i >= 0; i--) {  // solve_upper_triangular (src/fgmres.cpp:118-128)
+            double2 e = gm[i];
+            for (int j = i + 1; j < maxIt; j++) e = e - cmul(Hij(i, j), eta[j]);
+            eta[i] = cdiv(e, Hij(i, i));
+        }
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(h->dcoef, eta.data(), sizeof(double2) * maxIt, cudaMemcpyHostToDevice, s));
+        launch_multiaxpy<V>(s, K.Z, n, 0, maxIt, h->dcoef, x, 0, n, 1, +1.0);
+        A(x, K.w);
+        launch_sub<V>(s, b, K.w, K.r, n);
+        launch_norm2<V>(s, K.r, n, n, 1, h->dpart, h->dn);
+        double rr;
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(&rr, h->dn, sizeof(double), cudaMemcpyDeviceToHost, s));
+        sync(h);
+        err = std::sqrt(rr);
+        if (!(err == err)) throw ParamFailure{"NaN residual"};
+        if (err < tol * norm_b) {
+            ret = k * m + maxIt;
+            break;
+        }
+    }
+    if (final_rel) *final_rel = norm_b > 0 ? err / norm_b : 0.0;
+    return ret;
+}
+
+// ------------------------------------------------------------------ cycles
+static void cycle(ddamg_handle* h, int l, const void* eta, void* psi, bool psi_zero, int kind);
+
+// the next level's input: restrict r (level l, type V) into level l+1's eta (its own type)
+template <typename V> static void* restrict_into_next(ddamg_handle* h, int l, const V* r) {
+    LevelData& D = h->lv[l];
+    LevelData& N = h->lv[l + 1];
+    const bool next32 = N.fp32;
+    const bool cur32 = std::is_same<V, float2>::value;
+    if (next32 == cur32) {
+        V* out = B<V>(N).eta;
+        launch_restrict<V>(h->s, D.g, B<V>(D).tv, r, out, 1);
+        return out;
+    }
+    // only float -> double happens (mixed: FP32 level above the FP64 coarsest level)
+    launch_restrict<V>(h->s, D.g, B<V>(D).tv, r, reinterpret_cast<V*>(N.f.xfer), 1);
+    launch_convert<float2, double2>(h->s, N.f.xfer, N.d.eta, N.g.size());
+    return N.d.eta;
+}
+template <typename V> static void prolong_from_next(ddamg_handle* h, int l, const void* psi_next, V* psi) {
+    LevelData& D = h->lv[l];
+    LevelData& N = h->lv[l + 1];
+    const bool cur32 = std::is_same<V, float2>::value;
+    if (N.fp32 == cur32) {
+        launch_prolong<V>(h->s, D.g, B<V>(D).tv, static_cast<const V*>(psi_next), psi, 1, 1);
+        return;
+    }
+    launch_convert<double2, float2>(h->s, static_cast<const double2*>(psi_next), N.f.xfer, N.g.size());
+    launch_prolong<V>(h->s, D.g, B<V>(D).tv, reinterpret_cast<const V*>(N.f.xfer), psi, 1, 1);
+}
+static void* next_psi(ddamg_handle* h, int l) {
+    LevelData& N = h->lv[l + 1];
+    return N.fp32 ? (void*)N.f.psi : (void*)N.d.psi;
+}
+
+// AlgebraicMG::v_cycle / k_cycle (src/amg.cpp:64-174) on one vector of level l
+template <typename V> static void cycle_t(ddamg_handle* h, int l, const V* eta, V* psi, bool psi_zero, int kind) {
+    const ddamg_params& p = h->p;
+    if (l == h->L - 1) {
+        coarse_solve(h, reinterpret_cast<const double2*>(eta), reinterpret_cast<double2*>(psi));
+        return;
+    }
+    LevelData& D = h->lv[l];
+    const long n = D.g.size();
+    if (psi_zero) DDAMG_CUDA_TRY(cudaMemsetAsync(psi, 0, sizeof(V) * n, h->s));
+    bool zero = psi_zero;
+    if (p.nu1 > 0) {
+        sap_t<V>(h, l, eta, psi, p.nu1, p.smoother_tolerance, zero, 1, false);
+        zero = false;
+    }
+    V* r = B<V>(D).r;
+    // r = eta - D psi (psi == 0 gives r = eta exactly)
+    const V* rin = eta;
+    if (!zero) {
+        level_op<V>(h, l, psi, r, eta, 1);
+        rin = r;
+    }
+    void* en = restrict_into_next<V>(h, l, rin);
+    void* pn = next_psi(h, l);
+    LevelData& N = h->lv[l + 1];
+    if (kind == DDAMG_CYCLE_V) {
+        cycle(h, l + 1, en, pn, true, kind);
+    } else {
+        // FGMRES_k_cycle at level l+1 (include/amg.h:16-94), x0 = rhs
+        const long nn = N.g.size();
+        auto run = [&](auto tag) {
+            typedef decltype(tag) W;
+            LevelBufs<W>& nb = B<W>(N);
+            std::function<void(const W*, W*)> A = [h, l](const W* in, W* out) {
+                level_op<W>(h, l + 1, in, out, nullptr, 1);
+            };
+            std::function<void(const W*, W*, int)> M = [h, l](const W* in, W* out, int restart) {
+                cycle(h, l + 1, in, out, restart == 0, DDAMG_CYCLE_K);
+            };
+            Krylov<W> K{nb.kV, nb.kZ, nb.kw, nb.kr};
+            fgmres_host<W>(h, nn, p.kcycle_restart_length, p.kcycle_restarts, p.kcycle_tolerance, A, &M,
+                           static_cast<const W*>(en), static_cast<const W*>(en), false, static_cast<W*>(pn), K,
+                           nullptr);
+        };
+        if (N.fp32) run(float2{});
+        else run(double2{});
+    }
+    prolong_from_next<V>(h, l, pn, psi);
+    if (p.nu2 > 0) sap_t<V>(h, l, eta, psi, p.nu2, p.smoother_tolerance, false, 1, false);
+}
+static void cycle(ddamg_handle* h, int l, const void* eta, void* psi, bool psi_zero, int kind) {
+    if (h->lv[l].fp32) cycle_t<float2>(h, l, static_cast<const float2*>(eta), static_cast<float2*>(psi), psi_zero, kind);
+    else cycle_t<double2>(h, l, static_cast<const double2*>(eta), static_cast<double2*>(psi), psi_zero, kind);
+    if (l == h->L - 1) check_coarse_status(h, nullptr);
+}
+
+// the outer preconditioner (FGMRES_AMG_*::preconditioner, include/amg.h:240-269): zero, one cycle
+static void outer_prec(ddamg_handle* h, const double2* in, double2* out) {
+    LevelData& D = h->lv[0];
+    const long n = D.g.size();
+    if (D.fp32) {
+        launch_convert<double2, float2>(h->s, in, D.f.eta, n);
+        cycle(h, 0, D.f.eta, D.f.psi, true, h->p.cycle);
+        launch_convert<float2, double2>(h->s, D.f.psi, out, n);
+    } else {
+        cycle(h, 0, in, out, true, h->p.cycle);
+    }
+}
+
+// ------------------------------------------------------------------ setup
+static void make_fp32_copies(ddamg_handle* h) {
+    for (int l = 0; l < h->L; l++) {
+        LevelData& D = h->lv[l];
+        if (!D.fp32) continue;
+        if (l == 0) launch_convert<double2, float2>(h->s, D.d.U, D.f.U, 2L * D.g.sites);
+        else launch_convert<double2, float2>(h->s, D.d.links, D.f.links, (long)D.g.sites * 5 * D.g.dof * D.g.dof);
+        if (l < h->L - 1) launch_convert<double2, float2>(h->s, D.d.tv, D.f.tv, (long)D.g.ntest * D.g.size());
+    }
+}
+
+static long setup_random_count(const ddamg_handle* h) {
+    long n = (long)h->lv[0].g.ntest * h->lv[0].g.size();
+    for (int l = 1; l < h->L - 1; l++) {
+        int extra = h->lv[l].g.ntest - h->lv[l - 1].g.ntest;
+        if (extra > 0) n += (long)extra * h->lv[l].g.size();
+    }
+    return n;
+}
+
+// AlgebraicMG::setUpPhase (src/amg.cpp:4-56).  rnd: device stream of random complex values
+// (or null with a seed: drawn on the device with the same counter RNG as the oracle).
+static void setup(ddamg_handle* h, const double2* rnd_host, uint64_t seed) {
+    if (!h->gauge) throw ParamFailure{"load the gauge field before the setup"};
+    cudaStream_t s = h->s;
+    DDAMG_CUDA_TRY(cudaEventRecord(h->ev0, s));
+    long pos = 0;
+    auto draw = [&](double2* dst, long count) {
+        if (rnd_host)
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(dst, rnd_host + pos, sizeof(double2) * count, cudaMemcpyHostToDevice, s));
+        else launch_fill_uniform(s, dst, count, seed, pos);
+        pos += count;
+    };
+    LevelData& L0 = h->lv[0];
+    draw(L0.d.tv, (long)L0.g.ntest * L0.g.size());
+    for (int l = 1; l < h->L - 1; l++) {
+        LevelData& D = h->lv[l];
+        LevelData& P = h->lv[l - 1];
+        const int from_prev = std::min(D.g.ntest, P.g.ntest);
+        // tvec_l[cc] = P^dagger tvec_{l-1}[cc] before level l-1 is smoothed (src/amg.cpp:25-41)
+        launch_restrict<double2>(s, P.g, P.d.tv, P.d.tv, D.d.tv, from_prev);
+        for (int cc = from_prev; cc < D.g.ntest; cc++) draw(D.d.tv + (long)cc * D.g.size(), D.g.size());
+    }
+    for (int l = 0; l < h->L - 1; l++) {
+        LevelData& D = h->lv[l];
+        const long n = D.g.size();
+        const int nv = D.g.ntest;
+        // SAP(rhs = 0, tvec, nu = SAP_test_vectors_iterations) on all test vectors at once
+        DDAMG_CUDA_TRY(cudaMemsetAsync(D.d.eta, 0, sizeof(double2) * n * nv, s));
+        sap_t<double2>(h, l, D.d.eta, D.d.tv, h->p.sap_test_vectors_iterations, 1e-10, false, nv, false);
+        launch_orthonormalize(s, D.g, D.d.tv);
+        launch_build_coarse_links(s, D.g, D.d.U, D.d.links, D.d.tv, h->lv[l + 1].d.links);
+    }
+    make_fp32_copies(h);
+    DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, s));
+    sync(h);
+    float ms = 0;
+    DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->last_setup_s = ms * 1e-3;
+    h->setup_done = true;
+}
+
+// ------------------------------------------------------------------ solve
+static ddamg_status solve_device(ddamg_handle* h, const double2* b, double2* x, int nrhs, ddamg_solve_info* info) {
+    if (!h->setup_done) throw ParamFailure{"run the setup before solving"};
+    const ddamg_params& p = h->p;
+    const long n = h->lv[0].g.size();
+    const Geom& g0 = h->lv[0].g;
+    ddamg_status st = DDAMG_OK;
+    for (int r = 0; r < nrhs; r++) {
+        DDAMG_CUDA_TRY(cudaEventRecord(h->ev0, h->s));
+        std::function<void(const double2*, double2*)> A = [h, &g0](const double2* in, double2* out) {
+            launch_wilson<double2>(h->s, h->lv[0].d.U, in, out, nullptr, g0.Nx, g0.Nt, h->p.m0, 0, 1);
+        };
+        std::function<void(const double2*, double2*, int)> M = [h](const double2* in, double2* out, int) {
+            outer_prec(h, in, out);
+        };
+        Krylov<double2> K{h->oV, h->oZ, h->ow, h->orr};
+        double rel = 0;
+        int it = fgmres_host<double2>(h, n, p.fgmres_restart_length, p.fgmres_restarts, p.fgmres_tolerance, A, &M,
+                                      b + r * n, nullptr, true, x + r * n, K, &rel);
+        DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, h->s));
+        sync(h);
+        float ms = 0;
+        DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        const bool conv = rel < p.fgmres_tolerance;
+        if (!conv) st = DDAMG_NOT_CONVERGED;
+        if (info) {
+            info[r].iterations = it;
+            info[r].converged = conv ? 1 : 0;
+            info[r].rel_residual = rel;
+            info[r].setup_seconds = h->last_setup_s;
+            info[r].solve_seconds = ms * 1e-3;
+        }
+    }
+    return st;
+}
+
+}  // namespace ddamg
+
+// ====================================================================== C API
+using namespace ddamg;
+
+#define API_BEGIN try {
+#define API_END                                                                                  \
+    }                                                                                            \
+    catch (const ParamFailure& e) {                                                              \
+        set_error(e.msg);                                                                        \
+        return DDAMG_ERR_BAD_PARAM;                                                              \
+    }                                                                                            \
+    catch (const CudaFailure&) {                                                                 \
+        return DDAMG_ERR_CUDA;                                                                   \
+    }                                                                                            \
+    catch (const TimeoutFailure&) {                                                              \
+        set_error("a bounded device-side wait gave up (grid barrier timeout)");                  \
+        return DDAMG_ERR_DEVICE_TIMEOUT;                                                         \
+    }                                                                                            \
+    catch (const std::exception& e) {                                                            \
+        set_error(e.what());                                                                     \
+        return DDAMG_ERR_STATE;                                                                  \
+    }                                                                                            \
+    return DDAMG_OK;
+
+#define CHECK_HANDLE(h)                                                                          \
+    if (!(h)) {                                                                                  \
+        set_error("null handle");                                                                \
+        return DDAMG_ERR_BAD_PARAM;                                                              \
+    }                                                                                            \
+    DDAMG_CUDA_TRY(cudaSetDevice((h)->p.device));
+
+static void need_level(ddamg_handle* h, int l, bool allow_coarsest) {
+    if (l < 0 || l >= h->L || (!allow_coarsest && l == h->L - 1)) throw ParamFailure{"level out of range"};
+}
+static void need_setup(ddamg_handle* h) {
+    if (!h->setup_done) throw ParamFailure{"run the setup first"};
+}
+
+extern "C" {
+
+const char* ddamg_last_error(void) { return t_last_error.c_str(); }
+
+ddamg_status ddamg_params_default(ddamg_params* p) {
+    if (!p) return DDAMG_ERR_BAD_PARAM;
+    std::memset(p, 0, sizeof(*p));
+    p->sap_gmres_restart_length = 5;
+    p->sap_gmres_restarts = 5;
+    p->sap_gmres_tolerance = 1e-3;
+    p->sap_test_vectors_iterations = 4;
+    p->coarse_gmres_restart_length = 400;
+    p->coarse_gmres_restarts = 10;
+    p->coarse_gmres_tolerance = 0.1;
+    p->nu1 = 0;
+    p->nu2 = 2;
+    p->kcycle_restart_length = 5;
+    p->kcycle_restarts = 2;
+    p->kcycle_tolerance = 0.1;
+    p->fgmres_restart_length = 20;
+    p->fgmres_restarts = 50;
+    p->fgmres_tolerance = 1e-10;
+    p->smoother_tolerance = 1e-10;
+    p->cycle = DDAMG_CYCLE_V;
+    p->precision = DDAMG_PREC_DOUBLE;
+    p->max_rhs = 1;
+    p->device = 0;
+    return DDAMG_OK;
+}
+
+ddamg_status ddamg_parse_params_file(const char* path, int levels, ddamg_params* p) {
+    if (!path || !p) return DDAMG_ERR_BAD_PARAM;
+    std::ifstream f(path);
+    if (!f) {
+        set_error(std::string("File ") + path + " not found");
+        return DDAMG_ERR_IO;
+    }
+    int v[6], count = 0;
+    while (f >> v[0] >> v[1] >> v[2] >> v[3] >> v[4] >> v[5]) {
+        if (count >= DDAMG_MAX_LEVELS - 1) {
+            set_error("too many rows in the parameters file");
+            return DDAMG_ERR_BAD_PARAM;
+        }
+        for (int k = 0; k < 6; k++) p->rows[count][k] = v[k];
+        count++;
+    }
+    if (!f.eof()) {
+        set_error("malformed parameters file (expected 6 integers per row)");
+        return DDAMG_ERR_BAD_PARAM;
+    }
+    if (count != levels - 1) {
+        set_error("The number of levels in the inputs file does not match the number of levels assigned");
+        return DDAMG_ERR_BAD_PARAM;
+    }
+    p->levels = levels;
+    return DDAMG_OK;
+}
+
+ddamg_status ddamg_create(const ddamg_params* p, ddamg_t** out) {
+    if (!p || !out) return DDAMG_ERR_BAD_PARAM;
+    *out = nullptr;
+    auto* h = new ddamg_handle();
+    h->p = *p;
+    try {
+        DDAMG_CUDA_TRY(cudaSetDevice(p->device));
+        build_geometry(h);
+        DDAMG_CUDA_TRY(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
+        DDAMG_CUDA_TRY(cudaEventCreate(&h->ev0));
+        DDAMG_CUDA_TRY(cudaEventCreate(&h->ev1));
+        allocate(h);
+    } catch (const ParamFailure& e) {
+        set_error(e.msg);
+        ddamg_destroy(h);
+        return DDAMG_ERR_BAD_PARAM;
+    } catch (const CudaFailure&) {
+        ddamg_destroy(h);
+        return DDAMG_ERR_CUDA;
+    }
+    h->launches_at_create = g_launches;
+    *out = h;
+    return DDAMG_OK;
+}
+
+ddamg_status ddamg_destroy(ddamg_t* h) {
+    if (!h) return DDAMG_OK;
+    cudaSetDevice(h->p.device);
+    if (h->s) cudaStreamSynchronize(h->s);
+    for (void* a : h->allocs) cudaFree(a);
+    if (h->hpin) cudaFreeHost(h->hpin);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->s) cudaStreamDestroy(h->s);
+    delete h;
+    return DDAMG_OK;
+}
+
+ddamg_status ddamg_get_stream(ddamg_t* h, void** stream) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    *stream = (void*)h->s;
+    API_END
+}
+ddamg_status ddamg_launch_count(ddamg_t* h, long long* count) {
+    if (!count) return DDAMG_ERR_BAD_PARAM;
+    *count = g_launches;
+    (void)h;
+    return DDAMG_OK;
+}
+
+ddamg_status ddamg_read_binary(const char* path, int Nx, int Nt, double* out) {
+    if (!path || !out || Nx <= 0 || Nt <= 0) return DDAMG_ERR_BAD_PARAM;
+    std::ifstream f(path, std::ios::binary);
+    if (!f) {
+        set_error(std::string("File ") + path + " not found");
+        return DDAMG_ERR_IO;
+    }
+    for (long i = 0; i < 2L * Nx * Nt; i++) {
+        int32_t hdr[3];
+        double re_im[2];
+        f.read(reinterpret_cast<char*>(hdr), sizeof(hdr));
+        f.read(reinterpret_cast<char*>(re_im), sizeof(re_im));
+        if (!f) {
+            set_error(std::string("short file ") + path);
+            return DDAMG_ERR_IO;
+        }
+        out[2 * i] = re_im[0];
+        out[2 * i + 1] = re_im[1];
+    }
+    return DDAMG_OK;
+}
+ddamg_status ddamg_write_binary(const char* path, int Nx, int Nt, const double* field) {
+    if (!path || !field || Nx <= 0 || Nt <= 0) return DDAMG_ERR_BAD_PARAM;
+    std::ofstream f(path, std::ios::binary);
+    if (!f) return DDAMG_ERR_IO;
+    for (int x = 0; x < Nx; x++)
+        for (int t = 0; t < Nt; t++)
+            for (int mu = 0; mu < 2; mu++) {
+                int32_t hdr[3] = {x, t, mu};
+                long i = ((long)x * Nt + t) * 2 + mu;
+                f.write(reinterpret_cast<const char*>(hdr), sizeof(hdr));
+                f.write(reinterpret_cast<const char*>(field + 2 * i), 2 * sizeof(double));
+            }
+    return f ? DDAMG_OK : DDAMG_ERR_IO;
+}
+
+ddamg_status ddamg_load_gauge(ddamg_t* h, const double* U) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (!U) throw ParamFailure{"null gauge field"};
+    LevelData& D = h->lv[0];
+    const long n = 2L * D.g.sites;
+    for (long i = 0; i < 2 * n; i++)
+        if (!std::isfinite(U[i])) {
+            set_error("non-finite value in the gauge field");
+            return DDAMG_ERR_NAN;
+        }
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.U, U, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    if (D.fp32) launch_convert<double2, float2>(h->s, D.d.U, D.f.U, n);
+    sync(h);
+    h->gauge = true;
+    h->setup_done = false;
+    API_END
+}
+
+static ddamg_status apply_dirac_dev(ddamg_t* h, int dagger, const double2* in, double2* out, int nrhs) {
+    const Geom& g = h->lv[0].g;
+    launch_wilson<double2>(h->s, h->lv[0].d.U, in, out, nullptr, g.Nx, g.Nt, h->p.m0, dagger, nrhs);
+    return DDAMG_OK;
+}
+
+ddamg_status ddamg_apply_dirac(ddamg_t* h, int dagger, const double* in, double* out, int nrhs) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (!h->gauge) throw ParamFailure{"no gauge field loaded"};
+    if (nrhs < 1 || nrhs > h->W) throw ParamFailure{"nrhs out of range"};
+    const long n = h->lv[0].g.size() * nrhs;
+    LevelData& D = h->lv[0];
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.eta, in, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    apply_dirac_dev(h, dagger, D.d.eta, D.d.psi, nrhs);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(out, D.d.psi, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    API_END
+}
+ddamg_status ddamg_apply_dirac_device(ddamg_t* h, int dagger, const void* in, void* out, int nrhs) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (!h->gauge) throw ParamFailure{"no gauge field loaded"};
+    apply_dirac_dev(h, dagger, static_cast<const double2*>(in), static_cast<double2*>(out), nrhs);
+    API_END
+}
+ddamg_status ddamg_apply_dirac_f32_device(ddamg_t* h, int dagger, const void* in, void* out, int nrhs) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (!h->gauge) throw ParamFailure{"no gauge field loaded"};
+    LevelData& D = h->lv[0];
+    if (!D.f.U) {
+        D.f.U = dalloc_t<float2>(h, 2L * D.g.sites);
+        launch_convert<double2, float2>(h->s, D.d.U, D.f.U, 2L * D.g.sites);
+    }
+    launch_wilson<float2>(h->s, D.f.U, static_cast<const float2*>(in), static_cast<float2*>(out), nullptr, D.g.Nx,
+                          D.g.Nt, h->p.m0, dagger, nrhs);
+    API_END
+}
+
+ddamg_status ddamg_apply_level_op(ddamg_t* h, int level, const double* in, double* out) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    need_level(h, level, true);
+    if (level == 0 && !h->gauge) throw ParamFailure{"no gauge field loaded"};
+    if (level > 0) need_setup(h);
+    LevelData& D = h->lv[level];
+    const long n = D.g.size();
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.eta, in, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    level_op<double2>(h, level, D.d.eta, D.d.psi, nullptr, 1);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(out, D.d.psi, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    API_END
+}
+
+ddamg_status ddamg_restrict(ddamg_t* h, int level, const double* in, double* out) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    need_level(h, level, false);
+    need_setup(h);
+    LevelData& D = h->lv[level];
+    LevelData& N = h->lv[level + 1];
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.eta, in, sizeof(double2) * D.g.size(), cudaMemcpyHostToDevice, h->s));
+    launch_restrict<double2>(h->s, D.g, D.d.tv, D.d.eta, N.d.psi, 1);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(out, N.d.psi, sizeof(double2) * N.g.size(), cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    API_END
+}
+ddamg_status ddamg_prolong(ddamg_t* h, int level, const double* in, double* out) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    need_level(h, level, false);
+    need_setup(h);
+    LevelData& D = h->lv[level];
+    LevelData& N = h->lv[level + 1];
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(N.d.eta, in, sizeof(double2) * N.g.size(), cudaMemcpyHostToDevice, h->s));
+    launch_prolong<double2>(h->s, D.g, D.d.tv, N.d.eta, D.d.psi, 0, 1);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(out, D.d.psi, sizeof(double2) * D.g.size(), cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    API_END
+}
+
+ddamg_status ddamg_sap(ddamg_t* h, int level, const double* v, double* x, int nu, double tol, int* iters) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    need_level(h, level, false);
+    if (level == 0 && !h->gauge) throw ParamFailure{"no gauge field loaded"};
+    if (level > 0) need_setup(h);
+    if (nu < 0) throw ParamFailure{"nu must be >= 0"};
+    LevelData& D = h->lv[level];
+    const long n = D.g.size();
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.eta, v, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.psi, x, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    int it = sap_t<double2>(h, level, D.d.eta, D.d.psi, nu, tol, false, 1, true);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(x, D.d.psi, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    if (iters) *iters = it;
+    API_END
+}
+
+ddamg_status ddamg_setup(ddamg_t* h, uint64_t seed) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    setup(h, nullptr, seed);
+    API_END
+}
+ddamg_status ddamg_setup_random_count(ddamg_t* h, int64_t* n) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    *n = setup_random_count(h);
+    API_END
+}
+ddamg_status ddamg_setup_with_vectors(ddamg_t* h, const double* rnd, int64_t n) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (!rnd || n < setup_random_count(h)) throw ParamFailure{"random stream too short"};
+    setup(h, reinterpret_cast<const double2*>(rnd), 0);
+    API_END
+}
+ddamg_status ddamg_get_test_vectors(ddamg_t* h, int level, double* out) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    need_level(h, level, false);
+    LevelData& D = h->lv[level];
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(out, D.d.tv, sizeof(double2) * D.g.ntest * D.g.size(), cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    API_END
+}
+ddamg_status ddamg_set_test_vectors(ddamg_t* h, int level, const double* in) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    need_level(h, level, false);
+    LevelData& D = h->lv[level];
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.tv, in, sizeof(double2) * D.g.ntest * D.g.size(), cudaMemcpyHostToDevice, h->s));
+    if (D.fp32) launch_convert<double2, float2>(h->s, D.d.tv, D.f.tv, (long)D.g.ntest * D.g.size());
+    sync(h);
+    API_END
+}
+ddamg_status ddamg_orthonormalize(ddamg_t* h, int level) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    need_level(h, level, false);
+    LevelData& D = h->lv[level];
+    launch_orthonormalize(h->s, D.g, D.d.tv);
+    if (D.fp32) launch_convert<double2, float2>(h->s, D.d.tv, D.f.tv, (long)D.g.ntest * D.g.size());
+    sync(h);
+    API_END
+}
+ddamg_status ddamg_build_coarse_links(ddamg_t* h, int level) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    need_level(h, level, false);
+    if (!h->gauge) throw ParamFailure{"no gauge field loaded"};
+    LevelData& D = h->lv[level];
+    LevelData& N = h->lv[level + 1];
+    launch_build_coarse_links(h->s, D.g, D.d.U, D.d.links, D.d.tv, N.d.links);
+    if (N.fp32) launch_convert<double2, float2>(h->s, N.d.links, N.f.links, (long)N.g.sites * 5 * N.g.dof * N.g.dof);
+    sync(h);
+    API_END
+}
+ddamg_status ddamg_get_coarse_links(ddamg_t* h, int level, int which, double* out) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (level < 1 || level >= h->L) throw ParamFailure{"coarse links exist on levels >= 1"};
+    if (which < 1 || which > 3) throw ParamFailure{"which must be 1, 2 or 3"};
+    LevelData& D = h->lv[level];
+    const int dof = D.g.dof, C = D.g.colors;
+    std::vector<double2> M((size_t)D.g.sites * 5 * dof * dof);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(M.data(), D.d.links, sizeof(double2) * M.size(), cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    double2* o = reinterpret_cast<double2*>(out);
+    for (int n = 0; n < D.g.sites; n++)
+        for (int alf = 0; alf < 2; alf++)
+            for (int bet = 0; bet < 2; bet++)
+                for (int c = 0; c < C; c++)
+                    for (int b = 0; b < C; b++) {
+                        const int i = c * 2 + alf, j = b * 2 + bet;
+                        auto get = [&](int d) { return M[(((size_t)n * 5 + d) * dof + j) * dof + i]; };
+                        const size_t base = ((((size_t)n * 2 + alf) * 2 + bet) * C + c) * C + b;
+                        if (which == 1) o[base] = get(0);
+                        else
+                            for (int mu = 0; mu < 2; mu++) o[base * 2 + mu] = get(which == 2 ? 1 + mu : 3 + mu);
+                    }
+    API_END
+}
+
+ddamg_status ddamg_coarse_solve(ddamg_t* h, const double* b, double* x, int* iters) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    need_setup(h);
+    LevelData& D = h->lv[h->L - 1];
+    const long n = D.g.size();
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.eta, b, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    coarse_solve(h, D.d.eta, D.d.psi);
+    int it = 0;
+    check_coarse_status(h, &it);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(x, D.d.psi, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    if (iters) *iters = it;
+    API_END
+}
+
+static ddamg_status run_cycle(ddamg_t* h, const double* eta, double* psi, int kind) {
+    need_setup(h);
+    const long n = h->lv[0].g.size();
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(h->ow, eta, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    const int saved = h->p.cycle;
+    h->p.cycle = kind;
+    try {
+        outer_prec(h, h->ow, h->orr);
+    } catch (...) {
+        h->p.cycle = saved;
+        throw;
+    }
+    h->p.cycle = saved;
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(psi, h->orr, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    return DDAMG_OK;
+}
+ddamg_status ddamg_vcycle(ddamg_t* h, const double* eta, double* psi) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    return run_cycle(h, eta, psi, DDAMG_CYCLE_V);
+    API_END
+}
+ddamg_status ddamg_kcycle(ddamg_t* h, const double* eta, double* psi) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (h->p.cycle != DDAMG_CYCLE_K) throw ParamFailure{"the K-cycle needs a handle created with cycle = DDAMG_CYCLE_K"};
+    return run_cycle(h, eta, psi, DDAMG_CYCLE_K);
+    API_END
+}
+
+ddamg_status ddamg_solve_device(ddamg_t* h, const void* b, void* x, int nrhs, ddamg_solve_info* info) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (nrhs < 1) throw ParamFailure{"nrhs must be >= 1"};
+    return solve_device(h, static_cast<const double2*>(b), static_cast<double2*>(x), nrhs, info);
+    API_END
+}
+ddamg_status ddamg_solve(ddamg_t* h, const double* b, double* x, int nrhs, ddamg_solve_info* info) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (nrhs < 1 || nrhs > h->p.max_rhs) throw ParamFailure{"nrhs must be in [1, max_rhs]"};
+    const long n = h->lv[0].g.size() * nrhs;
+    for (long i = 0; i < 2 * n; i++)
+        if (!std::isfinite(b[i])) {
+            set_error("non-finite value in the right-hand side");
+            return DDAMG_ERR_NAN;
+        }
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(h->ob, b, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    ddamg_status st = solve_device(h, h->ob, h->ox, nrhs, info);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(x, h->ox, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    return st;
+    API_END
+}
+
+ddamg_status ddamg_gmres_plain(ddamg_t* h, const double* b, double* x, int m, int restarts, double tol,
+                               ddamg_solve_info* info) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (!h->gauge) throw ParamFailure{"no gauge field loaded"};
+    if (m < 1 || restarts < 1) throw ParamFailure{"m and restarts must be >= 1"};
+    const Geom& g0 = h->lv[0].g;
+    const long n = g0.size();
+    double2* Vb = dalloc_t<double2>(h, (size_t)(m + 1) * n);
+    double2* Z = dalloc_t<double2>(h, (size_t)m * n);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(h->ob, b, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    std::function<void(const double2*, double2*)> A = [h, &g0](const double2* in, double2* out) {
+        launch_wilson<double2>(h->s, h->lv[0].d.U, in, out, nullptr, g0.Nx, g0.Nt, h->p.m0, 0, 1);
+    };
+    Krylov<double2> K{Vb, Z, h->ow, h->orr};
+    double rel = 0;
+    DDAMG_CUDA_TRY(cudaEventRecord(h->ev0, h->s));
+    int it = fgmres_host<double2>(h, n, m, restarts, tol, A, nullptr, h->ob, nullptr, true, h->ox, K, &rel);
+    DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, h->s));
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(x, h->ox, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    float ms = 0;
+    DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    // release the temporary basis
+    for (void* q : {(void*)Vb, (void*)Z}) {
+        cudaFree(q);
+        h->allocs.erase(std::find(h->allocs.begin(), h->allocs.end(), q));
+    }
+    if (info) {
+        info->iterations = it;
+        info->converged = rel < tol;
+        info->rel_residual = rel;
+        info->setup_seconds = 0;
+        info->solve_seconds = ms * 1e-3;
+    }
+    if (!(rel < tol)) return DDAMG_NOT_CONVERGED;
+    API_END
+}
+
+ddamg_status ddamg_link_derivative(ddamg_t* h, const double* psi, const double* lambda, double* out) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (!h->gauge) throw ParamFailure{"no gauge field loaded"};
+    LevelData& D = h->lv[0];
+    const long n = D.g.size();
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.eta, psi, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.psi, lambda, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    double* g = reinterpret_cast<double*>(D.d.r);
+    launch_link_derivative(h->s, D.d.U, D.d.eta, D.d.psi, g, D.g.Nx, D.g.Nt);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(out, g, sizeof(double) * 2 * D.g.sites, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    API_END
+}
+
+ddamg_status ddamg_gradient(ddamg_t* h, const double* eta, const double* b, double* out, ddamg_solve_info* info) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    need_setup(h);
+    LevelData& D = h->lv[0];
+    const long n = D.g.size();
+    const long sites = D.g.sites;
+    ddamg_solve_info inf[2];
+    if (!h->grad) h->grad = dalloc_t<double2>(h, 3 * (size_t)n);
+    double2 *gpsi = h->grad, *glam = h->grad + n, *gtmp = h->grad + 2 * n;
+    // psi = D^-1 b
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(h->ob, b, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    ddamg_status s1 = solve_device(h, h->ob, gpsi, 1, &inf[0]);
+    // lambda = D^-dagger eta = sigma_3 D^-1 sigma_3 eta (gamma_5-hermiticity)
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(gtmp, eta, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    launch_sigma3(h->s, gtmp, h->ob, sites);
+    ddamg_status s2 = solve_device(h, h->ob, gtmp, 1, &inf[1]);
+    launch_sigma3(h->s, gtmp, glam, sites);
+    double* g = reinterpret_cast<double*>(gtmp);
+    launch_link_derivative(h->s, D.d.U, gpsi, glam, g, D.g.Nx, D.g.Nt);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(out, g, sizeof(double) * 2 * sites, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    if (info) {
+        info[0] = inf[0];
+        info[1] = inf[1];
+    }
+    if (s1 != DDAMG_OK) return s1;
+    if (s2 != DDAMG_OK) return s2;
+    API_END
+}
+
+ddamg_status ddamg_gauge_metropolis(int Nx, int Nt, double beta, int sweeps, uint64_t seed, double delta,
+                                    double* theta, double* acceptance, int device) {
+    if (!theta || Nx < 2 || Nt < 2 || (Nx & 1) || (Nt & 1) || sweeps < 0) return DDAMG_ERR_BAD_PARAM;
+    try {
+        DDAMG_CUDA_TRY(cudaSetDevice(device));
+        cudaStream_t s;
+        DDAMG_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        double* th = nullptr;
+        unsigned long long* acc = nullptr;
+        DDAMG_CUDA_TRY(cudaMalloc(&th, sizeof(double) * 2 * Nx * Nt));
+        DDAMG_CUDA_TRY(cudaMalloc(&acc, sizeof(unsigned long long)));
+        launch_metropolis_init(s, th, Nx, Nt, seed);
+        for (int sw = 0; sw < sweeps; sw++) {
+            if (sw == sweeps - 1) DDAMG_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(unsigned long long), s));
+            for (int sub = 0; sub < 4; sub++) launch_metropolis_sub(s, th, Nx, Nt, beta, delta, seed, sw, sub, acc);
+        }
+        unsigned long long a = 0;
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(theta, th, sizeof(double) * 2 * Nx * Nt, cudaMemcpyDeviceToHost, s));
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(&a, acc, sizeof(a), cudaMemcpyDeviceToHost, s));
+        DDAMG_CUDA_TRY(cudaStreamSynchronize(s));
+        cudaFree(th);
+        cudaFree(acc);
+        cudaStreamDestroy(s);
+        if (acceptance) *acceptance = sweeps > 0 ? (double)a / (2.0 * Nx * Nt) : 0.0;
+    } catch (const CudaFailure&) {
+        return DDAMG_ERR_CUDA;
+    }
+    return DDAMG_OK;
+}
+
+ddamg_status ddamg_gaussian_field(int64_t n, uint64_t seed, double* out) {
+    if (!out || n < 0) return DDAMG_ERR_BAD_PARAM;
+    const double pi = 3.14159265358979323846;
+    for (int64_t i = 0; i < n; i++) {
+        double u1 = u01(rng64(seed, kStreamGauss, (uint64_t)(2 * i)));
+        double u2 = u01(rng64(seed, kStreamGauss, (uint64_t)(2 * i + 1)));
+        double r = std::sqrt(-std::log(1.0 - u1));
+        out[2 * i] = r * std::cos(2.0 * pi * u2);
+        out[2 * i + 1] = r * std::sin(2.0 * pi * u2);
+    }
+    return DDAMG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,253 @@
+"""Python host API of the B200 DD-alphaAMG solver for the 2D Schwinger-model Wilson-Dirac operator.
+
+A thin layer over the C ABI (include/ddamg.h, libddamg.so) that keeps the reference's
+operator names (JFNCastellanos/DDalphaAMG-SM): D_phi / D_dagger_phi, Level.D_operator,
+P_vc / Pdagg_v, SAP, setUpPhase, v_cycle / k_cycle, FGMRES with a multigrid preconditioner.
+Fields are numpy complex128 arrays laid out [site][dof] with site = x*Nt + t (x slow),
+mu = 0 along t, mu = 1 along x.  Every call runs on the GPU; a missing library raises.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import CYCLE_K, CYCLE_V, PREC_DOUBLE, PREC_MIXED, DDAMGError, Params, SolveInfo, check
+
+__all__ = ["Solver", "Params", "SolveInfo", "DDAMGError", "default_params", "read_parameters", "read_binary",
+           "write_binary", "gauge_metropolis", "gaussian_field", "PREC_DOUBLE", "PREC_MIXED", "CYCLE_V", "CYCLE_K"]
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def default_params(Nx=0, Nt=0, levels=2, m0=0.0, rows=(), **kw):
+    """Reference defaults (src/variables.cpp:100-134) plus geometry; keyword overrides any field."""
+    p = Params()
+    check(_lib.load().ddamg_params_default(ctypes.byref(p)))
+    p.Nx, p.Nt, p.levels, p.m0 = Nx, Nt, levels, m0
+    for i, r in enumerate(rows):
+        for k in range(6):
+            p.rows[i][k] = int(r[k])
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def read_parameters(path, levels, params=None):
+    """readParameters (include/params.h:18-111)."""
+    p = params if params is not None else default_params()
+    check(_lib.load().ddamg_parse_params_file(path.encode(), levels, ctypes.byref(p)))
+    return p
+
+
+def read_binary(path, Nx, Nt):
+    """read_binary (src/io.cpp:4-55): returns [site][mu] complex128."""
+    out = np.zeros(2 * Nx * Nt, dtype=np.complex128)
+    check(_lib.load().ddamg_read_binary(path.encode(), Nx, Nt, _dp(out)))
+    return out
+
+
+def write_binary(path, Nx, Nt, field):
+    f = _c(field)
+    check(_lib.load().ddamg_write_binary(path.encode(), Nx, Nt, _dp(f)))
+
+
+def gauge_metropolis(Nx, Nt, beta, sweeps, seed, delta=1.0, device=0):
+    """U(1) Metropolis on the GPU; returns (theta [site][mu], acceptance of the last sweep)."""
+    th = np.zeros(2 * Nx * Nt)
+    acc = ctypes.c_double(0)
+    check(_lib.load().ddamg_gauge_metropolis(Nx, Nt, beta, sweeps, seed, delta, _dp(th), ctypes.byref(acc), device))
+    return th, acc.value
+
+
+def gaussian_field(n, seed):
+    out = np.zeros(n, dtype=np.complex128)
+    check(_lib.load().ddamg_gaussian_field(n, seed, _dp(out)))
+    return out
+
+
+class Solver:
+    """One multigrid hierarchy on one GPU (AlgebraicMG + FGMRES_AMG of the reference)."""
+
+    def __init__(self, params):
+        self.L = _lib.load()
+        self.params = params
+        h = ctypes.c_void_p()
+        check(self.L.ddamg_create(ctypes.byref(params), ctypes.byref(h)))
+        self.h = h
+        self.Nx, self.Nt, self.levels = params.Nx, params.Nt, params.levels
+        self._sizes = [self.Nx * self.Nt * 2]
+        self._ntest = []
+        for l in range(self.levels - 1):
+            r = params.rows[l]
+            self._ntest.append(r[3])
+            self._sizes.append(r[1] * r[2] * 2 * r[3])
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ddamg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def size(self, level):
+        return self._sizes[level]
+
+    # ------------------------------------------------------------ inputs
+    def load_gauge(self, U):
+        U = _c(U)
+        check(self.L.ddamg_load_gauge(self.h, _dp(U)))
+
+    # ------------------------------------------------------------ operators
+    def D_phi(self, phi, nrhs=1):
+        phi = _c(phi)
+        out = np.empty_like(phi)
+        check(self.L.ddamg_apply_dirac(self.h, 0, _dp(phi), _dp(out), nrhs))
+        return out
+
+    def D_dagger_phi(self, phi, nrhs=1):
+        phi = _c(phi)
+        out = np.empty_like(phi)
+        check(self.L.ddamg_apply_dirac(self.h, 1, _dp(phi), _dp(out), nrhs))
+        return out
+
+    def D_operator(self, level, v):
+        v = _c(v)
+        out = np.empty(self.size(level), dtype=np.complex128)
+        check(self.L.ddamg_apply_level_op(self.h, level, _dp(v), _dp(out)))
+        return out
+
+    def Pdagg_v(self, level, v):
+        v = _c(v)
+        out = np.empty(self.size(level + 1), dtype=np.complex128)
+        check(self.L.ddamg_restrict(self.h, level, _dp(v), _dp(out)))
+        return out
+
+    def P_vc(self, level, vc):
+        vc = _c(vc)
+        out = np.empty(self.size(level), dtype=np.complex128)
+        check(self.L.ddamg_prolong(self.h, level, _dp(vc), _dp(out)))
+        return out
+
+    def SAP(self, level, v, x0=None, nu=2, tol=1e-10):
+        """SAP_C::SAP (src/sap.cpp:81-165); returns (x, iterations)."""
+        v = _c(v)
+        x = np.zeros(self.size(level), dtype=np.complex128) if x0 is None else np.array(x0, dtype=np.complex128)
+        it = ctypes.c_int(0)
+        check(self.L.ddamg_sap(self.h, level, _dp(v), _dp(x), nu, tol, ctypes.byref(it)))
+        return x, it.value
+
+    # ------------------------------------------------------------ setup
+    def setup_random_count(self):
+        n = ctypes.c_int64(0)
+        check(self.L.ddamg_setup_random_count(self.h, ctypes.byref(n)))
+        return n.value
+
+    def setUpPhase(self, seed=None, vectors=None):
+        """AlgebraicMG::setUpPhase (src/amg.cpp:4-62) from a seed or an explicit random stream."""
+        if vectors is not None:
+            v = _c(vectors)
+            check(self.L.ddamg_setup_with_vectors(self.h, _dp(v), v.size))
+        else:
+            check(self.L.ddamg_setup(self.h, 0 if seed is None else int(seed)))
+
+    def test_vectors(self, level):
+        out = np.empty(self._ntest[level] * self.size(level), dtype=np.complex128)
+        check(self.L.ddamg_get_test_vectors(self.h, level, _dp(out)))
+        return out
+
+    def set_test_vectors(self, level, tv):
+        tv = _c(tv)
+        check(self.L.ddamg_set_test_vectors(self.h, level, _dp(tv)))
+
+    def orthonormalize(self, level):
+        check(self.L.ddamg_orthonormalize(self.h, level))
+
+    def makeCoarseLinks(self, level):
+        check(self.L.ddamg_build_coarse_links(self.h, level))
+
+    def coarse_links(self, level, which):
+        """G1 (which=1), G2 (2), G3 (3) of level >= 1 in the reference layout (include/level.h:349-365)."""
+        C = self._ntest[level - 1]
+        n = (self.size(level) // (2 * C)) * 4 * C * C * (1 if which == 1 else 2)
+        out = np.empty(n, dtype=np.complex128)
+        check(self.L.ddamg_get_coarse_links(self.h, level, which, _dp(out)))
+        return out
+
+    # ------------------------------------------------------------ solvers
+    def coarse_gmres(self, b):
+        b = _c(b)
+        x = np.empty_like(b)
+        it = ctypes.c_int(0)
+        check(self.L.ddamg_coarse_solve(self.h, _dp(b), _dp(x), ctypes.byref(it)))
+        return x, it.value
+
+    def v_cycle(self, eta):
+        eta = _c(eta)
+        psi = np.empty_like(eta)
+        check(self.L.ddamg_vcycle(self.h, _dp(eta), _dp(psi)))
+        return psi
+
+    def k_cycle(self, eta):
+        eta = _c(eta)
+        psi = np.empty_like(eta)
+        check(self.L.ddamg_kcycle(self.h, _dp(eta), _dp(psi)))
+        return psi
+
+    def solve(self, b, nrhs=1, allow_not_converged=False):
+        """FGMRES_AMG_{v,k}_cycle::fgmres from x0 = 0; returns (x, [SolveInfo])."""
+        b = _c(b)
+        x = np.empty_like(b)
+        info = (SolveInfo * nrhs)()
+        check(self.L.ddamg_solve(self.h, _dp(b), _dp(x), nrhs, info),
+              allow=(_lib.NOT_CONVERGED,) if allow_not_converged else ())
+        return x, list(info)
+
+    def solve_device(self, b_ptr, x_ptr, nrhs=1):
+        info = (SolveInfo * nrhs)()
+        check(self.L.ddamg_solve_device(self.h, ctypes.c_void_p(b_ptr), ctypes.c_void_p(x_ptr), nrhs, info))
+        return list(info)
+
+    def gmres_plain(self, b, m=50, restarts=200, tol=1e-10):
+        b = _c(b)
+        x = np.empty_like(b)
+        info = SolveInfo()
+        check(self.L.ddamg_gmres_plain(self.h, _dp(b), _dp(x), m, restarts, tol, ctypes.byref(info)),
+              allow=(_lib.NOT_CONVERGED,))
+        return x, info
+
+    def gradient(self, eta, b):
+        """dL/dtheta_mu(x) for L = Re(eta^dagger D^-1 b); returns ([site][mu] float64, infos)."""
+        eta, b = _c(eta), _c(b)
+        out = np.empty(2 * self.Nx * self.Nt)
+        info = (SolveInfo * 2)()
+        check(self.L.ddamg_gradient(self.h, _dp(eta), _dp(b), _dp(out), info))
+        return out, list(info)
+
+    def link_derivative(self, psi, lam):
+        psi, lam = _c(psi), _c(lam)
+        out = np.empty(2 * self.Nx * self.Nt)
+        check(self.L.ddamg_link_derivative(self.h, _dp(psi), _dp(lam), _dp(out)))
+        return out
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        check(self.L.ddamg_get_stream(self.h, ctypes.byref(s)))
+        return s.value or 0
+
+    @staticmethod
+    def launch_count():
+        c = ctypes.c_longlong(0)
+        check(_lib.load().ddamg_launch_count(None, ctypes.byref(c)))
+        return c.value

@@ -1,0 +1,180 @@
+/*
+ * ddamg.h — C ABI of the B200-native DD-alphaAMG solver for the 2D Schwinger-model
+ * Wilson-Dirac operator.  Drop-in for the solve path of the reference
+ * (JFNCastellanos/DDalphaAMG-SM); each entry point names the reference interface it
+ * replaces.
+ *
+ * Conventions (identical to the reference):
+ *   - lattice Nx (x, slow) by Nt (t, fast); site = x*Nt + t; no halo;
+ *   - mu = 0 is the t direction, mu = 1 the x direction (include/boundary.h:32-36);
+ *   - fermions periodic in x, antiperiodic in t; links periodic (include/boundary.h:38-46);
+ *   - a level-l vector is [site][c][alpha] with dof = c*2 + alpha (src/level.cpp:403);
+ *   - every complex number is two doubles (re, im), interleaved; a field of n complex
+ *     numbers is a double[2n];
+ *   - several right-hand sides are stored one after another: [rhs][site][dof].
+ *
+ * Host pointers are caller-owned and may be pageable; *_device variants take device
+ * pointers on the handle's device.  One handle owns its device memory and one CUDA stream
+ * and is not thread-safe; different handles are independent.  Every call returns a
+ * ddamg_status; ddamg_last_error() describes the last failure on the calling thread.
+ */
+#ifndef DDAMG_H
+#define DDAMG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DDAMG_MAX_LEVELS 6
+
+typedef enum {
+    DDAMG_OK = 0,
+    DDAMG_ERR_BAD_PARAM = 1,      /* reference: exit(1)/MPI_Abort on bad input (include/params.h:22-25,101-104) */
+    DDAMG_ERR_IO = 2,             /* reference: exit(1) in read_binary / readParameters (src/io.cpp:7-10) */
+    DDAMG_NOT_CONVERGED = 3,      /* reference: only the returned count restarts*m (src/fgmres.cpp:93-96) */
+    DDAMG_ERR_NAN = 4,            /* NaN/Inf found in an input or a residual */
+    DDAMG_ERR_DEVICE_TIMEOUT = 5, /* a bounded device-side wait (grid barrier) gave up */
+    DDAMG_ERR_CUDA = 6,           /* a CUDA runtime error */
+    DDAMG_ERR_STATE = 7           /* call out of order (e.g. solve before setup) */
+} ddamg_status;
+
+typedef enum { DDAMG_PREC_DOUBLE = 0, DDAMG_PREC_MIXED = 1 } ddamg_precision;
+typedef enum { DDAMG_CYCLE_V = 0, DDAMG_CYCLE_K = 1 } ddamg_cycle;
+
+/* Solver parameters.  Geometry comes from the parameters file (include/params.h:18-111),
+ * the constants from the reference's globals (src/variables.cpp:100-134); defaults are
+ * the reference's values. */
+typedef struct {
+    int Nx, Nt;          /* lattice (reference: compile-time NS, NT from config.h) */
+    int levels;          /* reference: stdin "Levels" (src/main.cpp:33-46) */
+    double m0;           /* bare mass (mass::m0) */
+    /* parameters-file rows: level block_x block_t ntest sap_block_x sap_block_t;
+     * block_* and sap_block_* are block COUNTS (include/params.h:7-16) */
+    int rows[DDAMG_MAX_LEVELS - 1][6];
+    int sap_gmres_restart_length;     /* 5    SAPV::sap_gmres_restart_length */
+    int sap_gmres_restarts;           /* 5    SAPV::sap_gmres_restarts */
+    double sap_gmres_tolerance;       /* 1e-3 SAPV::sap_gmres_tolerance */
+    int sap_test_vectors_iterations;  /* 4    AMGV::SAP_test_vectors_iterations */
+    int coarse_gmres_restart_length;  /* 400  AMGV::gmres_restart_length_coarse_level */
+    int coarse_gmres_restarts;        /* 10   AMGV::gmres_restarts_coarse_level */
+    double coarse_gmres_tolerance;    /* 0.1  AMGV::gmres_tol_coarse_level */
+    int nu1, nu2;                     /* 0, 2 AMGV::nu1, AMGV::nu2 */
+    int kcycle_restart_length;        /* 5    AMGV::fgmres_k_cycle_restart_length */
+    int kcycle_restarts;              /* 2    AMGV::fgmres_k_cycle_restarts */
+    double kcycle_tolerance;          /* 0.1  AMGV::fgmres_k_cycle_tol */
+    int fgmres_restart_length;        /* 20   FGMRESV::fgmres_restart_length */
+    int fgmres_restarts;              /* 50   FGMRESV::fgmres_restarts */
+    double fgmres_tolerance;          /* 1e-10 FGMRESV::fgmres_tolerance */
+    double smoother_tolerance;        /* 1e-10, the tol the cycles pass to SAP (src/amg.cpp:65) */
+    int cycle;                        /* ddamg_cycle; reference: AMGV::cycle */
+    int precision;                    /* ddamg_precision; the reference is FP64 only */
+    int max_rhs;                      /* right-hand sides one ddamg_solve call may carry (>= 1) */
+    int device;                       /* CUDA device ordinal */
+} ddamg_params;
+
+typedef struct {
+    int iterations;        /* outer FGMRES iterations, as FGMRES::fgmres returns (src/fgmres.cpp:89,96) */
+    int converged;         /* 1 if the true residual met the tolerance */
+    double rel_residual;   /* ||b - D x|| / ||b|| with the FP64 operator */
+    double setup_seconds;  /* device time of the last setup */
+    double solve_seconds;  /* device time of this solve */
+} ddamg_solve_info;
+
+typedef struct ddamg_handle ddamg_t;
+
+/* ------------------------------------------------------------------ configuration */
+/* fills the reference defaults (src/variables.cpp:100-134); geometry zeroed */
+ddamg_status ddamg_params_default(ddamg_params* p);
+/* readParameters (include/params.h:18-111): one row per non-coarsest level; the number
+ * of rows must equal levels-1 (include/params.h:101-104) */
+ddamg_status ddamg_parse_params_file(const char* path, int levels, ddamg_params* p);
+/* Level / AlgebraicMG construction (include/level.h:147-233, include/amg.h:96-114):
+ * validates the geometry and allocates every level's device storage */
+ddamg_status ddamg_create(const ddamg_params* p, ddamg_t** h);
+ddamg_status ddamg_destroy(ddamg_t* h);
+const char* ddamg_last_error(void);
+/* the cudaStream_t the handle launches on (as void*) */
+ddamg_status ddamg_get_stream(ddamg_t* h, void** stream);
+/* number of kernels this handle has launched so far */
+ddamg_status ddamg_launch_count(ddamg_t* h, long long* count);
+
+/* ------------------------------------------------------------------ I/O */
+/* read_binary (src/io.cpp:4-55): records int32 x, t, mu, f64 re, im, x slowest; out: [site][mu] */
+ddamg_status ddamg_read_binary(const char* path, int Nx, int Nt, double* out);
+/* writer of the same format (the reference has none; its inputs come from HMC) */
+ddamg_status ddamg_write_binary(const char* path, int Nx, int Nt, const double* field);
+/* gauge links U_mu(x) (spinor U of src/main.cpp:74-78), [site][mu] complex */
+ddamg_status ddamg_load_gauge(ddamg_t* h, const double* U);
+
+/* ------------------------------------------------------------------ operators */
+/* D_phi / D_dagger_phi (src/dirac_operator.cpp:24-85); nrhs fields back to back */
+ddamg_status ddamg_apply_dirac(ddamg_t* h, int dagger, const double* in, double* out, int nrhs);
+ddamg_status ddamg_apply_dirac_device(ddamg_t* h, int dagger, const void* in, void* out, int nrhs);
+/* the same stencil in FP32 on device buffers of float pairs (mixed-precision smoother operator) */
+ddamg_status ddamg_apply_dirac_f32_device(ddamg_t* h, int dagger, const void* in, void* out, int nrhs);
+/* Level::D_operator (src/level.cpp:394-426) at level l >= 0, FP64 */
+ddamg_status ddamg_apply_level_op(ddamg_t* h, int level, const double* in, double* out);
+/* Level::Pdagg_v (src/level.cpp:145-189): level l -> l+1 */
+ddamg_status ddamg_restrict(ddamg_t* h, int level, const double* in, double* out);
+/* Level::P_vc (src/level.cpp:92-141): level l+1 -> l */
+ddamg_status ddamg_prolong(ddamg_t* h, int level, const double* in, double* out);
+/* SAP_C::SAP (src/sap.cpp:81-165) at level l: x is the initial guess on entry and the
+ * result on exit; *iters gets SAP's return value */
+ddamg_status ddamg_sap(ddamg_t* h, int level, const double* v, double* x, int nu, double tol, int* iters);
+
+/* ------------------------------------------------------------------ setup */
+/* AlgebraicMG::setUpPhase (src/amg.cpp:4-62) with test vectors drawn on the device from a
+ * counter-based generator (splitmix64) seeded by `seed`: re, im ~ U(-1, 1) as in src/amg.cpp:7 */
+ddamg_status ddamg_setup(ddamg_t* h, uint64_t seed);
+/* the same with every random vector supplied, in the order setUpPhase draws them
+ * (src/amg.cpp:12-41): level-0 vectors, then the extra vectors of each level >= 1 */
+ddamg_status ddamg_setup_with_vectors(ddamg_t* h, const double* rnd, int64_t n_complex);
+/* number of complex values ddamg_setup_with_vectors consumes */
+ddamg_status ddamg_setup_random_count(ddamg_t* h, int64_t* n_complex);
+/* Level::tvec access (include/level.h:251): [ntest][site][dof] */
+ddamg_status ddamg_get_test_vectors(ddamg_t* h, int level, double* out);
+ddamg_status ddamg_set_test_vectors(ddamg_t* h, int level, const double* in);
+/* Level::orthonormalize (src/level.cpp:193-284) */
+ddamg_status ddamg_orthonormalize(ddamg_t* h, int level);
+/* Level::makeCoarseLinks (src/level.cpp:431-542): builds level+1's operator */
+ddamg_status ddamg_build_coarse_links(ddamg_t* h, int level);
+/* coarse links of level l >= 1 in the reference layout (include/level.h:349-365):
+ * which = 1: G1[site][alf][bet][c][b]; 2: G2 and 3: G3 [site][alf][bet][c][b][mu] */
+ddamg_status ddamg_get_coarse_links(ddamg_t* h, int level, int which, double* out);
+
+/* ------------------------------------------------------------------ solvers */
+/* coarsest solve Level::GMRES_level_l (include/level.h:70-140), x0 = b (src/amg.cpp:69) */
+ddamg_status ddamg_coarse_solve(ddamg_t* h, const double* b, double* x, int* iters);
+/* one cycle from psi = 0: AlgebraicMG::v_cycle / k_cycle (src/amg.cpp:64-174) */
+ddamg_status ddamg_vcycle(ddamg_t* h, const double* eta, double* psi);
+ddamg_status ddamg_kcycle(ddamg_t* h, const double* eta, double* psi);
+/* FGMRES_AMG_v_cycle / _k_cycle::fgmres (include/amg.h:147-270, src/fgmres.cpp:5-97) from
+ * x0 = 0 for nrhs right-hand sides; info may be NULL or point to nrhs entries */
+ddamg_status ddamg_solve(ddamg_t* h, const double* b, double* x, int nrhs, ddamg_solve_info* info);
+ddamg_status ddamg_solve_device(ddamg_t* h, const void* b, void* x, int nrhs, ddamg_solve_info* info);
+/* FGMRES_fine_level (include/fgmres.h:153-236): unpreconditioned GMRES(m) on D_W */
+ddamg_status ddamg_gmres_plain(ddamg_t* h, const double* b, double* x, int m, int restarts, double tol,
+                               ddamg_solve_info* info);
+
+/* ------------------------------------------------------------------ gradient (no reference counterpart) */
+/* L = Re(eta^dagger D^-1 b): solves D psi = b and D^dagger lambda = eta through the same
+ * multigrid (D^dagger = sigma_3 D sigma_3) and forms dL/dtheta_mu(x) = out[site*2 + mu] */
+ddamg_status ddamg_gradient(ddamg_t* h, const double* eta, const double* b, double* dL_dtheta,
+                            ddamg_solve_info* info);
+/* the link-derivative kernel alone, given psi = D^-1 b and lambda = D^-dagger eta */
+ddamg_status ddamg_link_derivative(ddamg_t* h, const double* psi, const double* lambda, double* dL_dtheta);
+
+/* ------------------------------------------------------------------ inputs (no reference counterpart) */
+/* U(1) Metropolis of S = beta sum_P (1 - cos theta_P), hot start theta ~ U[-pi, pi), on the
+ * device; theta: [site][mu]; *acceptance: acceptance rate of the last sweep (may be NULL) */
+ddamg_status ddamg_gauge_metropolis(int Nx, int Nt, double beta, int sweeps, uint64_t seed, double delta,
+                                    double* theta, double* acceptance, int device);
+/* complex Gaussian right-hand sides, E|z|^2 = 1 */
+ddamg_status ddamg_gaussian_field(int64_t n_complex, uint64_t seed, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
