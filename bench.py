@@ -1,0 +1,449 @@
+"""Benchmark: DD-alphaAMG time-to-solution on one B200 (per rank), with the reference's CPU solve beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the reference's FP64 3-level configuration): 256x256 lattice, U(1) links from 1000
+seeded Metropolis sweeps of the Wilson plaquette action at beta = 3 (hot start), m0 = -0.10,
+parameters "0 64 64 12 64 64 / 1 16 16 12 16 16" (4x4-site aggregates and SAP blocks, Nv = 12),
+FGMRES(30) with a V-cycle to relative residual 1e-10, one complex Gaussian right-hand side.
+A step is one time-to-solution: the adaptive setup from a seed plus the preconditioned FGMRES
+solve, as the reference times it (src/methods.cpp:153-170 starts the clock before the setup).
+
+Our arm prints one JSON line (rank 0); `value` has the inputs resident in HBM, `e2e` goes through
+the public C ABI with pinned host buffers.  The reference arm runs the reference's own code
+(oracle/_ref/ref_harness_256x256, built from its sources against a single-rank MPI stand-in):
+one full solve per step, steps run as concurrent single-core processes.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "ddalphaamg-sm_b200"))
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+
+WORKLOAD = dict(Nx=256, Nt=256, levels=3, m0=-0.10, beta=3.0, sweeps=1000, seed=2025, delta=1.0,
+                rows=[[0, 64, 64, 12, 64, 64], [1, 16, 16, 12, 16, 16]], fgmres_m=30, fgmres_restarts=50, tol=1e-10,
+                rhs_seed=77, setup_seed=5)
+WORKLOAD_NAME = ("DD-alphaAMG FP64 3-level time-to-solution (setup + FGMRES(30) V-cycle to 1e-10, one RHS): 256x256 "
+                 "U(1) beta=3 (1000 Metropolis sweeps), m0=-0.10, 4x4 aggregates / SAP blocks, Nv=12")
+REF_BIN = os.path.join(REPO, "oracle", "_ref", "ref_harness_256x256")
+L2_FLUSH_BYTES = 512 << 20
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------- inputs (CPU generators, identical in both arms)
+def make_inputs():
+    import pyoracle as po
+
+    w = WORKLOAD
+    theta, acc = po.metropolis(w["Nx"], w["Nt"], w["beta"], w["sweeps"], w["seed"], w["delta"])
+    U = po.links_from_theta(theta)
+    b = po.gaussian(2 * w["Nx"] * w["Nt"], w["rhs_seed"])
+    return U, b, acc, po.plaquette(w["Nx"], w["Nt"], theta)
+
+
+def write_ref_inputs(d, U, b):
+    import pyoracle as po
+
+    w = WORKLOAD
+    conf, rhs, par = os.path.join(d, "conf.bin"), os.path.join(d, "rhs.bin"), os.path.join(d, "params")
+    po.write_binary(conf, w["Nx"], w["Nt"], U)
+    po.write_binary(rhs, w["Nx"], w["Nt"], b)
+    with open(par, "w") as f:
+        for r in w["rows"]:
+            f.write(" ".join(map(str, r)) + "\n")
+    return conf, rhs, par
+
+
+def start_reference_solve(d, conf, rhs, par, tag):
+    """The reference's own FGMRES_AMG_v_cycle path with its stock mt19937 setup, one core."""
+    w = WORKLOAD
+    out = os.path.join(d, f"out_{tag}")
+    os.makedirs(out, exist_ok=True)
+    cmd = [REF_BIN, "solve", str(w["levels"]), repr(w["m0"]), par, conf, rhs, "-", out, "0", str(w["fgmres_m"]),
+           str(w["fgmres_restarts"]), repr(w["tol"])]
+    return subprocess.Popen(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE), out
+
+
+def read_reference(out):
+    meta = dict(line.split() for line in open(os.path.join(out, "solve.txt")))
+    return dict(iterations=int(meta["iterations"]), setup_s=float(meta["setup_s"]), solve_s=float(meta["solve_s"]),
+                relres=float(meta["relres"]), x=np.fromfile(os.path.join(out, "x.bin"), dtype=np.complex128))
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            t = [v.strip() for v in line.split(",")]
+            if len(t) < 9:
+                continue
+            try:
+                rows.append((float(t[1]), float(t[2]), float(t[3]), t[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[3]) if v.lower().startswith("active")})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
+
+
+# ---------------------------------------------------------------- helpers
+def peaks():
+    try:
+        p = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+        return p["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel_key):
+    """dram bytes per launch from a committed ncu summary (profiles/<...>.txt line 'traffic_bytes_per_launch')."""
+    path = os.path.join(REPO, "profiles", "sap_sweep_l1_256x256.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch") and kernel_key in line:
+            try:
+                return float(line.split()[-1])
+            except ValueError:
+                return None
+    return None
+
+
+def sap_sweep_bytes(level_geom, fp_bytes):
+    """Algorithmic HBM bytes of one SAP colour sweep: the colour's links read once, r read, x read and written."""
+    g = level_geom
+    sites_colour = g["sites"] / 2
+    if g["level"] == 0:
+        links = sites_colour * 2 * 2 * fp_bytes  # U_0, U_1 complex per site
+    else:
+        links = sites_colour * 5 * g["dof"] ** 2 * 2 * fp_bytes
+    vecs = 3 * sites_colour * g["dof"] * 2 * fp_bytes
+    return links + vecs
+
+
+def level_geoms():
+    w = WORKLOAD
+    gs = [dict(level=0, sites=w["Nx"] * w["Nt"], dof=2)]
+    for l, r in enumerate(w["rows"]):
+        gs.append(dict(level=l + 1, sites=r[1] * r[2], dof=2 * r[3]))
+    return gs
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    if not os.path.exists(REF_BIN):
+        print(json.dumps({"impl": "reference", "unavailable": f"{REF_BIN} not built (needs the reference sources)"}))
+        return 0
+    U, b, _, _ = make_inputs()
+    d = tempfile.mkdtemp(prefix="refarm_")
+    conf, rhs, par = write_ref_inputs(d, U, b)
+    n = args.warmup + args.steps
+    ncpu = os.cpu_count() or 1
+    par_n = max(1, min(n, ncpu - 1))
+    results = []
+    t0 = time.time()
+    i = 0
+    while i < n:
+        batch = []
+        for j in range(i, min(n, i + par_n)):
+            batch.append(start_reference_solve(d, conf, rhs, par, j))
+        for p, out in batch:
+            p.wait()
+            if p.returncode != 0:
+                print(json.dumps({"impl": "reference", "unavailable": f"reference solve failed: {p.stderr.read()[-300:]}"}))
+                return 0
+            results.append(read_reference(out))
+        i += par_n
+    wall = time.time() - t0
+    timed = results[args.warmup:]
+    tts = [1e3 * (r["setup_s"] + r["solve_s"]) for r in timed]
+    v = statistics.median(tts)
+    line = {
+        "impl": "reference", "metric": "time_to_solution", "value": v, "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": {"workload": WORKLOAD_NAME},
+        "iterations": timed[0]["iterations"], "rel_residual": timed[0]["relres"],
+        "setup_ms": statistics.median(1e3 * r["setup_s"] for r in timed),
+        "solve_ms": statistics.median(1e3 * r["solve_s"] for r in timed),
+        "cpu_baseline": {"value": v, "unit": "ms", "cores": 1, "kind": "reference",
+                         "sample": f"{n} full 256x256 solves of the reference's own code (single rank, MPI stand-in), "
+                                   f"run {par_n} at a time as separate single-core processes; first {args.warmup} "
+                                   f"discarded; median of {args.steps}; wall {wall:.0f} s"},
+        "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    import ddamg
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    w = WORKLOAD
+    U, b, acc, plaq = make_inputs()
+    cpu_proc = None
+    want_cpu = (rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_BIN))
+    if want_cpu:  # the single-core reference solve runs while the GPU is measured (disjoint resources)
+        dref = tempfile.mkdtemp(prefix="cpubase_")
+        cpu_proc = start_reference_solve(dref, *write_ref_inputs(dref, U, b), "base")
+
+    def params(precision):
+        return ddamg.default_params(w["Nx"], w["Nt"], w["levels"], w["m0"], w["rows"], precision=precision,
+                                    fgmres_restart_length=w["fgmres_m"], fgmres_restarts=w["fgmres_restarts"],
+                                    fgmres_tolerance=w["tol"], device=local_rank)
+
+    s = ddamg.Solver(params(ddamg.PREC_DOUBLE))
+    s.load_gauge(U)
+    stream = torch.cuda.ExternalStream(s.stream())
+    n = b.size
+    b_dev = torch.from_numpy(b.view(np.float64).copy()).to(f"cuda:{local_rank}")
+    x_dev = torch.zeros_like(b_dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
+
+    def step():
+        s.setUpPhase(seed=w["setup_seed"])
+        return s.solve_device(b_dev.data_ptr(), x_dev.data_ptr())[0]
+
+    for _ in range(args.warmup):
+        info = step()
+    # ---- timed region: K steps, L2 flushed between steps, events on the library's stream
+    launches0 = ddamg.Solver.launch_count()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    infos = []
+    s.profile(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                starts[k].record(stream)
+            infos.append(step())
+            with torch.cuda.stream(stream):
+                ends[k].record(stream)
+        torch.cuda.synchronize()
+    s.profile(False)
+    if dist:
+        dist.barrier()
+    launches = ddamg.Solver.launch_count() - launches0
+    step_ms = [starts[k].elapsed_time(ends[k]) for k in range(args.steps)]
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{local_rank}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    clocks = clk.summary()
+    x = x_dev.cpu().numpy().view(np.complex128)
+    # dominant kernel of the timed region
+    best = None
+    for kind in (0, 1, 2):
+        for l in range(w["levels"]):
+            ms, cnt = s.profile_query(kind, l)
+            if cnt and (best is None or ms > best[2]):
+                best = (kind, l, ms, cnt)
+    kinds = {0: "sap_block_kernel (SAP colour sweep)", 1: "coarse_gmres_kernel", 2: "level operator"}
+    hbm, peak_kind = peaks()
+    roof = None
+    if best and best[0] == 0:
+        g = level_geoms()[best[1]]
+        bytes_per = sap_sweep_bytes(g, 8)
+        avg_ms = best[2] / best[3]
+        ach = bytes_per / (avg_ms * 1e-3) / 1e9
+        roof = {"kernel": f"{kinds[0]} level {best[1]}", "bound": "hbm", "achieved": ach, "peak": hbm,
+                "unit": "GB/s", "frac": ach / hbm, "traffic": profiled_traffic(f"level{best[1]}"),
+                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_per, "avg_launch_ms": avg_ms,
+                "launches": best[3], "share_of_step": best[2] / total_ms if total_ms else None}
+    elif best:
+        roof = {"kernel": kinds[best[0]] + f" level {best[1]}", "bound": "hbm", "achieved": None, "peak": hbm,
+                "unit": "GB/s", "frac": None, "traffic": None, "avg_launch_ms": best[2] / best[3]}
+    # ---- e2e through the public API with pinned host buffers
+    Ut = torch.from_numpy(U.view(np.float64).copy()).pin_memory()
+    bt = torch.from_numpy(b.view(np.float64).copy()).pin_memory()
+    xt = torch.zeros_like(bt).pin_memory()
+    L = s.L
+    import ctypes
+
+    dp = ctypes.POINTER(ctypes.c_double)
+    e2e_ms = []
+    for k in range(args.warmup + args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ddamg.check(L.ddamg_load_gauge(s.h, ctypes.cast(Ut.data_ptr(), dp)))
+        ddamg.check(L.ddamg_setup(s.h, w["setup_seed"]))
+        info_e = (ddamg.SolveInfo * 1)()
+        ddamg.check(L.ddamg_solve(s.h, ctypes.cast(bt.data_ptr(), dp), ctypes.cast(xt.data_ptr(), dp), 1, info_e))
+        t1 = time.perf_counter()
+        if k >= args.warmup:
+            e2e_ms.append(1e3 * (t1 - t0))
+    e2e = statistics.median(e2e_ms)
+    if dist:
+        t = torch.tensor([e2e], device=f"cuda:{local_rank}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = float(t.item())
+    # ---- secondary: mixed precision on the same workload, D_W bandwidth
+    sec = {}
+    if rank == 0:
+        sm = ddamg.Solver(params(ddamg.PREC_MIXED))
+        sm.load_gauge(U)
+        xm = torch.zeros_like(b_dev)
+        for _ in range(2):
+            sm.setUpPhase(seed=w["setup_seed"])
+            im = sm.solve_device(b_dev.data_ptr(), xm.data_ptr())[0]
+        sec["mixed_same_workload"] = {
+            "time_to_solution_ms": 1e3 * (im.setup_seconds + im.solve_seconds), "setup_ms": 1e3 * im.setup_seconds,
+            "solve_ms": 1e3 * im.solve_seconds, "iterations": im.iterations, "rel_residual": im.rel_residual,
+            "rel_err_vs_fp64": float(np.linalg.norm(xm.cpu().numpy().view(np.complex128) - x) / np.linalg.norm(x))}
+        sm.close()
+        sec["dw_gbs"] = dw_bandwidth(ddamg, torch, local_rank)
+    # ---- CPU baseline (the reference's own code, one core, the same workload)
+    cpu = None
+    err_vs_ref = None
+    if cpu_proc:
+        p, out = cpu_proc
+        p.wait()
+        if p.returncode == 0:
+            r = read_reference(out)
+            tts = 1e3 * (r["setup_s"] + r["solve_s"])
+            cpu = {"value": tts, "unit": "ms", "cores": 1, "kind": "reference",
+                   "sample": "one full 256x256 solve (setup + FGMRES(30) V-cycle) of the reference's own code, single "
+                             "rank via the MPI stand-in; its stock mt19937 setup",
+                   "iterations": r["iterations"], "setup_ms": 1e3 * r["setup_s"], "solve_ms": 1e3 * r["solve_s"]}
+            err_vs_ref = float(np.linalg.norm(x - r["x"]) / np.linalg.norm(r["x"]))
+    if rank == 0:
+        h2d = U.nbytes + b.nbytes
+        line = {
+            "metric": "time_to_solution", "value": ms_per_step, "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_NAME, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": f"flushed between steps ({L2_FLUSH_BYTES >> 20} MiB write)",
+                       "metropolis_acceptance": acc, "plaquette": plaq},
+            "iterations": infos[-1].iterations, "rel_residual": infos[-1].rel_residual,
+            "setup_ms": 1e3 * infos[-1].setup_seconds, "solve_ms": 1e3 * infos[-1].solve_seconds,
+            "rel_err_vs_reference_solution": err_vs_ref,
+            "e2e": {"value": e2e, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": b.nbytes},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "secondary": sec,
+        }
+        print(json.dumps(line))
+    s.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def dw_bandwidth(ddamg, torch, dev):
+    """D_W GB/s on a 1024x1024 lattice: 96 B/site FP64, 48 B/site FP32 (psi in, U, out; neighbour reuse perfect)."""
+    Nx = Nt = 1024
+    th, _ = ddamg.gauge_metropolis(Nx, Nt, 4.0, 10, 3, device=dev)
+    U = np.exp(1j * th)
+    p = ddamg.default_params(Nx, Nt, 2, -0.07, [[0, 128, 128, 4, 128, 128]], device=dev, precision=ddamg.PREC_MIXED)
+    s = ddamg.Solver(p)
+    s.load_gauge(U)
+    stream = torch.cuda.ExternalStream(s.stream())
+    out = {}
+    for name, dt, bps in (("f64", torch.float64, 96), ("f32", torch.float32, 48)):
+        x = torch.randn(2 * 2 * Nx * Nt, dtype=dt, device=f"cuda:{dev}")
+        y = torch.empty_like(x)
+        fn = s.L.ddamg_apply_dirac_device if dt == torch.float64 else s.L.ddamg_apply_dirac_f32_device
+        for _ in range(3):
+            ddamg.check(fn(s.h, 0, x.data_ptr(), y.data_ptr(), 1))
+        reps = 50
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(reps):
+                ddamg.check(fn(s.h, 0, x.data_ptr(), y.data_ptr(), 1))
+            e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"GB_s": bps * Nx * Nt / (ms * 1e-3) / 1e9, "us_per_apply": 1e3 * ms}
+    hbm, kind = peaks()
+    for v in out.values():
+        v["frac_of_hbm"] = v["GB_s"] / hbm
+    out["peak_kind"] = kind
+    s.close()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

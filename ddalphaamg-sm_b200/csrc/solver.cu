@@ -77,6 +77,17 @@ struct ddamg_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_setup_s = 0;
     long long launches_at_create = 0;
+    // per-kernel event timing (ddamg_profile)
+    struct ProfRec {
+        int kind, level;
+        cudaEvent_t a, b;
+    };
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_next = 0;
+    std::vector<ProfRec> prof_recs;
+    double prof_ms[3][DDAMG_MAX_LEVELS] = {};
+    long long prof_n[3][DDAMG_MAX_LEVELS] = {};
 };
 
 namespace ddamg {
@@ -93,6 +104,42 @@ template <typename V> static V* dalloc_t(ddamg_handle* h, size_t count) {
     return static_cast<V*>(dalloc(h, count * sizeof(V)));
 }
 static void sync(ddamg_handle* h) { DDAMG_CUDA_TRY(cudaStreamSynchronize(h->s)); }
+
+// ------------------------------------------------------------------ per-kernel timing
+static cudaEvent_t prof_event(ddamg_handle* h) {
+    if (h->ev_next == h->ev_pool.size()) {
+        cudaEvent_t e;
+        DDAMG_CUDA_TRY(cudaEventCreate(&e));
+        h->ev_pool.push_back(e);
+    }
+    return h->ev_pool[h->ev_next++];
+}
+struct ProfScope {
+    ddamg_handle* h;
+    int idx = -1;
+    ProfScope(ddamg_handle* hh, int kind, int level) : h(hh) {
+        if (!h->prof) return;
+        cudaEvent_t a = prof_event(h), b = prof_event(h);
+        DDAMG_CUDA_TRY(cudaEventRecord(a, h->s));
+        h->prof_recs.push_back({kind, level, a, b});
+        idx = (int)h->prof_recs.size() - 1;
+    }
+    ~ProfScope() {
+        if (idx >= 0) cudaEventRecord(h->prof_recs[idx].b, h->s);
+    }
+};
+static void prof_flush(ddamg_handle* h) {
+    if (h->prof_recs.empty()) return;
+    sync(h);
+    for (auto& r : h->prof_recs) {
+        float ms = 0;
+        DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, r.a, r.b));
+        h->prof_ms[r.kind][r.level] += ms;
+        h->prof_n[r.kind][r.level] += 1;
+    }
+    h->prof_recs.clear();
+    h->ev_next = 0;
+}
 static void bad(const std::string& m) { throw ParamFailure{m}; }
 
 // ------------------------------------------------------------------ geometry
@@ -266,6 +313,7 @@ static void allocate(ddamg_handle* h) {
 
 // ------------------------------------------------------------------ operators
 template <typename V> static void level_op(ddamg_handle* h, int l, const V* in, V* out, const V* b, int nrhs) {
+    ProfScope ps(h, 2, l);
     LevelData& D = h->lv[l];
     const Geom& g = D.g;
     if (l == 0) launch_wilson<V>(h->s, B<V>(D).U, in, out, b, g.Nx, g.Nt, h->p.m0, 0, nrhs);
@@ -291,8 +339,11 @@ static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, b
         for (int colour = 0; colour < 2; colour++) {
             a.blocks = colour == 0 ? D.red : D.black;
             a.nblocks = colour == 0 ? D.nred : D.nblack;
-            if (l == 0) launch_sap_sweep_fine<V>(h->s, g, B<V>(D).U, r, x, a, nrhs);
-            else launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs);
+            {
+                ProfScope ps(h, 0, l);
+                if (l == 0) launch_sap_sweep_fine<V>(h->s, g, B<V>(D).U, r, x, a, nrhs);
+                else launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs);
+            }
             // the residual after the last black sweep only feeds the convergence test
             const bool last = (colour == 1 && it == nu - 1);
             if (!last || (check && want_iters)) level_op<V>(h, l, x, r, v, nrhs);
@@ -310,6 +361,7 @@ static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, b
 }
 
 static int coarse_solve(ddamg_handle* h, const double2* b, double2* x) {
+    ProfScope ps(h, 1, h->L - 1);
     LevelData& D = h->lv[h->L - 1];
     const Geom& g = D.g;
     launch_coarse_gmres(h->s, h->cg, D.d.links, b, x, g.Nx, g.Nt, g.dof, h->p.m0, h->p.coarse_gmres_restart_length,
@@ -755,6 +807,7 @@ ddamg_status ddamg_destroy(ddamg_t* h) {
     cudaSetDevice(h->p.device);
     if (h->s) cudaStreamSynchronize(h->s);
     for (void* a : h->allocs) cudaFree(a);
+    for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     if (h->hpin) cudaFreeHost(h->hpin);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -767,6 +820,28 @@ ddamg_status ddamg_get_stream(ddamg_t* h, void** stream) {
     CHECK_HANDLE(h);
     API_BEGIN
     *stream = (void*)h->s;
+    API_END
+}
+ddamg_status ddamg_profile(ddamg_t* h, int enable) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (enable && !h->prof) {
+        for (auto& row : h->prof_ms)
+            for (double& v : row) v = 0;
+        for (auto& row : h->prof_n)
+            for (long long& v : row) v = 0;
+    }
+    if (!enable) prof_flush(h);
+    h->prof = enable != 0;
+    API_END
+}
+ddamg_status ddamg_profile_query(ddamg_t* h, int kind, int level, double* total_ms, long long* launches) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (kind < 0 || kind > 2 || level < 0 || level >= h->L) throw ParamFailure{"kind or level out of range"};
+    prof_flush(h);
+    if (total_ms) *total_ms = h->prof_ms[kind][level];
+    if (launches) *launches = h->prof_n[kind][level];
     API_END
 }
 ddamg_status ddamg_launch_count(ddamg_t* h, long long* count) {

@@ -246,6 +246,16 @@ class Solver:
         check(self.L.ddamg_get_stream(self.h, ctypes.byref(s)))
         return s.value or 0
 
+    def profile(self, enable):
+        check(self.L.ddamg_profile(self.h, int(bool(enable))))
+
+    def profile_query(self, kind, level):
+        """(total ms, launches) of kind 0 SAP sweep / 1 coarsest GMRES / 2 level operator at a level."""
+        ms = ctypes.c_double(0)
+        n = ctypes.c_longlong(0)
+        check(self.L.ddamg_profile_query(self.h, kind, level, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
     @staticmethod
     def launch_count():
         c = ctypes.c_longlong(0)

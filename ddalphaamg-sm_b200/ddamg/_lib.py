@@ -48,6 +48,8 @@ SIGNATURES = {
     "ddamg_last_error": (ctypes.c_char_p, []),
     "ddamg_get_stream": (_st, [_h, ctypes.POINTER(_vp)]),
     "ddamg_launch_count": (_st, [_h, ctypes.POINTER(ctypes.c_longlong)]),
+    "ddamg_profile": (_st, [_h, _i]),
+    "ddamg_profile_query": (_st, [_h, _i, _i, _dp, ctypes.POINTER(ctypes.c_longlong)]),
     "ddamg_read_binary": (_st, [ctypes.c_char_p, _i, _i, _dp]),
     "ddamg_write_binary": (_st, [ctypes.c_char_p, _i, _i, _dp]),
     "ddamg_load_gauge": (_st, [_h, _dp]),

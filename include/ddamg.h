@@ -97,8 +97,14 @@ ddamg_status ddamg_destroy(ddamg_t* h);
 const char* ddamg_last_error(void);
 /* the cudaStream_t the handle launches on (as void*) */
 ddamg_status ddamg_get_stream(ddamg_t* h, void** stream);
-/* number of kernels this handle has launched so far */
+/* number of kernels the library has launched so far (all handles) */
 ddamg_status ddamg_launch_count(ddamg_t* h, long long* count);
+/* per-kernel device timing: while enabled, the handle brackets every SAP sweep, coarsest solve
+ * and level-operator launch with CUDA events on its stream; disabling folds the elapsed times
+ * into per (kind, level) totals.  kind: 0 SAP colour sweep, 1 coarsest GMRES, 2 level operator.
+ * (No reference counterpart: the reference counts FLOPs, include/utils.h:141-150.) */
+ddamg_status ddamg_profile(ddamg_t* h, int enable);
+ddamg_status ddamg_profile_query(ddamg_t* h, int kind, int level, double* total_ms, long long* launches);
 
 /* ------------------------------------------------------------------ I/O */
 /* read_binary (src/io.cpp:4-55): records int32 x, t, mu, f64 re, im, x slowest; out: [site][mu] */
