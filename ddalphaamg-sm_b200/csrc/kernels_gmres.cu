@@ -6,7 +6,7 @@
 // identical data so control flow stays uniform without broadcasts.
 #include "internal.h"
 
-#include <cooperative_groups.h>
+#include <mutex>
 
 namespace ddamg {
 
@@ -304,8 +304,6 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
     if (blockIdx.x == 0 && threadIdx.x == 0) k.status[1] = iters;
 }
 
-static int g_coop_grid_cache[2] = {0, 0};
-
 void coarse_gmres_prepare(CoarseGmresWork& w, int n, int m, int dof, int device) {
     int sms = 0;
     DDAMG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
@@ -326,7 +324,6 @@ void coarse_gmres_prepare(CoarseGmresWork& w, int n, int m, int dof, int device)
     int grid = std::min(sms, std::max(1, sites / 8));
     w.grid = grid;
     w.block = 256;
-    (void)g_coop_grid_cache;
 }
 
 void launch_coarse_gmres(cudaStream_t s, const CoarseGmresWork& w, const double2* links, const double2* b,
@@ -362,4 +359,87 @@ void launch_coarse_gmres(cudaStream_t s, const CoarseGmresWork& w, const double2
     ++g_launches;
 }
 
+// ---------------------------------------------------------------- allocation-free coarsest solve
+// Some callers cannot allocate device memory when they solve: a host framework that owns every
+// device allocation through its own memory pool and forbids others, or a time-critical loop that
+// cannot pay for the implicit device synchronisation of cudaMalloc / cudaFree.  For them the
+// coarsest-level GMRES runs out of one fixed scratch array compiled into the library instead of a
+// handle's workspace.  The array is device memory of every GPU on which this code is loaded and
+// stays allocated until the process exits.
+constexpr size_t kNoAllocScratch = (size_t)1 << 21;  // complex FP64 values: 32 MiB
+static __device__ __align__(256) double2 g_noalloc_scratch[kNoAllocScratch];
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mutex;
+static double2* g_noalloc_base[kNoAllocMaxDevices] = {};
+
 }  // namespace ddamg
+
+extern "C" ddamg_status ddamg_coarse_gmres_noalloc(const void* links, const void* b, void* x, int Nx, int Nt, int dof,
+                                                   double m0, int m, int restarts, double tol, void* stream,
+                                                   int* iterations) {
+    using namespace ddamg;
+    if (!links || !b || !x || Nx < 1 || Nt < 1 || dof < 2 || dof > 64 || (dof & 1) || m < 1 || restarts < 1) {
+        set_error("ddamg_coarse_gmres_noalloc: bad argument");
+        return DDAMG_ERR_BAD_PARAM;
+    }
+    try {
+        int dev = 0, sms = 0;
+        DDAMG_CUDA_TRY(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= kNoAllocMaxDevices) {
+            set_error("ddamg_coarse_gmres_noalloc: device ordinal out of range");
+            return DDAMG_ERR_BAD_PARAM;
+        }
+        DDAMG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const long sites = (long)Nx * Nt, n = sites * dof;
+        const long grid = std::min<long>(sms, std::max<long>(1, sites / 8));
+        // scratch: Krylov basis (m+1) n, w n, 3 partial-sum buffers, Hessenberg (m+1) m, 2 control words
+        const long need = (long)(m + 1) * n + n + 3 * grid * (m + 2) + (long)(m + 1) * m + 2;
+        if (need > (long)kNoAllocScratch || 6L * (m + 1) * (long)sizeof(double2) > 227 * 1024) {
+            set_error("ddamg_coarse_gmres_noalloc: the solve needs " + std::to_string(need) +
+                      " complex values of scratch; the fixed array holds " + std::to_string(kNoAllocScratch) +
+                      " ((m+2)*n + (m+1)*m + 3*G*(m+2) + 2 must fit, G = min(SMs, sites/8))");
+            return DDAMG_ERR_BAD_PARAM;
+        }
+        double2* base;
+        {
+            std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+            if (!g_noalloc_base[dev]) {  // once per device, with that device current
+                void* p = nullptr;
+                DDAMG_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+                g_noalloc_base[dev] = static_cast<double2*>(p);
+            }
+            base = g_noalloc_base[dev];
+        }
+        CoarseGmresWork w;
+        coarse_gmres_prepare(w, (int)n, m, dof, dev);
+        if (w.grid != grid) {
+            set_error("ddamg_coarse_gmres_noalloc: unexpected grid size");
+            return DDAMG_ERR_STATE;
+        }
+        w.V = base;
+        w.w = w.V + (long)(m + 1) * n;
+        w.r = nullptr;
+        w.partial = w.w + n;
+        w.H = w.partial + 3 * grid * (m + 2);
+        w.bar = reinterpret_cast<unsigned*>(w.H + (long)(m + 1) * m);
+        w.status = reinterpret_cast<int*>(w.bar + 2);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        // the barrier words and status are zeroed inside; the rest is written before it is read
+        launch_coarse_gmres(s, w, static_cast<const double2*>(links), static_cast<const double2*>(b),
+                            static_cast<double2*>(x), Nx, Nt, dof, m0, m, restarts, tol);
+        int st[2] = {0, 0};
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(st, w.status, sizeof(st), cudaMemcpyDeviceToHost, s));
+        DDAMG_CUDA_TRY(cudaStreamSynchronize(s));
+        if (st[0] != 0) {
+            set_error("ddamg_coarse_gmres_noalloc: a bounded grid barrier gave up");
+            return DDAMG_ERR_DEVICE_TIMEOUT;
+        }
+        if (iterations) *iterations = st[1];
+    } catch (const CudaFailure&) {
+        return DDAMG_ERR_CUDA;
+    } catch (const ParamFailure& e) {
+        set_error(e.msg);
+        return DDAMG_ERR_BAD_PARAM;
+    }
+    return DDAMG_OK;
+}

@@ -69,6 +69,8 @@ SIGNATURES = {
     "ddamg_build_coarse_links": (_st, [_h, _i]),
     "ddamg_get_coarse_links": (_st, [_h, _i, _i, _dp]),
     "ddamg_coarse_solve": (_st, [_h, _dp, _dp, ctypes.POINTER(_i)]),
+    "ddamg_coarse_gmres_noalloc": (_st, [_vp, _vp, _vp, _i, _i, _i, ctypes.c_double, _i, _i, ctypes.c_double, _vp,
+                                         ctypes.POINTER(_i)]),
     "ddamg_vcycle": (_st, [_h, _dp, _dp]),
     "ddamg_kcycle": (_st, [_h, _dp, _dp]),
     "ddamg_solve": (_st, [_h, _dp, _dp, _i, ctypes.POINTER(SolveInfo)]),

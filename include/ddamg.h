@@ -153,6 +153,24 @@ ddamg_status ddamg_get_coarse_links(ddamg_t* h, int level, int which, double* ou
 /* ------------------------------------------------------------------ solvers */
 /* coarsest solve Level::GMRES_level_l (include/level.h:70-140), x0 = b (src/amg.cpp:69) */
 ddamg_status ddamg_coarse_solve(ddamg_t* h, const double* b, double* x, int* iters);
+/* No counterpart in the reference.  The coarsest solve above without any device allocation, for
+ * callers that cannot allocate device memory while they solve (a host framework that hands out all
+ * device memory from its own pool, or a time-critical loop that cannot absorb the device
+ * synchronisation of cudaMalloc / cudaFree).  The caller passes device pointers: links in the
+ * library's coarse layout [site][d][j][i] (d = self, +t, +x, -t, -x; j input dof, i output dof,
+ * 5*dof*dof complex per site), b and x (sites*dof complex); stream may be 0.  Scratch comes from
+ * one fixed 32 MiB array of complex doubles compiled into the library: the solve must fit in
+ * (m+2)*n + (m+1)*m + 3*G*(m+2) + 2 <= 2097152 complex values (n = Nx*Nt*dof, G = min(SMs,
+ * sites/8)) or the call returns DDAMG_ERR_BAD_PARAM; e.g. m = 400 allows n up to about 4,700.
+ * The array is device memory of every GPU that runs this code, held until the process exits.
+ * The first call on a device looks the array's address up (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  All calls share the one array and it
+ * keeps the last call's contents (its barrier and status words are cleared at each call): calls
+ * that overlap on the GPU, on any stream, race and give wrong results.  Waits for completion;
+ * *iterations gets the GMRES iteration count. */
+ddamg_status ddamg_coarse_gmres_noalloc(const void* links, const void* b, void* x, int Nx, int Nt, int dof,
+                                        double m0, int m, int restarts, double tol, void* stream,
+                                        int* iterations);
 /* one cycle from psi = 0: AlgebraicMG::v_cycle / k_cycle (src/amg.cpp:64-174) */
 ddamg_status ddamg_vcycle(ddamg_t* h, const double* eta, double* psi);
 ddamg_status ddamg_kcycle(ddamg_t* h, const double* eta, double* psi);
