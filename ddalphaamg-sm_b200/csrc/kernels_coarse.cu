@@ -53,13 +53,21 @@ __global__ void __launch_bounds__(128) coarse_op_kernel(const V* __restrict__ li
 #pragma unroll
         for (int jq = 0; jq < NI; jq++) {
             const int jn = min(32, dof - 32 * jq);
-            for (int jl = 0; jl < jn; jl++) {
-                const V vj = shflc(vd[jq], jl);
-                const V* Mj = M + (long)(32 * jq + jl) * dof;
+            for (int j0 = 0; j0 < jn; j0 += 8) {  // 8 column loads in flight per lane
+                V mv[8][NI];
 #pragma unroll
-                for (int q = 0; q < NI; q++) {
-                    int i = lane + 32 * q;
-                    if (i < dof) acc[q] = cfma(__ldg(Mj + i), vj, acc[q]);
+                for (int u = 0; u < 8; u++)
+#pragma unroll
+                    for (int q = 0; q < NI; q++) {
+                        const int i = lane + 32 * q;
+                        mv[u][q] = (j0 + u < jn && i < dof) ? __ldg(M + (long)(32 * jq + j0 + u) * dof + i) : czero<V>();
+                    }
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    if (j0 + u >= jn) break;
+                    const V vj = shflc(vd[jq], j0 + u);
+#pragma unroll
+                    for (int q = 0; q < NI; q++) acc[q] = cfma(mv[u][q], vj, acc[q]);
                 }
             }
         }

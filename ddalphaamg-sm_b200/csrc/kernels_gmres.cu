@@ -100,14 +100,23 @@ __device__ void apply_own(const GmresK& k, const double2* __restrict__ in, doubl
 #pragma unroll
             for (int jq = 0; jq < NI; jq++) {
                 const int jn = min(32, dof - 32 * jq);
-                for (int jl = 0; jl < jn; jl++) {
-                    const double2 vj = make_double2(__shfl_sync(0xffffffffu, vd[jq].x, jl),
-                                                    __shfl_sync(0xffffffffu, vd[jq].y, jl));
-                    const double2* Mj = M + (long)(32 * jq + jl) * dof;
+                for (int j0 = 0; j0 < jn; j0 += 8) {  // 8 column loads in flight per lane
+                    double2 mv[8][NI];
 #pragma unroll
-                    for (int q = 0; q < NI; q++) {
-                        const int i = lane + 32 * q;
-                        if (i < dof) acc[q] = cfma(__ldg(Mj + i), vj, acc[q]);
+                    for (int u = 0; u < 8; u++)
+#pragma unroll
+                        for (int q = 0; q < NI; q++) {
+                            const int i = lane + 32 * q;
+                            mv[u][q] = (j0 + u < jn && i < dof) ? __ldg(M + (long)(32 * jq + j0 + u) * dof + i)
+                                                                : make_double2(0.0, 0.0);
+                        }
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        if (j0 + u >= jn) break;
+                        const double2 vj = make_double2(__shfl_sync(0xffffffffu, vd[jq].x, j0 + u),
+                                                        __shfl_sync(0xffffffffu, vd[jq].y, j0 + u));
+#pragma unroll
+                        for (int q = 0; q < NI; q++) acc[q] = cfma(mv[u][q], vj, acc[q]);
                     }
                 }
             }

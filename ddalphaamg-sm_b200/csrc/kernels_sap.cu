@@ -49,55 +49,74 @@ struct SapKParams {
     const int* blocks;
     int nblocks;
     const int* done;
+    int nrhs;     // vectors in the sweep
+    int ngroups;  // CTAs per Schwarz block: ceil(nrhs / RB)
 };
 
-// Shared-memory layout of one block solve
-template <typename V> struct SapSmem {
-    V* basis;      // (m+1) x NE
-    V* op;         // NE: operand of D_B
-    double2* red;  // 33
-    double2* H;    // (m+1) x m, H[i*m + j]
-    double2* gm;   // m+1
-    double2* cn;   // m
-    double2* sn;   // m
-    double2* eta;  // m
-    int* flag;     // [0] = maxIt
-    __device__ SapSmem(unsigned char* raw, int m, int NE) {
+constexpr int kSapMaxM = 8;  // block GMRES restart length supported by the on-chip solver
+
+// Shared memory of one CTA: RB right-hand sides of one Schwarz block.  Vectors are stored
+// [element][rhs] so that the RB values a link element multiplies sit side by side.
+template <typename V, int RB> struct SapSmem {
+    V* basis;      // (m+1) x NE x RB
+    V* op;         // NE x RB: operand of D_B
+    double2* red;  // 2 buffers x warps x RB*(kSapMaxM+1): reductions
+    double2* H;    // RB x (m+1) x m, H[r][i*m + j]
+    double2* gm;   // RB x (m+1)
+    double2* cn;   // RB x m
+    double2* sn;   // RB x m
+    double2* eta;  // RB x m
+    int* flag;     // RB: the Arnoldi estimate met tol
+    __device__ SapSmem(unsigned char* raw, int m, int NE, int nw) {
         double2* d = reinterpret_cast<double2*>(raw);
         red = d;
-        H = red + 33;
-        gm = H + (m + 1) * m;
-        cn = gm + (m + 1);
-        sn = cn + m;
-        eta = sn + m;
-        flag = reinterpret_cast<int*>(eta + m);
-        basis = reinterpret_cast<V*>(flag + 4);
-        op = basis + (long)(m + 1) * NE;
+        H = red + (size_t)2 * nw * RB * (kSapMaxM + 1);
+        gm = H + RB * (m + 1) * m;
+        cn = gm + RB * (m + 1);
+        sn = cn + RB * m;
+        eta = sn + RB * m;
+        flag = reinterpret_cast<int*>(eta + RB * m);
+        basis = reinterpret_cast<V*>(flag + ((RB + 3) / 4) * 4);
+        op = basis + (size_t)(m + 1) * NE * RB;
     }
-    static size_t bytes(int m, int NE) {
-        return sizeof(double2) * (33 + (m + 1) * m + (m + 1) + 3 * m) + 4 * sizeof(int) +
-               sizeof(V) * (size_t)(m + 2) * NE;
+    static size_t bytes(int m, int NE, int nw) {
+        return sizeof(double2) * ((size_t)2 * nw * RB * (kSapMaxM + 1) + (size_t)RB * ((m + 1) * m + (m + 1) + 3 * m)) +
+               sizeof(int) * ((RB + 3) / 4) * 4 + sizeof(V) * (size_t)(m + 2) * NE * RB;
     }
 };
 
-template <typename V, bool DENSE, int EPT>
-__global__ void __launch_bounds__(1024) sap_block_kernel(Geom g, const V* __restrict__ L, const V* __restrict__ rg,
+// One SAP colour sweep for RB right-hand sides of one Schwarz block in lockstep: each link
+// element is loaded once and applied to all RB vectors; every right-hand side keeps its own
+// Hessenberg matrix, rotations, break point (maxIt) and convergence state, and freezes once it
+// has finished, so each follows exactly the single-vector algorithm of FGMRES::fgmres.
+template <typename V, bool DENSE, int EPT, int MAXT, int RB>
+__global__ void __launch_bounds__(MAXT) sap_block_kernel(Geom g, const V* __restrict__ L, const V* __restrict__ rg,
                                                          V* __restrict__ xg, SapKParams p) {
     typedef typename RealOf<V>::R R;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int S = g.sel_x * g.sel_t, dof = g.dof, NE = S * dof;
-    const int rhs = blockIdx.x / p.nblocks, kb = blockIdx.x - rhs * p.nblocks;
-    if (p.done && p.done[rhs]) return;
-    SapSmem<V> sm(smraw, p.m, NE);
+    const int nw = (blockDim.x + 31) >> 5, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    // block-major order: the CTAs of one Schwarz block run side by side and share its links in L2
+    const int kb = blockIdx.x / p.ngroups, r0 = (blockIdx.x - kb * p.ngroups) * RB;
+    bool act[RB];
+    bool any = false;
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+        act[r] = (r0 + r < p.nrhs) && !(p.done && p.done[r0 + r]);
+        any |= act[r];
+    }
+    if (!any) return;
+    SapSmem<V, RB> sm(smraw, p.m, NE, nw);
     const int blk = p.blocks[kb];
     const int bx = blk / g.sap_t, bt = blk - bx * g.sap_t;
-    const long ro = (long)rhs * g.size();
     const R mm = R(p.m0) + R(2);
+    const int m = p.m;
+    constexpr int SL = RB * (kSapMaxM + 1);  // reduction slots per warp
+    int rbuf = 0;
 
-    // element ownership: e = tid + q * blockDim
     int ek[EPT], ei[EPT], en[EPT], nbk[EPT][5];
     bool ev[EPT];
-    V b[EPT], x[EPT], w[EPT];
+    V b[EPT][RB], x[EPT][RB], w[EPT][RB];
 #pragma unroll
     for (int q = 0; q < EPT; q++) {
         const int e = threadIdx.x + q * blockDim.x;
@@ -112,186 +131,331 @@ __global__ void __launch_bounds__(1024) sap_block_kernel(Geom g, const V* __rest
         nbk[q][2] = (kx + 1 < g.sel_x) ? k + g.sel_t : -1;
         nbk[q][3] = (kt > 0) ? k - 1 : -1;
         nbk[q][4] = (kx > 0) ? k - g.sel_t : -1;
-        b[q] = ev[q] ? rg[ro + (long)en[q] * dof + i] : czero<V>();
-        x[q] = b[q];
+#pragma unroll
+        for (int r = 0; r < RB; r++) {
+            b[q][r] = (ev[q] && act[r]) ? rg[(long)(r0 + r) * g.size() + (long)en[q] * dof + i] : czero<V>();
+            x[q][r] = b[q][r];
+        }
     }
+    auto sidx = [&](int q) { return threadIdx.x + q * blockDim.x; };
+    // warp partial of one reduction slot; totals are read after the next __syncthreads
+    auto partial = [&](double2 v, int slot) {
+        v = warp_sum(v);
+        if (lane == 0) sm.red[((size_t)rbuf * nw + wid) * SL + slot] = v;
+    };
+    auto total = [&](int buf, int slot) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int ww = 0; ww < nw; ww++) t += sm.red[((size_t)buf * nw + ww) * SL + slot];
+        return t;
+    };
 
-    // w = D_B op   (op in shared memory, fully written before the call)
+    // w = D_B op for all RB vectors (op in shared memory, fully written before the call)
     auto apply = [&](const V* op) {
 #pragma unroll
         for (int q = 0; q < EPT; q++) {
+            V acc[RB][2];
+#pragma unroll
+            for (int r = 0; r < RB; r++) acc[r][0] = acc[r][1] = czero<V>();
             if (!ev[q]) {
-                w[q] = czero<V>();
+#pragma unroll
+                for (int r = 0; r < RB; r++) w[q][r] = czero<V>();
                 continue;
             }
             const int k = ek[q], i = ei[q], n = en[q];
-            V acc = czero<V>();
             if (DENSE) {
 #pragma unroll
                 for (int d = 0; d < 5; d++) {
                     const int kk = nbk[q][d];
                     if (kk < 0) continue;
                     const V* M = L + ((long)n * 5 + d) * dof * dof + i;
-                    const V* o = op + kk * dof;
-                    for (int j = 0; j < dof; j++) acc = cfma(__ldg(M + (long)j * dof), o[j], acc);
+                    const V* o = op + (size_t)kk * dof * RB;
+                    int j = 0;
+                    for (; j + 8 <= dof; j += 8) {  // 8 link loads in flight
+                        V mv[8];
+#pragma unroll
+                        for (int u = 0; u < 8; u++) mv[u] = __ldg(M + (long)(j + u) * dof);
+#pragma unroll
+                        for (int u = 0; u < 8; u++)
+#pragma unroll
+                            for (int r = 0; r < RB; r++) acc[r][u & 1] = cfma(mv[u], o[(j + u) * RB + r], acc[r][u & 1]);
+                    }
+                    for (; j < dof; j++) {
+                        const V mv = __ldg(M + (long)j * dof);
+#pragma unroll
+                        for (int r = 0; r < RB; r++) acc[r][0] = cfma(mv, o[j * RB + r], acc[r][0]);
+                    }
                 }
             } else {
 #pragma unroll
                 for (int d = 1; d < 5; d++) {
                     const int kk = nbk[q][d];
                     if (kk < 0) continue;
-                    acc = cfma(level0_hop(L, g.Nx, g.Nt, n, d, i, 0), op[kk * 2], acc);
-                    acc = cfma(level0_hop(L, g.Nx, g.Nt, n, d, i, 1), op[kk * 2 + 1], acc);
+                    const V h0 = level0_hop(L, g.Nx, g.Nt, n, d, i, 0), h1 = level0_hop(L, g.Nx, g.Nt, n, d, i, 1);
+#pragma unroll
+                    for (int r = 0; r < RB; r++) {
+                        acc[r][0] = cfma(h0, op[(kk * 2) * RB + r], acc[r][0]);
+                        acc[r][1] = cfma(h1, op[(kk * 2 + 1) * RB + r], acc[r][1]);
+                    }
                 }
             }
-            w[q] = mm * op[k * dof + i] - acc;
+#pragma unroll
+            for (int r = 0; r < RB; r++) w[q][r] = mm * op[(k * dof + i) * RB + r] - (acc[r][0] + acc[r][1]);
         }
     };
-    auto dot_own = [&](const V* a_sm) -> double2 {  // sum_own w * conj(a)
-        double2 s = make_double2(0.0, 0.0);
+    auto store_op = [&](V (&v)[EPT][RB]) {
 #pragma unroll
         for (int q = 0; q < EPT; q++)
-            if (ev[q]) s = cfmac(to_d(a_sm[threadIdx.x + q * blockDim.x]), to_d(w[q]), s);
-        return block_sum(s, sm.red);
-    };
-    auto norm_of = [&](const V* v) -> double {  // over own registers v[EPT]
-        double s = 0.0;
+            if (ev[q])
 #pragma unroll
-        for (int q = 0; q < EPT; q++)
-            if (ev[q]) s += (double)cnorm2(v[q]);
-        return sqrt(block_sum(make_double2(s, 0.0), sm.red).x);
+                for (int r = 0; r < RB; r++) sm.op[(size_t)sidx(q) * RB + r] = v[q][r];
     };
 
-    const int m = p.m;
     // x = x0 = b; r = b - D_B x
-#pragma unroll
-    for (int q = 0; q < EPT; q++)
-        if (ev[q]) sm.op[threadIdx.x + q * blockDim.x] = x[q];
+    store_op(x);
     __syncthreads();
     apply(sm.op);
+    double norm_b[RB], err[RB];
+    bool fin[RB];  // converged, inactive, or a zero right-hand side
+    int maxIt[RB];
 #pragma unroll
-    for (int q = 0; q < EPT; q++) w[q] = b[q] - w[q];  // w holds r
-    const double norm_b = norm_of(b);
-    double err = norm_of(w);
-    int maxIt = m;
-    // a zero block right-hand side has the zero solution (the reference would divide by zero)
-    if (norm_b == 0.0) return;
+    for (int r = 0; r < RB; r++) {
+        double bb = 0.0, rr = 0.0;
+#pragma unroll
+        for (int q = 0; q < EPT; q++) {
+            w[q][r] = b[q][r] - w[q][r];
+            if (ev[q]) {
+                bb += (double)cnorm2(b[q][r]);
+                rr += (double)cnorm2(w[q][r]);
+            }
+        }
+        partial(make_double2(bb, rr), r);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+        const double2 t = total(rbuf, r);
+        norm_b[r] = sqrt(t.x);
+        err[r] = sqrt(t.y);
+        // a zero block right-hand side has the zero solution (the reference would divide by zero)
+        fin[r] = !act[r] || norm_b[r] == 0.0;
+        maxIt[r] = m;
+    }
+    rbuf ^= 1;
     for (int k = 0; k < p.restarts; k++) {
-        // V_0 = r / beta
-        {
-            const R inv = R(1.0 / err);
+        bool arn[RB], anyarn = false;
+#pragma unroll
+        for (int r = 0; r < RB; r++) {
+            arn[r] = !fin[r];
+            anyarn |= arn[r];
+        }
+        if (!anyarn) break;
+#pragma unroll
+        for (int r = 0; r < RB; r++) {  // V_0 = r / beta
+            if (!arn[r]) continue;
+            const R inv = R(1.0 / err[r]);
 #pragma unroll
             for (int q = 0; q < EPT; q++)
-                if (ev[q]) sm.basis[threadIdx.x + q * blockDim.x] = inv * w[q];
-            if (threadIdx.x == 0) sm.gm[0] = make_double2(err, 0.0);
+                if (ev[q]) sm.basis[(size_t)sidx(q) * RB + r] = inv * w[q][r];
+            if (threadIdx.x == 0) sm.gm[r * (m + 1)] = make_double2(err[r], 0.0);
         }
-        bool brk = false;
         for (int j = 0; j < m; j++) {
+            anyarn = false;
+#pragma unroll
+            for (int r = 0; r < RB; r++) anyarn |= arn[r];
+            if (!anyarn) break;
             __syncthreads();
-            apply(sm.basis + (long)j * NE);  // w = D_B V_j
-            for (int i = 0; i <= j; i++) {   // modified Gram-Schmidt (src/fgmres.cpp:28-40)
-                const V* vi = sm.basis + (long)i * NE;
-                const double2 h = dot_own(vi);
-                if (threadIdx.x == 0) sm.H[i * m + j] = h;
-                const V hv = from_d<V>(h);
+            apply(sm.basis + (size_t)j * NE * RB);  // w = D_B V_j
+            // classical Gram-Schmidt coefficients <w, V_i>, i <= j, in one reduction
+            const int dbuf = rbuf;
 #pragma unroll
-                for (int q = 0; q < EPT; q++)
-                    if (ev[q]) w[q] = w[q] - cmul(hv, vi[threadIdx.x + q * blockDim.x]);
-            }
-            const double hn = norm_of(w);
-            if (hn > 0) {
-                const R inv = R(1.0 / hn);
+            for (int r = 0; r < RB; r++) {
+                if (!arn[r]) continue;
+                for (int i = 0; i <= j; i++) {
+                    double2 s = make_double2(0.0, 0.0);
 #pragma unroll
-                for (int q = 0; q < EPT; q++)
-                    if (ev[q]) sm.basis[(long)(j + 1) * NE + threadIdx.x + q * blockDim.x] = inv * w[q];
+                    for (int q = 0; q < EPT; q++)
+                        if (ev[q]) s = cfmac(to_d(sm.basis[((size_t)i * NE + sidx(q)) * RB + r]), to_d(w[q][r]), s);
+                    partial(s, r * (kSapMaxM + 1) + i);
+                }
             }
-            if (threadIdx.x == 0) {
-                double2* H = sm.H;
-                H[(j + 1) * m + j] = make_double2(hn, 0.0);
+            __syncthreads();
+            rbuf ^= 1;
+#pragma unroll
+            for (int r = 0; r < RB; r++) {
+                double ww = 0.0;
+                if (arn[r]) {
+                    for (int i = 0; i <= j; i++) {
+                        const V h = from_d<V>(total(dbuf, r * (kSapMaxM + 1) + i));
+#pragma unroll
+                        for (int q = 0; q < EPT; q++)
+                            if (ev[q]) w[q][r] = w[q][r] - cmul(h, sm.basis[((size_t)i * NE + sidx(q)) * RB + r]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < EPT; q++)
+                        if (ev[q]) ww += (double)cnorm2(w[q][r]);
+                }
+                partial(make_double2(ww, 0.0), r);
+            }
+            __syncthreads();
+            double hn[RB];
+#pragma unroll
+            for (int r = 0; r < RB; r++) {
+                hn[r] = sqrt(total(rbuf, r).x);
+                if (arn[r] && hn[r] > 0) {
+                    const R inv = R(1.0 / hn[r]);
+#pragma unroll
+                    for (int q = 0; q < EPT; q++)
+                        if (ev[q]) sm.basis[((size_t)(j + 1) * NE + sidx(q)) * RB + r] = inv * w[q][r];
+                }
+            }
+            rbuf ^= 1;
+            if (threadIdx.x < RB && arn[threadIdx.x]) {  // thread r: Hessenberg column j of RHS r
+                const int r = threadIdx.x;
+                double2* H = sm.H + r * (m + 1) * m;
+                double2* cn = sm.cn + r * m;
+                double2* sn = sm.sn + r * m;
+                double2* gm = sm.gm + r * (m + 1);
+                for (int i = 0; i <= j; i++) H[i * m + j] = total(dbuf, r * (kSapMaxM + 1) + i);
+                H[(j + 1) * m + j] = make_double2(hn[r], 0.0);
                 for (int i = 0; i < j; i++) {  // FGMRES::rotation (src/fgmres.cpp:99-115)
                     double2 hij = H[i * m + j], hi1 = H[(i + 1) * m + j];
-                    double2 tmp = cmulc(sm.cn[i], hij) + cmulc(sm.sn[i], hi1);
-                    H[(i + 1) * m + j] = cmul(sm.cn[i], hi1) - cmul(sm.sn[i], hij);
+                    double2 tmp = cmulc(cn[i], hij) + cmulc(sn[i], hi1);
+                    H[(i + 1) * m + j] = cmul(cn[i], hi1) - cmul(sn[i], hij);
                     H[i * m + j] = tmp;
                 }
                 double2 hjj = H[j * m + j], hj1 = H[(j + 1) * m + j];
                 double den = sqrt(cnorm2(hjj) + cnorm2(hj1));
-                sm.sn[j] = make_double2(hj1.x / den, hj1.y / den);
-                sm.cn[j] = make_double2(hjj.x / den, hjj.y / den);
-                H[j * m + j] = cmulc(sm.cn[j], hjj) + cmulc(sm.sn[j], hj1);
+                sn[j] = make_double2(hj1.x / den, hj1.y / den);
+                cn[j] = make_double2(hjj.x / den, hjj.y / den);
+                H[j * m + j] = cmulc(cn[j], hjj) + cmulc(sn[j], hj1);
                 H[(j + 1) * m + j] = make_double2(0.0, 0.0);
-                sm.gm[j + 1] = -cmul(sm.sn[j], sm.gm[j]);
-                sm.gm[j] = cmulc(sm.cn[j], sm.gm[j]);
-                sm.flag[0] = (sqrt(cnorm2(sm.gm[j + 1])) < p.tol * norm_b) ? 1 : 0;
+                gm[j + 1] = -cmul(sn[j], gm[j]);
+                gm[j] = cmulc(cn[j], gm[j]);
+                sm.flag[r] = (sqrt(cnorm2(gm[j + 1])) < p.tol * norm_b[r]) ? 1 : 0;
             }
             __syncthreads();
-            if (sm.flag[0]) {
-                maxIt = j + 1;
-                brk = true;
-                break;
-            }
+#pragma unroll
+            for (int r = 0; r < RB; r++)
+                if (arn[r] && sm.flag[r]) {
+                    maxIt[r] = j + 1;  // not reset at the next restart (src/fgmres.cpp:14,56)
+                    arn[r] = false;
+                }
         }
-        (void)brk;
-        // solve_upper_triangular (src/fgmres.cpp:118-128)
-        if (threadIdx.x == 0) {
-            for (int i = maxIt - 1; i >= 0; i--) {
-                double2 e = sm.gm[i];
-                for (int jj = i + 1; jj < maxIt; jj++) e = e - cmul(sm.H[i * m + jj], sm.eta[jj]);
-                sm.eta[i] = cdiv(e, sm.H[i * m + i]);
+        // solve_upper_triangular (src/fgmres.cpp:118-128), thread r for RHS r
+        if (threadIdx.x < RB && !fin[threadIdx.x]) {
+            const int r = threadIdx.x;
+            const double2* H = sm.H + r * (m + 1) * m;
+            double2* eta = sm.eta + r * m;
+            for (int i = maxIt[r] - 1; i >= 0; i--) {
+                double2 e = sm.gm[r * (m + 1) + i];
+                for (int jj = i + 1; jj < maxIt[r]; jj++) e = e - cmul(H[i * m + jj], eta[jj]);
+                eta[i] = cdiv(e, H[i * m + i]);
             }
         }
         __syncthreads();
 #pragma unroll
-        for (int q = 0; q < EPT; q++) {
-            if (!ev[q]) continue;
-            V acc = x[q];
-            for (int jj = 0; jj < maxIt; jj++)
-                acc = cfma(from_d<V>(sm.eta[jj]), sm.basis[(long)jj * NE + threadIdx.x + q * blockDim.x], acc);
-            x[q] = acc;
-            sm.op[threadIdx.x + q * blockDim.x] = acc;
+        for (int r = 0; r < RB; r++) {
+            if (fin[r]) continue;
+#pragma unroll
+            for (int q = 0; q < EPT; q++) {
+                if (!ev[q]) continue;
+                V a = x[q][r];
+                for (int jj = 0; jj < maxIt[r]; jj++)
+                    a = cfma(from_d<V>(sm.eta[r * m + jj]), sm.basis[((size_t)jj * NE + sidx(q)) * RB + r], a);
+                x[q][r] = a;
+            }
         }
+        store_op(x);
         __syncthreads();
         apply(sm.op);
 #pragma unroll
-        for (int q = 0; q < EPT; q++) w[q] = b[q] - w[q];
-        err = norm_of(w);
-        if (err < p.tol * norm_b) break;
+        for (int r = 0; r < RB; r++) {
+            double rr = 0.0;
+#pragma unroll
+            for (int q = 0; q < EPT; q++) {
+                w[q][r] = b[q][r] - w[q][r];
+                if (ev[q]) rr += (double)cnorm2(w[q][r]);
+            }
+            partial(make_double2(rr, 0.0), r);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < RB; r++) {
+            err[r] = sqrt(total(rbuf, r).x);
+            if (!fin[r] && err[r] < p.tol * norm_b[r]) fin[r] = true;
+        }
+        rbuf ^= 1;
     }
     // x_B += e  (src/sap.cpp:106-113)
 #pragma unroll
-    for (int q = 0; q < EPT; q++)
-        if (ev[q]) {
-            V* o = xg + ro + (long)en[q] * dof + ei[q];
-            *o = *o + x[q];
-        }
+    for (int r = 0; r < RB; r++) {
+        if (!act[r] || norm_b[r] == 0.0) continue;
+#pragma unroll
+        for (int q = 0; q < EPT; q++)
+            if (ev[q]) {
+                V* o = xg + (long)(r0 + r) * g.size() + (long)en[q] * dof + ei[q];
+                *o = *o + x[q][r];
+            }
+    }
+}
+
+template <typename V, bool DENSE, int EPT, int MAXT, int RB>
+static void launch_sap_k(cudaStream_t s, int threads, const Geom& g, const V* L, const V* r, V* x, SapKParams p) {
+    const int NE = g.sel_x * g.sel_t * g.dof;
+    p.ngroups = (p.nrhs + RB - 1) / RB;
+    const size_t smem = SapSmem<V, RB>::bytes(p.m, NE, threads / 32);
+    DDAMG_CUDA_TRY(cudaFuncSetAttribute(sap_block_kernel<V, DENSE, EPT, MAXT, RB>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DDAMG_LAUNCH((sap_block_kernel<V, DENSE, EPT, MAXT, RB>), dim3(p.nblocks * p.ngroups), threads, smem, s, g, L, r,
+                 x, p);
+}
+
+// right-hand sides per CTA: as many as fit in shared memory (and in registers for small
+// element counts), preferring a count that divides nrhs
+static int pick_rb(int nrhs, int ept, int m, int NE, int threads, size_t vbytes) {
+    auto fits = [&](int rb) {
+        const size_t smem = sizeof(double2) * ((size_t)2 * (threads / 32) * rb * (kSapMaxM + 1) +
+                                               (size_t)rb * ((m + 1) * m + (m + 1) + 3 * m)) +
+                            16 + vbytes * (size_t)(m + 2) * NE * rb;
+        return smem <= 227 * 1024 && ept * rb * (int)(vbytes / 8) <= 8;  // register budget
+    };
+    if (nrhs <= 1) return 1;
+    int best = 1;
+    for (int rb : {8, 4, 2}) {
+        if (rb > nrhs || !fits(rb)) continue;
+        if (nrhs % rb == 0) return rb;
+        if (best == 1) best = rb;
+    }
+    return best;
 }
 
 template <typename V, bool DENSE>
 static void launch_sap(cudaStream_t s, const Geom& g, const V* L, const V* r, V* x, const SapArgs& a, int nrhs) {
+    if (a.m > kSapMaxM) throw ParamFailure{"SAP block GMRES restart length above 8 is not supported"};
     const int NE = g.sel_x * g.sel_t * g.dof;
-    int threads = std::min(1024, ((NE + 31) / 32) * 32);
-    int ept = (NE + threads - 1) / threads;
-    size_t smem = SapSmem<V>::bytes(a.m, NE);
-    SapKParams p{a.m, a.restarts, a.tol, a.m0, a.blocks, a.nblocks, a.done};
-    dim3 grid(a.nblocks * nrhs);
-    if (ept == 1) {
-        DDAMG_CUDA_TRY(cudaFuncSetAttribute(sap_block_kernel<V, DENSE, 1>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        DDAMG_LAUNCH((sap_block_kernel<V, DENSE, 1>), grid, threads, smem, s, g, L, r, x, p);
+    const int threads = std::min(1024, ((NE + 31) / 32) * 32);
+    const int ept = (NE + threads - 1) / threads;
+    SapKParams p{a.m, a.restarts, a.tol, a.m0, a.blocks, a.nblocks, a.done, nrhs, 1};
+    const int rb = pick_rb(nrhs, ept, a.m, NE, threads, sizeof(V));
+    if (ept == 1 && threads <= 512) {
+        if (rb == 8) launch_sap_k<V, DENSE, 1, 512, 8>(s, threads, g, L, r, x, p);
+        else if (rb == 4) launch_sap_k<V, DENSE, 1, 512, 4>(s, threads, g, L, r, x, p);
+        else if (rb == 2) launch_sap_k<V, DENSE, 1, 512, 2>(s, threads, g, L, r, x, p);
+        else launch_sap_k<V, DENSE, 1, 512, 1>(s, threads, g, L, r, x, p);
+    } else if (ept == 1) {
+        if (rb >= 2) launch_sap_k<V, DENSE, 1, 1024, 2>(s, threads, g, L, r, x, p);
+        else launch_sap_k<V, DENSE, 1, 1024, 1>(s, threads, g, L, r, x, p);
     } else if (ept == 2) {
-        DDAMG_CUDA_TRY(cudaFuncSetAttribute(sap_block_kernel<V, DENSE, 2>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        DDAMG_LAUNCH((sap_block_kernel<V, DENSE, 2>), grid, threads, smem, s, g, L, r, x, p);
+        launch_sap_k<V, DENSE, 2, 1024, 1>(s, threads, g, L, r, x, p);
     } else if (ept <= 4) {
-        DDAMG_CUDA_TRY(cudaFuncSetAttribute(sap_block_kernel<V, DENSE, 4>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        DDAMG_LAUNCH((sap_block_kernel<V, DENSE, 4>), grid, threads, smem, s, g, L, r, x, p);
+        launch_sap_k<V, DENSE, 4, 1024, 1>(s, threads, g, L, r, x, p);
     } else {
         throw ParamFailure{"SAP block too large (more than 4096 unknowns per block)"};
     }
 }
 size_t sap_smem_bytes(int m, int NE, bool fp64) {
-    return fp64 ? SapSmem<double2>::bytes(m, NE) : SapSmem<float2>::bytes(m, NE);
+    const int nw = std::min(32, (NE + 31) / 32);
+    return fp64 ? SapSmem<double2, 1>::bytes(m, NE, nw) : SapSmem<float2, 1>::bytes(m, NE, nw);
 }
 
 template <typename V>

@@ -202,6 +202,7 @@ static void build_geometry(ddamg_handle* h) {
         const Geom& g = h->lv[l].g;
         if (g.Nx != pg.agg_x || g.Nt != pg.agg_t || g.colors != pg.ntest) bad("inconsistent level sizes");
     }
+    if (p.sap_gmres_restart_length > 8) bad("SAP block GMRES restart length above 8 is not supported");
     if (p.sap_gmres_restart_length < 1 || p.sap_gmres_restarts < 1 || p.coarse_gmres_restart_length < 1 ||
         p.coarse_gmres_restarts < 1 || p.kcycle_restart_length < 1 || p.kcycle_restarts < 1 ||
         p.fgmres_restart_length < 1 || p.fgmres_restarts < 1)
