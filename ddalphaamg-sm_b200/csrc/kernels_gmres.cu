@@ -64,72 +64,73 @@ struct GmresK {
     double m0, tol;
 };
 
-// out = [b -] D in on this CTA's sites (warp per site, lane per dof, NI = dof/32 rounded up)
+// out = [b -] D in on this CTA's sites.  The CTA's (site, direction) pairs are spread over its
+// warps (lane = output dof, NI = dof/32 rounded up); each pair leaves its partial product in
+// shared memory and the five partials of a site are summed in a fixed order.
 template <int NI>
 __device__ void apply_own(const GmresK& k, const double2* __restrict__ in, double2* __restrict__ out,
-                          const double2* __restrict__ bsub, int s0, int s1) {
+                          const double2* __restrict__ bsub, int s0, int s1, double2* __restrict__ part) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int dof = k.dof, Nt = k.Nt, Nx = k.Nx;
-    for (int n = s0 + wid; n < s1; n += nw) {
+    const int ntask = (s1 - s0) * 5;
+    for (int task = wid; task < ntask; task += nw) {
+        const int sl = task / 5, d = task - sl * 5;
+        const int n = s0 + sl;
         const int x = n / Nt, t = n - x * Nt;
-        int nb[5];
-        double sg[5];
-        nb[0] = n;
-        nb[1] = x * Nt + ((t + 1 == Nt) ? 0 : t + 1);
-        nb[2] = ((x + 1 == Nx) ? 0 : x + 1) * Nt + t;
-        nb[3] = x * Nt + ((t == 0) ? Nt - 1 : t - 1);
-        nb[4] = ((x == 0) ? Nx - 1 : x - 1) * Nt + t;
-        sg[0] = 1.0;
-        sg[1] = (t == Nt - 1) ? -1.0 : 1.0;
-        sg[2] = 1.0;
-        sg[3] = (t == 0) ? -1.0 : 1.0;
-        sg[4] = 1.0;
-        double2 acc[NI], self[NI];
+        int nb;
+        double sg = 1.0;
+        switch (d) {
+            case 0: nb = n; break;
+            case 1: nb = x * Nt + ((t + 1 == Nt) ? 0 : t + 1); sg = (t == Nt - 1) ? -1.0 : 1.0; break;
+            case 2: nb = ((x + 1 == Nx) ? 0 : x + 1) * Nt + t; break;
+            case 3: nb = x * Nt + ((t == 0) ? Nt - 1 : t - 1); sg = (t == 0) ? -1.0 : 1.0; break;
+            default: nb = ((x == 0) ? Nx - 1 : x - 1) * Nt + t; break;
+        }
+        double2 vd[NI], acc[NI];
 #pragma unroll
-        for (int q = 0; q < NI; q++) acc[q] = make_double2(0.0, 0.0);
+        for (int q = 0; q < NI; q++) {
+            const int i = lane + 32 * q;
+            vd[q] = (i < dof) ? sg * in[(long)nb * dof + i] : make_double2(0.0, 0.0);
+            acc[q] = make_double2(0.0, 0.0);
+        }
+        const double2* M = k.links + ((long)n * 5 + d) * dof * dof;
 #pragma unroll
-        for (int d = 0; d < 5; d++) {
-            double2 vd[NI];
+        for (int jq = 0; jq < NI; jq++) {
+            const int jn = min(32, dof - 32 * jq);
+            for (int j0 = 0; j0 < jn; j0 += 8) {  // 8 column loads in flight per lane
+                double2 mv[8][NI];
 #pragma unroll
-            for (int q = 0; q < NI; q++) {
-                const int i = lane + 32 * q;
-                vd[q] = (i < dof) ? sg[d] * in[(long)nb[d] * dof + i] : make_double2(0.0, 0.0);
-                if (d == 0) self[q] = vd[q];
-            }
-            const double2* M = k.links + ((long)n * 5 + d) * dof * dof;
+                for (int u = 0; u < 8; u++)
 #pragma unroll
-            for (int jq = 0; jq < NI; jq++) {
-                const int jn = min(32, dof - 32 * jq);
-                for (int j0 = 0; j0 < jn; j0 += 8) {  // 8 column loads in flight per lane
-                    double2 mv[8][NI];
-#pragma unroll
-                    for (int u = 0; u < 8; u++)
-#pragma unroll
-                        for (int q = 0; q < NI; q++) {
-                            const int i = lane + 32 * q;
-                            mv[u][q] = (j0 + u < jn && i < dof) ? __ldg(M + (long)(32 * jq + j0 + u) * dof + i)
-                                                                : make_double2(0.0, 0.0);
-                        }
-#pragma unroll
-                    for (int u = 0; u < 8; u++) {
-                        if (j0 + u >= jn) break;
-                        const double2 vj = make_double2(__shfl_sync(0xffffffffu, vd[jq].x, j0 + u),
-                                                        __shfl_sync(0xffffffffu, vd[jq].y, j0 + u));
-#pragma unroll
-                        for (int q = 0; q < NI; q++) acc[q] = cfma(mv[u][q], vj, acc[q]);
+                    for (int q = 0; q < NI; q++) {
+                        const int i = lane + 32 * q;
+                        mv[u][q] = (j0 + u < jn && i < dof) ? __ldg(M + (long)(32 * jq + j0 + u) * dof + i)
+                                                            : make_double2(0.0, 0.0);
                     }
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    if (j0 + u >= jn) break;
+                    const double2 vj = make_double2(__shfl_sync(0xffffffffu, vd[jq].x, j0 + u),
+                                                    __shfl_sync(0xffffffffu, vd[jq].y, j0 + u));
+#pragma unroll
+                    for (int q = 0; q < NI; q++) acc[q] = cfma(mv[u][q], vj, acc[q]);
                 }
             }
         }
 #pragma unroll
         for (int q = 0; q < NI; q++) {
             const int i = lane + 32 * q;
-            if (i < dof) {
-                double2 o = (k.m0 + 2.0) * self[q] - acc[q];
-                if (bsub) o = bsub[(long)n * dof + i] - o;
-                out[(long)n * dof + i] = o;
-            }
+            if (i < dof) part[(sl * 5 + d) * dof + i] = (d == 0) ? (k.m0 + 2.0) * vd[q] - acc[q] : acc[q];
         }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < (s1 - s0) * dof; e += blockDim.x) {
+        const int sl = e / dof, i = e - sl * dof;
+        const double2* pp = part + sl * 5 * dof + i;
+        double2 o = pp[0] - pp[dof] - pp[2 * dof] - pp[3 * dof] - pp[4 * dof];
+        const long ge = (long)(s0 + sl) * dof + i;
+        if (bsub) o = bsub[ge] - o;
+        out[ge] = o;
     }
 }
 
@@ -165,6 +166,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
     double2* cn = gm + (m + 1);   // m
     double2* sn = cn + m;         // m
     double2* eta = sn + m;        // m
+    double2* part = eta + m;      // sites per CTA x 5 x dof: per-direction partial products
     __shared__ int s_flag;
     const unsigned G = gridDim.x;
     const int sites = k.Nx * k.Nt;
@@ -179,7 +181,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
     // x = x0 = b
     for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) k.x[e] = k.b[e];
     if (!grid_barrier(k.bar, k.status, G)) return;
-    apply_own<NI>(k, k.x, k.w, k.b, s0, s1);  // w = r = b - D x
+    apply_own<NI>(k, k.x, k.w, k.b, s0, s1, part);  // w = r = b - D x
     __syncthreads();
     {
         double rr = 0.0, bb = 0.0;
@@ -201,6 +203,11 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
     }
     int maxIt = m, iters = k.restarts * m;
     bool converged = false;
+    if (norm_b == 0.0) {  // zero right-hand side: x = 0 (the reference would divide by zero)
+        for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) k.x[e] = make_double2(0.0, 0.0);
+        iters = 0;
+        converged = true;
+    }
     for (int kk = 0; kk < k.restarts && !converged; kk++) {
         const double inv = 1.0 / err;
         for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) k.V[e] = inv * k.w[e];
@@ -208,7 +215,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
         if (!grid_barrier(k.bar, k.status, G)) return;
         for (int j = 0; j < m; j++) {
             const double2* vj = k.V + (long)j * n;
-            apply_own<NI>(k, vj, k.w, nullptr, s0, s1);
+            apply_own<NI>(k, vj, k.w, nullptr, s0, s1, part);
             __syncthreads();
             partial_dots(k, k.w, j + 1, pA, e0, e1, n);
             if (!grid_barrier(k.bar, k.status, G)) return;
@@ -289,7 +296,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
             k.x[e] = a;
         }
         if (!grid_barrier(k.bar, k.status, G)) return;
-        apply_own<NI>(k, k.x, k.w, k.b, s0, s1);
+        apply_own<NI>(k, k.x, k.w, k.b, s0, s1, part);
         __syncthreads();
         {
             double rr = 0.0;
@@ -313,10 +320,19 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
     if (blockIdx.x == 0 && threadIdx.x == 0) k.status[1] = iters;
 }
 
+// CTAs of the coarsest solve: about two coarse sites per CTA, at most one CTA per SM
+int coarse_gmres_grid(long sites, int sms) { return (int)std::min<long>(sms, std::max<long>(1, (sites + 1) / 2)); }
+static size_t coarse_gmres_smem(long sites, int grid, int m, int dof) {
+    const long spc = (sites + grid - 1) / grid;
+    return sizeof(double2) * ((size_t)6 * (m + 1) + (size_t)spc * 5 * dof);
+}
+
 void coarse_gmres_prepare(CoarseGmresWork& w, int n, int m, int dof, int device) {
     int sms = 0;
     DDAMG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    size_t smem = sizeof(double2) * (size_t)(6 * (m + 1));
+    const int grid = coarse_gmres_grid(n / dof, sms);
+    size_t smem = coarse_gmres_smem(n / dof, grid, m, dof);
+    if (smem > 227 * 1024) throw ParamFailure{"coarsest GMRES restart length too large for shared memory"};
     int per_sm = 0;
     if (dof <= 32) {
         DDAMG_CUDA_TRY(cudaFuncSetAttribute(coarse_gmres_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -328,9 +344,6 @@ void coarse_gmres_prepare(CoarseGmresWork& w, int n, int m, int dof, int device)
         DDAMG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_gmres_kernel<2>, 256, smem));
     }
     if (per_sm < 1) throw ParamFailure{"coarsest GMRES kernel cannot be resident"};
-    const int sites = n / dof;
-    // one CTA per SM at most, and at least 8 sites per CTA so the phases have work
-    int grid = std::min(sms, std::max(1, sites / 8));
     w.grid = grid;
     w.block = 256;
 }
@@ -357,7 +370,7 @@ void launch_coarse_gmres(cudaStream_t s, const CoarseGmresWork& w, const double2
     k.tol = tol;
     DDAMG_CUDA_TRY(cudaMemsetAsync(w.bar, 0, 2 * sizeof(unsigned), s));
     DDAMG_CUDA_TRY(cudaMemsetAsync(w.status, 0, 2 * sizeof(int), s));
-    size_t smem = sizeof(double2) * (size_t)(6 * (m + 1));
+    size_t smem = coarse_gmres_smem((long)Nx * Nt, w.grid, m, dof);
     void* args[] = {&k};
     if (dof <= 32)
         DDAMG_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)coarse_gmres_kernel<1>, dim3(w.grid), dim3(w.block),
@@ -400,13 +413,13 @@ extern "C" ddamg_status ddamg_coarse_gmres_noalloc(const void* links, const void
         }
         DDAMG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         const long sites = (long)Nx * Nt, n = sites * dof;
-        const long grid = std::min<long>(sms, std::max<long>(1, sites / 8));
+        const long grid = coarse_gmres_grid(sites, sms);
         // scratch: Krylov basis (m+1) n, w n, 3 partial-sum buffers, Hessenberg (m+1) m, 2 control words
         const long need = (long)(m + 1) * n + n + 3 * grid * (m + 2) + (long)(m + 1) * m + 2;
-        if (need > (long)kNoAllocScratch || 6L * (m + 1) * (long)sizeof(double2) > 227 * 1024) {
+        if (need > (long)kNoAllocScratch || coarse_gmres_smem(sites, (int)grid, m, dof) > 227 * 1024) {
             set_error("ddamg_coarse_gmres_noalloc: the solve needs " + std::to_string(need) +
                       " complex values of scratch; the fixed array holds " + std::to_string(kNoAllocScratch) +
-                      " ((m+2)*n + (m+1)*m + 3*G*(m+2) + 2 must fit, G = min(SMs, sites/8))");
+                      " ((m+2)*n + (m+1)*m + 3*G*(m+2) + 2 must fit, G = min(SMs, sites/2))");
             return DDAMG_ERR_BAD_PARAM;
         }
         double2* base;

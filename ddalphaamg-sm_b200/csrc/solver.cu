@@ -71,7 +71,9 @@ struct ddamg_handle {
     double2* dh = nullptr;     // multidot results (2 x (max m + 1))
     double2* dcoef = nullptr;  // coefficients for multiaxpy
     double* dn = nullptr;      // norms
-    double2* hpin = nullptr;   // pinned host mirror
+    double2* hpin = nullptr;   // pinned host mirror (downloads)
+    double2* hpin2 = nullptr;  // pinned host staging (uploads)
+    double2* dalpha = nullptr; // per-rhs scale factors
     double2* grad = nullptr;   // gradient work: psi, lambda, sigma_3 eta (3 fine vectors)
     ddamg::CoarseGmresWork cg;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -244,18 +246,17 @@ static void allocate(ddamg_handle* h) {
         if (l > 0 && h->lv[l - 1].fp32 && !D.fp32) D.f.xfer = dalloc_t<float2>(h, (size_t)W * n);
         if (l > 0 && p.cycle == DDAMG_CYCLE_K) {
             const int km = p.kcycle_restart_length;
+            const size_t Rn = (size_t)p.max_rhs * n;
             if (D.fp32) {
-                D.f.kV = dalloc_t<float2>(h, (size_t)(km + 1) * n);
-                D.f.kZ = dalloc_t<float2>(h, (size_t)km * n);
-                D.f.kw = dalloc_t<float2>(h, n);
-                D.f.kr = dalloc_t<float2>(h, n);
-                D.f.kx = dalloc_t<float2>(h, n);
+                D.f.kV = dalloc_t<float2>(h, (km + 1) * Rn);
+                D.f.kZ = dalloc_t<float2>(h, km * Rn);
+                D.f.kw = dalloc_t<float2>(h, Rn);
+                D.f.kr = dalloc_t<float2>(h, Rn);
             } else {
-                D.d.kV = dalloc_t<double2>(h, (size_t)(km + 1) * n);
-                D.d.kZ = dalloc_t<double2>(h, (size_t)km * n);
-                D.d.kw = dalloc_t<double2>(h, n);
-                D.d.kr = dalloc_t<double2>(h, n);
-                D.d.kx = dalloc_t<double2>(h, n);
+                D.d.kV = dalloc_t<double2>(h, (km + 1) * Rn);
+                D.d.kZ = dalloc_t<double2>(h, km * Rn);
+                D.d.kw = dalloc_t<double2>(h, Rn);
+                D.d.kr = dalloc_t<double2>(h, Rn);
             }
         }
         D.done = dalloc_t<int>(h, W);
@@ -283,21 +284,24 @@ static void allocate(ddamg_handle* h) {
             sync(h);
         }
     }
-    // outer FGMRES (one right-hand side at a time)
+    // outer FGMRES, all right-hand sides of one call in lockstep
     const long n0 = h->lv[0].g.size();
     const int m = p.fgmres_restart_length;
-    h->oV = dalloc_t<double2>(h, (size_t)(m + 1) * n0);
-    h->oZ = dalloc_t<double2>(h, (size_t)m * n0);
-    h->ow = dalloc_t<double2>(h, n0);
-    h->orr = dalloc_t<double2>(h, n0);
-    h->ob = dalloc_t<double2>(h, (size_t)p.max_rhs * n0);
-    h->ox = dalloc_t<double2>(h, (size_t)p.max_rhs * n0);
+    const size_t Rn0 = (size_t)p.max_rhs * n0;
+    h->oV = dalloc_t<double2>(h, (m + 1) * Rn0);
+    h->oZ = dalloc_t<double2>(h, m * Rn0);
+    h->ow = dalloc_t<double2>(h, Rn0);
+    h->orr = dalloc_t<double2>(h, Rn0);
+    h->ob = dalloc_t<double2>(h, Rn0);
+    h->ox = dalloc_t<double2>(h, Rn0);
     const int mm = std::max(m, std::max(p.kcycle_restart_length, 1)) + 2;
-    h->dpart = dalloc_t<double2>(h, (size_t)kRedBlocks * std::max(2 * mm, 2 * W + 2));
-    h->dh = dalloc_t<double2>(h, 2 * mm + 2);
-    h->dcoef = dalloc_t<double2>(h, 2 * mm + 2);
+    h->dpart = dalloc_t<double2>(h, (size_t)kRedBlocks * (2 * (size_t)W * mm + 2));
+    h->dh = dalloc_t<double2>(h, 2 * (size_t)W * mm + 2);
+    h->dcoef = dalloc_t<double2>(h, (size_t)W * mm + 2);
+    h->dalpha = dalloc_t<double2>(h, (size_t)W + 2);
     h->dn = dalloc_t<double>(h, 2 * W + 4);
-    DDAMG_CUDA_TRY(cudaMallocHost(&h->hpin, sizeof(double2) * (4 * mm + 8)));
+    DDAMG_CUDA_TRY(cudaMallocHost(&h->hpin, sizeof(double2) * (2 * (size_t)W * mm + 2 * W + 8)));
+    DDAMG_CUDA_TRY(cudaMallocHost(&h->hpin2, sizeof(double2) * ((size_t)W * (mm + 1) + 8)));
     // coarsest GMRES
     const Geom& gc = h->lv[L - 1].g;
     const int cm = p.coarse_gmres_restart_length;
@@ -378,208 +382,261 @@ static void check_coarse_status(ddamg_handle* h, int* iters) {
 }
 
 // ------------------------------------------------------------------ FGMRES (host driven)
-// FGMRES::fgmres (src/fgmres.cpp:5-97) with CGS2 for the Arnoldi step; the Hessenberg matrix,
-// Givens rotations and back substitution run on the host in FP64 (one sync per step).
-// prec(in, out, restart): out = M in, out holds the previous restart's Z_j (src/amg.cpp:43-45).
+// FGMRES::fgmres (src/fgmres.cpp:5-97) for R right-hand sides in lockstep, with CGS2 for the
+// Arnoldi step.  Every right-hand side keeps its own Hessenberg matrix, rotations, break point
+// (maxIt, not reset between restarts: src/fgmres.cpp:14,56) and convergence state; one that has
+// finished is fed zero vectors so the shared launches leave it unchanged.  The small dense work
+// (Givens, back substitution) runs on the host in FP64: one sync per Arnoldi step.
+// A(in, out, R): out = A in.  M(in, out, R, restart): out = M in, where out still holds the
+// previous restart's Z_j (the K-cycle's initial guess, src/amg.cpp:43-45).
 template <typename V> struct Krylov {
-    V* Vb;
-    V* Z;
-    V* w;
-    V* r;
+    V* Vb;  // (m+1) x R x n
+    V* Z;   // m x R x n
+    V* w;   // R x n
+    V* r;   // R x n
 };
 template <typename V>
-static int fgmres_host(ddamg_handle* h, long n, int m, int restarts, double tol,
-                       const std::function<void(const V*, V*)>& A,
-                       const std::function<void(const V*, V*, int)>* M, const V* b, const V* x0, bool x0_zero, V* x,
-                       Krylov<V> K, double* final_rel) {
+static void fgmres_host(ddamg_handle* h, long n, int R, int m, int restarts, double tol,
+                        const std::function<void(const V*, V*, int)>& A,
+                        const std::function<void(const V*, V*, int, int)>* M, const V* b, const V* x0, bool x0_zero,
+                        V* x, Krylov<V> K, int* iters, double* rel) {
     cudaStream_t s = h->s;
-    if (x0_zero) DDAMG_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(V) * n, s));
-    else if (x0 != x) DDAMG_CUDA_TRY(cudaMemcpyAsync(x, x0, sizeof(V) * n, cudaMemcpyDeviceToDevice, s));
-    DDAMG_CUDA_TRY(cudaMemsetAsync(K.Z, 0, sizeof(V) * n * m, s));  // setZeros (include/fgmres.h:119-143)
-    if (x0_zero) DDAMG_CUDA_TRY(cudaMemcpyAsync(K.r, b, sizeof(V) * n, cudaMemcpyDeviceToDevice, s));
+    const long Rn = (long)R * n;
+    if (x0_zero) DDAMG_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(V) * Rn, s));
+    else if (x0 != x) DDAMG_CUDA_TRY(cudaMemcpyAsync(x, x0, sizeof(V) * Rn, cudaMemcpyDeviceToDevice, s));
+    DDAMG_CUDA_TRY(cudaMemsetAsync(K.Z, 0, sizeof(V) * Rn * m, s));  // setZeros (include/fgmres.h:119-143)
+    if (x0_zero) DDAMG_CUDA_TRY(cudaMemcpyAsync(K.r, b, sizeof(V) * Rn, cudaMemcpyDeviceToDevice, s));
     else {
-        A(x, K.w);
-        launch_sub<V>(s, b, K.w, K.r, n);
+        A(x, K.w, R);
+        launch_sub<V>(s, b, K.w, K.r, Rn);
     }
-    launch_norm2<V>(s, b, n, n, 1, h->dpart, h->dn);
-    launch_norm2<V>(s, K.r, n, n, 1, h->dpart, h->dn + 1);
-    double nrm[2];
-    DDAMG_CUDA_TRY(cudaMemcpyAsync(nrm, h->dn, sizeof(nrm), cudaMemcpyDeviceToHost, s));
+    launch_norm2<V>(s, b, n, n, R, h->dpart, h->dn);
+    launch_norm2<V>(s, K.r, n, n, R, h->dpart, h->dn + R);
+    double* hn_pin = reinterpret_cast<double*>(h->hpin);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(hn_pin, h->dn, sizeof(double) * 2 * R, cudaMemcpyDeviceToHost, s));
     sync(h);
-    const double norm_b = std::sqrt(nrm[0]);
-    double err = std::sqrt(nrm[1]);
-    if (!(err == err) || !(norm_b == norm_b)) throw ParamFailure{"NaN in the right-hand side"};
-    std::vector<double2> H((size_t)(m + 1) * m), gm(m + 1), cn(m), sn(m), eta(m);
-    auto Hij = [&](int i, int j) -> double2& { return H[(size_t)i * m + j]; };
-    int maxIt = m;
-    int ret = restarts * m;
+    std::vector<double> norm_b(R), err(R);
+    for (int r = 0; r < R; r++) {
+        norm_b[r] = std::sqrt(hn_pin[r]);
+        err[r] = std::sqrt(hn_pin[R + r]);
+        if (!(err[r] == err[r]) || !(norm_b[r] == norm_b[r])) throw ParamFailure{"NaN in the right-hand side"};
+    }
+    std::vector<double2> H((size_t)R * (m + 1) * m), gm((size_t)R * (m + 1)), cn((size_t)R * m), sn((size_t)R * m);
+    std::vector<int> maxIt(R, m), ret(R, restarts * m);
+    std::vector<char> done(R, 0), arn(R, 0);
+    for (int r = 0; r < R; r++) done[r] = norm_b[r] == 0.0;  // zero right-hand side: x = x0 = 0
+    double2* alpha = h->hpin2;            // R values uploaded to h->dalpha
+    double2* coef = h->hpin2 + R;         // R x m back-substitution results uploaded to h->dcoef
+    auto upload_alpha = [&]() {
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(h->dalpha, alpha, sizeof(double2) * R, cudaMemcpyHostToDevice, s));
+    };
     for (int k = 0; k < restarts; k++) {
-        launch_scale_host<V>(s, make_double2(1.0 / err, 0.0), K.r, K.Vb, n);
-        gm[0] = make_double2(err, 0.0);
-        bool brk = false;
+        bool any = false;
+        for (int r = 0; r < R; r++) {
+            arn[r] = !done[r];
+            any |= !done[r];
+            alpha[r] = make_double2(done[r] ? 0.0 : 1.0 / err[r], 0.0);
+            gm[(size_t)r * (m + 1)] = make_double2(err[r], 0.0);
+        }
+        if (!any) break;
+        upload_alpha();
+        launch_scale<V>(s, h->dalpha, K.r, K.Vb, n, R);  // V_0 = r / beta
         for (int j = 0; j < m; j++) {
-            const V* vj = K.Vb + (long)j * n;
-            V* zj = K.Z + (long)j * n;
-            if (M) (*M)(vj, zj, k);
-            else DDAMG_CUDA_TRY(cudaMemcpyAsync(zj, vj, sizeof(V) * n, cudaMemcpyDeviceToDevice, s));
-            A(zj, K.w);
-            launch_multidot<V>(s, K.Vb, n, 0, j + 1, K.w, 0, n, 1, h->dpart, h->dh);
-            launch_multiaxpy<V>(s, K.Vb, n, 0, j + 1, h->dh, K.w, 0, n, 1, -1.0);
-            launch_multidot<V>(s, K.Vb, n, 0, j + 1, K.w, 0, n, 1, h->dpart, h->dh + (j + 1));
-            launch_multiaxpy<V>(s, K.Vb, n, 0, j + 1, h->dh + (j + 1), K.w, 0, n, 1, -1.0);
-            launch_norm2<V>(s, K.w, n, n, 1, h->dpart, h->dn);
-            DDAMG_CUDA_TRY(cudaMemcpyAsync(h->hpin, h->dh, sizeof(double2) * 2 * (j + 1), cudaMemcpyDeviceToHost, s));
-            DDAMG_CUDA_TRY(cudaMemcpyAsync(h->hpin + 2 * (j + 1), h->dn, sizeof(double), cudaMemcpyDeviceToHost, s));
+            bool anyarn = false;
+            for (int r = 0; r < R; r++) anyarn |= arn[r] != 0;
+            if (!anyarn) break;
+            const V* vj = K.Vb + (long)j * Rn;
+            V* zj = K.Z + (long)j * Rn;
+            if (M) (*M)(vj, zj, R, k);
+            else DDAMG_CUDA_TRY(cudaMemcpyAsync(zj, vj, sizeof(V) * Rn, cudaMemcpyDeviceToDevice, s));
+            A(zj, K.w, R);
+            double2* h1 = h->dh;
+            double2* h2 = h->dh + (long)R * (j + 1);
+            launch_multidot<V>(s, K.Vb, Rn, n, j + 1, K.w, n, n, R, h->dpart, h1);
+            launch_multiaxpy<V>(s, K.Vb, Rn, n, j + 1, h1, K.w, n, n, R, -1.0);
+            launch_multidot<V>(s, K.Vb, Rn, n, j + 1, K.w, n, n, R, h->dpart, h2);
+            launch_multiaxpy<V>(s, K.Vb, Rn, n, j + 1, h2, K.w, n, n, R, -1.0);
+            launch_norm2<V>(s, K.w, n, n, R, h->dpart, h->dn);
+            DDAMG_CUDA_TRY(
+                cudaMemcpyAsync(h->hpin, h->dh, sizeof(double2) * 2 * R * (j + 1), cudaMemcpyDeviceToHost, s));
+            double* dn_pin = reinterpret_cast<double*>(h->hpin + 2 * R * (j + 1));
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(dn_pin, h->dn, sizeof(double) * R, cudaMemcpyDeviceToHost, s));
             sync(h);
-            for (int i = 0; i <= j; i++) Hij(i, j) = h->hpin[i] + h->hpin[j + 1 + i];
-            const double hn = std::sqrt(reinterpret_cast<double*>(h->hpin + 2 * (j + 1))[0]);
-            if (!(hn == hn)) throw ParamFailure{"NaN in the Krylov basis"};
-            Hij(j + 1, j) = make_double2(hn, 0.0);
-            if (hn > 0) launch_scale_host<V>(s, make_double2(1.0 / hn, 0.0), K.w, K.Vb + (long)(j + 1) * n, n);
-            for (int i = 0; i < j; i++) {  // FGMRES::rotation (src/fgmres.cpp:99-115)
-                double2 tmp = cmulc(cn[i], Hij(i, j)) + cmulc(sn[i], Hij(i + 1, j));
-                Hij(i + 1, j) = cmul(cn[i], Hij(i + 1, j)) - cmul(sn[i], Hij(i, j));
-                Hij(i, j) = tmp;
+            for (int r = 0; r < R; r++) {
+                alpha[r] = make_double2(0.0, 0.0);
+                if (!arn[r]) continue;
+                double2* Hr = H.data() + (size_t)r * (m + 1) * m;
+                double2* gr = gm.data() + (size_t)r * (m + 1);
+                double2* cr = cn.data() + (size_t)r * m;
+                double2* sr = sn.data() + (size_t)r * m;
+                auto Hij = [&](int i, int jj) -> double2& { return Hr[(size_t)i * m + jj]; };
+                for (int i = 0; i <= j; i++)
+                    Hij(i, j) = h->hpin[(size_t)r * (j + 1) + i] + h->hpin[(size_t)R * (j + 1) + r * (j + 1) + i];
+                const double hn = std::sqrt(dn_pin[r]);
+                if (!(hn == hn)) throw ParamFailure{"NaN in the Krylov basis"};
+                Hij(j + 1, j) = make_double2(hn, 0.0);
+                if (hn > 0) alpha[r] = make_double2(1.0 / hn, 0.0);
+                for (int i = 0; i < j; i++) {  // FGMRES::rotation (src/fgmres.cpp:99-115)
+                    double2 tmp = cmulc(cr[i], Hij(i, j)) + cmulc(sr[i], Hij(i + 1, j));
+                    Hij(i + 1, j) = cmul(cr[i], Hij(i + 1, j)) - cmul(sr[i], Hij(i, j));
+                    Hij(i, j) = tmp;
+                }
+                const double den = std::sqrt(cnorm2(Hij(j, j)) + cnorm2(Hij(j + 1, j)));
+                sr[j] = make_double2(Hij(j + 1, j).x / den, Hij(j + 1, j).y / den);
+                cr[j] = make_double2(Hij(j, j).x / den, Hij(j, j).y / den);
+                Hij(j, j) = cmulc(cr[j], Hij(j, j)) + cmulc(sr[j], Hij(j + 1, j));
+                Hij(j + 1, j) = make_double2(0.0, 0.0);
+                gr[j + 1] = -cmul(sr[j], gr[j]);
+                gr[j] = cmulc(cr[j], gr[j]);
+                if (std::sqrt(cnorm2(gr[j + 1])) < tol * norm_b[r]) {
+                    maxIt[r] = j + 1;
+                    arn[r] = 0;
+                    alpha[r] = make_double2(0.0, 0.0);  // V_{j+1} is not used again
+                }
             }
-            const double den = std::sqrt(cnorm2(Hij(j, j)) + cnorm2(Hij(j + 1, j)));
-            sn[j] = make_double2(Hij(j + 1, j).x / den, Hij(j + 1, j).y / den);
-            cn[j] = make_double2(Hij(j, j).x / den, Hij(j, j).y / den);
-            Hij(j, j) = cmulc(cn[j], Hij(j, j)) + cmulc(sn[j], Hij(j + 1, j));
-            Hij(j + 1, j) = make_double2(0.0, 0.0);
-            gm[j + 1] = -cmul(sn[j], gm[j]);
-            gm[j] = cmulc(cn[j], gm[j]);
-            if (std::sqrt(cnorm2(gm[j + 1])) < tol * norm_b) {
-                maxIt = j + 1;  // not reset at the next restart (src/fgmres.cpp:14,56)
-                brk = true;
-                break;
+            upload_alpha();
+            launch_scale<V>(s, h->dalpha, K.w, K.Vb + (long)(j + 1) * Rn, n, R);
+        }
+        // solve_upper_triangular (src/fgmres.cpp:118-128); x += sum_j eta_j Z_j
+        for (int r = 0; r < R; r++) {
+            double2* cf = coef + (size_t)r * m;
+            for (int i = 0; i < m; i++) cf[i] = make_double2(0.0, 0.0);
+            if (done[r]) continue;
+            const double2* Hr = H.data() + (size_t)r * (m + 1) * m;
+            const double2* gr = gm.data() + (size_t)r * (m + 1);
+            for (int i = maxIt[r] - 1; i >= 0; i--) {
+                double2 e = gr[i];
+                for (int jj = i + 1; jj < maxIt[r]; jj++) e = e - cmul(Hr[(size_t)i * m + jj], cf[jj]);
+                cf[i] = cdiv(e, Hr[(size_t)i * m + i]);
             }
         }
-        (void)brk;
-        for (int i = maxIt - 1; i >= 0; i--) {  // solve_upper_triangular (src/fgmres.cpp:118-128)
-            double2 e = gm[i];
-            for (int j = i + 1; j < maxIt; j++) e = e - cmul(Hij(i, j), eta[j]);
-            eta[i] = cdiv(e, Hij(i, i));
-        }
-        DDAMG_CUDA_TRY(cudaMemcpyAsync(h->dcoef, eta.data(), sizeof(double2) * maxIt, cudaMemcpyHostToDevice, s));
-        launch_multiaxpy<V>(s, K.Z, n, 0, maxIt, h->dcoef, x, 0, n, 1, +1.0);
-        A(x, K.w);
-        launch_sub<V>(s, b, K.w, K.r, n);
-        launch_norm2<V>(s, K.r, n, n, 1, h->dpart, h->dn);
-        double rr;
-        DDAMG_CUDA_TRY(cudaMemcpyAsync(&rr, h->dn, sizeof(double), cudaMemcpyDeviceToHost, s));
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(h->dcoef, coef, sizeof(double2) * R * m, cudaMemcpyHostToDevice, s));
+        launch_multiaxpy<V>(s, K.Z, Rn, n, m, h->dcoef, x, n, n, R, +1.0);
+        A(x, K.w, R);
+        launch_sub<V>(s, b, K.w, K.r, Rn);
+        launch_norm2<V>(s, K.r, n, n, R, h->dpart, h->dn);
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(hn_pin, h->dn, sizeof(double) * R, cudaMemcpyDeviceToHost, s));
         sync(h);
-        err = std::sqrt(rr);
-        if (!(err == err)) throw ParamFailure{"NaN residual"};
-        if (err < tol * norm_b) {
-            ret = k * m + maxIt;
-            break;
+        for (int r = 0; r < R; r++) {
+            if (done[r]) continue;
+            err[r] = std::sqrt(hn_pin[r]);
+            if (!(err[r] == err[r])) throw ParamFailure{"NaN residual"};
+            if (err[r] < tol * norm_b[r]) {
+                ret[r] = k * m + maxIt[r];
+                done[r] = 1;
+            }
         }
     }
-    if (final_rel) *final_rel = norm_b > 0 ? err / norm_b : 0.0;
-    return ret;
+    for (int r = 0; r < R; r++) {
+        if (iters) iters[r] = (norm_b[r] == 0.0) ? 0 : ret[r];
+        if (rel) rel[r] = norm_b[r] > 0 ? err[r] / norm_b[r] : 0.0;
+    }
 }
 
 // ------------------------------------------------------------------ cycles
-static void cycle(ddamg_handle* h, int l, const void* eta, void* psi, bool psi_zero, int kind);
+static void cycle(ddamg_handle* h, int l, const void* eta, void* psi, bool psi_zero, int kind, int R);
 
 // the next level's input: restrict r (level l, type V) into level l+1's eta (its own type)
-template <typename V> static void* restrict_into_next(ddamg_handle* h, int l, const V* r) {
-    LevelData& D = h->lv[l];
-    LevelData& N = h->lv[l + 1];
-    const bool next32 = N.fp32;
-    const bool cur32 = std::is_same<V, float2>::value;
-    if (next32 == cur32) {
-        V* out = B<V>(N).eta;
-        launch_restrict<V>(h->s, D.g, B<V>(D).tv, r, out, 1);
-        return out;
-    }
-    // only float -> double happens (mixed: FP32 level above the FP64 coarsest level)
-    launch_restrict<V>(h->s, D.g, B<V>(D).tv, r, reinterpret_cast<V*>(N.f.xfer), 1);
-    launch_convert<float2, double2>(h->s, N.f.xfer, N.d.eta, N.g.size());
-    return N.d.eta;
-}
-template <typename V> static void prolong_from_next(ddamg_handle* h, int l, const void* psi_next, V* psi) {
+template <typename V> static void* restrict_into_next(ddamg_handle* h, int l, const V* r, int R) {
     LevelData& D = h->lv[l];
     LevelData& N = h->lv[l + 1];
     const bool cur32 = std::is_same<V, float2>::value;
     if (N.fp32 == cur32) {
-        launch_prolong<V>(h->s, D.g, B<V>(D).tv, static_cast<const V*>(psi_next), psi, 1, 1);
+        V* out = B<V>(N).eta;
+        launch_restrict<V>(h->s, D.g, B<V>(D).tv, r, out, R);
+        return out;
+    }
+    // only float -> double happens (mixed: FP32 level above the FP64 coarsest level)
+    launch_restrict<V>(h->s, D.g, B<V>(D).tv, r, reinterpret_cast<V*>(N.f.xfer), R);
+    launch_convert<float2, double2>(h->s, N.f.xfer, N.d.eta, N.g.size() * R);
+    return N.d.eta;
+}
+template <typename V> static void prolong_from_next(ddamg_handle* h, int l, const void* psi_next, V* psi, int R) {
+    LevelData& D = h->lv[l];
+    LevelData& N = h->lv[l + 1];
+    const bool cur32 = std::is_same<V, float2>::value;
+    if (N.fp32 == cur32) {
+        launch_prolong<V>(h->s, D.g, B<V>(D).tv, static_cast<const V*>(psi_next), psi, 1, R);
         return;
     }
-    launch_convert<double2, float2>(h->s, static_cast<const double2*>(psi_next), N.f.xfer, N.g.size());
-    launch_prolong<V>(h->s, D.g, B<V>(D).tv, reinterpret_cast<const V*>(N.f.xfer), psi, 1, 1);
+    launch_convert<double2, float2>(h->s, static_cast<const double2*>(psi_next), N.f.xfer, N.g.size() * R);
+    launch_prolong<V>(h->s, D.g, B<V>(D).tv, reinterpret_cast<const V*>(N.f.xfer), psi, 1, R);
 }
 static void* next_psi(ddamg_handle* h, int l) {
     LevelData& N = h->lv[l + 1];
     return N.fp32 ? (void*)N.f.psi : (void*)N.d.psi;
 }
 
-// AlgebraicMG::v_cycle / k_cycle (src/amg.cpp:64-174) on one vector of level l
-template <typename V> static void cycle_t(ddamg_handle* h, int l, const V* eta, V* psi, bool psi_zero, int kind) {
+// AlgebraicMG::v_cycle / k_cycle (src/amg.cpp:64-174) on R vectors of level l
+template <typename V>
+static void cycle_t(ddamg_handle* h, int l, const V* eta, V* psi, bool psi_zero, int kind, int R) {
     const ddamg_params& p = h->p;
     if (l == h->L - 1) {
-        coarse_solve(h, reinterpret_cast<const double2*>(eta), reinterpret_cast<double2*>(psi));
+        const long n = h->lv[l].g.size();
+        for (int r = 0; r < R; r++)
+            coarse_solve(h, reinterpret_cast<const double2*>(eta) + r * n, reinterpret_cast<double2*>(psi) + r * n);
         return;
     }
     LevelData& D = h->lv[l];
     const long n = D.g.size();
-    if (psi_zero) DDAMG_CUDA_TRY(cudaMemsetAsync(psi, 0, sizeof(V) * n, h->s));
+    if (psi_zero) DDAMG_CUDA_TRY(cudaMemsetAsync(psi, 0, sizeof(V) * n * R, h->s));
     bool zero = psi_zero;
     if (p.nu1 > 0) {
-        sap_t<V>(h, l, eta, psi, p.nu1, p.smoother_tolerance, zero, 1, false);
+        sap_t<V>(h, l, eta, psi, p.nu1, p.smoother_tolerance, zero, R, false);
         zero = false;
     }
     V* r = B<V>(D).r;
     // r = eta - D psi (psi == 0 gives r = eta exactly)
     const V* rin = eta;
     if (!zero) {
-        level_op<V>(h, l, psi, r, eta, 1);
+        level_op<V>(h, l, psi, r, eta, R);
         rin = r;
     }
-    void* en = restrict_into_next<V>(h, l, rin);
+    void* en = restrict_into_next<V>(h, l, rin, R);
     void* pn = next_psi(h, l);
     LevelData& N = h->lv[l + 1];
     if (kind == DDAMG_CYCLE_V) {
-        cycle(h, l + 1, en, pn, true, kind);
+        cycle(h, l + 1, en, pn, true, kind, R);
     } else {
         // FGMRES_k_cycle at level l+1 (include/amg.h:16-94), x0 = rhs
         const long nn = N.g.size();
         auto run = [&](auto tag) {
             typedef decltype(tag) W;
             LevelBufs<W>& nb = B<W>(N);
-            std::function<void(const W*, W*)> A = [h, l](const W* in, W* out) {
-                level_op<W>(h, l + 1, in, out, nullptr, 1);
+            std::function<void(const W*, W*, int)> A = [h, l](const W* in, W* out, int RR) {
+                level_op<W>(h, l + 1, in, out, nullptr, RR);
             };
-            std::function<void(const W*, W*, int)> M = [h, l](const W* in, W* out, int restart) {
-                cycle(h, l + 1, in, out, restart == 0, DDAMG_CYCLE_K);
+            std::function<void(const W*, W*, int, int)> M = [h, l](const W* in, W* out, int RR, int restart) {
+                cycle(h, l + 1, in, out, restart == 0, DDAMG_CYCLE_K, RR);
             };
             Krylov<W> K{nb.kV, nb.kZ, nb.kw, nb.kr};
-            fgmres_host<W>(h, nn, p.kcycle_restart_length, p.kcycle_restarts, p.kcycle_tolerance, A, &M,
+            fgmres_host<W>(h, nn, R, p.kcycle_restart_length, p.kcycle_restarts, p.kcycle_tolerance, A, &M,
                            static_cast<const W*>(en), static_cast<const W*>(en), false, static_cast<W*>(pn), K,
-                           nullptr);
+                           nullptr, nullptr);
         };
         if (N.fp32) run(float2{});
         else run(double2{});
     }
-    prolong_from_next<V>(h, l, pn, psi);
-    if (p.nu2 > 0) sap_t<V>(h, l, eta, psi, p.nu2, p.smoother_tolerance, false, 1, false);
+    prolong_from_next<V>(h, l, pn, psi, R);
+    if (p.nu2 > 0) sap_t<V>(h, l, eta, psi, p.nu2, p.smoother_tolerance, false, R, false);
 }
-static void cycle(ddamg_handle* h, int l, const void* eta, void* psi, bool psi_zero, int kind) {
-    if (h->lv[l].fp32) cycle_t<float2>(h, l, static_cast<const float2*>(eta), static_cast<float2*>(psi), psi_zero, kind);
-    else cycle_t<double2>(h, l, static_cast<const double2*>(eta), static_cast<double2*>(psi), psi_zero, kind);
+static void cycle(ddamg_handle* h, int l, const void* eta, void* psi, bool psi_zero, int kind, int R) {
+    if (h->lv[l].fp32)
+        cycle_t<float2>(h, l, static_cast<const float2*>(eta), static_cast<float2*>(psi), psi_zero, kind, R);
+    else cycle_t<double2>(h, l, static_cast<const double2*>(eta), static_cast<double2*>(psi), psi_zero, kind, R);
     if (l == h->L - 1) check_coarse_status(h, nullptr);
 }
 
 // the outer preconditioner (FGMRES_AMG_*::preconditioner, include/amg.h:240-269): zero, one cycle
-static void outer_prec(ddamg_handle* h, const double2* in, double2* out) {
+static void outer_prec(ddamg_handle* h, const double2* in, double2* out, int R) {
     LevelData& D = h->lv[0];
-    const long n = D.g.size();
+    const long n = D.g.size() * R;
     if (D.fp32) {
         launch_convert<double2, float2>(h->s, in, D.f.eta, n);
-        cycle(h, 0, D.f.eta, D.f.psi, true, h->p.cycle);
+        cycle(h, 0, D.f.eta, D.f.psi, true, h->p.cycle, R);
         launch_convert<float2, double2>(h->s, D.f.psi, out, n);
     } else {
-        cycle(h, 0, in, out, true, h->p.cycle);
+        cycle(h, 0, in, out, true, h->p.cycle, R);
     }
 }
 
@@ -651,29 +708,30 @@ static ddamg_status solve_device(ddamg_handle* h, const double2* b, double2* x, 
     const ddamg_params& p = h->p;
     const long n = h->lv[0].g.size();
     const Geom& g0 = h->lv[0].g;
+    DDAMG_CUDA_TRY(cudaEventRecord(h->ev0, h->s));
+    std::function<void(const double2*, double2*, int)> A = [h, &g0](const double2* in, double2* out, int R) {
+        launch_wilson<double2>(h->s, h->lv[0].d.U, in, out, nullptr, g0.Nx, g0.Nt, h->p.m0, 0, R);
+    };
+    std::function<void(const double2*, double2*, int, int)> M = [h](const double2* in, double2* out, int R, int) {
+        outer_prec(h, in, out, R);
+    };
+    Krylov<double2> K{h->oV, h->oZ, h->ow, h->orr};
+    std::vector<int> it(nrhs);
+    std::vector<double> rel(nrhs);
+    fgmres_host<double2>(h, n, nrhs, p.fgmres_restart_length, p.fgmres_restarts, p.fgmres_tolerance, A, &M, b,
+                         nullptr, true, x, K, it.data(), rel.data());
+    DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, h->s));
+    sync(h);
+    float ms = 0;
+    DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     ddamg_status st = DDAMG_OK;
     for (int r = 0; r < nrhs; r++) {
-        DDAMG_CUDA_TRY(cudaEventRecord(h->ev0, h->s));
-        std::function<void(const double2*, double2*)> A = [h, &g0](const double2* in, double2* out) {
-            launch_wilson<double2>(h->s, h->lv[0].d.U, in, out, nullptr, g0.Nx, g0.Nt, h->p.m0, 0, 1);
-        };
-        std::function<void(const double2*, double2*, int)> M = [h](const double2* in, double2* out, int) {
-            outer_prec(h, in, out);
-        };
-        Krylov<double2> K{h->oV, h->oZ, h->ow, h->orr};
-        double rel = 0;
-        int it = fgmres_host<double2>(h, n, p.fgmres_restart_length, p.fgmres_restarts, p.fgmres_tolerance, A, &M,
-                                      b + r * n, nullptr, true, x + r * n, K, &rel);
-        DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, h->s));
-        sync(h);
-        float ms = 0;
-        DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-        const bool conv = rel < p.fgmres_tolerance;
+        const bool conv = rel[r] < p.fgmres_tolerance;
         if (!conv) st = DDAMG_NOT_CONVERGED;
         if (info) {
-            info[r].iterations = it;
+            info[r].iterations = it[r];
             info[r].converged = conv ? 1 : 0;
-            info[r].rel_residual = rel;
+            info[r].rel_residual = rel[r];
             info[r].setup_seconds = h->last_setup_s;
             info[r].solve_seconds = ms * 1e-3;
         }
@@ -810,6 +868,7 @@ ddamg_status ddamg_destroy(ddamg_t* h) {
     for (void* a : h->allocs) cudaFree(a);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     if (h->hpin) cudaFreeHost(h->hpin);
+    if (h->hpin2) cudaFreeHost(h->hpin2);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->s) cudaStreamDestroy(h->s);
@@ -1116,7 +1175,7 @@ static ddamg_status run_cycle(ddamg_t* h, const double* eta, double* psi, int ki
     const int saved = h->p.cycle;
     h->p.cycle = kind;
     try {
-        outer_prec(h, h->ow, h->orr);
+        outer_prec(h, h->ow, h->orr, 1);
     } catch (...) {
         h->p.cycle = saved;
         throw;
@@ -1143,7 +1202,7 @@ ddamg_status ddamg_kcycle(ddamg_t* h, const double* eta, double* psi) {
 ddamg_status ddamg_solve_device(ddamg_t* h, const void* b, void* x, int nrhs, ddamg_solve_info* info) {
     CHECK_HANDLE(h);
     API_BEGIN
-    if (nrhs < 1) throw ParamFailure{"nrhs must be >= 1"};
+    if (nrhs < 1 || nrhs > h->p.max_rhs) throw ParamFailure{"nrhs must be in [1, max_rhs]"};
     return solve_device(h, static_cast<const double2*>(b), static_cast<double2*>(x), nrhs, info);
     API_END
 }
@@ -1176,13 +1235,14 @@ ddamg_status ddamg_gmres_plain(ddamg_t* h, const double* b, double* x, int m, in
     double2* Vb = dalloc_t<double2>(h, (size_t)(m + 1) * n);
     double2* Z = dalloc_t<double2>(h, (size_t)m * n);
     DDAMG_CUDA_TRY(cudaMemcpyAsync(h->ob, b, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
-    std::function<void(const double2*, double2*)> A = [h, &g0](const double2* in, double2* out) {
-        launch_wilson<double2>(h->s, h->lv[0].d.U, in, out, nullptr, g0.Nx, g0.Nt, h->p.m0, 0, 1);
+    std::function<void(const double2*, double2*, int)> A = [h, &g0](const double2* in, double2* out, int R) {
+        launch_wilson<double2>(h->s, h->lv[0].d.U, in, out, nullptr, g0.Nx, g0.Nt, h->p.m0, 0, R);
     };
     Krylov<double2> K{Vb, Z, h->ow, h->orr};
     double rel = 0;
+    int it = 0;
     DDAMG_CUDA_TRY(cudaEventRecord(h->ev0, h->s));
-    int it = fgmres_host<double2>(h, n, m, restarts, tol, A, nullptr, h->ob, nullptr, true, h->ox, K, &rel);
+    fgmres_host<double2>(h, n, 1, m, restarts, tol, A, nullptr, h->ob, nullptr, true, h->ox, K, &it, &rel);
     DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, h->s));
     DDAMG_CUDA_TRY(cudaMemcpyAsync(x, h->ox, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
     sync(h);

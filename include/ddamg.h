@@ -161,7 +161,7 @@ ddamg_status ddamg_coarse_solve(ddamg_t* h, const double* b, double* x, int* ite
  * 5*dof*dof complex per site), b and x (sites*dof complex); stream may be 0.  Scratch comes from
  * one fixed 32 MiB array of complex doubles compiled into the library: the solve must fit in
  * (m+2)*n + (m+1)*m + 3*G*(m+2) + 2 <= 2097152 complex values (n = Nx*Nt*dof, G = min(SMs,
- * sites/8)) or the call returns DDAMG_ERR_BAD_PARAM; e.g. m = 400 allows n up to about 4,700.
+ * (sites+1)/2)) or the call returns DDAMG_ERR_BAD_PARAM; e.g. m = 400 allows n up to about 4,600.
  * The array is device memory of every GPU that runs this code, held until the process exits.
  * The first call on a device looks the array's address up (cudaGetSymbolAddress) with that device
  * current; make that first call before any stream capture.  All calls share the one array and it

@@ -221,3 +221,35 @@ def test_metropolis_matches_oracle():
     # same chain: identical proposals and acceptance draws; cos/exp may differ by an ulp
     assert np.max(np.abs(th_g - th_o)) < 1e-12
     assert abs(acc_g - acc_o) < 1e-12
+
+
+@pytest.mark.parametrize("cycle", [ddamg.CYCLE_V, ddamg.CYCLE_K])
+@pytest.mark.parametrize("precision", [ddamg.PREC_DOUBLE, ddamg.PREC_MIXED])
+def test_solve_batched_matches_single(golden, cycle, precision):
+    """R right-hand sides in one lockstep solve follow exactly the single-RHS algorithm each."""
+    z = golden("ops_16x32_l3")
+    R = 3
+    s1, o = make_pair(z, precision=precision, cycle=cycle)
+    sb, _ = make_pair(z, precision=precision, cycle=cycle, max_rhs=R)
+    n = z["rhs"].size
+    bs = [po.gaussian(n, 300 + r) for r in range(R)]
+    xb, infob = sb.solve(np.concatenate(bs), nrhs=R)
+    for r in range(R):
+        x1, info1 = s1.solve(bs[r])
+        assert infob[r].iterations == info1[0].iterations
+        assert infob[r].converged == 1
+        assert rel(xb[r * n:(r + 1) * n], x1) < 1e-12
+        assert rel(o.dirac(xb[r * n:(r + 1) * n]), bs[r]) < 1e-10
+    s1.close()
+    sb.close()
+
+
+def test_solve_batched_with_zero_rhs(golden):
+    z = golden("ops_16x32_l3")
+    s, o = make_pair(z, max_rhs=2)
+    n = z["rhs"].size
+    b = np.concatenate([np.zeros(n, dtype=np.complex128), z["rhs"]])
+    x, info = s.solve(b, nrhs=2)
+    assert np.all(x[:n] == 0) and info[0].iterations == 0
+    assert info[1].converged == 1 and rel(o.dirac(x[n:]), z["rhs"]) < 1e-10
+    s.close()
