@@ -146,14 +146,28 @@ __device__ void partial_dots(const GmresK& k, const double2* __restrict__ w, int
         if (lane == 0) part[(long)blockIdx.x * k.P + i] = s;
     }
 }
-// h[i] = sum_blk partial[blk*P + i], identical order in every CTA
+// h[i] = sum_blk partial[blk*P + i]: one warp per coefficient, lanes stride over the CTAs' partials,
+// a shuffle tree finishes; every CTA runs the identical order, so all CTAs hold identical sums
 __device__ void reduce_partials(const GmresK& k, const double2* __restrict__ part, int cnt, double2* h) {
-    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = wid; i < cnt; i += nw) {
         double2 s = make_double2(0.0, 0.0);
-        for (int bk = 0; bk < (int)gridDim.x; bk++) s += part[(long)bk * k.P + i];
-        h[i] = s;
+        for (int bk = lane; bk < (int)gridDim.x; bk += 32) s += part[(long)bk * k.P + i];
+        s = warp_sum(s);
+        if (lane == 0) h[i] = s;
     }
     __syncthreads();
+}
+// sum over the CTAs of the first slot of pC (norms), same order in every CTA
+__device__ double2 reduce_slot0(const GmresK& k, const double2* __restrict__ part, double2* tmp) {
+    if (threadIdx.x < 32) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int bk = threadIdx.x; bk < (int)gridDim.x; bk += 32) s += part[(long)bk * k.P];
+        s = warp_sum(s);
+        if (threadIdx.x == 0) *tmp = s;
+    }
+    __syncthreads();
+    return *tmp;
 }
 
 template <int NI>
@@ -168,6 +182,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
     double2* eta = sn + m;        // m
     double2* part = eta + m;      // sites per CTA x 5 x dof: per-direction partial products
     __shared__ int s_flag;
+    __shared__ double2 s_sum;
     const unsigned G = gridDim.x;
     const int sites = k.Nx * k.Nt;
     const long n = (long)sites * k.dof;
@@ -196,8 +211,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
     if (!grid_barrier(k.bar, k.status, G)) return;
     double err, norm_b;
     {
-        double2 t = make_double2(0.0, 0.0);
-        for (unsigned bk = 0; bk < G; bk++) t += pC[(long)bk * k.P];
+        const double2 t = reduce_slot0(k, pC, &s_sum);
         err = sqrt(t.x);
         norm_b = sqrt(t.y);
     }
@@ -244,12 +258,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
             }
             for (int i = threadIdx.x; i <= j; i += blockDim.x) h[i] = h[i] + h2[i];
             if (!grid_barrier(k.bar, k.status, G)) return;
-            double hn;
-            {
-                double t = 0.0;
-                for (unsigned bk = 0; bk < G; bk++) t += pC[(long)bk * k.P].x;
-                hn = sqrt(t);
-            }
+            const double hn = sqrt(reduce_slot0(k, pC, &s_sum).x);
             if (hn > 0) {
                 const double ih = 1.0 / hn;
                 double2* vn = k.V + (long)(j + 1) * n;
@@ -306,11 +315,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
             if (threadIdx.x == 0) pC[(long)blockIdx.x * k.P] = t;
         }
         if (!grid_barrier(k.bar, k.status, G)) return;
-        {
-            double t = 0.0;
-            for (unsigned bk = 0; bk < G; bk++) t += pC[(long)bk * k.P].x;
-            err = sqrt(t);
-        }
+        err = sqrt(reduce_slot0(k, pC, &s_sum).x);
         if (err < k.tol * norm_b) {
             iters = kk * m + maxIt;
             converged = true;

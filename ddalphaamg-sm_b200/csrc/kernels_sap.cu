@@ -137,6 +137,19 @@ __global__ void __launch_bounds__(MAXT) sap_block_kernel(Geom g, const V* __rest
             x[q][r] = b[q][r];
         }
     }
+    // level 0: the block operator's eight 2x2-hop coefficients of each owned element are
+    // formed once from U (they do not change during the block solve)
+    V hop[EPT][DENSE ? 1 : 8];
+    if (!DENSE) {
+#pragma unroll
+        for (int q = 0; q < EPT; q++)
+#pragma unroll
+            for (int d = 1; d < 5; d++)
+#pragma unroll
+                for (int bet = 0; bet < 2; bet++)
+                    hop[q][DENSE ? 0 : (d - 1) * 2 + bet] =
+                        (ev[q] && nbk[q][d] >= 0) ? level0_hop(L, g.Nx, g.Nt, en[q], d, ei[q], bet) : czero<V>();
+    }
     auto sidx = [&](int q) { return threadIdx.x + q * blockDim.x; };
     // warp partial of one reduction slot; totals are read after the next __syncthreads
     auto partial = [&](double2 v, int slot) {
@@ -190,7 +203,7 @@ __global__ void __launch_bounds__(MAXT) sap_block_kernel(Geom g, const V* __rest
                 for (int d = 1; d < 5; d++) {
                     const int kk = nbk[q][d];
                     if (kk < 0) continue;
-                    const V h0 = level0_hop(L, g.Nx, g.Nt, n, d, i, 0), h1 = level0_hop(L, g.Nx, g.Nt, n, d, i, 1);
+                    const V h0 = hop[q][DENSE ? 0 : (d - 1) * 2], h1 = hop[q][DENSE ? 0 : (d - 1) * 2 + 1];
 #pragma unroll
                     for (int r = 0; r < RB; r++) {
                         acc[r][0] = cfma(h0, op[(kk * 2) * RB + r], acc[r][0]);
@@ -399,6 +412,243 @@ __global__ void __launch_bounds__(MAXT) sap_block_kernel(Geom g, const V* __rest
     }
 }
 
+// ---------------------------------------------------------------- level 0: one warp per block
+// The fine-level block solve is small (2 * sites unknowns), so a whole warp owns one Schwarz block:
+// lane l owns sites l, l+32, ...; the block operator is the Wilson stencil restricted to the block
+// (Level::SAP_level_l::D_local at level 0, src/level.cpp:607-653, with makeDirac's links), applied
+// in spin-projected form from links held in registers; every reduction is a warp shuffle and the
+// only synchronisation is __syncwarp.  Per-warp shared memory: Krylov basis, operand, Hessenberg.
+template <typename V> struct WarpSmem {
+    V* basis;      // (m+1) x S x 2
+    V* op;         // S x 2
+    double2* H;    // (m+1) x m
+    double2* gm;   // m+1
+    double2* cn;   // m
+    double2* sn;   // m
+    double2* eta;  // m
+    __device__ WarpSmem(unsigned char* raw, int m, int S) {
+        double2* d = reinterpret_cast<double2*>(raw);
+        H = d;
+        gm = H + (m + 1) * m;
+        cn = gm + (m + 1);
+        sn = cn + m;
+        eta = sn + m;
+        basis = reinterpret_cast<V*>(eta + m);
+        op = basis + (size_t)(m + 1) * S * 2;
+    }
+    static size_t bytes(int m, int S) {
+        return sizeof(double2) * ((size_t)(m + 1) * m + (m + 1) + 3 * m) + sizeof(V) * (size_t)(m + 2) * S * 2;
+    }
+};
+
+template <typename V, int SPL>
+__global__ void __launch_bounds__(128) sap_fine_warp_kernel(Geom g, const V* __restrict__ U, const V* __restrict__ rg,
+                                                            V* __restrict__ xg, SapKParams p, int wpc, size_t wbytes) {
+    typedef typename RealOf<V>::R R;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int task = blockIdx.x * wpc + wib;
+    if (wib >= wpc || task >= p.nblocks * p.nrhs) return;
+    const int kb = task / p.nrhs, rhs = task - kb * p.nrhs;  // block-major
+    if (p.done && p.done[rhs]) return;
+    const int et = g.sel_t, ex = g.sel_x, S = ex * et, m = p.m;
+    WarpSmem<V> sm(smraw + wib * wbytes, m, S);
+    const int blk = p.blocks[kb];
+    const int bx = blk / g.sap_t, bt = blk - bx * g.sap_t;
+    const long ro = (long)rhs * g.size();
+    const R mm = R(p.m0) + R(2), half = R(0.5);
+
+    bool sv[SPL];
+    int sk[SPL], sn_[SPL];
+    V u0[SPL], u1[SPL], ul0[SPL], ul1[SPL];
+    V b[SPL][2], x[SPL][2], w[SPL][2];
+#pragma unroll
+    for (int q = 0; q < SPL; q++) {
+        const int k = lane + 32 * q;
+        sv[q] = k < S;
+        const int kk = sv[q] ? k : 0;
+        const int kx = kk / et, kt = kk - kx * et;
+        const int xx = bx * ex + kx, tt = bt * et + kt;
+        const int n = xx * g.Nt + tt;
+        sk[q] = kk;
+        sn_[q] = n;
+        u0[q] = sv[q] ? __ldg(U + 2 * n) : czero<V>();
+        u1[q] = sv[q] ? __ldg(U + 2 * n + 1) : czero<V>();
+        ul0[q] = (sv[q] && kt > 0) ? conjc(__ldg(U + 2 * (n - 1))) : czero<V>();
+        ul1[q] = (sv[q] && kx > 0) ? conjc(__ldg(U + 2 * (n - g.Nt) + 1)) : czero<V>();
+#pragma unroll
+        for (int a = 0; a < 2; a++) {
+            b[q][a] = sv[q] ? rg[ro + (long)n * 2 + a] : czero<V>();
+            x[q][a] = b[q][a];
+        }
+    }
+    // w = D_B op  (op in per-warp shared memory, written and __syncwarp'ed by the caller)
+    auto apply = [&](const V* op) {
+#pragma unroll
+        for (int q = 0; q < SPL; q++) {
+            if (!sv[q]) {
+                w[q][0] = w[q][1] = czero<V>();
+                continue;
+            }
+            const int k = sk[q], kx = k / et, kt = k - kx * et;
+            const V p0 = op[2 * k], p1 = op[2 * k + 1];
+            V a = czero<V>(), c = czero<V>(), e = czero<V>(), gg = czero<V>();
+            if (kt + 1 < et) a = cmul(u0[q], op[2 * (k + 1)] - op[2 * (k + 1) + 1]);          // +t: (1 - sigma_x)
+            if (kx + 1 < ex) c = cmul(u1[q], op[2 * (k + et)] + imul(op[2 * (k + et) + 1]));  // +x: (1 - sigma_y)
+            if (kt > 0) e = cmul(ul0[q], op[2 * (k - 1)] + op[2 * (k - 1) + 1]);              // -t: (1 + sigma_x)
+            if (kx > 0) gg = cmul(ul1[q], op[2 * (k - et)] - imul(op[2 * (k - et) + 1]));      // -x: (1 + sigma_y)
+            w[q][0] = mm * p0 - half * (a + c + e + gg);
+            w[q][1] = mm * p1 - half * (imul(gg) - imul(c) + e - a);
+        }
+    };
+    auto store = [&](V* dst, V (&v)[SPL][2]) {
+#pragma unroll
+        for (int q = 0; q < SPL; q++)
+            if (sv[q]) {
+                dst[2 * sk[q]] = v[q][0];
+                dst[2 * sk[q] + 1] = v[q][1];
+            }
+    };
+    auto dotw = [&](const V* vi) {  // sum_own w * conj(vi)
+        double2 s = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int q = 0; q < SPL; q++)
+            if (sv[q])
+#pragma unroll
+                for (int a = 0; a < 2; a++) s = cfmac(to_d(vi[2 * sk[q] + a]), to_d(w[q][a]), s);
+        return warp_sum(s);
+    };
+    auto nrm2 = [&](V (&v)[SPL][2]) {
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < SPL; q++)
+            if (sv[q]) s += (double)cnorm2(v[q][0]) + (double)cnorm2(v[q][1]);
+        return warp_sum(s);
+    };
+
+    store(sm.op, x);
+    __syncwarp();
+    apply(sm.op);
+#pragma unroll
+    for (int q = 0; q < SPL; q++)
+#pragma unroll
+        for (int a = 0; a < 2; a++) w[q][a] = b[q][a] - w[q][a];
+    const double norm_b = sqrt(nrm2(b));
+    double err = sqrt(nrm2(w));
+    // a zero block right-hand side has the zero solution (the reference would divide by zero)
+    if (norm_b == 0.0) return;
+    int maxIt = m;
+    for (int k = 0; k < p.restarts; k++) {
+        const R inv = R(1.0 / err);
+#pragma unroll
+        for (int q = 0; q < SPL; q++)
+#pragma unroll
+            for (int a = 0; a < 2; a++) w[q][a] = inv * w[q][a];
+        store(sm.basis, w);
+        if (lane == 0) sm.gm[0] = make_double2(err, 0.0);
+        __syncwarp();
+        for (int j = 0; j < m; j++) {
+            const V* vj = sm.basis + (size_t)j * S * 2;
+            apply(vj);
+            for (int i = 0; i <= j; i++) {  // modified Gram-Schmidt (src/fgmres.cpp:28-40)
+                const V* vi = sm.basis + (size_t)i * S * 2;
+                const double2 h = dotw(vi);
+                if (lane == 0) sm.H[i * m + j] = h;
+                const V hv = from_d<V>(h);
+#pragma unroll
+                for (int q = 0; q < SPL; q++)
+                    if (sv[q])
+#pragma unroll
+                        for (int a = 0; a < 2; a++) w[q][a] = w[q][a] - cmul(hv, vi[2 * sk[q] + a]);
+            }
+            const double hn = sqrt(nrm2(w));
+            if (hn > 0) {
+                const R ih = R(1.0 / hn);
+                V t[SPL][2];
+#pragma unroll
+                for (int q = 0; q < SPL; q++)
+#pragma unroll
+                    for (int a = 0; a < 2; a++) t[q][a] = ih * w[q][a];
+                store(sm.basis + (size_t)(j + 1) * S * 2, t);
+            }
+            int brk = 0;
+            if (lane == 0) {
+                double2* H = sm.H;
+                H[(j + 1) * m + j] = make_double2(hn, 0.0);
+                for (int i = 0; i < j; i++) {  // FGMRES::rotation (src/fgmres.cpp:99-115)
+                    double2 hij = H[i * m + j], hi1 = H[(i + 1) * m + j];
+                    double2 tmp = cmulc(sm.cn[i], hij) + cmulc(sm.sn[i], hi1);
+                    H[(i + 1) * m + j] = cmul(sm.cn[i], hi1) - cmul(sm.sn[i], hij);
+                    H[i * m + j] = tmp;
+                }
+                double2 hjj = H[j * m + j], hj1 = H[(j + 1) * m + j];
+                double den = sqrt(cnorm2(hjj) + cnorm2(hj1));
+                sm.sn[j] = make_double2(hj1.x / den, hj1.y / den);
+                sm.cn[j] = make_double2(hjj.x / den, hjj.y / den);
+                H[j * m + j] = cmulc(sm.cn[j], hjj) + cmulc(sm.sn[j], hj1);
+                H[(j + 1) * m + j] = make_double2(0.0, 0.0);
+                sm.gm[j + 1] = -cmul(sm.sn[j], sm.gm[j]);
+                sm.gm[j] = cmulc(sm.cn[j], sm.gm[j]);
+                brk = (sqrt(cnorm2(sm.gm[j + 1])) < p.tol * norm_b) ? 1 : 0;
+            }
+            brk = __shfl_sync(0xffffffffu, brk, 0);
+            __syncwarp();
+            if (brk) {
+                maxIt = j + 1;  // not reset at the next restart (src/fgmres.cpp:14,56)
+                break;
+            }
+        }
+        if (lane == 0) {  // solve_upper_triangular (src/fgmres.cpp:118-128)
+            for (int i = maxIt - 1; i >= 0; i--) {
+                double2 e = sm.gm[i];
+                for (int jj = i + 1; jj < maxIt; jj++) e = e - cmul(sm.H[i * m + jj], sm.eta[jj]);
+                sm.eta[i] = cdiv(e, sm.H[i * m + i]);
+            }
+        }
+        __syncwarp();
+        for (int jj = 0; jj < maxIt; jj++) {
+            const V ej = from_d<V>(sm.eta[jj]);
+            const V* vj = sm.basis + (size_t)jj * S * 2;
+#pragma unroll
+            for (int q = 0; q < SPL; q++)
+                if (sv[q])
+#pragma unroll
+                    for (int a = 0; a < 2; a++) x[q][a] = cfma(ej, vj[2 * sk[q] + a], x[q][a]);
+        }
+        __syncwarp();
+        store(sm.op, x);
+        __syncwarp();
+        apply(sm.op);
+#pragma unroll
+        for (int q = 0; q < SPL; q++)
+#pragma unroll
+            for (int a = 0; a < 2; a++) w[q][a] = b[q][a] - w[q][a];
+        err = sqrt(nrm2(w));
+        if (err < p.tol * norm_b) break;
+    }
+    // x_B += e  (src/sap.cpp:106-113)
+#pragma unroll
+    for (int q = 0; q < SPL; q++)
+        if (sv[q])
+#pragma unroll
+            for (int a = 0; a < 2; a++) {
+                V* o = xg + ro + (long)sn_[q] * 2 + a;
+                *o = *o + x[q][a];
+            }
+}
+
+template <typename V, int SPL>
+static void launch_fine_warp(cudaStream_t s, const Geom& g, const V* U, const V* r, V* x, SapKParams p) {
+    const int S = g.sel_x * g.sel_t;
+    const size_t wb = (WarpSmem<V>::bytes(p.m, S) + 15) / 16 * 16;
+    const int wpc = (int)std::max<size_t>(1, std::min<size_t>(4, (48 * 1024) / wb));
+    const size_t smem = wb * wpc;
+    const int tasks = p.nblocks * p.nrhs;
+    DDAMG_CUDA_TRY(cudaFuncSetAttribute(sap_fine_warp_kernel<V, SPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+    DDAMG_LAUNCH((sap_fine_warp_kernel<V, SPL>), ceil_div(tasks, wpc), 32 * wpc, smem, s, g, U, r, x, p, wpc, wb);
+}
+
 template <typename V, bool DENSE, int EPT, int MAXT, int RB>
 static void launch_sap_k(cudaStream_t s, int threads, const Geom& g, const V* L, const V* r, V* x, SapKParams p) {
     const int NE = g.sel_x * g.sel_t * g.dof;
@@ -436,7 +686,9 @@ static void launch_sap(cudaStream_t s, const Geom& g, const V* L, const V* r, V*
     const int threads = std::min(1024, ((NE + 31) / 32) * 32);
     const int ept = (NE + threads - 1) / threads;
     SapKParams p{a.m, a.restarts, a.tol, a.m0, a.blocks, a.nblocks, a.done, nrhs, 1};
-    const int rb = pick_rb(nrhs, ept, a.m, NE, threads, sizeof(V));
+    // level 0 keeps one vector per CTA: its links are 32 B per site, so there is nothing to share,
+    // and a wider CTA would only cost shared memory and occupancy
+    const int rb = DENSE ? pick_rb(nrhs, ept, a.m, NE, threads, sizeof(V)) : 1;
     if (ept == 1 && threads <= 512) {
         if (rb == 8) launch_sap_k<V, DENSE, 1, 512, 8>(s, threads, g, L, r, x, p);
         else if (rb == 4) launch_sap_k<V, DENSE, 1, 512, 4>(s, threads, g, L, r, x, p);
@@ -460,7 +712,14 @@ size_t sap_smem_bytes(int m, int NE, bool fp64) {
 
 template <typename V>
 void launch_sap_sweep_fine(cudaStream_t s, const Geom& g, const V* U, const V* r, V* x, const SapArgs& a, int nrhs) {
-    launch_sap<V, false>(s, g, U, r, x, a, nrhs);
+    const int S = g.sel_x * g.sel_t;
+    if (a.m > kSapMaxM) throw ParamFailure{"SAP block GMRES restart length above 8 is not supported"};
+    SapKParams p{a.m, a.restarts, a.tol, a.m0, a.blocks, a.nblocks, a.done, nrhs, 1};
+    if (S <= 32) launch_fine_warp<V, 1>(s, g, U, r, x, p);
+    else if (S <= 64) launch_fine_warp<V, 2>(s, g, U, r, x, p);
+    else if (S <= 128) launch_fine_warp<V, 4>(s, g, U, r, x, p);
+    else if (S <= 256) launch_fine_warp<V, 8>(s, g, U, r, x, p);
+    else launch_sap<V, false>(s, g, U, r, x, a, nrhs);
 }
 template <typename V>
 void launch_sap_sweep_coarse(cudaStream_t s, const Geom& g, const V* links, const V* r, V* x, const SapArgs& a,

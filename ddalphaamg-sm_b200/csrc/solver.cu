@@ -75,7 +75,11 @@ struct ddamg_handle {
     double2* hpin2 = nullptr;  // pinned host staging (uploads)
     double2* dalpha = nullptr; // per-rhs scale factors
     double2* grad = nullptr;   // gradient work: psi, lambda, sigma_3 eta (3 fine vectors)
-    ddamg::CoarseGmresWork cg;
+    ddamg::CoarseGmresWork cg;                      // lane 0: the handle's stream
+    std::vector<ddamg::CoarseGmresWork> cg_lane;    // lanes 1..: concurrent coarsest solves of a batch
+    std::vector<cudaStream_t> lane_s;
+    std::vector<cudaEvent_t> lane_ev;
+    cudaEvent_t fork_ev = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_setup_s = 0;
     long long launches_at_create = 0;
@@ -313,6 +317,26 @@ static void allocate(ddamg_handle* h) {
     h->cg.H = dalloc_t<double2>(h, (size_t)(cm + 1) * cm);
     h->cg.bar = dalloc_t<unsigned>(h, 2);
     h->cg.status = dalloc_t<int>(h, 2);
+    // extra lanes so the coarsest solves of a batch run side by side (each a cooperative grid)
+    const int lanes = std::min(p.max_rhs, 8);
+    DDAMG_CUDA_TRY(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
+    for (int k = 1; k < lanes; k++) {
+        CoarseGmresWork w = h->cg;
+        w.V = dalloc_t<double2>(h, (size_t)(cm + 1) * gc.size());
+        w.w = dalloc_t<double2>(h, gc.size());
+        w.r = nullptr;
+        w.partial = dalloc_t<double2>(h, (size_t)3 * h->cg.grid * (cm + 2));
+        w.H = dalloc_t<double2>(h, (size_t)(cm + 1) * cm);
+        w.bar = dalloc_t<unsigned>(h, 2);
+        w.status = dalloc_t<int>(h, 2);
+        h->cg_lane.push_back(w);
+        cudaStream_t ls;
+        cudaEvent_t le;
+        DDAMG_CUDA_TRY(cudaStreamCreateWithFlags(&ls, cudaStreamNonBlocking));
+        DDAMG_CUDA_TRY(cudaEventCreateWithFlags(&le, cudaEventDisableTiming));
+        h->lane_s.push_back(ls);
+        h->lane_ev.push_back(le);
+    }
     sync(h);
 }
 
@@ -373,11 +397,43 @@ static int coarse_solve(ddamg_handle* h, const double2* b, double2* x) {
                         h->p.coarse_gmres_restarts, h->p.coarse_gmres_tolerance);
     return 0;
 }
+// coarsest solves of R right-hand sides: right-hand side r runs on lane r mod K; lanes other than
+// 0 have their own stream, forked from and joined back into the handle's stream with events
+static void coarse_solve_batch(ddamg_handle* h, const double2* b, double2* x, int R) {
+    if (R == 1) {
+        coarse_solve(h, b, x);
+        return;
+    }
+    ProfScope ps(h, 1, h->L - 1);
+    LevelData& D = h->lv[h->L - 1];
+    const Geom& g = D.g;
+    const long n = g.size();
+    const int K = 1 + (int)h->cg_lane.size();
+    DDAMG_CUDA_TRY(cudaEventRecord(h->fork_ev, h->s));
+    for (int k = 1; k < K && k < R; k++) DDAMG_CUDA_TRY(cudaStreamWaitEvent(h->lane_s[k - 1], h->fork_ev, 0));
+    for (int r = 0; r < R; r++) {
+        const int k = r % K;
+        cudaStream_t st = k == 0 ? h->s : h->lane_s[k - 1];
+        const CoarseGmresWork& w = k == 0 ? h->cg : h->cg_lane[k - 1];
+        launch_coarse_gmres(st, w, D.d.links, b + r * n, x + r * n, g.Nx, g.Nt, g.dof, h->p.m0,
+                            h->p.coarse_gmres_restart_length, h->p.coarse_gmres_restarts,
+                            h->p.coarse_gmres_tolerance);
+    }
+    for (int k = 1; k < K && k < R; k++) {
+        DDAMG_CUDA_TRY(cudaEventRecord(h->lane_ev[k - 1], h->lane_s[k - 1]));
+        DDAMG_CUDA_TRY(cudaStreamWaitEvent(h->s, h->lane_ev[k - 1], 0));
+    }
+}
 static void check_coarse_status(ddamg_handle* h, int* iters) {
-    int st[2];
-    DDAMG_CUDA_TRY(cudaMemcpyAsync(st, h->cg.status, sizeof(st), cudaMemcpyDeviceToHost, h->s));
+    const int K = 1 + (int)h->cg_lane.size();
+    std::vector<int> st(2 * K);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(st.data(), h->cg.status, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->s));
+    for (int k = 1; k < K; k++)
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(st.data() + 2 * k, h->cg_lane[k - 1].status, 2 * sizeof(int),
+                                       cudaMemcpyDeviceToHost, h->s));
     sync(h);
-    if (st[0] != 0) throw TimeoutFailure();
+    for (int k = 0; k < K; k++)
+        if (st[2 * k] != 0) throw TimeoutFailure();
     if (iters) *iters = st[1];
 }
 
@@ -572,9 +628,7 @@ template <typename V>
 static void cycle_t(ddamg_handle* h, int l, const V* eta, V* psi, bool psi_zero, int kind, int R) {
     const ddamg_params& p = h->p;
     if (l == h->L - 1) {
-        const long n = h->lv[l].g.size();
-        for (int r = 0; r < R; r++)
-            coarse_solve(h, reinterpret_cast<const double2*>(eta) + r * n, reinterpret_cast<double2*>(psi) + r * n);
+        coarse_solve_batch(h, reinterpret_cast<const double2*>(eta), reinterpret_cast<double2*>(psi), R);
         return;
     }
     LevelData& D = h->lv[l];
@@ -867,6 +921,9 @@ ddamg_status ddamg_destroy(ddamg_t* h) {
     if (h->s) cudaStreamSynchronize(h->s);
     for (void* a : h->allocs) cudaFree(a);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->lane_ev) cudaEventDestroy(e);
+    for (cudaStream_t q : h->lane_s) cudaStreamDestroy(q);
+    if (h->fork_ev) cudaEventDestroy(h->fork_ev);
     if (h->hpin) cudaFreeHost(h->hpin);
     if (h->hpin2) cudaFreeHost(h->hpin2);
     if (h->ev0) cudaEventDestroy(h->ev0);
