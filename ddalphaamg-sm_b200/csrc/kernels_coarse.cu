@@ -83,12 +83,88 @@ __global__ void __launch_bounds__(128) coarse_op_kernel(const V* __restrict__ li
         }
     }
 }
+// The same operator for several vectors at once: one warp per (site, chunk of RC vectors), lane =
+// output dof (dof <= 32).  Each link element is loaded once and applied to all RC vectors; the
+// neighbour vectors of the chunk are staged in per-warp shared memory and read as broadcasts.
+// Tasks run site-major, so the chunks of one site are neighbours in the grid and share its links
+// through L2.
+template <typename V, int RC>
+__global__ void __launch_bounds__(128) coarse_op_multi_kernel(const V* __restrict__ links, const V* __restrict__ in,
+                                                              V* __restrict__ out, const V* __restrict__ b, int Nx,
+                                                              int Nt, int dof, typename RealOf<V>::R m0, long stride,
+                                                              int nrhs) {
+    typedef typename RealOf<V>::R R;
+    __shared__ V sv[4][RC][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int nchunk = (nrhs + RC - 1) / RC;
+    const long task = (long)blockIdx.x * 4 + wib;
+    const int sites = Nx * Nt;
+    if (task >= (long)sites * nchunk) return;
+    const int n = (int)(task / nchunk), r0 = (int)(task - (long)n * nchunk) * RC;
+    const int rc = min(RC, nrhs - r0);
+    const int x = n / Nt, t = n - x * Nt;
+    int nb[5];
+    R sg[5];
+    nb[0] = n;
+    nb[1] = x * Nt + ((t + 1 == Nt) ? 0 : t + 1);
+    nb[2] = ((x + 1 == Nx) ? 0 : x + 1) * Nt + t;
+    nb[3] = x * Nt + ((t == 0) ? Nt - 1 : t - 1);
+    nb[4] = ((x == 0) ? Nx - 1 : x - 1) * Nt + t;
+    sg[0] = R(1);
+    sg[1] = (t == Nt - 1) ? R(-1) : R(1);
+    sg[2] = R(1);
+    sg[3] = (t == 0) ? R(-1) : R(1);
+    sg[4] = R(1);
+    V acc[RC], self[RC];
+#pragma unroll
+    for (int r = 0; r < RC; r++) acc[r] = self[r] = czero<V>();
+    const bool li = lane < dof;
+    for (int d = 0; d < 5; d++) {
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < RC; r++) {
+            V v = (li && r < rc) ? sg[d] * in[(long)(r0 + r) * stride + (long)nb[d] * dof + lane] : czero<V>();
+            sv[wib][r][lane] = v;
+            if (d == 0) self[r] = v;
+        }
+        __syncwarp();
+        const V* M = links + ((long)n * 5 + d) * dof * dof;
+        for (int j0 = 0; j0 < dof; j0 += 8) {  // 8 column loads in flight
+            V mv[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) mv[u] = (j0 + u < dof && li) ? __ldg(M + (long)(j0 + u) * dof + lane) : czero<V>();
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                if (j0 + u >= dof) break;
+#pragma unroll
+                for (int r = 0; r < RC; r++) acc[r] = cfma(mv[u], sv[wib][r][j0 + u], acc[r]);
+            }
+        }
+    }
+    if (!li) return;
+    const R mm = m0 + R(2);
+#pragma unroll
+    for (int r = 0; r < RC; r++) {
+        if (r >= rc) break;
+        V o = mm * self[r] - acc[r];
+        const long idx = (long)(r0 + r) * stride + (long)n * dof + lane;
+        if (b) o = b[idx] - o;
+        out[idx] = o;
+    }
+}
+
 template <typename V>
 void launch_coarse_op(cudaStream_t s, const V* links, const V* in, V* out, const V* b, int Nx, int Nt, int dof,
                       double m0, int nrhs) {
     typedef typename RealOf<V>::R R;
-    dim3 grid(ceil_div((long)Nx * Nt, 4), nrhs);
     long stride = (long)Nx * Nt * dof;
+    if (nrhs > 1 && dof <= 32) {
+        const long tasks = (long)Nx * Nt * ((nrhs + 7) / 8);
+        DDAMG_LAUNCH((coarse_op_multi_kernel<V, 8>), ceil_div(tasks, 4), 128, 0, s, links, in, out, b, Nx, Nt, dof,
+                     (R)m0, stride, nrhs);
+        return;
+    }
+    dim3 grid(ceil_div((long)Nx * Nt, 4), nrhs);
     if (dof <= 32)
         DDAMG_LAUNCH((coarse_op_kernel<V, 1>), grid, 128, 0, s, links, in, out, b, Nx, Nt, dof, (R)m0, stride);
     else
