@@ -355,6 +355,9 @@ def run_ours(args, rank, world, local_rank):
             "rel_err_vs_fp64": float(np.linalg.norm(xm.cpu().numpy().view(np.complex128) - x) / np.linalg.norm(x))}
         sm.close()
         sec["dw_gbs"] = dw_bandwidth(ddamg, torch, local_rank)
+        if not args.no_secondary:
+            sec["mixed_1024"] = mixed_1024(ddamg, torch, local_rank)
+            sec["batched_512"] = batched_512(ddamg, torch, local_rank)
     # ---- CPU baseline (the reference's own code, one core, the same workload)
     cpu = None
     err_vs_ref = None
@@ -393,6 +396,140 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def timed_solves(ddamg, torch, dev, p, U, b_dev, R, reps=2):
+    """setup + solve of R right-hand sides on one handle; returns (setup_ms, solve_ms, infos, x) of the
+    last of `reps` repetitions, times from the library's own events (device time)."""
+    s = ddamg.Solver(p)
+    s.load_gauge(U)
+    x = torch.zeros(b_dev.numel(), dtype=torch.float64, device=f"cuda:{dev}")
+    for _ in range(reps):
+        s.setUpPhase(seed=5)
+        infos = s.solve_device(b_dev.data_ptr(), x.data_ptr(), R)
+    s.close()
+    xs = x.cpu().numpy().view(np.complex128)
+    return 1e3 * infos[0].setup_seconds, 1e3 * infos[0].solve_seconds, infos, xs
+
+
+def rel_errs(xs, ref, n):
+    return [float(np.linalg.norm(xs[r * n:(r + 1) * n] - ref[r * n:(r + 1) * n]) / np.linalg.norm(ref[r * n:(r + 1) * n]))
+            for r in range(len(xs) // n)]
+
+
+def mixed_1024(ddamg, torch, dev, R=16):
+    """1024x1024, beta=4, 2000 Metropolis sweeps, m0=-0.07, 3 levels, Nv=16 (8x8 aggregates and SAP blocks, then
+    4x4), FGMRES(30) to 1e-10: plain FP64 single-RHS solve against the mixed solve, single and batched (R RHS in
+    one lockstep solve), with every mixed solution compared to the FP64 one of the same right-hand side."""
+    N = 1024
+    th, acc = ddamg.gauge_metropolis(N, N, 4.0, 2000, 1024, device=dev)
+    U = np.exp(1j * th)
+    n = 2 * N * N
+    b = ddamg.gaussian_field(n * R, 1025)
+    b_dev = torch.from_numpy(b.view(np.float64).copy()).to(f"cuda:{dev}")
+    rows = [[0, 128, 128, 16, 128, 128], [1, 32, 32, 16, 32, 32]]
+
+    def p(prec, R_):
+        return ddamg.default_params(N, N, 3, -0.07, rows, precision=prec, max_rhs=R_, fgmres_restart_length=30,
+                                    fgmres_tolerance=1e-10, device=dev)
+
+    s64, t64, i64, x64 = timed_solves(ddamg, torch, dev, p(ddamg.PREC_DOUBLE, 1), U, b_dev[:2 * n], 1)
+    sB64, tB64, iB64, xB64 = timed_solves(ddamg, torch, dev, p(ddamg.PREC_DOUBLE, R), U, b_dev, R, reps=1)
+    sm, tm, im, xm = timed_solves(ddamg, torch, dev, p(ddamg.PREC_MIXED, 1), U, b_dev[:2 * n], 1)
+    sb, tb, ib, xb = timed_solves(ddamg, torch, dev, p(ddamg.PREC_MIXED, R), U, b_dev, R)
+    assert np.linalg.norm(xB64[:n] - x64) / np.linalg.norm(x64) < 1e-8
+    errs = rel_errs(xb, xB64, n)
+    return {
+        "workload": f"1024x1024 beta=4 (2000 sweeps, acceptance {acc:.3f}), m0=-0.07, 3 levels Nv=16, "
+                    f"FGMRES(30) V-cycle to 1e-10; {R} Gaussian RHS",
+        "fp64_single": {"setup_ms": s64, "solve_ms": t64, "iterations": i64[0].iterations,
+                        "rel_residual": i64[0].rel_residual},
+        "fp64_batched": {"R": R, "setup_ms": sB64, "solve_ms": tB64, "solve_ms_per_rhs": tB64 / R,
+                         "iterations": [i.iterations for i in iB64]},
+        "mixed_single": {"setup_ms": sm, "solve_ms": tm, "iterations": im[0].iterations,
+                         "rel_residual": im[0].rel_residual,
+                         "rel_err_vs_fp64": float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))},
+        "mixed_batched": {"R": R, "setup_ms": sb, "solve_ms": tb, "solve_ms_per_rhs": tb / R,
+                          "time_to_solution_ms_per_rhs": (sb + tb) / R,
+                          "iterations": [i.iterations for i in ib],
+                          "max_rel_residual": max(i.rel_residual for i in ib),
+                          "max_rel_err_vs_fp64": max(errs)},
+        "speedup_per_rhs_solve": t64 / (tb / R),
+        "speedup_per_rhs_time_to_solution": (s64 + t64) / ((sb + tb) / R),
+    }
+
+
+def batched_512(ddamg, torch, dev):
+    """512x512, beta=3 (1000 sweeps), m0=-0.10, 3 levels, Nv=16 (8x8 aggregates and SAP blocks, then 4x4... as
+    rows 0 64 64 16 64 64 / 1 16 16 16 16 16), FGMRES(30) to 1e-10: 64 Gaussian RHS in one lockstep mixed solve,
+    and 8 independent configurations x 8 RHS (8 handles driven from 8 host threads, each on its own stream),
+    both per RHS against the FP64 single-RHS solve; errors against FP64 batched solutions of the same systems."""
+    import threading
+
+    N, R = 512, 64
+    rows = [[0, 64, 64, 16, 64, 64], [1, 16, 16, 16, 16, 16]]
+    n = 2 * N * N
+
+    def p(prec, R_):
+        return ddamg.default_params(N, N, 3, -0.10, rows, precision=prec, max_rhs=R_, fgmres_restart_length=30,
+                                    fgmres_tolerance=1e-10, device=dev)
+
+    th, acc = ddamg.gauge_metropolis(N, N, 3.0, 1000, 512, device=dev)
+    U = np.exp(1j * th)
+    b = ddamg.gaussian_field(n * R, 513)
+    b_dev = torch.from_numpy(b.view(np.float64).copy()).to(f"cuda:{dev}")
+    s64, t64, i64, x64 = timed_solves(ddamg, torch, dev, p(ddamg.PREC_DOUBLE, 1), U, b_dev[:2 * n], 1)
+    sB, tB, iB, xB = timed_solves(ddamg, torch, dev, p(ddamg.PREC_DOUBLE, R), U, b_dev, R, reps=1)
+    sb, tb, ib, xb = timed_solves(ddamg, torch, dev, p(ddamg.PREC_MIXED, R), U, b_dev, R)
+    errs = rel_errs(xb, xB, n)
+    out = {
+        "workload": f"512x512 beta=3 (1000 sweeps, acceptance {acc:.3f}), m0=-0.10, 3 levels Nv=16, FGMRES(30) "
+                    "V-cycle to 1e-10",
+        "fp64_single": {"setup_ms": s64, "solve_ms": t64, "iterations": i64[0].iterations},
+        "mixed_batched_64": {"setup_ms": sb, "solve_ms": tb, "solve_ms_per_rhs": tb / R,
+                             "time_to_solution_ms_per_rhs": (sb + tb) / R,
+                             "iterations": sorted(set(i.iterations for i in ib)),
+                             "max_rel_residual": max(i.rel_residual for i in ib), "max_rel_err_vs_fp64": max(errs),
+                             "speedup_per_rhs_solve": t64 / (tb / R),
+                             "speedup_per_rhs_time_to_solution": (s64 + t64) / ((sb + tb) / R)},
+    }
+    # 8 configurations x 8 RHS: one handle per configuration, all set up and solved concurrently
+    C, RC = 8, 8
+    handles, bufs = [], []
+    for c in range(C):
+        thc, _ = ddamg.gauge_metropolis(N, N, 3.0, 1000, 600 + c, device=dev)
+        h = ddamg.Solver(p(ddamg.PREC_MIXED, RC))
+        h.load_gauge(np.exp(1j * thc))
+        bc = torch.from_numpy(ddamg.gaussian_field(n * RC, 700 + c).view(np.float64).copy()).to(f"cuda:{dev}")
+        bufs.append((bc, torch.zeros_like(bc)))
+        handles.append(h)
+    res = [None] * C
+
+    def work(c):
+        h, (bc, xc) = handles[c], bufs[c]
+        h.setUpPhase(seed=5)
+        res[c] = h.solve_device(bc.data_ptr(), xc.data_ptr(), RC)
+
+    walls = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ts = [threading.Thread(target=work, args=(c,)) for c in range(C)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        torch.cuda.synchronize()
+        walls.append(1e3 * (time.perf_counter() - t0))
+    its = [i.iterations for r in res for i in r]
+    out["mixed_8configs_x_8rhs"] = {
+        "wall_ms": walls[-1], "time_to_solution_ms_per_rhs": walls[-1] / (C * RC),
+        "iterations": sorted(set(its)), "max_rel_residual": max(i.rel_residual for r in res for i in r),
+        "speedup_per_rhs_time_to_solution_vs_fp64_single": (s64 + t64) / (walls[-1] / (C * RC)),
+        "timing": "host wall clock around setup + solve of all 8 handles (8 threads, 8 streams)"}
+    for h in handles:
+        h.close()
+    return out
 
 
 def dw_bandwidth(ddamg, torch, dev):
@@ -436,6 +573,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the 1024x1024 and 512x512 batched lines")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -55,6 +55,10 @@ template <> LevelBufs<float2>& B<float2>(LevelData& L) { return L.f; }
 
 }  // namespace ddamg
 
+// timing kinds: 0 SAP colour sweep, 1 coarsest GMRES, 2 level operator, 3 orthonormalisation,
+// 4 coarse-link construction
+constexpr int kProfKinds = 5;
+
 struct ddamg_handle {
     ddamg_params p;
     int L = 0;          // levels
@@ -92,8 +96,8 @@ struct ddamg_handle {
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_next = 0;
     std::vector<ProfRec> prof_recs;
-    double prof_ms[3][DDAMG_MAX_LEVELS] = {};
-    long long prof_n[3][DDAMG_MAX_LEVELS] = {};
+    double prof_ms[kProfKinds][DDAMG_MAX_LEVELS] = {};
+    long long prof_n[kProfKinds][DDAMG_MAX_LEVELS] = {};
 };
 
 namespace ddamg {
@@ -744,7 +748,11 @@ static void setup(ddamg_handle* h, const double2* rnd_host, uint64_t seed) {
         // SAP(rhs = 0, tvec, nu = SAP_test_vectors_iterations) on all test vectors at once
         DDAMG_CUDA_TRY(cudaMemsetAsync(D.d.eta, 0, sizeof(double2) * n * nv, s));
         sap_t<double2>(h, l, D.d.eta, D.d.tv, h->p.sap_test_vectors_iterations, 1e-10, false, nv, false);
-        launch_orthonormalize(s, D.g, D.d.tv);
+        {
+            ProfScope ps(h, 3, l);
+            launch_orthonormalize(s, D.g, D.d.tv);
+        }
+        ProfScope ps(h, 4, l);
         launch_build_coarse_links(s, D.g, D.d.U, D.d.links, D.d.tv, h->lv[l + 1].d.links);
     }
     make_fp32_copies(h);
@@ -955,7 +963,7 @@ ddamg_status ddamg_profile(ddamg_t* h, int enable) {
 ddamg_status ddamg_profile_query(ddamg_t* h, int kind, int level, double* total_ms, long long* launches) {
     CHECK_HANDLE(h);
     API_BEGIN
-    if (kind < 0 || kind > 2 || level < 0 || level >= h->L) throw ParamFailure{"kind or level out of range"};
+    if (kind < 0 || kind >= kProfKinds || level < 0 || level >= h->L) throw ParamFailure{"kind or level out of range"};
     prof_flush(h);
     if (total_ms) *total_ms = h->prof_ms[kind][level];
     if (launches) *launches = h->prof_n[kind][level];
@@ -1346,13 +1354,20 @@ ddamg_status ddamg_gradient(ddamg_t* h, const double* eta, const double* b, doub
     ddamg_solve_info inf[2];
     if (!h->grad) h->grad = dalloc_t<double2>(h, 3 * (size_t)n);
     double2 *gpsi = h->grad, *glam = h->grad + n, *gtmp = h->grad + 2 * n;
-    // psi = D^-1 b
+    // psi = D^-1 b and lambda = D^-dagger eta = sigma_3 D^-1 sigma_3 eta (gamma_5-hermiticity):
+    // one lockstep solve of both when the handle batches, else two solves
     DDAMG_CUDA_TRY(cudaMemcpyAsync(h->ob, b, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
-    ddamg_status s1 = solve_device(h, h->ob, gpsi, 1, &inf[0]);
-    // lambda = D^-dagger eta = sigma_3 D^-1 sigma_3 eta (gamma_5-hermiticity)
     DDAMG_CUDA_TRY(cudaMemcpyAsync(gtmp, eta, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
-    launch_sigma3(h->s, gtmp, h->ob, sites);
-    ddamg_status s2 = solve_device(h, h->ob, gtmp, 1, &inf[1]);
+    ddamg_status s1, s2;
+    if (h->p.max_rhs >= 2) {
+        launch_sigma3(h->s, gtmp, h->ob + n, sites);
+        s1 = s2 = solve_device(h, h->ob, gpsi, 2, inf);  // psi then sigma_3 lambda, back to back
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(gtmp, glam, sizeof(double2) * n, cudaMemcpyDeviceToDevice, h->s));
+    } else {
+        s1 = solve_device(h, h->ob, gpsi, 1, &inf[0]);
+        launch_sigma3(h->s, gtmp, h->ob, sites);
+        s2 = solve_device(h, h->ob, gtmp, 1, &inf[1]);
+    }
     launch_sigma3(h->s, gtmp, glam, sites);
     double* g = reinterpret_cast<double*>(gtmp);
     launch_link_derivative(h->s, D.d.U, gpsi, glam, g, D.g.Nx, D.g.Nt);

@@ -250,7 +250,8 @@ class Solver:
         check(self.L.ddamg_profile(self.h, int(bool(enable))))
 
     def profile_query(self, kind, level):
-        """(total ms, launches) of kind 0 SAP sweep / 1 coarsest GMRES / 2 level operator at a level."""
+        """(total ms, launches) of kind 0 SAP sweep / 1 coarsest GMRES / 2 level operator /
+        3 orthonormalisation / 4 coarse-link construction at a level."""
         ms = ctypes.c_double(0)
         n = ctypes.c_longlong(0)
         check(self.L.ddamg_profile_query(self.h, kind, level, ctypes.byref(ms), ctypes.byref(n)))

@@ -101,7 +101,8 @@ ddamg_status ddamg_get_stream(ddamg_t* h, void** stream);
 ddamg_status ddamg_launch_count(ddamg_t* h, long long* count);
 /* per-kernel device timing: while enabled, the handle brackets every SAP sweep, coarsest solve
  * and level-operator launch with CUDA events on its stream; disabling folds the elapsed times
- * into per (kind, level) totals.  kind: 0 SAP colour sweep, 1 coarsest GMRES, 2 level operator.
+ * into per (kind, level) totals.  kind: 0 SAP colour sweep, 1 coarsest GMRES, 2 level operator,
+ * 3 orthonormalisation of the test vectors, 4 coarse-link construction (the last two: setup).
  * (No reference counterpart: the reference counts FLOPs, include/utils.h:141-150.) */
 ddamg_status ddamg_profile(ddamg_t* h, int enable);
 ddamg_status ddamg_profile_query(ddamg_t* h, int kind, int level, double* total_ms, long long* launches);
