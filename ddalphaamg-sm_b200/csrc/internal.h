@@ -84,6 +84,7 @@ void launch_build_coarse_links(cudaStream_t s, const Geom& g, const double2* U, 
 // ------------------------------------------------------------ SAP (kernels_sap.cu)
 // One colour sweep of SAP_C::SAP: x_B += D_B^-1 r_B for every block of the colour, block
 // GMRES(m) x restarts to tol with x0 = r_B (src/sap.cpp:48-77).  blocks: device list.
+constexpr int kSapMaxM = 8;  // block GMRES restart length supported by the SAP block solvers
 struct SapArgs {
     int m, restarts;
     double tol;
@@ -98,6 +99,27 @@ void launch_sap_sweep_fine(cudaStream_t s, const Geom& g, const V* U, const V* r
 template <typename V>
 void launch_sap_sweep_coarse(cudaStream_t s, const Geom& g, const V* links, const V* r, V* x, const SapArgs& a,
                              int nrhs);
+
+// ------------------------------------------------------------ tensor-core SAP (kernels_tcsap.cu)
+// Batched FP32 coarse-level SAP colour sweep whose block operator runs on tcgen05 tensor cores
+// (TF32 inputs, FP32 accumulation), with the per-(block, rhs) GMRES bookkeeping on CUDA cores.
+// Block vectors are [kb][r][s][dof] (kb: block of the colour, r: rhs, s: site in the block).
+struct TcSapWork {
+    float2 *b = nullptr, *x = nullptr, *w = nullptr, *V = nullptr;  // V holds m+1 block vectors
+    long vec = 0;                                                    // float2 per block vector
+    int *act = nullptr, *fin = nullptr, *arn = nullptr, *maxit = nullptr;
+    double *normb = nullptr, *err = nullptr;
+    double2 *H = nullptr, *gm = nullptr, *cn = nullptr, *sn = nullptr;
+    float* tiles = nullptr;  // operator tiles of the level, kTcTileFloats per (site, direction)
+    int* status = nullptr;   // set when a bounded wait inside the apply kernel gave up
+};
+constexpr int kTcTileFloats = 64 * 64;
+// the level's geometry admits the tensor-core sweep (dof <= 32, at most 1024 unknowns per block,
+// and a block-vector window that fits in shared memory)
+bool tc_sap_supported(const Geom& g);
+void launch_pack_tc_links(cudaStream_t s, const Geom& g, const float2* links, float* tiles);
+void launch_sap_sweep_tc(cudaStream_t s, const Geom& g, const TcSapWork& w, const float2* r, float2* x,
+                         const SapArgs& a, int nrhs);
 
 // ------------------------------------------------------------ coarsest GMRES (kernels_gmres.cu)
 struct CoarseGmresWork {

@@ -53,7 +53,6 @@ struct SapKParams {
     int ngroups;  // CTAs per Schwarz block: ceil(nrhs / RB)
 };
 
-constexpr int kSapMaxM = 8;  // block GMRES restart length supported by the on-chip solver
 
 // Shared memory of one CTA: RB right-hand sides of one Schwarz block.  Vectors are stored
 // [element][rhs] so that the RB values a link element multiplies sit side by side.

@@ -1,0 +1,571 @@
+// Batched coarse-level SAP colour sweep with the block operator on tcgen05 tensor cores.
+//
+// A colour sweep solves, for every Schwarz block B of the colour and every right-hand side r,
+// D_B e = r_B by GMRES(m) x restarts with x0 = r_B (SAP_C::SAP, src/sap.cpp:48-77,104-139;
+// FGMRES::fgmres, src/fgmres.cpp:5-98).  With R right-hand sides in lockstep the operator
+// application of one block is, per site s and hop d, the contraction of a dof x dof complex link
+// with a dof x R block of vectors: in the real embedding a GEMM with M = 2 dof, K = 2 dof, N = R.
+//
+//   tc_block_apply_kernel   one CTA per (block, group of RG right-hand sides):
+//                           w = D_B v (or b - D_B v) on tensor cores.  The embedded link tiles
+//                           (one per site and hop, packed once after the setup) arrive by bulk
+//                           copy; the vector tiles of the block's sites arrive by TMA straight from
+//                           the interleaved block vectors into a shared-memory window holding sites
+//                           s - sel_t .. s + sel_t + 1, so every vector tile is read once per
+//                           application; the accumulators live in tensor memory, two buffers so
+//                           the epilogue of site s overlaps the MMAs of site s + 1.
+//   tcs_* kernels           one warp per (block, right-hand side): Gram-Schmidt, Givens rotations,
+//                           restarts, and the gather / scatter between the level vectors and the
+//                           block vectors, with the same per-rhs control flow (break point maxIt,
+//                           convergence freeze) as the on-chip solver in kernels_sap.cu.
+//
+// Warp roles of the apply kernel: warps 0-3 epilogue (warp q reads tensor-memory lanes
+// 32q..32q+31), warp 4 lane 0 issues the copies, warp 5 lane 0 the MMAs.  Every mbarrier wait is
+// bounded; a wait that gives up sets the status word and the CTA winds down.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "internal.h"
+#include "tc_sm100.cuh"
+
+namespace ddamg {
+
+using namespace tc;
+
+namespace {
+constexpr int kNA = 3;  // link-tile ring depth
+constexpr int kEpiWarps = 4;
+constexpr int kProdWarp = 4, kMmaWarp = 5;
+constexpr int kApplyThreads = 6 * 32;
+constexpr uint32_t kTileBytes = kTcTileFloats * 4;  // 64 rows x 64 fp32
+
+__host__ __device__ inline int release_lag(int sel_t) { return sel_t > 2 ? sel_t : 2; }
+__host__ __device__ inline int window_slots(int sel_t) { return sel_t + release_lag(sel_t) + 2; }
+inline size_t apply_smem(int RG, int sel_t) {
+    const int nw = window_slots(sel_t);
+    return 1024 + (size_t)kNA * kTileBytes + (size_t)nw * 256 * RG + sizeof(uint64_t) * (2 * kNA + 2 * nw + 5);
+}
+inline int pick_rg(int nrhs, int sel_t) {
+    int rg = 16;
+    while (rg < 64 && rg < nrhs) rg *= 2;
+    while (rg > 16 && apply_smem(rg, sel_t) > 227 * 1024) rg /= 2;
+    return rg;
+}
+
+struct ApplyArgs {
+    const float* tiles;  // operator tiles (site, hop)
+    float2* dst;
+    const float2* bsub;  // non-null: dst = bsub - D_B src
+    const int* flag;     // per (kb, r): the rhs takes part when (flag != 0) != invert
+    int invert;
+    const int* blocks;
+    int R, S, sel_x, sel_t, Nt, sap_t, dof;
+    int ks;  // MMA K steps of 8: ceil(2 dof / 8)
+    float mm;  // m0 + 2
+    int* status;
+};
+}  // namespace
+
+bool tc_sap_supported(const Geom& g) {
+    const int S = g.sel_x * g.sel_t;
+    return g.level >= 1 && g.dof <= 32 && S * g.dof <= 1024 && apply_smem(16, g.sel_t) <= 227 * 1024;
+}
+
+// Operator tile (n, d): the real 2dof x 2dof embedding of T = -s_d M_d, M_d the coarse link of hop
+// d at site n and s_d the antiperiodic sign of a hop across the t boundary (the mass term of d = 0
+// is added in FP32 by the epilogue):  rows m = 2i + p (p: real / imaginary part of output dof i),
+// columns k = 2j + q (q: real / imaginary part of input dof j),
+//     [Re T_ij  -Im T_ij]
+//     [Im T_ij   Re T_ij],
+// zero outside i, j < dof; 64 x 64 fp32 stored as two K-major 128B-swizzled 64 x 32 blocks (the
+// shared-memory image, so one bulk copy lands it ready for tcgen05.mma).  A vector stored as
+// interleaved (re, im) pairs is then the K-major B operand as it lies in memory.
+__global__ void pack_tc_links_kernel(const float2* __restrict__ L, float* __restrict__ tiles, int Nt, int dof) {
+    const long tile = blockIdx.x;
+    const int n = (int)(tile / 5), d = (int)(tile - (long)n * 5);
+    const int t = n % Nt;
+    const float sg = ((d == 1 && t == Nt - 1) || (d == 3 && t == 0)) ? -1.f : 1.f;
+    const float2* M = L + tile * dof * dof;
+    char* base = reinterpret_cast<char*>(tiles + tile * kTcTileFloats);
+    for (int e = threadIdx.x; e < kTcTileFloats; e += blockDim.x) {
+        const int m = e >> 6, k = e & 63, i = m >> 1, p = m & 1, j = k >> 1, q = k & 1;
+        float v = 0.f;
+        if (i < dof && j < dof) {
+            const float2 l = M[(long)j * dof + i];
+            const float re = -sg * l.x, im = -sg * l.y;
+            v = (p == q) ? re : (p ? im : -im);
+        }
+        *reinterpret_cast<float*>(base + (k >> 5) * 8192 + swz_off(m, k & 31)) = v;
+    }
+}
+
+void launch_pack_tc_links(cudaStream_t s, const Geom& g, const float2* links, float* tiles) {
+    DDAMG_LAUNCH(pack_tc_links_kernel, (long)g.sites * 5, 256, 0, s, links, tiles, g.Nt, g.dof);
+}
+
+// w = D_B src (or bsub - D_B src) for one block and RG right-hand sides.  src enters through the
+// tensor map vmap: dims (2 dof floats, S sites, NB*R block-rhs rows), box (32, 1, RG), 128B swizzle,
+// so a box lands as RG rows of 32 fp32 -- one K-major 128B-swizzled operand block.
+template <int RG>
+__global__ void __launch_bounds__(kApplyThreads, 1)
+    tc_block_apply_kernel(const __grid_constant__ CUtensorMap vmap, ApplyArgs a) {
+    extern __shared__ unsigned char smraw[];
+    __shared__ int s_any;
+    __shared__ volatile int s_abort;
+    __shared__ uint32_t s_taddr;
+    constexpr uint32_t kBBytes = RG * 256;  // two 128-byte column blocks of RG rows
+    unsigned char* sm =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
+    const int kb = blockIdx.x, r0 = blockIdx.y * RG;
+    const int nr = min(RG, a.R - r0);
+    const int S = a.S, NW = window_slots(a.sel_t), RL = release_lag(a.sel_t);
+    const int katoms = (a.ks + 3) >> 2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        s_any = 0;
+        s_abort = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x < nr && ((a.flag[(long)kb * a.R + r0 + threadIdx.x] != 0) != (a.invert != 0))) s_any = 1;
+    __syncthreads();
+    if (!s_any) return;
+
+    unsigned char* Abuf = sm;
+    unsigned char* Bbuf = sm + kNA * kTileBytes;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Bbuf + (size_t)NW * kBBytes);
+    uint64_t* fullA = bar;
+    uint64_t* emptyA = bar + kNA;
+    uint64_t* fullB = bar + 2 * kNA;
+    uint64_t* emptyB = fullB + NW;
+    uint64_t* accF = emptyB + NW;
+    uint64_t* accE = accF + 2;
+    uint64_t* drain = accE + 2;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kNA; i++) {
+            mbar_init(&fullA[i], 1);
+            mbar_init(&emptyA[i], 1);
+        }
+        for (int i = 0; i < NW; i++) {
+            mbar_init(&fullB[i], 1);
+            mbar_init(&emptyB[i], 1);
+        }
+        for (int i = 0; i < 2; i++) {
+            mbar_init(&accF[i], 1);
+            mbar_init(&accE[i], kEpiWarps * 32);
+        }
+        mbar_init(drain, 1);
+        mbar_fence_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(&s_taddr, 2 * RG);
+        tmem_relinquish();
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t taddr = s_taddr;
+
+    const int blk = a.blocks[kb];
+    const int bx = blk / a.sap_t, bt = blk - bx * a.sap_t;
+    auto nbr = [&](int s, int d) -> int {
+        const int kx = s / a.sel_t, kt = s - kx * a.sel_t;
+        if (d == 0) return s;
+        if (d == 1) return kt + 1 < a.sel_t ? s + 1 : -1;
+        if (d == 2) return kx + 1 < a.sel_x ? s + a.sel_t : -1;
+        if (d == 3) return kt > 0 ? s - 1 : -1;
+        return kx > 0 ? s - a.sel_t : -1;
+    };
+    auto gsite = [&](int s) -> long {
+        const int kx = s / a.sel_t, kt = s - kx * a.sel_t;
+        return (long)(bx * a.sel_x + kx) * a.Nt + bt * a.sel_t + kt;
+    };
+    auto wait = [&](uint64_t* b, uint32_t parity) -> bool {
+        if (s_abort) return false;
+        if (mbar_wait(b, parity, a.status)) return true;
+        s_abort = 1;
+        return false;
+    };
+
+    if (warp == kProdWarp) {
+        // ---------------- producer (one thread): vector tiles by TMA, link tiles by bulk copy
+        if (lane == 0) {
+            int a_idx = 0, t_next = 0;
+            bool ok = true;
+            for (int s = 0; s < S && ok; s++) {
+                const int tmax = min(S - 1, s + a.sel_t + 1);
+                for (; t_next <= tmax; t_next++) {
+                    const int slot = t_next % NW, k = t_next / NW;
+                    if (k > 0 && !(ok = wait(&emptyB[slot], (k - 1) & 1))) break;
+                    unsigned char* tb = Bbuf + (size_t)slot * kBBytes;
+                    mbar_arrive_expect_tx(&fullB[slot], (uint32_t)katoms * RG * 128);
+                    for (int at = 0; at < katoms; at++)
+                        tma_load_3d(tb + at * RG * 128, &vmap, 32 * at, t_next, kb * a.R + r0, &fullB[slot]);
+                }
+                if (!ok) break;
+                for (int d = 0; d < 5; d++) {
+                    if (nbr(s, d) < 0) continue;
+                    const int stage = a_idx % kNA, k = a_idx / kNA;
+                    if (k > 0 && !(ok = wait(&emptyA[stage], (k - 1) & 1))) break;
+                    mbar_arrive_expect_tx(&fullA[stage], kTileBytes);
+                    bulk_g2s(Abuf + (size_t)stage * kTileBytes, a.tiles + (gsite(s) * 5 + d) * kTcTileFloats,
+                             kTileBytes, &fullA[stage]);
+                    a_idx++;
+                }
+            }
+            // every copy issued has landed before the CTA may exit
+            for (int st = 0; st < kNA; st++) {
+                const int issued = a_idx > st ? (a_idx - 1 - st) / kNA + 1 : 0;
+                if (issued > 0) mbar_wait(&fullA[st], (issued - 1) & 1, a.status);
+            }
+            for (int sl = 0; sl < NW; sl++) {
+                const int issued = t_next > sl ? (t_next - 1 - sl) / NW + 1 : 0;
+                if (issued > 0) mbar_wait(&fullB[sl], (issued - 1) & 1, a.status);
+            }
+        }
+    } else if (warp == kMmaWarp) {
+        // ---------------- MMA issuer (one thread)
+        if (lane == 0) {
+            const uint32_t idesc = idesc_tf32(64, RG);
+            int a_idx = 0;
+            for (int s = 0; s < S; s++) {
+                const int b = s & 1;
+                if (s >= 2 && !wait(&accE[b], ((s >> 1) - 1) & 1)) break;
+                tc_fence_after();
+                const uint32_t dt = taddr + (uint32_t)(b * RG);
+                bool first = true, ok = true;
+                for (int d = 0; d < 5; d++) {
+                    const int nb = nbr(s, d);
+                    if (nb < 0) continue;
+                    const int stage = a_idx % kNA;
+                    if (!wait(&fullB[nb % NW], (nb / NW) & 1) || !wait(&fullA[stage], (a_idx / kNA) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t as = smem_u32(Abuf + (size_t)stage * kTileBytes);
+                    const uint32_t bs = smem_u32(Bbuf + (size_t)(nb % NW) * kBBytes);
+                    for (int k = 0; k < a.ks; k++)  // K steps of 8 fp32 = 32 bytes within a 128-byte block
+                        mma_tf32(dt, sdesc_k128(as + (k >> 2) * 8192 + (k & 3) * 32),
+                                 sdesc_k128(bs + (k >> 2) * RG * 128 + (k & 3) * 32), idesc,
+                                 (first && k == 0) ? 0u : 1u);
+                    first = false;
+                    mma_commit(&emptyA[stage]);
+                    a_idx++;
+                }
+                if (!ok) break;
+                mma_commit(&accF[b]);
+                // site s is the last to read vector tile s - sel_t; the epilogue of site s - RL
+                // (which reads that site's own tile) has finished before site s could start
+                if (s >= RL) mma_commit(&emptyB[(s - RL) % NW]);
+            }
+            mma_commit(drain);  // every MMA of this CTA has finished before TMEM is released
+            mbar_wait(drain, 0, a.status);
+        }
+    } else {
+        // ---------------- epilogue: warp q owns accumulator rows 16q .. 16q+15 (lanes 0-15);
+        // row m = 2i + p is part p of output dof i for each right-hand side (column)
+        const int q = warp;
+        const int m = 16 * q + (lane & 15);
+        const bool rowok = lane < 16 && m < 2 * a.dof;
+        const float* bf = reinterpret_cast<const float*>(a.bsub);
+        float* dstf = reinterpret_cast<float*>(a.dst);
+        const uint32_t selfoff = (uint32_t)(m >> 5) * RG * 128;
+        for (int s = 0; s < S; s++) {
+            const int b = s & 1;
+            if (!wait(&accF[b], (s >> 1) & 1)) break;
+            tc_fence_after();
+            const uint32_t tb = taddr + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * RG);
+            const unsigned char* self = Bbuf + (size_t)(s % NW) * kBBytes + selfoff;
+            const long o0 = (((long)kb * a.R + r0) * S + s) * a.dof * 2 + m;  // float index, rhs r0
+            const long ostride = (long)S * a.dof * 2;
+#pragma unroll 1
+            for (int c0 = 0; c0 < RG; c0 += 16) {
+                float acc[16], bv[16];
+                tmem_ld16(tb + c0, acc);
+#pragma unroll
+                for (int c = 0; c < 16; c++)
+                    bv[c] = (bf && rowok && c0 + c < nr) ? bf[o0 + (c0 + c) * ostride] : 0.f;
+#pragma unroll
+                for (int c = 0; c < 16; c++) {
+                    if (rowok && c0 + c < nr) {
+                        const float v = *reinterpret_cast<const float*>(self + swz_off(c0 + c, m & 31));
+                        float w = a.mm * v + acc[c];
+                        if (bf) w = bv[c] - w;
+                        dstf[o0 + (c0 + c) * ostride] = w;
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&accE[b]);
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(taddr, 2 * RG);
+    }
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        DDAMG_CUDA_TRY(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p) throw ParamFailure{"cuTensorMapEncodeTiled is unavailable"};
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// block vectors [kb*R + r][s][dof] (interleaved complex) as a 3-D fp32 tensor
+static CUtensorMap vector_map(const float2* base, int dof, int S, long rows, int RG) {
+    CUtensorMap m;
+    cuuint64_t dims[3] = {(cuuint64_t)(2 * dof), (cuuint64_t)S, (cuuint64_t)rows};
+    cuuint64_t strides[2] = {(cuuint64_t)(2 * dof * 4), (cuuint64_t)S * 2 * dof * 4};
+    cuuint32_t box[3] = {32, 1, (cuuint32_t)RG};
+    cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float2*>(base), dims,
+                                            strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw ParamFailure{"tensor map encoding failed"};
+    return m;
+}
+
+template <int RG>
+static void launch_apply_rg(cudaStream_t s, const CUtensorMap& vmap, const ApplyArgs& a, int NB) {
+    const size_t smem = apply_smem(RG, a.sel_t);
+    DDAMG_CUDA_TRY(cudaFuncSetAttribute(tc_block_apply_kernel<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+    dim3 grid(NB, (a.R + RG - 1) / RG);
+    DDAMG_LAUNCH(tc_block_apply_kernel<RG>, grid, kApplyThreads, smem, s, vmap, a);
+}
+
+// ---------------------------------------------------------------- per (block, rhs) kernels
+// one warp per task = kb * R + r; lanes stride over the block's NE = S * dof unknowns
+struct TaskGeom {
+    int R, NB, S, dof, NE, sel_x, sel_t, Nt, sap_t;
+    long size;  // level vector length
+};
+
+__device__ __forceinline__ long level_index(const TaskGeom& t, int blk, int e) {
+    const int s = e / t.dof, i = e - s * t.dof;
+    const int kx = s / t.sel_t, kt = s - kx * t.sel_t;
+    const int bx = blk / t.sap_t, bt = blk - bx * t.sap_t;
+    return ((long)(bx * t.sel_x + kx) * t.Nt + bt * t.sel_t + kt) * t.dof + i;
+}
+
+__global__ void tcs_gather_kernel(TaskGeom t, TcSapWork w, const int* __restrict__ blocks,
+                                  const float2* __restrict__ rg, const int* __restrict__ done) {
+    const int task = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (task >= t.NB * t.R) return;
+    const int kb = task / t.R, r = task - kb * t.R;
+    const bool act = !(done && done[r]);
+    if (lane == 0) w.act[task] = act ? 1 : 0;
+    const int blk = blocks[kb];
+    float2* bv = w.b + (long)task * t.NE;
+    float2* xv = w.x + (long)task * t.NE;
+    for (int e = lane; e < t.NE; e += 32) {
+        const float2 v = act ? rg[(long)r * t.size + level_index(t, blk, e)] : make_float2(0.f, 0.f);
+        bv[e] = v;
+        xv[e] = v;
+    }
+}
+
+// after a residual w = b - D_B x: norms, convergence, and V_0 = w / ||w|| for the next restart
+__global__ void tcs_prep_kernel(TaskGeom t, TcSapWork w, int first, int m, double tol) {
+    const int task = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (task >= t.NB * t.R) return;
+    const float2* wv = w.w + (long)task * t.NE;
+    const float2* bv = w.b + (long)task * t.NE;
+    double rr = 0.0, bb = 0.0;
+    for (int e = lane; e < t.NE; e += 32) {
+        rr += (double)cnorm2(wv[e]);
+        if (first) bb += (double)cnorm2(bv[e]);
+    }
+    rr = warp_sum(rr);
+    bb = warp_sum(bb);
+    const double err = sqrt(rr);
+    int fin;
+    if (first) {
+        const double nb = sqrt(bb);
+        // a zero block right-hand side has the zero solution (the reference would divide by zero)
+        fin = (!w.act[task] || nb == 0.0) ? 1 : 0;
+        if (lane == 0) {
+            w.normb[task] = nb;
+            w.maxit[task] = m;
+        }
+    } else {
+        fin = w.fin[task];
+        if (!fin && err < tol * w.normb[task]) fin = 1;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        w.fin[task] = fin;
+        w.arn[task] = fin ? 0 : 1;
+        w.err[task] = err;
+        if (!fin) w.gm[(long)task * (m + 1)] = make_double2(err, 0.0);
+    }
+    if (fin) return;
+    const float inv = (float)(1.0 / err);
+    float2* v0 = w.V + (long)task * t.NE;
+    for (int e = lane; e < t.NE; e += 32) v0[e] = inv * wv[e];
+}
+
+// Arnoldi step j of every active (block, rhs): classical Gram-Schmidt against V_0..V_j, the new
+// basis vector, and the Givens update of Hessenberg column j (FGMRES::rotation,
+// src/fgmres.cpp:99-115); a rhs whose estimate meets tol stops its Arnoldi loop (maxIt = j + 1).
+template <int EPL>
+__global__ void tcs_arnoldi_kernel(TaskGeom t, TcSapWork w, int j, int m, double tol) {
+    const int task = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (task >= t.NB * t.R) return;
+    if (!w.arn[task]) return;
+    const long off = (long)task * t.NE;
+    float2 wl[EPL];
+#pragma unroll
+    for (int q = 0; q < EPL; q++) {
+        const int e = lane + 32 * q;
+        wl[q] = e < t.NE ? w.w[off + e] : make_float2(0.f, 0.f);
+    }
+    double2 h[kSapMaxM];
+    for (int i = 0; i <= j; i++) {
+        const float2* Vi = w.V + (long)i * w.vec + off;
+        double2 s = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int q = 0; q < EPL; q++) {
+            const int e = lane + 32 * q;
+            if (e < t.NE) s = cfmac(to_d(Vi[e]), to_d(wl[q]), s);
+        }
+        h[i] = warp_sum(s);
+    }
+    for (int i = 0; i <= j; i++) {
+        const float2* Vi = w.V + (long)i * w.vec + off;
+        const float2 hf = from_d<float2>(h[i]);
+#pragma unroll
+        for (int q = 0; q < EPL; q++) {
+            const int e = lane + 32 * q;
+            if (e < t.NE) wl[q] = wl[q] - cmul(hf, Vi[e]);
+        }
+    }
+    double ww = 0.0;
+#pragma unroll
+    for (int q = 0; q < EPL; q++) ww += (double)cnorm2(wl[q]);
+    const double hn = sqrt(warp_sum(ww));
+    if (hn > 0) {
+        float2* Vn = w.V + (long)(j + 1) * w.vec + off;
+        const float inv = (float)(1.0 / hn);
+#pragma unroll
+        for (int q = 0; q < EPL; q++) {
+            const int e = lane + 32 * q;
+            if (e < t.NE) Vn[e] = inv * wl[q];
+        }
+    }
+    if (lane != 0) return;
+    double2* H = w.H + (long)task * (m + 1) * m;
+    double2* cn = w.cn + (long)task * m;
+    double2* sn = w.sn + (long)task * m;
+    double2* gm = w.gm + (long)task * (m + 1);
+    for (int i = 0; i <= j; i++) H[i * m + j] = h[i];
+    H[(j + 1) * m + j] = make_double2(hn, 0.0);
+    for (int i = 0; i < j; i++) {
+        const double2 hij = H[i * m + j], hi1 = H[(i + 1) * m + j];
+        const double2 tmp = cmulc(cn[i], hij) + cmulc(sn[i], hi1);
+        H[(i + 1) * m + j] = cmul(cn[i], hi1) - cmul(sn[i], hij);
+        H[i * m + j] = tmp;
+    }
+    const double2 hjj = H[j * m + j], hj1 = H[(j + 1) * m + j];
+    const double den = sqrt(cnorm2(hjj) + cnorm2(hj1));
+    sn[j] = make_double2(hj1.x / den, hj1.y / den);
+    cn[j] = make_double2(hjj.x / den, hjj.y / den);
+    H[j * m + j] = cmulc(cn[j], hjj) + cmulc(sn[j], hj1);
+    H[(j + 1) * m + j] = make_double2(0.0, 0.0);
+    gm[j + 1] = -cmul(sn[j], gm[j]);
+    gm[j] = cmulc(cn[j], gm[j]);
+    if (sqrt(cnorm2(gm[j + 1])) < tol * w.normb[task]) {
+        w.maxit[task] = j + 1;  // not reset at the next restart (src/fgmres.cpp:14,56)
+        w.arn[task] = 0;
+    }
+}
+
+// solve_upper_triangular (src/fgmres.cpp:118-128) and x += sum_jj eta_jj V_jj
+__global__ void tcs_update_kernel(TaskGeom t, TcSapWork w, int m) {
+    __shared__ double2 eta_s[8][kSapMaxM];
+    const int wib = threadIdx.x >> 5;
+    const int task = blockIdx.x * (blockDim.x >> 5) + wib, lane = threadIdx.x & 31;
+    if (task >= t.NB * t.R) return;
+    if (w.fin[task]) return;
+    const int mi = w.maxit[task];
+    double2* eta = eta_s[wib];
+    if (lane == 0) {
+        const double2* H = w.H + (long)task * (m + 1) * m;
+        const double2* gm = w.gm + (long)task * (m + 1);
+        for (int i = mi - 1; i >= 0; i--) {
+            double2 e = gm[i];
+            for (int jj = i + 1; jj < mi; jj++) e = e - cmul(H[i * m + jj], eta[jj]);
+            eta[i] = cdiv(e, H[i * m + i]);
+        }
+    }
+    __syncwarp();
+    const long off = (long)task * t.NE;
+    for (int e = lane; e < t.NE; e += 32) {
+        float2 a = w.x[off + e];
+        for (int jj = 0; jj < mi; jj++) a = cfma(from_d<float2>(eta[jj]), w.V[(long)jj * w.vec + off + e], a);
+        w.x[off + e] = a;
+    }
+}
+
+// x_B += e  (src/sap.cpp:106-113)
+__global__ void tcs_scatter_kernel(TaskGeom t, TcSapWork w, const int* __restrict__ blocks, float2* __restrict__ xg) {
+    const int task = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (task >= t.NB * t.R) return;
+    if (!w.act[task] || w.normb[task] == 0.0) return;
+    const int kb = task / t.R, r = task - kb * t.R;
+    const int blk = blocks[kb];
+    const float2* xv = w.x + (long)task * t.NE;
+    for (int e = lane; e < t.NE; e += 32) {
+        float2* o = xg + (long)r * t.size + level_index(t, blk, e);
+        *o = *o + xv[e];
+    }
+}
+
+void launch_sap_sweep_tc(cudaStream_t s, const Geom& g, const TcSapWork& w, const float2* r, float2* x,
+                         const SapArgs& a, int nrhs) {
+    if (a.m > kSapMaxM) throw ParamFailure{"SAP block GMRES restart length above 8 is not supported"};
+    const int S = g.sel_x * g.sel_t;
+    TaskGeom t{nrhs, a.nblocks, S, g.dof, S * g.dof, g.sel_x, g.sel_t, g.Nt, g.sap_t, g.size()};
+    const int tasks = a.nblocks * nrhs;
+    const int tgrid = ceil_div(tasks, 8);
+    const int rg = pick_rg(nrhs, g.sel_t);
+    auto apply = [&](const float2* src, const float2* bsub, const int* flag, int invert) {
+        const CUtensorMap vmap = vector_map(src, g.dof, S, (long)a.nblocks * nrhs, rg);
+        ApplyArgs aa{w.tiles, w.w, bsub, flag, invert, a.blocks, nrhs, S, g.sel_x, g.sel_t, g.Nt, g.sap_t,
+                     g.dof, (2 * g.dof + 7) / 8, (float)a.m0 + 2.f, w.status};
+        switch (rg) {
+            case 16: launch_apply_rg<16>(s, vmap, aa, a.nblocks); break;
+            case 32: launch_apply_rg<32>(s, vmap, aa, a.nblocks); break;
+            default: launch_apply_rg<64>(s, vmap, aa, a.nblocks); break;
+        }
+    };
+    auto arnoldi = [&](int j) {
+        const int epl = (t.NE + 31) / 32;
+        if (epl <= 8) DDAMG_LAUNCH(tcs_arnoldi_kernel<8>, tgrid, 256, 0, s, t, w, j, a.m, a.tol);
+        else if (epl <= 16) DDAMG_LAUNCH(tcs_arnoldi_kernel<16>, tgrid, 256, 0, s, t, w, j, a.m, a.tol);
+        else DDAMG_LAUNCH(tcs_arnoldi_kernel<32>, tgrid, 256, 0, s, t, w, j, a.m, a.tol);
+    };
+    DDAMG_LAUNCH(tcs_gather_kernel, tgrid, 256, 0, s, t, w, a.blocks, r, a.done);
+    apply(w.x, w.b, w.act, 0);  // r = b - D_B x0 with x0 = b
+    DDAMG_LAUNCH(tcs_prep_kernel, tgrid, 256, 0, s, t, w, 1, a.m, a.tol);
+    for (int k = 0; k < a.restarts; k++) {
+        for (int j = 0; j < a.m; j++) {
+            apply(w.V + (long)j * w.vec, nullptr, w.arn, 0);  // w = D_B V_j
+            arnoldi(j);
+        }
+        DDAMG_LAUNCH(tcs_update_kernel, tgrid, 256, 0, s, t, w, a.m);
+        apply(w.x, w.b, w.fin, 1);  // r = b - D_B x for every rhs not yet converged
+        DDAMG_LAUNCH(tcs_prep_kernel, tgrid, 256, 0, s, t, w, 0, a.m, a.tol);
+    }
+    DDAMG_LAUNCH(tcs_scatter_kernel, tgrid, 256, 0, s, t, w, a.blocks, x);
+}
+
+}  // namespace ddamg

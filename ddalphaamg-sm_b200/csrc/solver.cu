@@ -48,7 +48,10 @@ struct LevelData {
     int* done = nullptr;    // W flags
     double* vv = nullptr;   // W norms
     double* rr = nullptr;   // W norms
+    bool tc = false;        // batched FP32 SAP sweeps of this level use the tensor-core block operator
+    TcSapWork tcw;
 };
+constexpr int kTcMinRhs = 8;  // fewer right-hand sides leave too little link reuse for the tensor cores
 template <typename V> LevelBufs<V>& B(LevelData& L);
 template <> LevelBufs<double2>& B<double2>(LevelData& L) { return L.d; }
 template <> LevelBufs<float2>& B<float2>(LevelData& L) { return L.f; }
@@ -291,6 +294,29 @@ static void allocate(ddamg_handle* h) {
             D.nblack = (int)black.size();
             sync(h);
         }
+        if (D.fp32 && l >= 1 && l < L - 1 && p.tensor_cores && W >= kTcMinRhs && tc_sap_supported(g)) {
+            TcSapWork& T = D.tcw;
+            const int m = p.sap_gmres_restart_length;
+            const long tasks = (long)std::max(D.nred, D.nblack) * W;
+            T.vec = tasks * g.sel_x * g.sel_t * g.dof;
+            T.b = dalloc_t<float2>(h, T.vec);
+            T.x = dalloc_t<float2>(h, T.vec);
+            T.w = dalloc_t<float2>(h, T.vec);
+            T.V = dalloc_t<float2>(h, (size_t)(m + 1) * T.vec);
+            T.act = dalloc_t<int>(h, tasks);
+            T.fin = dalloc_t<int>(h, tasks);
+            T.arn = dalloc_t<int>(h, tasks);
+            T.maxit = dalloc_t<int>(h, tasks);
+            T.normb = dalloc_t<double>(h, tasks);
+            T.err = dalloc_t<double>(h, tasks);
+            T.H = dalloc_t<double2>(h, (size_t)(m + 1) * m * tasks);
+            T.gm = dalloc_t<double2>(h, (size_t)(m + 1) * tasks);
+            T.cn = dalloc_t<double2>(h, (size_t)m * tasks);
+            T.sn = dalloc_t<double2>(h, (size_t)m * tasks);
+            T.tiles = dalloc_t<float>(h, (size_t)g.sites * 5 * kTcTileFloats);
+            T.status = dalloc_t<int>(h, 1);
+            D.tc = true;
+        }
     }
     // outer FGMRES, all right-hand sides of one call in lockstep
     const long n0 = h->lv[0].g.size();
@@ -375,6 +401,9 @@ static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, b
             {
                 ProfScope ps(h, 0, l);
                 if (l == 0) launch_sap_sweep_fine<V>(h->s, g, B<V>(D).U, r, x, a, nrhs);
+                else if (std::is_same<V, float2>::value && D.tc && nrhs >= kTcMinRhs)
+                    launch_sap_sweep_tc(h->s, g, D.tcw, reinterpret_cast<const float2*>(r),
+                                        reinterpret_cast<float2*>(x), a, nrhs);
                 else launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs);
             }
             // the residual after the last black sweep only feeds the convergence test
@@ -439,6 +468,18 @@ static void check_coarse_status(ddamg_handle* h, int* iters) {
     for (int k = 0; k < K; k++)
         if (st[2 * k] != 0) throw TimeoutFailure();
     if (iters) *iters = st[1];
+}
+
+// the tensor-core sweeps record a bounded wait that gave up in a status word per level
+static void check_tc_status(ddamg_handle* h) {
+    for (int l = 0; l < h->L; l++) {
+        LevelData& D = h->lv[l];
+        if (!D.tc) continue;
+        int st = 0;
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(&st, D.tcw.status, sizeof(int), cudaMemcpyDeviceToHost, h->s));
+        sync(h);
+        if (st != 0) throw TimeoutFailure();
+    }
 }
 
 // ------------------------------------------------------------------ FGMRES (host driven)
@@ -705,6 +746,7 @@ static void make_fp32_copies(ddamg_handle* h) {
         if (!D.fp32) continue;
         if (l == 0) launch_convert<double2, float2>(h->s, D.d.U, D.f.U, 2L * D.g.sites);
         else launch_convert<double2, float2>(h->s, D.d.links, D.f.links, (long)D.g.sites * 5 * D.g.dof * D.g.dof);
+        if (D.tc) launch_pack_tc_links(h->s, D.g, D.f.links, D.tcw.tiles);
         if (l < h->L - 1) launch_convert<double2, float2>(h->s, D.d.tv, D.f.tv, (long)D.g.ntest * D.g.size());
     }
 }
@@ -782,6 +824,7 @@ static ddamg_status solve_device(ddamg_handle* h, const double2* b, double2* x, 
     std::vector<double> rel(nrhs);
     fgmres_host<double2>(h, n, nrhs, p.fgmres_restart_length, p.fgmres_restarts, p.fgmres_tolerance, A, &M, b,
                          nullptr, true, x, K, it.data(), rel.data());
+    check_tc_status(h);
     DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, h->s));
     sync(h);
     float ms = 0;
@@ -867,6 +910,7 @@ ddamg_status ddamg_params_default(ddamg_params* p) {
     p->precision = DDAMG_PREC_DOUBLE;
     p->max_rhs = 1;
     p->device = 0;
+    p->tensor_cores = 1;
     return DDAMG_OK;
 }
 
@@ -1131,6 +1175,32 @@ ddamg_status ddamg_sap(ddamg_t* h, int level, const double* v, double* x, int nu
     API_END
 }
 
+ddamg_status ddamg_sap_batched(ddamg_t* h, int level, const double* v, double* x, int nrhs, int nu, double tol) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    need_level(h, level, false);
+    if (level == 0 && !h->gauge) throw ParamFailure{"no gauge field loaded"};
+    if (level > 0) need_setup(h);
+    if (nu < 0) throw ParamFailure{"nu must be >= 0"};
+    if (nrhs < 1 || nrhs > h->W) throw ParamFailure{"nrhs must be in [1, max(max_rhs, test vectors)]"};
+    LevelData& D = h->lv[level];
+    const long n = D.g.size() * nrhs;
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.eta, v, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.psi, x, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    if (D.fp32) {
+        launch_convert<double2, float2>(h->s, D.d.eta, D.f.eta, n);
+        launch_convert<double2, float2>(h->s, D.d.psi, D.f.psi, n);
+        sap_t<float2>(h, level, D.f.eta, D.f.psi, nu, tol, false, nrhs, false);
+        launch_convert<float2, double2>(h->s, D.f.psi, D.d.psi, n);
+    } else {
+        sap_t<double2>(h, level, D.d.eta, D.d.psi, nu, tol, false, nrhs, false);
+    }
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(x, D.d.psi, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    check_tc_status(h);
+    API_END
+}
+
 ddamg_status ddamg_setup(ddamg_t* h, uint64_t seed) {
     CHECK_HANDLE(h);
     API_BEGIN
@@ -1188,6 +1258,7 @@ ddamg_status ddamg_build_coarse_links(ddamg_t* h, int level) {
     LevelData& N = h->lv[level + 1];
     launch_build_coarse_links(h->s, D.g, D.d.U, D.d.links, D.d.tv, N.d.links);
     if (N.fp32) launch_convert<double2, float2>(h->s, N.d.links, N.f.links, (long)N.g.sites * 5 * N.g.dof * N.g.dof);
+    if (N.tc) launch_pack_tc_links(h->s, N.g, N.f.links, N.tcw.tiles);
     sync(h);
     API_END
 }

@@ -148,6 +148,13 @@ class Solver:
         check(self.L.ddamg_sap(self.h, level, _dp(v), _dp(x), nu, tol, ctypes.byref(it)))
         return x, it.value
 
+    def SAP_batched(self, level, v, nrhs, x0=None, nu=2, tol=1e-10):
+        """SAP on nrhs vectors stored back to back, in the level's working precision."""
+        v = _c(v)
+        x = np.zeros(v.size, dtype=np.complex128) if x0 is None else np.array(x0, dtype=np.complex128)
+        check(self.L.ddamg_sap_batched(self.h, level, _dp(v), _dp(x), nrhs, nu, tol))
+        return x
+
     # ------------------------------------------------------------ setup
     def setup_random_count(self):
         n = ctypes.c_int64(0)

@@ -25,7 +25,7 @@ class Params(ctypes.Structure):
         ("kcycle_tolerance", ctypes.c_double), ("fgmres_restart_length", ctypes.c_int),
         ("fgmres_restarts", ctypes.c_int), ("fgmres_tolerance", ctypes.c_double),
         ("smoother_tolerance", ctypes.c_double), ("cycle", ctypes.c_int), ("precision", ctypes.c_int),
-        ("max_rhs", ctypes.c_int), ("device", ctypes.c_int),
+        ("max_rhs", ctypes.c_int), ("device", ctypes.c_int), ("tensor_cores", ctypes.c_int),
     ]
 
 
@@ -60,6 +60,7 @@ SIGNATURES = {
     "ddamg_restrict": (_st, [_h, _i, _dp, _dp]),
     "ddamg_prolong": (_st, [_h, _i, _dp, _dp]),
     "ddamg_sap": (_st, [_h, _i, _dp, _dp, _i, ctypes.c_double, ctypes.POINTER(_i)]),
+    "ddamg_sap_batched": (_st, [_h, _i, _dp, _dp, _i, _i, ctypes.c_double]),
     "ddamg_setup": (_st, [_h, ctypes.c_uint64]),
     "ddamg_setup_with_vectors": (_st, [_h, _dp, ctypes.c_int64]),
     "ddamg_setup_random_count": (_st, [_h, ctypes.POINTER(ctypes.c_int64)]),

@@ -72,6 +72,10 @@ typedef struct {
     int precision;                    /* ddamg_precision; the reference is FP64 only */
     int max_rhs;                      /* right-hand sides one ddamg_solve call may carry (>= 1) */
     int device;                       /* CUDA device ordinal */
+    /* 1 (default): in mixed precision, coarse-level SAP sweeps over >= 8 right-hand sides run
+     * the block operator on tcgen05 tensor cores (TF32 inputs, FP32 accumulation); 0: CUDA
+     * cores only.  No reference counterpart. */
+    int tensor_cores;
 } ddamg_params;
 
 typedef struct {
@@ -130,6 +134,11 @@ ddamg_status ddamg_prolong(ddamg_t* h, int level, const double* in, double* out)
 /* SAP_C::SAP (src/sap.cpp:81-165) at level l: x is the initial guess on entry and the
  * result on exit; *iters gets SAP's return value */
 ddamg_status ddamg_sap(ddamg_t* h, int level, const double* v, double* x, int nu, double tol, int* iters);
+/* SAP_C::SAP (src/sap.cpp:81-165) on nrhs vectors at once ([rhs][site][dof]), in the level's
+ * working precision (FP32 in mixed precision below the coarsest level, where batches of >= 8
+ * right-hand sides of a coarse level use the tensor-core block operator); x: initial guesses in,
+ * results out.  nrhs <= max(max_rhs, test vectors of any level). */
+ddamg_status ddamg_sap_batched(ddamg_t* h, int level, const double* v, double* x, int nrhs, int nu, double tol);
 
 /* ------------------------------------------------------------------ setup */
 /* AlgebraicMG::setUpPhase (src/amg.cpp:4-62) with test vectors drawn on the device from a
