@@ -636,6 +636,217 @@ __global__ void __launch_bounds__(128) sap_fine_warp_kernel(Geom g, const V* __r
             }
 }
 
+// The same block solve with the Krylov basis in registers, for a restart length M fixed at compile
+// time: every lane keeps its own elements of V_0..V_M, so the Gram-Schmidt dots and updates and the
+// solution update touch no shared memory; only the stencil operand (whose neighbour values belong
+// to other lanes) passes through the warp's shared buffer.  Gram-Schmidt is classical: the j+1
+// dots of an Arnoldi step are reduced in one interleaved butterfly.  Dots and norms accumulate in
+// the working precision.
+template <typename V, int SPL, int M>
+__global__ void __launch_bounds__(128) sap_fine_reg_kernel(Geom g, const V* __restrict__ U, const V* __restrict__ rg,
+                                                           V* __restrict__ xg, SapKParams p, int wpc, size_t wbytes) {
+    typedef typename RealOf<V>::R R;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int task = blockIdx.x * wpc + wib;
+    if (wib >= wpc || task >= p.nblocks * p.nrhs) return;
+    const int kb = task / p.nrhs, rhs = task - kb * p.nrhs;  // block-major
+    if (p.done && p.done[rhs]) return;
+    const int et = g.sel_t, ex = g.sel_x, S = ex * et;
+    double2* H = reinterpret_cast<double2*>(smraw + wib * wbytes);  // (M+1) x M, lane 0 only
+    double2* gm = H + (M + 1) * M;
+    double2* cn = gm + (M + 1);
+    double2* sn = cn + M;
+    double2* eta = sn + M;
+    V* op = reinterpret_cast<V*>(eta + M);
+    const int blk = p.blocks[kb];
+    const int bx = blk / g.sap_t, bt = blk - bx * g.sap_t;
+    const long ro = (long)rhs * g.size();
+    const R mm = R(p.m0) + R(2), half = R(0.5);
+
+    bool sv[SPL];
+    int sk[SPL], sn_[SPL];
+    V u0[SPL], u1[SPL], ul0[SPL], ul1[SPL];
+    V b[SPL][2], x[SPL][2], w[SPL][2];
+    V Vb[M + 1][SPL][2];
+#pragma unroll
+    for (int q = 0; q < SPL; q++) {
+        const int k = lane + 32 * q;
+        sv[q] = k < S;
+        const int kk = sv[q] ? k : 0;
+        const int kx = kk / et, kt = kk - kx * et;
+        const int n = (bx * ex + kx) * g.Nt + bt * et + kt;
+        sk[q] = kk;
+        sn_[q] = n;
+        u0[q] = sv[q] ? __ldg(U + 2 * n) : czero<V>();
+        u1[q] = sv[q] ? __ldg(U + 2 * n + 1) : czero<V>();
+        ul0[q] = (sv[q] && kt > 0) ? conjc(__ldg(U + 2 * (n - 1))) : czero<V>();
+        ul1[q] = (sv[q] && kx > 0) ? conjc(__ldg(U + 2 * (n - g.Nt) + 1)) : czero<V>();
+#pragma unroll
+        for (int a = 0; a < 2; a++) {
+            b[q][a] = sv[q] ? rg[ro + (long)n * 2 + a] : czero<V>();
+            x[q][a] = b[q][a];
+        }
+    }
+    // w = D_B v: v goes to the shared operand buffer, the stencil reads the neighbours from it
+    auto apply = [&](const V (&v)[SPL][2]) {
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < SPL; q++)
+            if (sv[q]) {
+                op[2 * sk[q]] = v[q][0];
+                op[2 * sk[q] + 1] = v[q][1];
+            }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < SPL; q++) {
+            if (!sv[q]) {
+                w[q][0] = w[q][1] = czero<V>();
+                continue;
+            }
+            const int k = sk[q], kx = k / et, kt = k - kx * et;
+            V a = czero<V>(), c = czero<V>(), e = czero<V>(), gg = czero<V>();
+            if (kt + 1 < et) a = cmul(u0[q], op[2 * (k + 1)] - op[2 * (k + 1) + 1]);          // +t: (1 - sigma_x)
+            if (kx + 1 < ex) c = cmul(u1[q], op[2 * (k + et)] + imul(op[2 * (k + et) + 1]));  // +x: (1 - sigma_y)
+            if (kt > 0) e = cmul(ul0[q], op[2 * (k - 1)] + op[2 * (k - 1) + 1]);              // -t: (1 + sigma_x)
+            if (kx > 0) gg = cmul(ul1[q], op[2 * (k - et)] - imul(op[2 * (k - et) + 1]));      // -x: (1 + sigma_y)
+            w[q][0] = mm * v[q][0] - half * (a + c + e + gg);
+            w[q][1] = mm * v[q][1] - half * (imul(gg) - imul(c) + e - a);
+        }
+    };
+    auto nrm2 = [&](const V (&v)[SPL][2]) {
+        R s = R(0);
+#pragma unroll
+        for (int q = 0; q < SPL; q++)
+            if (sv[q]) s += cnorm2(v[q][0]) + cnorm2(v[q][1]);
+        return (double)warp_sum(s);
+    };
+
+    apply(x);
+#pragma unroll
+    for (int q = 0; q < SPL; q++)
+#pragma unroll
+        for (int a = 0; a < 2; a++) w[q][a] = b[q][a] - w[q][a];
+    const double norm_b = sqrt(nrm2(b));
+    double err = sqrt(nrm2(w));
+    // a zero block right-hand side has the zero solution (the reference would divide by zero)
+    if (norm_b == 0.0) return;
+    int maxIt = M;
+    for (int k = 0; k < p.restarts; k++) {
+        const R inv = R(1.0 / err);
+#pragma unroll
+        for (int q = 0; q < SPL; q++)
+#pragma unroll
+            for (int a = 0; a < 2; a++) Vb[0][q][a] = inv * w[q][a];
+        if (lane == 0) gm[0] = make_double2(err, 0.0);
+#pragma unroll
+        for (int j = 0; j < M; j++) {
+            apply(Vb[j]);
+            V h[M];
+#pragma unroll
+            for (int i = 0; i <= j; i++) {
+                V t = czero<V>();
+#pragma unroll
+                for (int q = 0; q < SPL; q++)
+                    if (sv[q])
+#pragma unroll
+                        for (int a = 0; a < 2; a++) t = cfmac(Vb[i][q][a], w[q][a], t);
+                h[i] = t;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int i = 0; i <= j; i++) {
+                    h[i].x += __shfl_xor_sync(0xffffffffu, h[i].x, o);
+                    h[i].y += __shfl_xor_sync(0xffffffffu, h[i].y, o);
+                }
+#pragma unroll
+            for (int i = 0; i <= j; i++)
+#pragma unroll
+                for (int q = 0; q < SPL; q++)
+#pragma unroll
+                    for (int a = 0; a < 2; a++) w[q][a] = w[q][a] - cmul(h[i], Vb[i][q][a]);
+            const double hn = sqrt(nrm2(w));
+            if (hn > 0) {
+                const R ih = R(1.0 / hn);
+#pragma unroll
+                for (int q = 0; q < SPL; q++)
+#pragma unroll
+                    for (int a = 0; a < 2; a++) Vb[j + 1][q][a] = ih * w[q][a];
+            }
+            int brk = 0;
+            if (lane == 0) {
+#pragma unroll
+                for (int i = 0; i <= j; i++) H[i * M + j] = to_d(h[i]);
+                H[(j + 1) * M + j] = make_double2(hn, 0.0);
+                for (int i = 0; i < j; i++) {  // FGMRES::rotation (src/fgmres.cpp:99-115)
+                    const double2 hij = H[i * M + j], hi1 = H[(i + 1) * M + j];
+                    const double2 tmp = cmulc(cn[i], hij) + cmulc(sn[i], hi1);
+                    H[(i + 1) * M + j] = cmul(cn[i], hi1) - cmul(sn[i], hij);
+                    H[i * M + j] = tmp;
+                }
+                const double2 hjj = H[j * M + j], hj1 = H[(j + 1) * M + j];
+                const double den = sqrt(cnorm2(hjj) + cnorm2(hj1));
+                sn[j] = make_double2(hj1.x / den, hj1.y / den);
+                cn[j] = make_double2(hjj.x / den, hjj.y / den);
+                H[j * M + j] = cmulc(cn[j], hjj) + cmulc(sn[j], hj1);
+                H[(j + 1) * M + j] = make_double2(0.0, 0.0);
+                gm[j + 1] = -cmul(sn[j], gm[j]);
+                gm[j] = cmulc(cn[j], gm[j]);
+                brk = (sqrt(cnorm2(gm[j + 1])) < p.tol * norm_b) ? 1 : 0;
+            }
+            brk = __shfl_sync(0xffffffffu, brk, 0);
+            if (brk) {
+                maxIt = j + 1;  // not reset at the next restart (src/fgmres.cpp:14,56)
+                break;
+            }
+        }
+        if (lane == 0) {  // solve_upper_triangular (src/fgmres.cpp:118-128)
+            for (int i = maxIt - 1; i >= 0; i--) {
+                double2 e = gm[i];
+                for (int jj = i + 1; jj < maxIt; jj++) e = e - cmul(H[i * M + jj], eta[jj]);
+                eta[i] = cdiv(e, H[i * M + i]);
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int jj = 0; jj < M; jj++) {
+            if (jj >= maxIt) break;
+            const V ej = from_d<V>(eta[jj]);
+#pragma unroll
+            for (int q = 0; q < SPL; q++)
+#pragma unroll
+                for (int a = 0; a < 2; a++) x[q][a] = cfma(ej, Vb[jj][q][a], x[q][a]);
+        }
+        apply(x);
+#pragma unroll
+        for (int q = 0; q < SPL; q++)
+#pragma unroll
+            for (int a = 0; a < 2; a++) w[q][a] = b[q][a] - w[q][a];
+        err = sqrt(nrm2(w));
+        if (err < p.tol * norm_b) break;
+    }
+    // x_B += e  (src/sap.cpp:106-113)
+#pragma unroll
+    for (int q = 0; q < SPL; q++)
+        if (sv[q])
+#pragma unroll
+            for (int a = 0; a < 2; a++) {
+                V* o = xg + ro + (long)sn_[q] * 2 + a;
+                *o = *o + x[q][a];
+            }
+}
+
+template <typename V, int SPL, int M>
+static void launch_fine_reg(cudaStream_t s, const Geom& g, const V* U, const V* r, V* x, SapKParams p) {
+    const int S = g.sel_x * g.sel_t;
+    const size_t wb = (sizeof(double2) * ((M + 1) * M + (M + 1) + 3 * M) + sizeof(V) * 2 * S + 15) / 16 * 16;
+    const int wpc = 4;
+    const int tasks = p.nblocks * p.nrhs;
+    DDAMG_LAUNCH((sap_fine_reg_kernel<V, SPL, M>), ceil_div(tasks, wpc), 32 * wpc, wb * wpc, s, g, U, r, x, p, wpc,
+                 wb);
+}
+
 template <typename V, int SPL>
 static void launch_fine_warp(cudaStream_t s, const Geom& g, const V* U, const V* r, V* x, SapKParams p) {
     const int S = g.sel_x * g.sel_t;
@@ -714,7 +925,9 @@ void launch_sap_sweep_fine(cudaStream_t s, const Geom& g, const V* U, const V* r
     const int S = g.sel_x * g.sel_t;
     if (a.m > kSapMaxM) throw ParamFailure{"SAP block GMRES restart length above 8 is not supported"};
     SapKParams p{a.m, a.restarts, a.tol, a.m0, a.blocks, a.nblocks, a.done, nrhs, 1};
-    if (S <= 32) launch_fine_warp<V, 1>(s, g, U, r, x, p);
+    if (a.m == 5 && S <= 32) launch_fine_reg<V, 1, 5>(s, g, U, r, x, p);
+    else if (a.m == 5 && S <= 64) launch_fine_reg<V, 2, 5>(s, g, U, r, x, p);
+    else if (S <= 32) launch_fine_warp<V, 1>(s, g, U, r, x, p);
     else if (S <= 64) launch_fine_warp<V, 2>(s, g, U, r, x, p);
     else if (S <= 128) launch_fine_warp<V, 4>(s, g, U, r, x, p);
     else if (S <= 256) launch_fine_warp<V, 8>(s, g, U, r, x, p);
