@@ -118,8 +118,15 @@ constexpr int kTcTileFloats = 64 * 64;
 // and a block-vector window that fits in shared memory)
 bool tc_sap_supported(const Geom& g);
 void launch_pack_tc_links(cudaStream_t s, const Geom& g, const float2* links, float* tiles);
+// shape: index of the apply kernel's tile shape (from tune_sap_tc; out of range: a default)
 void launch_sap_sweep_tc(cudaStream_t s, const Geom& g, const TcSapWork& w, const float2* r, float2* x,
-                         const SapArgs& a, int nrhs);
+                         const SapArgs& a, int nrhs, int shape);
+// autotuner: times each admissible tile shape on the sweep's data and returns the fastest;
+// us[tc_sweep_shapes()] receives the times (negative: not admissible)
+int tune_sap_tc(cudaStream_t s, const Geom& g, const TcSapWork& w, const float2* r, const SapArgs& a, int nrhs,
+                double* us);
+int tc_sweep_shapes();
+void tc_sweep_shape(int idx, int* rg, int* stages, int* chains);
 
 // ------------------------------------------------------------ coarsest GMRES (kernels_gmres.cu)
 struct CoarseGmresWork {

@@ -19,8 +19,9 @@
 //                           block vectors, with the same per-rhs control flow (break point maxIt,
 //                           convergence freeze) as the on-chip solver in kernels_sap.cu.
 //
-// Warp roles of the apply kernel: warps 0-3 epilogue (warp q reads tensor-memory lanes
-// 32q..32q+31), warp 4 lane 0 issues the copies, warp 5 lane 0 the MMAs.  Every mbarrier wait is
+// Warp roles of the apply kernel: EW = 8 or 16 epilogue warps (warp w reads tensor-memory lanes
+// 32 (w % 4) .. +31 and a quarter of the columns), then one warp whose lane 0 issues the copies
+// and one whose lane 0 issues the MMAs.  Every mbarrier wait is
 // bounded; a wait that gives up sets the status word and the CTA winds down.
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -33,23 +34,36 @@ namespace ddamg {
 using namespace tc;
 
 namespace {
-constexpr int kNA = 3;  // link-tile ring depth
-constexpr int kEpiWarps = 4;
-constexpr int kProdWarp = 4, kMmaWarp = 5;
-constexpr int kApplyThreads = 6 * 32;
+// epilogue warps (16 for groups of >= 32 right-hand sides, else 8), plus one copy warp and one MMA
+// warp
+__host__ __device__ constexpr int epi_warps(int RG) { return RG >= 32 ? 16 : 8; }
+__host__ __device__ constexpr int apply_threads(int RG) { return (epi_warps(RG) + 2) * 32; }
 constexpr uint32_t kTileBytes = kTcTileFloats * 4;  // 64 rows x 64 fp32
 
+constexpr int kMaxBlockSites = 256;  // sites per Schwarz block the apply kernel's tables hold
 __host__ __device__ inline int release_lag(int sel_t) { return sel_t > 2 ? sel_t : 2; }
 __host__ __device__ inline int window_slots(int sel_t) { return sel_t + release_lag(sel_t) + 2; }
-inline size_t apply_smem(int RG, int sel_t) {
+inline size_t apply_smem(int RG, int NA, int sel_t) {
     const int nw = window_slots(sel_t);
-    return 1024 + (size_t)kNA * kTileBytes + (size_t)nw * 256 * RG + sizeof(uint64_t) * (2 * kNA + 2 * nw + 5);
+    return 1024 + (size_t)NA * kTileBytes + (size_t)nw * 256 * RG + sizeof(uint64_t) * (2 * NA + 2 * nw + 5);
 }
-inline int pick_rg(int nrhs, int sel_t) {
-    int rg = 16;
-    while (rg < 64 && rg < nrhs) rg *= 2;
-    while (rg > 16 && apply_smem(rg, sel_t) > 227 * 1024) rg /= 2;
-    return rg;
+// tile shapes of the apply kernel the autotuner chooses from: right-hand sides per CTA and depth of
+// the link-tile ring
+struct TcShape {
+    int rg, na, nch;  // right-hand sides per CTA, link-tile ring depth, accumulator chains per site
+};
+constexpr TcShape kShapes[] = {{64, 3, 1}, {64, 3, 2}, {64, 3, 4}, {32, 8, 2}, {32, 8, 4}, {16, 8, 4}};
+constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+// dynamic shared memory plus the kernel's static tables (under 5 KB) within the 227 KB per CTA
+inline bool shape_fits(int idx, int sel_t) {
+    return apply_smem(kShapes[idx].rg, kShapes[idx].na, sel_t) + 5 * 1024 <= 227 * 1024 &&
+           2 * kShapes[idx].nch * kShapes[idx].rg <= 512;
+}
+// without a tuning result: the widest shape that fits, its width rounded up from the batch
+inline int default_shape(int nrhs, int sel_t) {
+    for (int i = 0; i < kNumShapes; i++)
+        if (shape_fits(i, sel_t) && (kShapes[i].rg / 2 < nrhs || kShapes[i].rg == 16)) return i;
+    return kNumShapes - 1;
 }
 
 struct ApplyArgs {
@@ -68,7 +82,8 @@ struct ApplyArgs {
 
 bool tc_sap_supported(const Geom& g) {
     const int S = g.sel_x * g.sel_t;
-    return g.level >= 1 && g.dof <= 32 && S * g.dof <= 1024 && apply_smem(16, g.sel_t) <= 227 * 1024;
+    return g.level >= 1 && g.dof <= 32 && S * g.dof <= 1024 && S <= kMaxBlockSites &&
+           apply_smem(16, 4, g.sel_t) + 5 * 1024 <= 227 * 1024;
 }
 
 // Operator tile (n, d): the real 2dof x 2dof embedding of T = -s_d M_d, M_d the coarse link of hop
@@ -103,17 +118,34 @@ void launch_pack_tc_links(cudaStream_t s, const Geom& g, const float2* links, fl
     DDAMG_LAUNCH(pack_tc_links_kernel, (long)g.sites * 5, 256, 0, s, links, tiles, g.Nt, g.dof);
 }
 
+// slow path of a barrier wait (kept out of line so the hot loops stay short): bounded, sets *abort
+__device__ __noinline__ bool wait_slow(uint64_t* bar, uint32_t parity, int* status, volatile int* abort) {
+    if (*abort) return false;
+    if (mbar_wait(bar, parity, status)) return true;
+    *abort = 1;
+    return false;
+}
+
 // w = D_B src (or bsub - D_B src) for one block and RG right-hand sides.  src enters through the
 // tensor map vmap: dims (2 dof floats, S sites, NB*R block-rhs rows), box (32, 1, RG), 128B swizzle,
 // so a box lands as RG rows of 32 fp32 -- one K-major 128B-swizzled operand block.
-template <int RG>
-__global__ void __launch_bounds__(kApplyThreads, 1)
+// Warps 0 .. EW-1 run the epilogue, warp EW issues the copies, warp EW+1 the MMAs (one thread
+// each); the control loops use tables built once per CTA (no divisions) and descriptor arithmetic
+// by addition, since a single thread's instruction latency is what bounds them.
+template <int RG, int NA, int NCH>
+__global__ void __launch_bounds__(apply_threads(RG), 1)
     tc_block_apply_kernel(const __grid_constant__ CUtensorMap vmap, ApplyArgs a) {
+    constexpr int EW = epi_warps(RG);
+    constexpr int CW = 4 * RG / EW;  // accumulator columns per epilogue warp: 16 or 8
+    constexpr uint32_t kBBytes = RG * 256;  // two 128-byte column blocks of RG rows
     extern __shared__ unsigned char smraw[];
     __shared__ int s_any;
     __shared__ volatile int s_abort;
     __shared__ uint32_t s_taddr;
-    constexpr uint32_t kBBytes = RG * 256;  // two 128-byte column blocks of RG rows
+    __shared__ short s_nb[kMaxBlockSites][5];         // neighbour site in the block, -1 outside
+    __shared__ int s_gsite[kMaxBlockSites];           // lattice site
+    __shared__ unsigned char s_slot[kMaxBlockSites];  // window slot of a site's vector tile
+    __shared__ unsigned char s_par[kMaxBlockSites];   // fill parity of that slot
     unsigned char* sm =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
     const int kb = blockIdx.x, r0 = blockIdx.y * RG;
@@ -132,17 +164,17 @@ __global__ void __launch_bounds__(kApplyThreads, 1)
     if (!s_any) return;
 
     unsigned char* Abuf = sm;
-    unsigned char* Bbuf = sm + kNA * kTileBytes;
+    unsigned char* Bbuf = sm + NA * kTileBytes;
     uint64_t* bar = reinterpret_cast<uint64_t*>(Bbuf + (size_t)NW * kBBytes);
     uint64_t* fullA = bar;
-    uint64_t* emptyA = bar + kNA;
-    uint64_t* fullB = bar + 2 * kNA;
+    uint64_t* emptyA = bar + NA;
+    uint64_t* fullB = bar + 2 * NA;
     uint64_t* emptyB = fullB + NW;
     uint64_t* accF = emptyB + NW;
     uint64_t* accE = accF + 2;
     uint64_t* drain = accE + 2;
     if (threadIdx.x == 0) {
-        for (int i = 0; i < kNA; i++) {
+        for (int i = 0; i < NA; i++) {
             mbar_init(&fullA[i], 1);
             mbar_init(&emptyA[i], 1);
         }
@@ -152,69 +184,69 @@ __global__ void __launch_bounds__(kApplyThreads, 1)
         }
         for (int i = 0; i < 2; i++) {
             mbar_init(&accF[i], 1);
-            mbar_init(&accE[i], kEpiWarps * 32);
+            mbar_init(&accE[i], EW);
         }
         mbar_init(drain, 1);
         mbar_fence_init();
     }
+    {
+        const int blk = a.blocks[kb];
+        const int bx = blk / a.sap_t, bt = blk - bx * a.sap_t;
+        for (int s = threadIdx.x; s < S; s += blockDim.x) {
+            const int kx = s / a.sel_t, kt = s - kx * a.sel_t;
+            s_nb[s][0] = (short)s;
+            s_nb[s][1] = (short)(kt + 1 < a.sel_t ? s + 1 : -1);
+            s_nb[s][2] = (short)(kx + 1 < a.sel_x ? s + a.sel_t : -1);
+            s_nb[s][3] = (short)(kt > 0 ? s - 1 : -1);
+            s_nb[s][4] = (short)(kx > 0 ? s - a.sel_t : -1);
+            s_gsite[s] = (bx * a.sel_x + kx) * a.Nt + bt * a.sel_t + kt;
+            s_slot[s] = (unsigned char)(s % NW);
+            s_par[s] = (unsigned char)((s / NW) & 1);
+        }
+    }
     if (warp == 0) {
-        tmem_alloc(&s_taddr, 2 * RG);
+        tmem_alloc(&s_taddr, 2 * NCH * RG);
         tmem_relinquish();
     }
     __syncthreads();
     tc_fence_after();
     const uint32_t taddr = s_taddr;
-
-    const int blk = a.blocks[kb];
-    const int bx = blk / a.sap_t, bt = blk - bx * a.sap_t;
-    auto nbr = [&](int s, int d) -> int {
-        const int kx = s / a.sel_t, kt = s - kx * a.sel_t;
-        if (d == 0) return s;
-        if (d == 1) return kt + 1 < a.sel_t ? s + 1 : -1;
-        if (d == 2) return kx + 1 < a.sel_x ? s + a.sel_t : -1;
-        if (d == 3) return kt > 0 ? s - 1 : -1;
-        return kx > 0 ? s - a.sel_t : -1;
-    };
-    auto gsite = [&](int s) -> long {
-        const int kx = s / a.sel_t, kt = s - kx * a.sel_t;
-        return (long)(bx * a.sel_x + kx) * a.Nt + bt * a.sel_t + kt;
-    };
     auto wait = [&](uint64_t* b, uint32_t parity) -> bool {
-        if (s_abort) return false;
-        if (mbar_wait(b, parity, a.status)) return true;
-        s_abort = 1;
-        return false;
+        return mbar_try_wait(b, parity) || wait_slow(b, parity, a.status, &s_abort);
     };
 
-    if (warp == kProdWarp) {
+    if (warp == EW) {
         // ---------------- producer (one thread): vector tiles by TMA, link tiles by bulk copy
         if (lane == 0) {
-            int a_idx = 0, t_next = 0;
+            int stage = 0, lap = 0, a_issued = 0, t_next = 0;
             bool ok = true;
             for (int s = 0; s < S && ok; s++) {
                 const int tmax = min(S - 1, s + a.sel_t + 1);
                 for (; t_next <= tmax; t_next++) {
-                    const int slot = t_next % NW, k = t_next / NW;
-                    if (k > 0 && !(ok = wait(&emptyB[slot], (k - 1) & 1))) break;
+                    const int slot = s_slot[t_next];
+                    if (t_next >= NW && !(ok = wait(&emptyB[slot], s_par[t_next] ^ 1u))) break;
                     unsigned char* tb = Bbuf + (size_t)slot * kBBytes;
                     mbar_arrive_expect_tx(&fullB[slot], (uint32_t)katoms * RG * 128);
                     for (int at = 0; at < katoms; at++)
                         tma_load_3d(tb + at * RG * 128, &vmap, 32 * at, t_next, kb * a.R + r0, &fullB[slot]);
                 }
                 if (!ok) break;
+                const float* tsite = a.tiles + (long)s_gsite[s] * 5 * kTcTileFloats;
                 for (int d = 0; d < 5; d++) {
-                    if (nbr(s, d) < 0) continue;
-                    const int stage = a_idx % kNA, k = a_idx / kNA;
-                    if (k > 0 && !(ok = wait(&emptyA[stage], (k - 1) & 1))) break;
+                    if (s_nb[s][d] < 0) continue;
+                    if (lap > 0 && !(ok = wait(&emptyA[stage], (uint32_t)(lap - 1) & 1u))) break;
                     mbar_arrive_expect_tx(&fullA[stage], kTileBytes);
-                    bulk_g2s(Abuf + (size_t)stage * kTileBytes, a.tiles + (gsite(s) * 5 + d) * kTcTileFloats,
-                             kTileBytes, &fullA[stage]);
-                    a_idx++;
+                    bulk_g2s(Abuf + (size_t)stage * kTileBytes, tsite + d * kTcTileFloats, kTileBytes, &fullA[stage]);
+                    a_issued++;
+                    if (++stage == NA) {
+                        stage = 0;
+                        lap++;
+                    }
                 }
             }
             // every copy issued has landed before the CTA may exit
-            for (int st = 0; st < kNA; st++) {
-                const int issued = a_idx > st ? (a_idx - 1 - st) / kNA + 1 : 0;
+            for (int st = 0; st < NA; st++) {
+                const int issued = a_issued > st ? (a_issued - 1 - st) / NA + 1 : 0;
                 if (issued > 0) mbar_wait(&fullA[st], (issued - 1) & 1, a.status);
             }
             for (int sl = 0; sl < NW; sl++) {
@@ -222,87 +254,116 @@ __global__ void __launch_bounds__(kApplyThreads, 1)
                 if (issued > 0) mbar_wait(&fullB[sl], (issued - 1) & 1, a.status);
             }
         }
-    } else if (warp == kMmaWarp) {
+    } else if (warp == EW + 1) {
         // ---------------- MMA issuer (one thread)
         if (lane == 0) {
             const uint32_t idesc = idesc_tf32(64, RG);
-            int a_idx = 0;
+            const uint64_t ad0 = sdesc_k128(smem_u32(Abuf)), bd0 = sdesc_k128(smem_u32(Bbuf));
+            int stage = 0;
+            uint32_t phA = 0;
+            const int ks = a.ks;
             for (int s = 0; s < S; s++) {
                 const int b = s & 1;
-                if (s >= 2 && !wait(&accE[b], ((s >> 1) - 1) & 1)) break;
+                if (s >= 2 && !wait(&accE[b], (uint32_t)((s >> 1) - 1) & 1u)) break;
                 tc_fence_after();
-                const uint32_t dt = taddr + (uint32_t)(b * RG);
+                // K step k of every hop accumulates into chain k % NCH: consecutive MMAs are
+                // independent, so the tensor pipe overlaps them instead of serialising one chain
+                const uint32_t dt = taddr + (uint32_t)(b * NCH * RG);
                 bool first = true, ok = true;
                 for (int d = 0; d < 5; d++) {
-                    const int nb = nbr(s, d);
+                    const int nb = s_nb[s][d];
                     if (nb < 0) continue;
-                    const int stage = a_idx % kNA;
-                    if (!wait(&fullB[nb % NW], (nb / NW) & 1) || !wait(&fullA[stage], (a_idx / kNA) & 1)) {
+                    const int slot = s_slot[nb];
+                    if (!wait(&fullB[slot], s_par[nb]) || !wait(&fullA[stage], phA)) {
                         ok = false;
                         break;
                     }
-                    tc_fence_after();
-                    const uint32_t as = smem_u32(Abuf + (size_t)stage * kTileBytes);
-                    const uint32_t bs = smem_u32(Bbuf + (size_t)(nb % NW) * kBBytes);
-                    for (int k = 0; k < a.ks; k++)  // K steps of 8 fp32 = 32 bytes within a 128-byte block
-                        mma_tf32(dt, sdesc_k128(as + (k >> 2) * 8192 + (k & 3) * 32),
-                                 sdesc_k128(bs + (k >> 2) * RG * 128 + (k & 3) * 32), idesc,
-                                 (first && k == 0) ? 0u : 1u);
+                    const uint64_t ad = ad0 + (uint64_t)(stage * (kTileBytes >> 4));
+                    const uint64_t bd = bd0 + (uint64_t)(slot * (kBBytes >> 4));
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {  // K steps of 8 fp32 = 32 bytes within a 128-byte block
+                        if (k >= ks) break;
+                        mma_tf32(dt + (uint32_t)((k % NCH) * RG), ad + (uint64_t)((k >> 2) * (8192 >> 4) + (k & 3) * 2),
+                                 bd + (uint64_t)((k >> 2) * (RG * 128 >> 4) + (k & 3) * 2), idesc,
+                                 (first && k < NCH) ? 0u : 1u);
+                    }
                     first = false;
                     mma_commit(&emptyA[stage]);
-                    a_idx++;
+                    if (++stage == NA) {
+                        stage = 0;
+                        phA ^= 1u;
+                    }
                 }
                 if (!ok) break;
                 mma_commit(&accF[b]);
                 // site s is the last to read vector tile s - sel_t; the epilogue of site s - RL
                 // (which reads that site's own tile) has finished before site s could start
-                if (s >= RL) mma_commit(&emptyB[(s - RL) % NW]);
+                if (s >= RL) mma_commit(&emptyB[s_slot[s - RL]]);
             }
             mma_commit(drain);  // every MMA of this CTA has finished before TMEM is released
             mbar_wait(drain, 0, a.status);
         }
     } else {
-        // ---------------- epilogue: warp q owns accumulator rows 16q .. 16q+15 (lanes 0-15);
-        // row m = 2i + p is part p of output dof i for each right-hand side (column)
-        const int q = warp;
+        // ---------------- epilogue: warp w owns accumulator rows 16 q .. 16 q + 15 (lanes 0-15,
+        // q = w % 4) and CW columns starting at (w / 4) CW; row m = 2i + p is part p of output
+        // dof i for each right-hand side (column)
+        const int q = warp & 3;
+        const int c0 = (warp >> 2) * CW;
         const int m = 16 * q + (lane & 15);
         const bool rowok = lane < 16 && m < 2 * a.dof;
-        const float* bf = reinterpret_cast<const float*>(a.bsub);
-        float* dstf = reinterpret_cast<float*>(a.dst);
-        const uint32_t selfoff = (uint32_t)(m >> 5) * RG * 128;
+        const long ostride = (long)S * a.dof * 2;
+        // shared-memory offsets of element (row c, column m) of a vector tile, for c % 8 = 0..7
+        uint32_t soff[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+            soff[j] = (uint32_t)(m >> 5) * RG * 128 + ((uint32_t)(((m & 31) >> 2) ^ j) << 4) + ((uint32_t)(m & 3) << 2);
+        const float mm = a.mm;
+        float* __restrict__ dst0 = reinterpret_cast<float*>(a.dst) + ((long)kb * a.R + r0 + c0) * ostride + m;
+        const float* __restrict__ b0 =
+            a.bsub ? reinterpret_cast<const float*>(a.bsub) + ((long)kb * a.R + r0 + c0) * ostride + m : nullptr;
+        const int ncol = min(CW, nr - c0);  // valid columns of this warp (may be <= 0)
         for (int s = 0; s < S; s++) {
             const int b = s & 1;
-            if (!wait(&accF[b], (s >> 1) & 1)) break;
+            if (!wait(&accF[b], (uint32_t)(s >> 1) & 1u)) break;
             tc_fence_after();
-            const uint32_t tb = taddr + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * RG);
-            const unsigned char* self = Bbuf + (size_t)(s % NW) * kBBytes + selfoff;
-            const long o0 = (((long)kb * a.R + r0) * S + s) * a.dof * 2 + m;  // float index, rhs r0
-            const long ostride = (long)S * a.dof * 2;
-#pragma unroll 1
-            for (int c0 = 0; c0 < RG; c0 += 16) {
-                float acc[16], bv[16];
-                tmem_ld16(tb + c0, acc);
+            const uint32_t tb = taddr + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * NCH * RG + c0);
+            float acc[CW];
+            if constexpr (CW == 16) tmem_ld16(tb, acc);
+            else tmem_ld8(tb, acc);
 #pragma unroll
-                for (int c = 0; c < 16; c++)
-                    bv[c] = (bf && rowok && c0 + c < nr) ? bf[o0 + (c0 + c) * ostride] : 0.f;
+            for (int ch = 1; ch < NCH; ch++) {
+                if (ch >= a.ks) break;
+                float part[CW];
+                if constexpr (CW == 16) tmem_ld16(tb + ch * RG, part);
+                else tmem_ld8(tb + ch * RG, part);
 #pragma unroll
-                for (int c = 0; c < 16; c++) {
-                    if (rowok && c0 + c < nr) {
-                        const float v = *reinterpret_cast<const float*>(self + swz_off(c0 + c, m & 31));
-                        float w = a.mm * v + acc[c];
-                        if (bf) w = bv[c] - w;
-                        dstf[o0 + (c0 + c) * ostride] = w;
+                for (int c = 0; c < CW; c++) acc[c] += part[c];
+            }
+            if (rowok) {
+                const unsigned char* self = Bbuf + (size_t)s_slot[s] * kBBytes + (size_t)c0 * 128;
+                const long so = (long)s * a.dof * 2;
+                float bv[CW];
+#pragma unroll
+                for (int c = 0; c < CW; c++) bv[c] = (b0 && c < ncol) ? b0[so + c * ostride] : 0.f;
+#pragma unroll
+                for (int c = 0; c < CW; c++) {
+                    if (c < ncol) {
+                        const float v = *reinterpret_cast<const float*>(self + c * 128 + soff[c & 7]);
+                        float w = mm * v + acc[c];
+                        if (b0) w = bv[c] - w;
+                        dst0[so + c * ostride] = w;
                     }
                 }
             }
             tc_fence_before();
-            mbar_arrive(&accE[b]);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&accE[b]);
         }
     }
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        tmem_dealloc(taddr, 2 * RG);
+        tmem_dealloc(taddr, 2 * NCH * RG);
     }
 }
 
@@ -333,13 +394,23 @@ static CUtensorMap vector_map(const float2* base, int dof, int S, long rows, int
     return m;
 }
 
-template <int RG>
-static void launch_apply_rg(cudaStream_t s, const CUtensorMap& vmap, const ApplyArgs& a, int NB) {
-    const size_t smem = apply_smem(RG, a.sel_t);
-    DDAMG_CUDA_TRY(cudaFuncSetAttribute(tc_block_apply_kernel<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem));
+template <int RG, int NA, int NCH>
+static void launch_apply_shape(cudaStream_t s, const CUtensorMap& vmap, const ApplyArgs& a, int NB) {
+    const size_t smem = apply_smem(RG, NA, a.sel_t);
+    DDAMG_CUDA_TRY(cudaFuncSetAttribute(tc_block_apply_kernel<RG, NA, NCH>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid(NB, (a.R + RG - 1) / RG);
-    DDAMG_LAUNCH(tc_block_apply_kernel<RG>, grid, kApplyThreads, smem, s, vmap, a);
+    DDAMG_LAUNCH((tc_block_apply_kernel<RG, NA, NCH>), grid, apply_threads(RG), smem, s, vmap, a);
+}
+static void launch_apply(int shape, cudaStream_t s, const CUtensorMap& vmap, const ApplyArgs& a, int NB) {
+    switch (shape) {
+        case 0: launch_apply_shape<64, 3, 1>(s, vmap, a, NB); break;
+        case 1: launch_apply_shape<64, 3, 2>(s, vmap, a, NB); break;
+        case 2: launch_apply_shape<64, 3, 4>(s, vmap, a, NB); break;
+        case 3: launch_apply_shape<32, 8, 2>(s, vmap, a, NB); break;
+        case 4: launch_apply_shape<32, 8, 4>(s, vmap, a, NB); break;
+        default: launch_apply_shape<16, 8, 4>(s, vmap, a, NB); break;
+    }
 }
 
 // ---------------------------------------------------------------- per (block, rhs) kernels
@@ -417,7 +488,7 @@ __global__ void tcs_prep_kernel(TaskGeom t, TcSapWork w, int first, int m, doubl
 // basis vector, and the Givens update of Hessenberg column j (FGMRES::rotation,
 // src/fgmres.cpp:99-115); a rhs whose estimate meets tol stops its Arnoldi loop (maxIt = j + 1).
 template <int EPL>
-__global__ void tcs_arnoldi_kernel(TaskGeom t, TcSapWork w, int j, int m, double tol) {
+__global__ void __launch_bounds__(256, EPL <= 16 ? 3 : 1) tcs_arnoldi_kernel(TaskGeom t, TcSapWork w, int j, int m, double tol) {
     const int task = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (task >= t.NB * t.R) return;
     if (!w.arn[task]) return;
@@ -426,26 +497,38 @@ __global__ void tcs_arnoldi_kernel(TaskGeom t, TcSapWork w, int j, int m, double
 #pragma unroll
     for (int q = 0; q < EPL; q++) {
         const int e = lane + 32 * q;
-        wl[q] = e < t.NE ? w.w[off + e] : make_float2(0.f, 0.f);
+        wl[q] = e < t.NE ? __ldg(w.w + off + e) : make_float2(0.f, 0.f);
     }
+    // all j+1 partial dots first, then one interleaved butterfly
     double2 h[kSapMaxM];
-    for (int i = 0; i <= j; i++) {
+#pragma unroll
+    for (int i = 0; i < kSapMaxM; i++) {
+        h[i] = make_double2(0.0, 0.0);
+        if (i > j) continue;
         const float2* Vi = w.V + (long)i * w.vec + off;
-        double2 s = make_double2(0.0, 0.0);
 #pragma unroll
         for (int q = 0; q < EPL; q++) {
             const int e = lane + 32 * q;
-            if (e < t.NE) s = cfmac(to_d(Vi[e]), to_d(wl[q]), s);
+            if (e < t.NE) h[i] = cfmac(to_d(__ldg(Vi + e)), to_d(wl[q]), h[i]);
         }
-        h[i] = warp_sum(s);
     }
-    for (int i = 0; i <= j; i++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int i = 0; i < kSapMaxM; i++) {
+            if (i > j) continue;
+            h[i].x += __shfl_xor_sync(0xffffffffu, h[i].x, o);
+            h[i].y += __shfl_xor_sync(0xffffffffu, h[i].y, o);
+        }
+#pragma unroll
+    for (int i = 0; i < kSapMaxM; i++) {
+        if (i > j) continue;
         const float2* Vi = w.V + (long)i * w.vec + off;
         const float2 hf = from_d<float2>(h[i]);
 #pragma unroll
         for (int q = 0; q < EPL; q++) {
             const int e = lane + 32 * q;
-            if (e < t.NE) wl[q] = wl[q] - cmul(hf, Vi[e]);
+            if (e < t.NE) wl[q] = wl[q] - cmul(hf, __ldg(Vi + e));
         }
     }
     double ww = 0.0;
@@ -466,7 +549,9 @@ __global__ void tcs_arnoldi_kernel(TaskGeom t, TcSapWork w, int j, int m, double
     double2* cn = w.cn + (long)task * m;
     double2* sn = w.sn + (long)task * m;
     double2* gm = w.gm + (long)task * (m + 1);
-    for (int i = 0; i <= j; i++) H[i * m + j] = h[i];
+#pragma unroll
+    for (int i = 0; i < kSapMaxM; i++)
+        if (i <= j) H[i * m + j] = h[i];
     H[(j + 1) * m + j] = make_double2(hn, 0.0);
     for (int i = 0; i < j; i++) {
         const double2 hij = H[i * m + j], hi1 = H[(i + 1) * m + j];
@@ -529,24 +614,69 @@ __global__ void tcs_scatter_kernel(TaskGeom t, TcSapWork w, const int* __restric
     }
 }
 
-void launch_sap_sweep_tc(cudaStream_t s, const Geom& g, const TcSapWork& w, const float2* r, float2* x,
-                         const SapArgs& a, int nrhs) {
-    if (a.m > kSapMaxM) throw ParamFailure{"SAP block GMRES restart length above 8 is not supported"};
-    const int S = g.sel_x * g.sel_t;
-    TaskGeom t{nrhs, a.nblocks, S, g.dof, S * g.dof, g.sel_x, g.sel_t, g.Nt, g.sap_t, g.size()};
-    const int tasks = a.nblocks * nrhs;
-    const int tgrid = ceil_div(tasks, 8);
-    const int rg = pick_rg(nrhs, g.sel_t);
-    auto apply = [&](const float2* src, const float2* bsub, const int* flag, int invert) {
-        const CUtensorMap vmap = vector_map(src, g.dof, S, (long)a.nblocks * nrhs, rg);
+namespace {
+struct SweepCtx {
+    cudaStream_t s;
+    const Geom& g;
+    const TcSapWork& w;
+    const SapArgs& a;
+    int nrhs, S;
+    void apply(int shape, const float2* src, const float2* bsub, const int* flag, int invert) const {
+        const CUtensorMap vmap = vector_map(src, g.dof, S, (long)a.nblocks * nrhs, kShapes[shape].rg);
         ApplyArgs aa{w.tiles, w.w, bsub, flag, invert, a.blocks, nrhs, S, g.sel_x, g.sel_t, g.Nt, g.sap_t,
                      g.dof, (2 * g.dof + 7) / 8, (float)a.m0 + 2.f, w.status};
-        switch (rg) {
-            case 16: launch_apply_rg<16>(s, vmap, aa, a.nblocks); break;
-            case 32: launch_apply_rg<32>(s, vmap, aa, a.nblocks); break;
-            default: launch_apply_rg<64>(s, vmap, aa, a.nblocks); break;
-        }
-    };
+        launch_apply(shape, s, vmap, aa, a.nblocks);
+    }
+    TaskGeom task_geom() const { return TaskGeom{nrhs, a.nblocks, S, g.dof, S * g.dof, g.sel_x, g.sel_t, g.Nt, g.sap_t, g.size()}; }
+};
+}  // namespace
+
+int tc_sweep_shapes() { return kNumShapes; }
+void tc_sweep_shape(int idx, int* rg, int* stages, int* chains) {
+    *rg = kShapes[idx].rg;
+    *stages = kShapes[idx].na;
+    *chains = kShapes[idx].nch;
+}
+
+// Times one block-operator application per admissible tile shape on the sweep's own data (gathered
+// from r first) and returns the fastest; us[i] gets the time of shape i (negative: not admissible).
+// Synchronises the stream: run it outside graph capture.
+int tune_sap_tc(cudaStream_t s, const Geom& g, const TcSapWork& w, const float2* r, const SapArgs& a, int nrhs,
+                double* us) {
+    const int S = g.sel_x * g.sel_t;
+    SweepCtx c{s, g, w, a, nrhs, S};
+    const TaskGeom t = c.task_geom();
+    DDAMG_LAUNCH(tcs_gather_kernel, ceil_div(a.nblocks * nrhs, 8), 256, 0, s, t, w, a.blocks, r, a.done);
+    cudaEvent_t e0, e1;
+    DDAMG_CUDA_TRY(cudaEventCreate(&e0));
+    DDAMG_CUDA_TRY(cudaEventCreate(&e1));
+    int best = -1;
+    for (int i = 0; i < kNumShapes; i++) {
+        us[i] = -1.0;
+        if (!shape_fits(i, g.sel_t) || kShapes[i].rg / 2 >= nrhs * 2) continue;  // at most 4x padding
+        c.apply(i, w.x, w.b, w.act, 0);  // warm-up
+        DDAMG_CUDA_TRY(cudaEventRecord(e0, s));
+        for (int k = 0; k < 3; k++) c.apply(i, w.x, w.b, w.act, 0);
+        DDAMG_CUDA_TRY(cudaEventRecord(e1, s));
+        DDAMG_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0;
+        DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        us[i] = 1e3 * ms / 3;
+        if (best < 0 || us[i] < us[best]) best = i;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best >= 0 ? best : default_shape(nrhs, g.sel_t);
+}
+
+void launch_sap_sweep_tc(cudaStream_t s, const Geom& g, const TcSapWork& w, const float2* r, float2* x,
+                         const SapArgs& a, int nrhs, int shape) {
+    if (a.m > kSapMaxM) throw ParamFailure{"SAP block GMRES restart length above 8 is not supported"};
+    const int S = g.sel_x * g.sel_t;
+    SweepCtx c{s, g, w, a, nrhs, S};
+    const TaskGeom t = c.task_geom();
+    const int tgrid = ceil_div(a.nblocks * nrhs, 8);
+    if (shape < 0 || shape >= kNumShapes || !shape_fits(shape, g.sel_t)) shape = default_shape(nrhs, g.sel_t);
     auto arnoldi = [&](int j) {
         const int epl = (t.NE + 31) / 32;
         if (epl <= 8) DDAMG_LAUNCH(tcs_arnoldi_kernel<8>, tgrid, 256, 0, s, t, w, j, a.m, a.tol);
@@ -554,15 +684,15 @@ void launch_sap_sweep_tc(cudaStream_t s, const Geom& g, const TcSapWork& w, cons
         else DDAMG_LAUNCH(tcs_arnoldi_kernel<32>, tgrid, 256, 0, s, t, w, j, a.m, a.tol);
     };
     DDAMG_LAUNCH(tcs_gather_kernel, tgrid, 256, 0, s, t, w, a.blocks, r, a.done);
-    apply(w.x, w.b, w.act, 0);  // r = b - D_B x0 with x0 = b
+    c.apply(shape, w.x, w.b, w.act, 0);  // r = b - D_B x0 with x0 = b
     DDAMG_LAUNCH(tcs_prep_kernel, tgrid, 256, 0, s, t, w, 1, a.m, a.tol);
     for (int k = 0; k < a.restarts; k++) {
         for (int j = 0; j < a.m; j++) {
-            apply(w.V + (long)j * w.vec, nullptr, w.arn, 0);  // w = D_B V_j
+            c.apply(shape, w.V + (long)j * w.vec, nullptr, w.arn, 0);  // w = D_B V_j
             arnoldi(j);
         }
         DDAMG_LAUNCH(tcs_update_kernel, tgrid, 256, 0, s, t, w, a.m);
-        apply(w.x, w.b, w.fin, 1);  // r = b - D_B x for every rhs not yet converged
+        c.apply(shape, w.x, w.b, w.fin, 1);  // r = b - D_B x for every rhs not yet converged
         DDAMG_LAUNCH(tcs_prep_kernel, tgrid, 256, 0, s, t, w, 0, a.m, a.tol);
     }
     DDAMG_LAUNCH(tcs_scatter_kernel, tgrid, 256, 0, s, t, w, a.blocks, x);

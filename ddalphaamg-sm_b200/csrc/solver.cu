@@ -6,6 +6,7 @@
 #include <cstring>
 #include <fstream>
 #include <functional>
+#include <map>
 #include <memory>
 #include <sstream>
 #include <string>
@@ -50,6 +51,7 @@ struct LevelData {
     double* rr = nullptr;   // W norms
     bool tc = false;        // batched FP32 SAP sweeps of this level use the tensor-core block operator
     TcSapWork tcw;
+    std::map<int, int> tc_shape;  // batch width -> tile shape chosen by the autotuner
 };
 constexpr int kTcMinRhs = 8;  // fewer right-hand sides leave too little link reuse for the tensor cores
 template <typename V> LevelBufs<V>& B(LevelData& L);
@@ -99,6 +101,7 @@ struct ddamg_handle {
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_next = 0;
     std::vector<ProfRec> prof_recs;
+    std::string tune_log;  // autotuner decisions, one line per (level, batch width)
     double prof_ms[kProfKinds][DDAMG_MAX_LEVELS] = {};
     long long prof_n[kProfKinds][DDAMG_MAX_LEVELS] = {};
 };
@@ -379,6 +382,28 @@ template <typename V> static void level_op(ddamg_handle* h, int l, const V* in, 
     else launch_coarse_op<V>(h->s, B<V>(D).links, in, out, b, g.Nx, g.Nt, g.dof, h->p.m0, nrhs);
 }
 
+// tile shape of the tensor-core sweep for this batch width: tuned on first use (the tuner times the
+// candidate shapes on the sweep's own data and syncs the stream), then cached
+static int tc_shape_for(ddamg_handle* h, int l, const float2* r, const SapArgs& a, int nrhs) {
+    LevelData& D = h->lv[l];
+    auto it = D.tc_shape.find(nrhs);
+    if (it != D.tc_shape.end()) return it->second;
+    std::vector<double> us(tc_sweep_shapes());
+    const int best = tune_sap_tc(h->s, D.g, D.tcw, r, a, nrhs, us.data());
+    D.tc_shape[nrhs] = best;
+    std::ostringstream o;
+    o << "level " << l << " rhs " << nrhs << ":";
+    for (int i = 0; i < (int)us.size(); i++) {
+        int rg, na, nch;
+        tc_sweep_shape(i, &rg, &na, &nch);
+        if (us[i] < 0) continue;
+        o << " [rhs/cta " << rg << " stages " << na << " chains " << nch << ": " << us[i] << " us"
+          << (i == best ? " *" : "") << "]";
+    }
+    h->tune_log += o.str() + "\n";
+    return best;
+}
+
 // SAP_C::SAP (src/sap.cpp:81-165) on nrhs independent vectors; returns the reference's value
 // for rhs 0 when want_iters (one host sync), else nu.
 template <typename V>
@@ -403,7 +428,8 @@ static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, b
                 if (l == 0) launch_sap_sweep_fine<V>(h->s, g, B<V>(D).U, r, x, a, nrhs);
                 else if (std::is_same<V, float2>::value && D.tc && nrhs >= kTcMinRhs)
                     launch_sap_sweep_tc(h->s, g, D.tcw, reinterpret_cast<const float2*>(r),
-                                        reinterpret_cast<float2*>(x), a, nrhs);
+                                        reinterpret_cast<float2*>(x), a, nrhs,
+                                        tc_shape_for(h, l, reinterpret_cast<const float2*>(r), a, nrhs));
                 else launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs);
             }
             // the residual after the last black sweep only feeds the convergence test
@@ -1011,6 +1037,16 @@ ddamg_status ddamg_profile_query(ddamg_t* h, int kind, int level, double* total_
     prof_flush(h);
     if (total_ms) *total_ms = h->prof_ms[kind][level];
     if (launches) *launches = h->prof_n[kind][level];
+    API_END
+}
+ddamg_status ddamg_autotune_report(ddamg_t* h, char* buf, int len) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (!buf || len < 1) throw ParamFailure{"buffer required"};
+    const std::string& t = h->tune_log;
+    const int n = std::min<int>((int)t.size(), len - 1);
+    std::memcpy(buf, t.data(), n);
+    buf[n] = 0;
     API_END
 }
 ddamg_status ddamg_launch_count(ddamg_t* h, long long* count) {

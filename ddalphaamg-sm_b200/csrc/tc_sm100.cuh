@@ -48,12 +48,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Waits until the phase with the given parity has completed.  Bounded: after about 2^22 polls
-// (well over a second with the back-off) it records the failure in *err and returns false.
+// Waits until the phase with the given parity has completed.  try_wait suspends the thread in
+// hardware until the phase completes or a short time limit passes, so the first 2^20 polls spin
+// without sleeping (a nanosleep here would add its full length to every hand-off); after that the
+// loop backs off by 1 us per poll.  Bounded: after about a second in all it records the failure in
+// *err and returns false.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-    for (uint32_t it = 0; it < (1u << 22); it++) {
+    for (uint32_t it = 0; it < (1u << 20); it++)
         if (mbar_try_wait(bar, parity)) return true;
-        if (it > 64) __nanosleep(it > 4096 ? 256 : 32);
+    for (uint32_t it = 0; it < (1u << 20); it++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        __nanosleep(1000);
     }
     if (err) atomicExch(err, 1);
     return false;
@@ -162,6 +167,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&a)[16]) {
         : "memory");
 #pragma unroll
     for (int i = 0; i < 16; i++) a[i] = __uint_as_float(r[i]);
+}
+// one load of 32 lanes x 32 bit x 8 consecutive columns, completed before returning
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&a)[8]) {
+    uint32_t r[8];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 8; i++) a[i] = __uint_as_float(r[i]);
 }
 // the same with 8 columns each
 __device__ __forceinline__ void tmem_ld8x2(uint32_t taddr_a, uint32_t taddr_b, float (&a)[8], float (&b)[8]) {

@@ -264,6 +264,12 @@ class Solver:
         check(self.L.ddamg_profile_query(self.h, kind, level, ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
 
+    def autotune_report(self):
+        """The tensor-core autotuner's measurements and choices, one line per (level, batch width)."""
+        buf = ctypes.create_string_buffer(1 << 14)
+        check(self.L.ddamg_autotune_report(self.h, buf, len(buf)))
+        return buf.value.decode()
+
     @staticmethod
     def launch_count():
         c = ctypes.c_longlong(0)

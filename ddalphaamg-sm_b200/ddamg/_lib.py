@@ -50,6 +50,7 @@ SIGNATURES = {
     "ddamg_launch_count": (_st, [_h, ctypes.POINTER(ctypes.c_longlong)]),
     "ddamg_profile": (_st, [_h, _i]),
     "ddamg_profile_query": (_st, [_h, _i, _i, _dp, ctypes.POINTER(ctypes.c_longlong)]),
+    "ddamg_autotune_report": (_st, [_h, ctypes.c_char_p, _i]),
     "ddamg_read_binary": (_st, [ctypes.c_char_p, _i, _i, _dp]),
     "ddamg_write_binary": (_st, [ctypes.c_char_p, _i, _i, _dp]),
     "ddamg_load_gauge": (_st, [_h, _dp]),

@@ -110,6 +110,11 @@ ddamg_status ddamg_launch_count(ddamg_t* h, long long* count);
  * (No reference counterpart: the reference counts FLOPs, include/utils.h:141-150.) */
 ddamg_status ddamg_profile(ddamg_t* h, int enable);
 ddamg_status ddamg_profile_query(ddamg_t* h, int kind, int level, double* total_ms, long long* launches);
+/* the autotuner's record: for each (level, batch width) whose SAP sweeps ran on the tensor cores,
+ * the measured time of one block-operator application per candidate tile shape (right-hand sides
+ * per CTA, link-tile pipeline depth, independent accumulator chains) and the chosen one (*); NUL-terminated text, truncated to
+ * len - 1 characters.  No reference counterpart. */
+ddamg_status ddamg_autotune_report(ddamg_t* h, char* buf, int len);
 
 /* ------------------------------------------------------------------ I/O */
 /* read_binary (src/io.cpp:4-55): records int32 x, t, mu, f64 re, im, x slowest; out: [site][mu] */
