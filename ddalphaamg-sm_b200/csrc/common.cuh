@@ -1,5 +1,6 @@
 // Shared device/host helpers for the DD-alphaAMG B200 library.
 #pragma once
+#include <atomic>
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -153,7 +154,7 @@ struct ParamFailure {
 struct TimeoutFailure {};
 
 // launch bookkeeping: every kernel launch in the library goes through this counter
-extern long long g_launches;
+extern std::atomic<long long> g_launches;  // kernels launched by the library (all handles)
 #define DDAMG_LAUNCH(kernel, grid, block, smem, stream, ...)                                      \
     do {                                                                                          \
         kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);                               \

@@ -7,6 +7,7 @@
 #include <fstream>
 #include <functional>
 #include <map>
+#include <set>
 #include <memory>
 #include <sstream>
 #include <string>
@@ -17,7 +18,7 @@
 
 namespace ddamg {
 
-long long g_launches = 0;
+std::atomic<long long> g_launches{0};
 static thread_local std::string t_last_error;
 void set_error(const std::string& msg) { t_last_error = msg; }
 
@@ -102,6 +103,15 @@ struct ddamg_handle {
     size_t ev_next = 0;
     std::vector<ProfRec> prof_recs;
     std::string tune_log;  // autotuner decisions, one line per (level, batch width)
+    // V-cycle preconditioner graphs, one per batch width; a width is captured on its second use
+    // (the first runs directly: autotuning and first-use set-up happen there)
+    struct CycleGraph {
+        cudaGraphExec_t exec;
+        long long kernels;
+    };
+    std::map<int, CycleGraph> graphs;
+    std::set<int> graph_warm;
+    bool graphs_off = false;  // a capture failed: launch directly from then on
     double prof_ms[kProfKinds][DDAMG_MAX_LEVELS] = {};
     long long prof_n[kProfKinds][DDAMG_MAX_LEVELS] = {};
 };
@@ -745,24 +755,76 @@ static void cycle_t(ddamg_handle* h, int l, const V* eta, V* psi, bool psi_zero,
     prolong_from_next<V>(h, l, pn, psi, R);
     if (p.nu2 > 0) sap_t<V>(h, l, eta, psi, p.nu2, p.smoother_tolerance, false, R, false);
 }
+// (the coarsest solves record a bounded wait that gave up in their status words; the callers of the
+// cycle check them once the whole solve is done: check_coarse_status)
 static void cycle(ddamg_handle* h, int l, const void* eta, void* psi, bool psi_zero, int kind, int R) {
     if (h->lv[l].fp32)
         cycle_t<float2>(h, l, static_cast<const float2*>(eta), static_cast<float2*>(psi), psi_zero, kind, R);
     else cycle_t<double2>(h, l, static_cast<const double2*>(eta), static_cast<double2*>(psi), psi_zero, kind, R);
-    if (l == h->L - 1) check_coarse_status(h, nullptr);
+}
+
+// One cycle on the level-0 buffers eta -> psi (fixed addresses, so a captured graph stays valid
+// across calls and set-ups).  V-cycles replay a CUDA graph per batch width: the first application
+// of a width runs directly, the second is captured and every later one replays it.
+static void level0_cycle(ddamg_handle* h, int R) {
+    LevelData& D = h->lv[0];
+    auto direct = [&]() {
+        if (D.fp32) cycle(h, 0, D.f.eta, D.f.psi, true, h->p.cycle, R);
+        else cycle(h, 0, D.d.eta, D.d.psi, true, h->p.cycle, R);
+    };
+    if (!h->p.cuda_graphs || h->graphs_off || h->p.cycle != DDAMG_CYCLE_V || h->prof) {
+        direct();
+        return;
+    }
+    auto it = h->graphs.find(R);
+    if (it != h->graphs.end()) {
+        DDAMG_CUDA_TRY(cudaGraphLaunch(it->second.exec, h->s));
+        g_launches += it->second.kernels;
+        return;
+    }
+    if (!h->graph_warm.count(R)) {
+        direct();
+        h->graph_warm.insert(R);
+        return;
+    }
+    const long long launches0 = g_launches;
+    cudaGraph_t graph = nullptr;
+    bool failed = cudaStreamBeginCapture(h->s, cudaStreamCaptureModeRelaxed) != cudaSuccess;
+    if (!failed) {
+        try {
+            direct();
+        } catch (...) {
+            failed = true;
+        }
+        if (cudaStreamEndCapture(h->s, &graph) != cudaSuccess || !graph) failed = true;
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (!failed && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) failed = true;
+    if (graph) cudaGraphDestroy(graph);
+    const long long kernels = g_launches - launches0;  // recorded, not yet run
+    g_launches -= kernels;
+    if (failed) {  // this configuration cannot be captured: keep launching directly
+        cudaGetLastError();
+        h->graphs_off = true;
+        h->tune_log += "cycle graph capture failed: launching kernels directly\n";
+        direct();
+        return;
+    }
+    h->graphs[R] = {exec, kernels};
+    h->tune_log += "cycle graph rhs " + std::to_string(R) + ": " + std::to_string(kernels) + " kernels\n";
+    DDAMG_CUDA_TRY(cudaGraphLaunch(exec, h->s));
+    g_launches += kernels;
 }
 
 // the outer preconditioner (FGMRES_AMG_*::preconditioner, include/amg.h:240-269): zero, one cycle
 static void outer_prec(ddamg_handle* h, const double2* in, double2* out, int R) {
     LevelData& D = h->lv[0];
     const long n = D.g.size() * R;
-    if (D.fp32) {
-        launch_convert<double2, float2>(h->s, in, D.f.eta, n);
-        cycle(h, 0, D.f.eta, D.f.psi, true, h->p.cycle, R);
-        launch_convert<float2, double2>(h->s, D.f.psi, out, n);
-    } else {
-        cycle(h, 0, in, out, true, h->p.cycle, R);
-    }
+    if (D.fp32) launch_convert<double2, float2>(h->s, in, D.f.eta, n);
+    else DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.eta, in, sizeof(double2) * n, cudaMemcpyDeviceToDevice, h->s));
+    level0_cycle(h, R);
+    if (D.fp32) launch_convert<float2, double2>(h->s, D.f.psi, out, n);
+    else DDAMG_CUDA_TRY(cudaMemcpyAsync(out, D.d.psi, sizeof(double2) * n, cudaMemcpyDeviceToDevice, h->s));
 }
 
 // ------------------------------------------------------------------ setup
@@ -850,6 +912,7 @@ static ddamg_status solve_device(ddamg_handle* h, const double2* b, double2* x, 
     std::vector<double> rel(nrhs);
     fgmres_host<double2>(h, n, nrhs, p.fgmres_restart_length, p.fgmres_restarts, p.fgmres_tolerance, A, &M, b,
                          nullptr, true, x, K, it.data(), rel.data());
+    check_coarse_status(h, nullptr);
     check_tc_status(h);
     DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, h->s));
     sync(h);
@@ -937,6 +1000,7 @@ ddamg_status ddamg_params_default(ddamg_params* p) {
     p->max_rhs = 1;
     p->device = 0;
     p->tensor_cores = 1;
+    p->cuda_graphs = 1;
     return DDAMG_OK;
 }
 
@@ -997,6 +1061,7 @@ ddamg_status ddamg_destroy(ddamg_t* h) {
     if (!h) return DDAMG_OK;
     cudaSetDevice(h->p.device);
     if (h->s) cudaStreamSynchronize(h->s);
+    for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second.exec);
     for (void* a : h->allocs) cudaFree(a);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : h->lane_ev) cudaEventDestroy(e);
@@ -1353,6 +1418,7 @@ static ddamg_status run_cycle(ddamg_t* h, const double* eta, double* psi, int ki
         throw;
     }
     h->p.cycle = saved;
+    check_coarse_status(h, nullptr);
     DDAMG_CUDA_TRY(cudaMemcpyAsync(psi, h->orr, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
     sync(h);
     return DDAMG_OK;

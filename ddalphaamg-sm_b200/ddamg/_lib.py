@@ -26,6 +26,7 @@ class Params(ctypes.Structure):
         ("fgmres_restarts", ctypes.c_int), ("fgmres_tolerance", ctypes.c_double),
         ("smoother_tolerance", ctypes.c_double), ("cycle", ctypes.c_int), ("precision", ctypes.c_int),
         ("max_rhs", ctypes.c_int), ("device", ctypes.c_int), ("tensor_cores", ctypes.c_int),
+        ("cuda_graphs", ctypes.c_int),
     ]
 
 

@@ -76,6 +76,11 @@ typedef struct {
      * the block operator on tcgen05 tensor cores (TF32 inputs, FP32 accumulation); 0: CUDA
      * cores only.  No reference counterpart. */
     int tensor_cores;
+    /* 1 (default): each V-cycle preconditioner application (per batch width) is captured once into
+     * a CUDA graph and replayed; 0: kernels are launched one by one.  Off while per-kernel timing
+     * (ddamg_profile) is on and for the K-cycle, whose inner FGMRES is host driven.  No reference
+     * counterpart. */
+    int cuda_graphs;
 } ddamg_params;
 
 typedef struct {
@@ -112,7 +117,8 @@ ddamg_status ddamg_profile(ddamg_t* h, int enable);
 ddamg_status ddamg_profile_query(ddamg_t* h, int kind, int level, double* total_ms, long long* launches);
 /* the autotuner's record: for each (level, batch width) whose SAP sweeps ran on the tensor cores,
  * the measured time of one block-operator application per candidate tile shape (right-hand sides
- * per CTA, link-tile pipeline depth, independent accumulator chains) and the chosen one (*); NUL-terminated text, truncated to
+ * per CTA, link-tile pipeline depth, independent accumulator chains) and the chosen one (*), and
+ * one line per captured V-cycle graph with its kernel count; NUL-terminated text, truncated to
  * len - 1 characters.  No reference counterpart. */
 ddamg_status ddamg_autotune_report(ddamg_t* h, char* buf, int len);
 
