@@ -96,9 +96,14 @@ struct SapArgs {
 template <typename V>
 void launch_sap_sweep_fine(cudaStream_t s, const Geom& g, const V* U, const V* r, V* x, const SapArgs& a,
                            int nrhs);
+// rb: right-hand sides per CTA (0: a default from the batch width and the block size)
 template <typename V>
 void launch_sap_sweep_coarse(cudaStream_t s, const Geom& g, const V* links, const V* r, V* x, const SapArgs& a,
-                             int nrhs);
+                             int nrhs, int rb = 0);
+// autotuner of rb: times one sweep per candidate (1, 2, 4, 8) into the scratch field xs; us[4]
+template <typename V>
+int tune_sap_rb(cudaStream_t s, const Geom& g, const V* links, const V* r, V* xs, const SapArgs& a, int nrhs,
+                double* us);
 
 // ------------------------------------------------------------ tensor-core SAP (kernels_tcsap.cu)
 // Batched FP32 coarse-level SAP colour sweep whose block operator runs on tcgen05 tensor cores

@@ -889,8 +889,21 @@ static int pick_rb(int nrhs, int ept, int m, int NE, int threads, size_t vbytes)
     return best;
 }
 
+// right-hand sides per CTA the launcher below supports for a block of NE unknowns
+static bool rb_admissible(int rb, int nrhs, int m, int NE, size_t vbytes) {
+    const int threads = std::min(1024, ((NE + 31) / 32) * 32);
+    const int ept = (NE + threads - 1) / threads;
+    if (rb == 1) return true;
+    if (rb > nrhs || ept != 1 || (threads > 512 && rb > 2)) return false;
+    const size_t smem = sizeof(double2) * ((size_t)2 * (threads / 32) * rb * (kSapMaxM + 1) +
+                                           (size_t)rb * ((m + 1) * m + (m + 1) + 3 * m)) +
+                        16 + vbytes * (size_t)(m + 2) * NE * rb;
+    return smem <= 227 * 1024 && rb * (int)(vbytes / 8) <= 8;  // shared memory and register budget
+}
+
 template <typename V, bool DENSE>
-static void launch_sap(cudaStream_t s, const Geom& g, const V* L, const V* r, V* x, const SapArgs& a, int nrhs) {
+static void launch_sap(cudaStream_t s, const Geom& g, const V* L, const V* r, V* x, const SapArgs& a, int nrhs,
+                       int rb_req = 0) {
     if (a.m > kSapMaxM) throw ParamFailure{"SAP block GMRES restart length above 8 is not supported"};
     const int NE = g.sel_x * g.sel_t * g.dof;
     const int threads = std::min(1024, ((NE + 31) / 32) * 32);
@@ -898,7 +911,8 @@ static void launch_sap(cudaStream_t s, const Geom& g, const V* L, const V* r, V*
     SapKParams p{a.m, a.restarts, a.tol, a.m0, a.blocks, a.nblocks, a.done, nrhs, 1};
     // level 0 keeps one vector per CTA: its links are 32 B per site, so there is nothing to share,
     // and a wider CTA would only cost shared memory and occupancy
-    const int rb = DENSE ? pick_rb(nrhs, ept, a.m, NE, threads, sizeof(V)) : 1;
+    int rb = DENSE ? pick_rb(nrhs, ept, a.m, NE, threads, sizeof(V)) : 1;
+    if (DENSE && rb_req > 0 && rb_admissible(rb_req, nrhs, a.m, NE, sizeof(V))) rb = rb_req;
     if (ept == 1 && threads <= 512) {
         if (rb == 8) launch_sap_k<V, DENSE, 1, 512, 8>(s, threads, g, L, r, x, p);
         else if (rb == 4) launch_sap_k<V, DENSE, 1, 512, 4>(s, threads, g, L, r, x, p);
@@ -935,16 +949,54 @@ void launch_sap_sweep_fine(cudaStream_t s, const Geom& g, const V* U, const V* r
 }
 template <typename V>
 void launch_sap_sweep_coarse(cudaStream_t s, const Geom& g, const V* links, const V* r, V* x, const SapArgs& a,
-                             int nrhs) {
-    launch_sap<V, true>(s, g, links, r, x, a, nrhs);
+                             int nrhs, int rb) {
+    launch_sap<V, true>(s, g, links, r, x, a, nrhs, rb);
 }
+
+// Autotuner for the CUDA-core coarse sweep: times one sweep per admissible count of right-hand sides
+// per CTA (1, 2, 4, 8), accumulating into the scratch field xs (its contents do not matter), and
+// returns the fastest; us[i] gets the time of candidate i (negative: not admissible).  Synchronises.
+template <typename V>
+int tune_sap_rb(cudaStream_t s, const Geom& g, const V* links, const V* r, V* xs, const SapArgs& a, int nrhs,
+                double* us) {
+    static const int cand[4] = {1, 2, 4, 8};
+    const int NE = g.sel_x * g.sel_t * g.dof;
+    cudaEvent_t e0, e1;
+    DDAMG_CUDA_TRY(cudaEventCreate(&e0));
+    DDAMG_CUDA_TRY(cudaEventCreate(&e1));
+    int best = 0;
+    double best_us = -1;
+    for (int i = 0; i < 4; i++) {
+        us[i] = -1;
+        if (!rb_admissible(cand[i], nrhs, a.m, NE, sizeof(V))) continue;
+        launch_sap<V, true>(s, g, links, r, xs, a, nrhs, cand[i]);  // warm-up
+        DDAMG_CUDA_TRY(cudaEventRecord(e0, s));
+        launch_sap<V, true>(s, g, links, r, xs, a, nrhs, cand[i]);
+        DDAMG_CUDA_TRY(cudaEventRecord(e1, s));
+        DDAMG_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0;
+        DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        us[i] = 1e3 * ms;
+        if (best_us < 0 || us[i] < best_us) {
+            best_us = us[i];
+            best = cand[i];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best > 0 ? best : 1;
+}
+template int tune_sap_rb<double2>(cudaStream_t, const Geom&, const double2*, const double2*, double2*,
+                                  const SapArgs&, int, double*);
+template int tune_sap_rb<float2>(cudaStream_t, const Geom&, const float2*, const float2*, float2*, const SapArgs&,
+                                 int, double*);
 template void launch_sap_sweep_fine<double2>(cudaStream_t, const Geom&, const double2*, const double2*, double2*,
                                              const SapArgs&, int);
 template void launch_sap_sweep_fine<float2>(cudaStream_t, const Geom&, const float2*, const float2*, float2*,
                                             const SapArgs&, int);
 template void launch_sap_sweep_coarse<double2>(cudaStream_t, const Geom&, const double2*, const double2*, double2*,
-                                               const SapArgs&, int);
+                                               const SapArgs&, int, int);
 template void launch_sap_sweep_coarse<float2>(cudaStream_t, const Geom&, const float2*, const float2*, float2*,
-                                              const SapArgs&, int);
+                                              const SapArgs&, int, int);
 
 }  // namespace ddamg

@@ -53,6 +53,7 @@ struct LevelData {
     bool tc = false;        // batched FP32 SAP sweeps of this level use the tensor-core block operator
     TcSapWork tcw;
     std::map<int, int> tc_shape;  // batch width -> tile shape chosen by the autotuner
+    std::map<int, int> rb_choice; // 2 * batch width + fp32 -> right-hand sides per CTA (CUDA cores)
 };
 constexpr int kTcMinRhs = 8;  // fewer right-hand sides leave too little link reuse for the tensor cores
 template <typename V> LevelBufs<V>& B(LevelData& L);
@@ -414,6 +415,25 @@ static int tc_shape_for(ddamg_handle* h, int l, const float2* r, const SapArgs& 
     return best;
 }
 
+// right-hand sides per CTA of the CUDA-core coarse sweep for this batch width and precision: tuned
+// on first use (one timed sweep per candidate into the level's scratch field t; syncs), then cached
+template <typename V> static int rb_for(ddamg_handle* h, int l, const V* r, const SapArgs& a, int nrhs) {
+    LevelData& D = h->lv[l];
+    const int key = nrhs * 2 + (std::is_same<V, float2>::value ? 1 : 0);
+    auto it = D.rb_choice.find(key);
+    if (it != D.rb_choice.end()) return it->second;
+    double us[4];
+    const int best = tune_sap_rb<V>(h->s, D.g, B<V>(D).links, r, B<V>(D).t, a, nrhs, us);
+    D.rb_choice[key] = best;
+    std::ostringstream o;
+    o << "level " << l << " rhs " << nrhs << (key & 1 ? " fp32" : " fp64") << " CUDA-core sweep:";
+    static const int cand[4] = {1, 2, 4, 8};
+    for (int i = 0; i < 4; i++)
+        if (us[i] >= 0) o << " [rhs/cta " << cand[i] << ": " << us[i] << " us" << (cand[i] == best ? " *" : "") << "]";
+    h->tune_log += o.str() + "\n";
+    return best;
+}
+
 // SAP_C::SAP (src/sap.cpp:81-165) on nrhs independent vectors; returns the reference's value
 // for rhs 0 when want_iters (one host sync), else nu.
 template <typename V>
@@ -440,7 +460,8 @@ static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, b
                     launch_sap_sweep_tc(h->s, g, D.tcw, reinterpret_cast<const float2*>(r),
                                         reinterpret_cast<float2*>(x), a, nrhs,
                                         tc_shape_for(h, l, reinterpret_cast<const float2*>(r), a, nrhs));
-                else launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs);
+                else launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs,
+                                                 nrhs > 1 ? rb_for<V>(h, l, r, a, nrhs) : 1);
             }
             // the residual after the last black sweep only feeds the convergence test
             const bool last = (colour == 1 && it == nu - 1);
