@@ -71,6 +71,15 @@ DDAMG_HD double2 cdiv(double2 a, double2 b) {
         return make_double2((a.x * r + a.y) / den, (a.y * r - a.x) / den);
     }
 }
+DDAMG_HD float2 cdiv(float2 a, float2 b) {
+    if (fabsf(b.x) >= fabsf(b.y)) {
+        float r = b.y / b.x, den = b.x + b.y * r;
+        return make_float2((a.x + a.y * r) / den, (a.y - a.x * r) / den);
+    } else {
+        float r = b.x / b.y, den = b.x * r + b.y;
+        return make_float2((a.x * r + a.y) / den, (a.y * r - a.x) / den);
+    }
+}
 
 // ---------------------------------------------------------------- warp / block reductions
 __device__ __forceinline__ double2 warp_sum(double2 v) {

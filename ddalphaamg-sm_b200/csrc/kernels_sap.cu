@@ -643,7 +643,7 @@ __global__ void __launch_bounds__(128) sap_fine_warp_kernel(Geom g, const V* __r
 // dots of an Arnoldi step are reduced in one interleaved butterfly.  Dots and norms accumulate in
 // the working precision.
 template <typename V, int SPL, int M>
-__global__ void __launch_bounds__(128) sap_fine_reg_kernel(Geom g, const V* __restrict__ U, const V* __restrict__ rg,
+__global__ void __launch_bounds__(128, (sizeof(V) == 8 || SPL == 1) ? 4 : 1) sap_fine_reg_kernel(Geom g, const V* __restrict__ U, const V* __restrict__ rg,
                                                            V* __restrict__ xg, SapKParams p, int wpc, size_t wbytes) {
     typedef typename RealOf<V>::R R;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -653,11 +653,12 @@ __global__ void __launch_bounds__(128) sap_fine_reg_kernel(Geom g, const V* __re
     const int kb = task / p.nrhs, rhs = task - kb * p.nrhs;  // block-major
     if (p.done && p.done[rhs]) return;
     const int et = g.sel_t, ex = g.sel_x, S = ex * et;
-    double2* H = reinterpret_cast<double2*>(smraw + wib * wbytes);  // (M+1) x M, lane 0 only
-    double2* gm = H + (M + 1) * M;
-    double2* cn = gm + (M + 1);
-    double2* sn = cn + M;
-    double2* eta = sn + M;
+    // Hessenberg matrix, rotations and triangular solve in the working precision (lane 0 only)
+    V* H = reinterpret_cast<V*>(smraw + wib * wbytes);  // (M+1) x M
+    V* gm = H + (M + 1) * M;
+    V* cn = gm + (M + 1);
+    V* sn = cn + M;
+    V* eta = sn + M;
     V* op = reinterpret_cast<V*>(eta + M);
     const int blk = p.blocks[kb];
     const int bx = blk / g.sap_t, bt = blk - bx * g.sap_t;
@@ -738,7 +739,7 @@ __global__ void __launch_bounds__(128) sap_fine_reg_kernel(Geom g, const V* __re
         for (int q = 0; q < SPL; q++)
 #pragma unroll
             for (int a = 0; a < 2; a++) Vb[0][q][a] = inv * w[q][a];
-        if (lane == 0) gm[0] = make_double2(err, 0.0);
+        if (lane == 0) gm[0] = mkc(R(err), R(0));
 #pragma unroll
         for (int j = 0; j < M; j++) {
             apply(Vb[j]);
@@ -777,20 +778,20 @@ __global__ void __launch_bounds__(128) sap_fine_reg_kernel(Geom g, const V* __re
             int brk = 0;
             if (lane == 0) {
 #pragma unroll
-                for (int i = 0; i <= j; i++) H[i * M + j] = to_d(h[i]);
-                H[(j + 1) * M + j] = make_double2(hn, 0.0);
+                for (int i = 0; i <= j; i++) H[i * M + j] = h[i];
+                H[(j + 1) * M + j] = mkc(R(hn), R(0));
                 for (int i = 0; i < j; i++) {  // FGMRES::rotation (src/fgmres.cpp:99-115)
-                    const double2 hij = H[i * M + j], hi1 = H[(i + 1) * M + j];
-                    const double2 tmp = cmulc(cn[i], hij) + cmulc(sn[i], hi1);
+                    const V hij = H[i * M + j], hi1 = H[(i + 1) * M + j];
+                    const V tmp = cmulc(cn[i], hij) + cmulc(sn[i], hi1);
                     H[(i + 1) * M + j] = cmul(cn[i], hi1) - cmul(sn[i], hij);
                     H[i * M + j] = tmp;
                 }
-                const double2 hjj = H[j * M + j], hj1 = H[(j + 1) * M + j];
-                const double den = sqrt(cnorm2(hjj) + cnorm2(hj1));
-                sn[j] = make_double2(hj1.x / den, hj1.y / den);
-                cn[j] = make_double2(hjj.x / den, hjj.y / den);
+                const V hjj = H[j * M + j], hj1 = H[(j + 1) * M + j];
+                const R den = sqrt(cnorm2(hjj) + cnorm2(hj1));
+                sn[j] = mkc(hj1.x / den, hj1.y / den);
+                cn[j] = mkc(hjj.x / den, hjj.y / den);
                 H[j * M + j] = cmulc(cn[j], hjj) + cmulc(sn[j], hj1);
-                H[(j + 1) * M + j] = make_double2(0.0, 0.0);
+                H[(j + 1) * M + j] = czero<V>();
                 gm[j + 1] = -cmul(sn[j], gm[j]);
                 gm[j] = cmulc(cn[j], gm[j]);
                 brk = (sqrt(cnorm2(gm[j + 1])) < p.tol * norm_b) ? 1 : 0;
@@ -803,7 +804,7 @@ __global__ void __launch_bounds__(128) sap_fine_reg_kernel(Geom g, const V* __re
         }
         if (lane == 0) {  // solve_upper_triangular (src/fgmres.cpp:118-128)
             for (int i = maxIt - 1; i >= 0; i--) {
-                double2 e = gm[i];
+                V e = gm[i];
                 for (int jj = i + 1; jj < maxIt; jj++) e = e - cmul(H[i * M + jj], eta[jj]);
                 eta[i] = cdiv(e, H[i * M + i]);
             }
@@ -812,7 +813,7 @@ __global__ void __launch_bounds__(128) sap_fine_reg_kernel(Geom g, const V* __re
 #pragma unroll
         for (int jj = 0; jj < M; jj++) {
             if (jj >= maxIt) break;
-            const V ej = from_d<V>(eta[jj]);
+            const V ej = eta[jj];
 #pragma unroll
             for (int q = 0; q < SPL; q++)
 #pragma unroll
@@ -840,7 +841,7 @@ __global__ void __launch_bounds__(128) sap_fine_reg_kernel(Geom g, const V* __re
 template <typename V, int SPL, int M>
 static void launch_fine_reg(cudaStream_t s, const Geom& g, const V* U, const V* r, V* x, SapKParams p) {
     const int S = g.sel_x * g.sel_t;
-    const size_t wb = (sizeof(double2) * ((M + 1) * M + (M + 1) + 3 * M) + sizeof(V) * 2 * S + 15) / 16 * 16;
+    const size_t wb = (sizeof(V) * ((M + 1) * M + (M + 1) + 3 * M) + sizeof(V) * 2 * S + 15) / 16 * 16;
     const int wpc = 4;
     const int tasks = p.nblocks * p.nrhs;
     DDAMG_LAUNCH((sap_fine_reg_kernel<V, SPL, M>), ceil_div(tasks, wpc), 32 * wpc, wb * wpc, s, g, U, r, x, p, wpc,
