@@ -88,8 +88,8 @@ template <typename V, int RB> struct SapSmem {
 // element is loaded once and applied to all RB vectors; every right-hand side keeps its own
 // Hessenberg matrix, rotations, break point (maxIt) and convergence state, and freezes once it
 // has finished, so each follows exactly the single-vector algorithm of FGMRES::fgmres.
-template <typename V, bool DENSE, int EPT, int MAXT, int RB>
-__global__ void __launch_bounds__(MAXT) sap_block_kernel(Geom g, const V* __restrict__ L, const V* __restrict__ rg,
+template <typename V, bool DENSE, int EPT, int MAXT, int RB, int CH>
+__global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __restrict__ L, const V* __restrict__ rg,
                                                          V* __restrict__ xg, SapKParams p) {
     typedef typename RealOf<V>::R R;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -182,6 +182,15 @@ __global__ void __launch_bounds__(MAXT) sap_block_kernel(Geom g, const V* __rest
                     const V* M = L + ((long)n * 5 + d) * dof * dof + i;
                     const V* o = op + (size_t)kk * dof * RB;
                     int j = 0;
+                    for (; j + CH <= dof; j += CH) {  // CH link loads in flight
+                        V mv[CH];
+#pragma unroll
+                        for (int u = 0; u < CH; u++) mv[u] = __ldg(M + (long)(j + u) * dof);
+#pragma unroll
+                        for (int u = 0; u < CH; u++)
+#pragma unroll
+                            for (int r = 0; r < RB; r++) acc[r][u & 1] = cfma(mv[u], o[(j + u) * RB + r], acc[r][u & 1]);
+                    }
                     for (; j + 8 <= dof; j += 8) {  // 8 link loads in flight
                         V mv[8];
 #pragma unroll
@@ -860,15 +869,15 @@ static void launch_fine_warp(cudaStream_t s, const Geom& g, const V* U, const V*
     DDAMG_LAUNCH((sap_fine_warp_kernel<V, SPL>), ceil_div(tasks, wpc), 32 * wpc, smem, s, g, U, r, x, p, wpc, wb);
 }
 
-template <typename V, bool DENSE, int EPT, int MAXT, int RB>
+template <typename V, bool DENSE, int EPT, int MAXT, int RB, int CH = 8>
 static void launch_sap_k(cudaStream_t s, int threads, const Geom& g, const V* L, const V* r, V* x, SapKParams p) {
     const int NE = g.sel_x * g.sel_t * g.dof;
     p.ngroups = (p.nrhs + RB - 1) / RB;
     const size_t smem = SapSmem<V, RB>::bytes(p.m, NE, threads / 32);
-    DDAMG_CUDA_TRY(cudaFuncSetAttribute(sap_block_kernel<V, DENSE, EPT, MAXT, RB>,
+    DDAMG_CUDA_TRY(cudaFuncSetAttribute(sap_block_kernel<V, DENSE, EPT, MAXT, RB, CH>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    DDAMG_LAUNCH((sap_block_kernel<V, DENSE, EPT, MAXT, RB>), dim3(p.nblocks * p.ngroups), threads, smem, s, g, L, r,
-                 x, p);
+    DDAMG_LAUNCH((sap_block_kernel<V, DENSE, EPT, MAXT, RB, CH>), dim3(p.nblocks * p.ngroups), threads, smem,
+                 s, g, L, r, x, p);
 }
 
 // right-hand sides per CTA: as many as fit in shared memory (and in registers for small
@@ -914,6 +923,13 @@ static void launch_sap(cudaStream_t s, const Geom& g, const V* L, const V* r, V*
     // and a wider CTA would only cost shared memory and occupancy
     int rb = DENSE ? pick_rb(nrhs, ept, a.m, NE, threads, sizeof(V)) : 1;
     if (DENSE && rb_req > 0 && rb_admissible(rb_req, nrhs, a.m, NE, sizeof(V))) rb = rb_req;
+    // blocks of at most 384 unknowns: a 384-thread bound leaves 168 registers per thread, enough to
+    // keep 12 link loads in flight per right-hand side group
+    if (DENSE && ept == 1 && threads <= 384 && (rb == 1 || rb == 4)) {
+        if (rb == 4) launch_sap_k<V, DENSE, 1, 384, 4, 12>(s, threads, g, L, r, x, p);
+        else launch_sap_k<V, DENSE, 1, 384, 1, 12>(s, threads, g, L, r, x, p);
+        return;
+    }
     if (ept == 1 && threads <= 512) {
         if (rb == 8) launch_sap_k<V, DENSE, 1, 512, 8>(s, threads, g, L, r, x, p);
         else if (rb == 4) launch_sap_k<V, DENSE, 1, 512, 4>(s, threads, g, L, r, x, p);
