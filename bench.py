@@ -364,6 +364,7 @@ def run_ours(args, rank, world, local_rank):
             "solve_ms": 1e3 * im.solve_seconds, "iterations": im.iterations, "rel_residual": im.rel_residual,
             "rel_err_vs_fp64": float(np.linalg.norm(xm.cpu().numpy().view(np.complex128) - x) / np.linalg.norm(x))}
         sm.close()
+        sec["krylov_256"] = krylov_256(ddamg, U, b, x, local_rank)
         sec["dw_gbs"] = dw_bandwidth(ddamg, torch, local_rank)
         if not args.no_secondary:
             sec["mixed_1024"] = mixed_1024(ddamg, torch, local_rank)
@@ -539,6 +540,50 @@ def batched_512(ddamg, torch, dev):
         "timing": "host wall clock around setup + solve of all 8 handles (8 threads, 8 streams)"}
     for h in handles:
         h.close()
+    return out
+
+
+# algorithmic HBM bytes per site and iteration of the fused comparison-solver kernels (FP64):
+# BiCGstab: direction pass (r, d, A d, U, r~ in; d, A d out) 224, s pass (r, A d, U in; s, t out) 160,
+# update pass (s, t, d, x, r~ in; r, x out) 224; CG on D^dagger D: 160 + 128 + 192
+KRYLOV_BYTES = {"bicgstab": 608, "cg_normal": 480}
+
+
+def krylov_256(ddamg, U, b, x_amg, dev):
+    """The reference's comparison solvers (src/conjugate_gradient.cpp) on the bench workload, to 1e-10 as
+    Methods::BiCG / Methods::CG run them, against the multigrid solve; plus a bandwidth probe: 300
+    BiCGstab iterations on a 1024x1024 field (larger than L2), per-iteration bytes from KRYLOV_BYTES."""
+    w = WORKLOAD
+    p = ddamg.default_params(w["Nx"], w["Nt"], w["levels"], w["m0"], w["rows"], device=dev)
+    s = ddamg.Solver(p)
+    s.load_gauge(U)
+    out = {}
+    sites = w["Nx"] * w["Nt"]
+    for name, fn in (("bicgstab", lambda: s.bi_cgstab(b)), ("cg_normal", lambda: s.CG(b))):
+        fn()  # warm-up (allocation, graph)
+        xs, info = fn()
+        ms = 1e3 * info.solve_seconds
+        out[name] = {"time_to_solution_ms": ms, "iterations": info.iterations, "converged": bool(info.converged),
+                     "rel_residual_iterated_system": info.rel_residual,
+                     "rel_err_vs_multigrid_fp64": float(np.linalg.norm(xs - x_amg) / np.linalg.norm(x_amg)),
+                     "us_per_iteration": 1e3 * ms / max(1, info.iterations),
+                     "gbs_algorithmic": KRYLOV_BYTES[name] * sites * info.iterations / (ms * 1e-3) / 1e9}
+    s.close()
+    N = 1024
+    th, _ = ddamg.gauge_metropolis(N, N, 4.0, 10, 3, device=dev)
+    p = ddamg.default_params(N, N, 2, -0.07, [[0, 128, 128, 4, 128, 128]], device=dev)
+    s = ddamg.Solver(p)
+    s.load_gauge(np.exp(1j * th))
+    bb = ddamg.gaussian_field(2 * N * N, 77)
+    s.bi_cgstab(bb, max_iter=50)
+    _, info = s.bi_cgstab(bb, max_iter=300)
+    ms = 1e3 * info.solve_seconds
+    gbs = KRYLOV_BYTES["bicgstab"] * N * N * info.iterations / (ms * 1e-3) / 1e9
+    hbm, kind = peaks()
+    out["bandwidth_probe_1024"] = {"iterations": info.iterations, "ms": ms, "us_per_iteration": 1e3 * ms / info.iterations,
+                                   "gbs_algorithmic": gbs, "frac_of_hbm": gbs / hbm, "peak_kind": kind,
+                                   "bytes_per_site_iteration": KRYLOV_BYTES["bicgstab"]}
+    s.close()
     return out
 
 

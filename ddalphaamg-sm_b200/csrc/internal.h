@@ -133,6 +133,28 @@ int tune_sap_tc(cudaStream_t s, const Geom& g, const TcSapWork& w, const float2*
 int tc_sweep_shapes();
 void tc_sweep_shape(int idx, int* rg, int* stages, int* chains);
 
+// ------------------------------------------------------------ comparison solvers (kernels_krylov.cu)
+// BiCGstab on D_W and CG on D^dagger D (src/conjugate_gradient.cpp) with device-resident scalars
+struct KrylovState {
+    double2 alpha, beta, omega, rho, rho_prev, rnorm2;
+    double norm_b, err;
+    int k, done, iters;  // done: 0 running, 1 BiCGstab converged with x += alpha d pending, 2 converged, 3 max_iter
+    unsigned ticket;     // CTAs finished in the current kernel (the last one reduces)
+};
+struct KrylovWork {
+    double2 *b = nullptr, *rt = nullptr, *x = nullptr, *r = nullptr, *s = nullptr, *t = nullptr, *y = nullptr;
+    double2* d[2] = {nullptr, nullptr};
+    double2* Ad[2] = {nullptr, nullptr};
+    double2* part = nullptr;  // 3 partial sums per CTA
+    KrylovState* st = nullptr;
+};
+int krylov_grid(int sites);
+// solver 0 = BiCGstab (x holds x0 on entry), 1 = CG on D^dagger D x = b (x0 = b)
+void launch_krylov_init(cudaStream_t s, int solver, const KrylovWork& w, const double2* U, int Nx, int Nt, double m0,
+                        double tol, int max_iter);
+void launch_krylov_iterations(cudaStream_t s, int solver, const KrylovWork& w, const double2* U, int Nx, int Nt,
+                              double m0, double tol, int max_iter, int count);
+
 // ------------------------------------------------------------ coarsest GMRES (kernels_gmres.cu)
 struct CoarseGmresWork {
     double2* V = nullptr;      // (m+1) x n

@@ -86,6 +86,7 @@ struct ddamg_handle {
     double2* hpin2 = nullptr;  // pinned host staging (uploads)
     double2* dalpha = nullptr; // per-rhs scale factors
     double2* grad = nullptr;   // gradient work: psi, lambda, sigma_3 eta (3 fine vectors)
+    ddamg::KrylovWork kry;                          // BiCGstab / CG comparison solvers (allocated on first use)
     ddamg::CoarseGmresWork cg;                      // lane 0: the handle's stream
     std::vector<ddamg::CoarseGmresWork> cg_lane;    // lanes 1..: concurrent coarsest solves of a batch
     std::vector<cudaStream_t> lane_s;
@@ -1520,6 +1521,165 @@ ddamg_status ddamg_gmres_plain(ddamg_t* h, const double* b, double* x, int m, in
         info->solve_seconds = ms * 1e-3;
     }
     if (!(rel < tol)) return DDAMG_NOT_CONVERGED;
+    API_END
+}
+
+// ------------------------------------------------------------------ comparison solvers
+namespace ddamg {
+static void krylov_alloc(ddamg_handle* h) {
+    KrylovWork& w = h->kry;
+    if (w.x) return;
+    const long n = h->lv[0].g.size();
+    for (double2** p : {&w.b, &w.rt, &w.x, &w.r, &w.s, &w.t, &w.y, &w.d[0], &w.d[1], &w.Ad[0], &w.Ad[1]})
+        *p = dalloc_t<double2>(h, n);
+    w.part = dalloc_t<double2>(h, 3 * (size_t)krylov_grid(h->lv[0].g.sites));
+    w.st = static_cast<KrylovState*>(dalloc(h, sizeof(KrylovState)));
+}
+
+// bi_cgstab (solver 0) or conjugate_gradient on D^dagger D (solver 1), src/conjugate_gradient.cpp.
+// Iterations are queued in batches of kKrylovBatch (replayed from a CUDA graph when cuda_graphs is
+// set); the next batch is queued before the device's done word of the current one is read, so
+// the GPU never waits for the host.  info->iterations follows the reference's count; the true
+// residual is recomputed for the system the solver iterates on.
+constexpr int kKrylovBatch = 16;
+static ddamg_status krylov_run(ddamg_handle* h, int solver, const double* b, const double* x0, double* x,
+                               int max_iter, double tol, ddamg_solve_info* info) {
+    if (!h->gauge) throw ParamFailure{"no gauge field loaded"};
+    if (max_iter < 1 || !(tol > 0)) throw ParamFailure{"max_iter must be >= 1 and tol > 0"};
+    const Geom& g = h->lv[0].g;
+    const long n = g.size();
+    double bb = 0.0;
+    for (long i = 0; i < 2 * n; i++) {
+        if (!std::isfinite(b[i]) || (x0 && !std::isfinite(x0[i]))) {
+            set_error("non-finite value in the right-hand side or the initial guess");
+            return DDAMG_ERR_NAN;
+        }
+        bb += b[i] * b[i];
+    }
+    if (bb == 0.0) {  // the zero right-hand side has the zero solution (the reference divides by zero)
+        std::fill(x, x + 2 * n, 0.0);
+        if (info) *info = ddamg_solve_info{};
+        if (info) info->converged = 1;
+        return DDAMG_OK;
+    }
+    krylov_alloc(h);
+    KrylovWork& w = h->kry;
+    const double2* U = h->lv[0].d.U;
+    cudaStream_t s = h->s;
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(w.b, b, sizeof(double2) * n, cudaMemcpyHostToDevice, s));
+    if (solver == 0) {
+        if (x0) DDAMG_CUDA_TRY(cudaMemcpyAsync(w.x, x0, sizeof(double2) * n, cudaMemcpyHostToDevice, s));
+        else DDAMG_CUDA_TRY(cudaMemsetAsync(w.x, 0, sizeof(double2) * n, s));
+    }
+    cudaGraphExec_t exec = nullptr;
+    long long graph_kernels = 0;
+    if (h->p.cuda_graphs && !h->prof) {  // one batch of iterations as a graph
+        cudaGraph_t graph = nullptr;
+        const long long l0 = g_launches;
+        bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+        if (ok) {
+            try {
+                launch_krylov_iterations(s, solver, w, U, g.Nx, g.Nt, h->p.m0, tol, max_iter, kKrylovBatch);
+            } catch (...) {
+                ok = false;
+            }
+            if (cudaStreamEndCapture(s, &graph) != cudaSuccess || !graph) ok = false;
+        }
+        if (ok && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) ok = false;
+        if (graph) cudaGraphDestroy(graph);
+        graph_kernels = g_launches - l0;
+        g_launches -= graph_kernels;
+        if (!ok) {
+            cudaGetLastError();
+            if (exec) cudaGraphExecDestroy(exec);
+            exec = nullptr;
+        }
+    }
+    cudaEvent_t evb[2] = {nullptr, nullptr};
+    int* hd = reinterpret_cast<int*>(h->hpin);
+    ddamg_status result = DDAMG_OK;
+    try {
+        for (cudaEvent_t& e : evb) DDAMG_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        DDAMG_CUDA_TRY(cudaEventRecord(h->ev0, s));
+        launch_krylov_init(s, solver, w, U, g.Nx, g.Nt, h->p.m0, tol, max_iter);
+        long launched = 0;
+        auto enqueue = [&](int slot) {
+            if (exec) {
+                DDAMG_CUDA_TRY(cudaGraphLaunch(exec, s));
+                g_launches += graph_kernels;
+            } else {
+                launch_krylov_iterations(s, solver, w, U, g.Nx, g.Nt, h->p.m0, tol, max_iter, kKrylovBatch);
+            }
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(hd + slot, &w.st->done, sizeof(int), cudaMemcpyDeviceToHost, s));
+            DDAMG_CUDA_TRY(cudaEventRecord(evb[slot], s));
+            launched += kKrylovBatch;
+        };
+        enqueue(0);
+        for (int i = 0;; i++) {
+            if (launched < max_iter) enqueue((i + 1) & 1);
+            DDAMG_CUDA_TRY(cudaEventSynchronize(evb[i & 1]));
+            if (hd[i & 1] >= 2) break;
+        }
+        DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, s));
+        // true residual of the iterated system: b - D x (BiCGstab), phi - D^dagger D x (CG)
+        if (solver == 0) {
+            launch_wilson<double2>(s, U, w.x, w.r, w.b, g.Nx, g.Nt, h->p.m0, 0, 1);
+        } else {
+            launch_wilson<double2>(s, U, w.x, w.y, nullptr, g.Nx, g.Nt, h->p.m0, 0, 1);
+            launch_wilson<double2>(s, U, w.y, w.r, w.b, g.Nx, g.Nt, h->p.m0, 1, 1);
+        }
+        launch_norm2<double2>(s, w.r, n, n, 1, h->dpart, h->dn);
+        launch_norm2<double2>(s, w.b, n, n, 1, h->dpart, h->dn + 1);
+        KrylovState st;
+        double nn[2];
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(&st, w.st, sizeof(st), cudaMemcpyDeviceToHost, s));
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(nn, h->dn, sizeof(nn), cudaMemcpyDeviceToHost, s));
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(x, w.x, sizeof(double2) * n, cudaMemcpyDeviceToHost, s));
+        sync(h);
+        float ms = 0;
+        DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        const double rel = nn[1] > 0 ? std::sqrt(nn[0] / nn[1]) : 0.0;
+        if (info) {
+            info->iterations = st.iters;
+            info->converged = st.done == 2;
+            info->rel_residual = rel;
+            info->setup_seconds = 0;
+            info->solve_seconds = ms * 1e-3;
+        }
+        if (!std::isfinite(rel)) {
+            set_error("the Krylov iteration produced a non-finite value");
+            result = DDAMG_ERR_NAN;
+        } else if (st.done != 2) {
+            set_error("no convergence within max_iter iterations");
+            result = DDAMG_NOT_CONVERGED;
+        }
+    } catch (...) {
+        for (cudaEvent_t e : evb)
+            if (e) cudaEventDestroy(e);
+        if (exec) cudaGraphExecDestroy(exec);
+        throw;
+    }
+    for (cudaEvent_t e : evb) cudaEventDestroy(e);
+    if (exec) cudaGraphExecDestroy(exec);
+    return result;
+}
+}  // namespace ddamg
+
+ddamg_status ddamg_bicgstab(ddamg_t* h, const double* b, const double* x0, double* x, int max_iter, double tol,
+                            ddamg_solve_info* info) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (!b || !x) throw ParamFailure{"null vector"};
+    return krylov_run(h, 0, b, x0, x, max_iter, tol, info);
+    API_END
+}
+
+ddamg_status ddamg_cg_normal(ddamg_t* h, const double* phi, double* x, int max_iter, double tol,
+                             ddamg_solve_info* info) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (!phi || !x) throw ParamFailure{"null vector"};
+    return krylov_run(h, 1, phi, nullptr, x, max_iter, tol, info);
     API_END
 }
 

@@ -234,6 +234,32 @@ class Solver:
               allow=(_lib.NOT_CONVERGED,))
         return x, info
 
+    def bi_cgstab(self, b, x0=None, max_iter=10000, tol=1e-10):
+        """bi_cgstab (src/conjugate_gradient.cpp:87-176) on D_W; returns (x, SolveInfo).  Like the
+        reference, info.iterations is k+1 at convergence and max_iter otherwise."""
+        b = _c(b)
+        x = np.empty_like(b)
+        info = SolveInfo()
+        x0c = _c(x0) if x0 is not None else None  # kept alive across the call
+        check(self.L.ddamg_bicgstab(self.h, _dp(b), _dp(x0c) if x0c is not None else None, _dp(x), max_iter, tol,
+                                    ctypes.byref(info)),
+              allow=(_lib.NOT_CONVERGED,))
+        return x, info
+
+    def conjugate_gradient(self, phi, max_iter=10000, tol=1e-10):
+        """conjugate_gradient (src/conjugate_gradient.cpp:4-83): CG on D^dagger D x = phi from x0 = phi;
+        returns (x, SolveInfo), info.iterations = k+1 at convergence."""
+        phi = _c(phi)
+        x = np.empty_like(phi)
+        info = SolveInfo()
+        check(self.L.ddamg_cg_normal(self.h, _dp(phi), _dp(x), max_iter, tol, ctypes.byref(info)),
+              allow=(_lib.NOT_CONVERGED,))
+        return x, info
+
+    def CG(self, b, max_iter=10000, tol=1e-10):
+        """Methods::CG (src/methods.cpp:42-58): D^dagger b, then conjugate_gradient; x solves D x = b."""
+        return self.conjugate_gradient(self.D_dagger_phi(b), max_iter=max_iter, tol=tol)
+
     def gradient(self, eta, b):
         """dL/dtheta_mu(x) for L = Re(eta^dagger D^-1 b); returns ([site][mu] float64, infos)."""
         eta, b = _c(eta), _c(b)

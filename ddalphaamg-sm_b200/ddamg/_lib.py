@@ -79,6 +79,8 @@ SIGNATURES = {
     "ddamg_solve": (_st, [_h, _dp, _dp, _i, ctypes.POINTER(SolveInfo)]),
     "ddamg_solve_device": (_st, [_h, _vp, _vp, _i, ctypes.POINTER(SolveInfo)]),
     "ddamg_gmres_plain": (_st, [_h, _dp, _dp, _i, _i, ctypes.c_double, ctypes.POINTER(SolveInfo)]),
+    "ddamg_bicgstab": (_st, [_h, _dp, _dp, _dp, _i, ctypes.c_double, ctypes.POINTER(SolveInfo)]),
+    "ddamg_cg_normal": (_st, [_h, _dp, _dp, _i, ctypes.c_double, ctypes.POINTER(SolveInfo)]),
     "ddamg_gradient": (_st, [_h, _dp, _dp, _dp, ctypes.POINTER(SolveInfo)]),
     "ddamg_link_derivative": (_st, [_h, _dp, _dp, _dp]),
     "ddamg_gauge_metropolis": (_st, [_i, _i, ctypes.c_double, _i, ctypes.c_uint64, ctypes.c_double, _dp, _dp, _i]),

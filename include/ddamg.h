@@ -203,6 +203,19 @@ ddamg_status ddamg_solve_device(ddamg_t* h, const void* b, void* x, int nrhs, dd
 ddamg_status ddamg_gmres_plain(ddamg_t* h, const double* b, double* x, int m, int restarts, double tol,
                                ddamg_solve_info* info);
 
+/* bi_cgstab (src/conjugate_gradient.cpp:87-176, driven as Methods::BiCG, src/methods.cpp:3-19):
+ * BiCGstab on D_W from x0 (NULL: zero) until ||s|| < tol ||b||; info->iterations is the
+ * reference's return value (k+1, or max_iter without convergence -> DDAMG_NOT_CONVERGED) */
+ddamg_status ddamg_bicgstab(ddamg_t* h, const double* b, const double* x0, double* x, int max_iter, double tol,
+                            ddamg_solve_info* info);
+/* conjugate_gradient (src/conjugate_gradient.cpp:4-83): CG on D^dagger D x = phi (the operator of
+ * D_D_dagger_phi, src/dirac_operator.cpp:88-92) from x0 = phi until ||r|| < tol ||phi||.
+ * Methods::CG (src/methods.cpp:42-58) calls it with phi = D^dagger b; info->rel_residual is
+ * ||phi - D^dagger D x|| / ||phi||; info->iterations is k+1 at convergence, max_iter without it
+ * (the reference returns 0 there), with DDAMG_NOT_CONVERGED */
+ddamg_status ddamg_cg_normal(ddamg_t* h, const double* phi, double* x, int max_iter, double tol,
+                             ddamg_solve_info* info);
+
 /* ------------------------------------------------------------------ gradient (no reference counterpart) */
 /* L = Re(eta^dagger D^-1 b): solves D psi = b and D^dagger lambda = eta through the same
  * multigrid (D^dagger = sigma_3 D sigma_3) and forms dL/dtheta_mu(x) = out[site*2 + mu] */

@@ -856,6 +856,101 @@ int orc_gmres_plain(const orc_mg* mg, int m, int restarts, double tol, const dou
     return it;
 }
 
+/* ------------------------------------------------------------------ comparison solvers */
+/* bi_cgstab, src/conjugate_gradient.cpp:87-176: BiCGstab on D_phi from x0, ||s|| < tol ||phi||;
+ * returns k+1 at convergence, max_iter otherwise (as the reference). */
+int orc_bicgstab(const orc_mg* mg, const double* phip, const double* x0p, double* xp, int max_iter, double tol) {
+    long n = (long)mg->lv[0].sites * 2;
+    const cplx* phi = (const cplx*)phip;
+    cplx* x = (cplx*)xp;
+    cplx* r = (cplx*)calloc(n, sizeof(cplx));
+    cplx* rt = (cplx*)calloc(n, sizeof(cplx));
+    cplx* d = (cplx*)calloc(n, sizeof(cplx));
+    cplx* s = (cplx*)calloc(n, sizeof(cplx));
+    cplx* t = (cplx*)calloc(n, sizeof(cplx));
+    cplx* Ad = (cplx*)calloc(n, sizeof(cplx));
+    cplx* Dx = (cplx*)calloc(n, sizeof(cplx));
+    cplx alpha = 0, beta, rho, omega = 0, rho2 = 0;
+    int k = 0, ret = max_iter;
+    memcpy(x, x0p, sizeof(cplx) * n);
+    orc_dirac(mg, 0, (const double*)x, (double*)Dx);
+    for (long i = 0; i < n; i++) r[i] = phi[i] + (-1.0) * Dx[i]; /* axpy(phi, Dphi, -1.0, r) */
+    memcpy(rt, r, sizeof(cplx) * n);
+    double norm_phi = sqrt(creal(vdot(phi, phi, n)));
+    while (k < max_iter) {
+        rho = vdot(r, rt, n);
+        if (k == 0) {
+            memcpy(d, r, sizeof(cplx) * n);
+        } else {
+            beta = alpha * rho / (omega * rho2);
+            for (long i = 0; i < n; i++) d[i] = r[i] + beta * (d[i] - omega * Ad[i]);
+        }
+        orc_dirac(mg, 0, (const double*)d, (double*)Ad);
+        alpha = rho / vdot(Ad, rt, n);
+        for (long i = 0; i < n; i++) s[i] = r[i] - alpha * Ad[i];
+        double err = sqrt(creal(vdot(s, s, n)));
+        if (err < tol * norm_phi) {
+            for (long i = 0; i < n; i++) x[i] = x[i] + alpha * d[i];
+            ret = k + 1;
+            break;
+        }
+        orc_dirac(mg, 0, (const double*)s, (double*)t);
+        omega = vdot(s, t, n) / vdot(t, t, n);
+        for (long i = 0; i < n; i++) r[i] = s[i] + (-omega) * t[i]; /* axpy(s, t, -omega, r) */
+        for (long i = 0; i < n; i++) x[i] = x[i] + alpha * d[i] + omega * s[i];
+        rho2 = rho;
+        k++;
+    }
+    free(r); free(rt); free(d); free(s); free(t); free(Ad); free(Dx);
+    return ret;
+}
+
+/* conjugate_gradient, src/conjugate_gradient.cpp:4-83: CG on D_D_dagger_phi (= D^dagger D,
+ * src/dirac_operator.cpp:88-92) with x0 = phi, ||r|| < tol ||phi||; returns k+1 at
+ * convergence, 0 otherwise (as the reference). */
+int orc_cg_normal(const orc_mg* mg, const double* phip, double* xp, int max_iter, double tol) {
+    long n = (long)mg->lv[0].sites * 2;
+    const cplx* phi = (const cplx*)phip;
+    cplx* x = (cplx*)xp;
+    cplx* r = (cplx*)calloc(n, sizeof(cplx));
+    cplx* d = (cplx*)calloc(n, sizeof(cplx));
+    cplx* Ad = (cplx*)calloc(n, sizeof(cplx));
+    cplx* y = (cplx*)calloc(n, sizeof(cplx));
+    cplx alpha, beta;
+    int k = 0, ret = 0;
+    memcpy(x, phi, sizeof(cplx) * n);
+    orc_dirac(mg, 0, (const double*)x, (double*)y);
+    orc_dirac(mg, 1, (const double*)y, (double*)Ad);
+    for (long i = 0; i < n; i++) r[i] = phi[i] - Ad[i];
+    memcpy(d, r, sizeof(cplx) * n);
+    cplx r_norm2 = vdot(r, r, n);
+    double phi_norm2 = sqrt(creal(vdot(phi, phi, n)));
+    while (k < max_iter) {
+        orc_dirac(mg, 0, (const double*)d, (double*)y);
+        orc_dirac(mg, 1, (const double*)y, (double*)Ad);
+        alpha = r_norm2 / vdot(d, Ad, n);
+        for (long i = 0; i < n; i++) {
+            x[i] += alpha * d[i];
+            r[i] -= alpha * Ad[i];
+        }
+        double err_sqr = creal(vdot(r, r, n));
+        double err = sqrt(err_sqr);
+        if (err < tol * phi_norm2) {
+            ret = k + 1;
+            break;
+        }
+        beta = err_sqr / r_norm2;
+        for (long i = 0; i < n; i++) {
+            d[i] *= beta;
+            d[i] += r[i];
+        }
+        r_norm2 = err_sqr;
+        k++;
+    }
+    free(r); free(d); free(Ad); free(y);
+    return ret;
+}
+
 /* ------------------------------------------------------------------ gradient (no reference counterpart) */
 /* dL/dtheta_mu(n) = -Re[ lam(n)^+ (-1/2)(1-sigma_mu)(i U_mu(n)) s psi(n+mu)
  *                       + lam(n+mu)^+ (-1/2)(1+sigma_mu)(-i U*_mu(n)) s psi(n) ]

@@ -82,6 +82,11 @@ int orc_solve(const orc_mg* mg, int cycle, int m, int restarts, double tol, cons
 /* plain GMRES(m) on D_W with no preconditioner (FGMRES_fine_level, include/fgmres.h:153-236) */
 int orc_gmres_plain(const orc_mg* mg, int m, int restarts, double tol, const double* b, double* x);
 
+/* comparison solvers (src/conjugate_gradient.cpp): BiCGstab on D_W from x0, returning k+1 or
+ * max_iter; CG on D^dagger D x = phi from x0 = phi, returning k+1 or 0 */
+int orc_bicgstab(const orc_mg* mg, const double* phi, const double* x0, double* x, int max_iter, double tol);
+int orc_cg_normal(const orc_mg* mg, const double* phi, double* x, int max_iter, double tol);
+
 /* link derivative of L = Re(eta^dagger D^-1 b) given psi = D^-1 b and
  * lambda = D^-dagger eta; out[site*2+mu] = dL/dtheta_mu(site) */
 void orc_link_gradient(const orc_mg* mg, const double* psi, const double* lambda, double* out);

@@ -80,6 +80,10 @@ def lib():
         L.orc_gmres_plain.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _c_dp, _c_dp]
         L.orc_gmres_plain.restype = ctypes.c_int
         L.orc_link_gradient.argtypes = [ctypes.c_void_p, _c_dp, _c_dp, _c_dp]
+        L.orc_bicgstab.argtypes = [ctypes.c_void_p, _c_dp, _c_dp, _c_dp, ctypes.c_int, ctypes.c_double]
+        L.orc_bicgstab.restype = ctypes.c_int
+        L.orc_cg_normal.argtypes = [ctypes.c_void_p, _c_dp, _c_dp, ctypes.c_int, ctypes.c_double]
+        L.orc_cg_normal.restype = ctypes.c_int
         L.orc_rng.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]
         L.orc_rng.restype = ctypes.c_uint64
         L.orc_metropolis.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_uint64,
@@ -287,6 +291,22 @@ class Oracle:
         b = np.ascontiguousarray(b, dtype=np.complex128)
         x = self._out(b.size)
         it = lib().orc_gmres_plain(self.h, m, restarts, tol, _p(b), _p(x))
+        return x, it
+
+    def bicgstab(self, b, x0=None, max_iter=10000, tol=1e-10):
+        """bi_cgstab (src/conjugate_gradient.cpp:87-176); returns (x, k+1 or max_iter)."""
+        b = np.ascontiguousarray(b, dtype=np.complex128)
+        x0 = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, dtype=np.complex128)
+        x = self._out(b.size)
+        it = lib().orc_bicgstab(self.h, _p(b), _p(x0), _p(x), max_iter, tol)
+        return x, it
+
+    def cg_normal(self, phi, max_iter=10000, tol=1e-10):
+        """conjugate_gradient (src/conjugate_gradient.cpp:4-83) on D^dagger D x = phi from x0 = phi;
+        returns (x, k+1 or 0)."""
+        phi = np.ascontiguousarray(phi, dtype=np.complex128)
+        x = self._out(phi.size)
+        it = lib().orc_cg_normal(self.h, _p(phi), _p(x), max_iter, tol)
         return x, it
 
     def link_gradient(self, psi, lam):

@@ -10,6 +10,8 @@
  *   ref_harness ops   <levels> <m0> <params> <conf.bin> <probe.bin> <tvec.bin> <outdir>
  *   ref_harness solve <levels> <m0> <params> <conf.bin> <rhs.bin> <tvec.bin|-> <outdir>
  *                     <cycle:0=V,1=K> <fgmres_m> <fgmres_restarts> <tol>
+ *   ref_harness krylov <levels> <m0> <params> <conf.bin> <rhs.bin> <x0.bin|-> <outdir> <max_iter> <tol>
+ *                     (bi_cgstab from x0, then Methods::CG: conjugate_gradient on D^dagger rhs)
  *
  * conf.bin / rhs.bin use the reference binary record format (src/io.cpp:32-44).
  * probe.bin / tvec.bin / outputs are raw little-endian complex128 arrays
@@ -33,6 +35,7 @@
 
 #define private public
 #include "amg.h"
+#include "conjugate_gradient.h"
 #include "params.h"
 #include "io.h"
 #undef private
@@ -277,6 +280,39 @@ int main(int argc, char** argv) {
         m.precision(17);
         m << "iterations " << iters << "\nsetup_s " << (t1 - t0) << "\nsolve_s " << (t2 - t1) << "\nrelres "
           << std::sqrt(nr / nb) << "\n";
+        return 0;
+    }
+    if (mode == "krylov") {
+        if (argc < 11) {
+            std::cerr << "krylov needs max_iter tol\n";
+            return 2;
+        }
+        const int max_iter = std::atoi(argv[9]);
+        const double tol = std::atof(argv[10]);
+        spinor rhs(mpi::maxSizeH), x0(mpi::maxSizeH), xb(mpi::maxSizeH), xc(mpi::maxSizeH), ddag(mpi::maxSizeH);
+        read_binary(vfile, rhs);
+        if (tfile != "-") {
+            Stream s0;
+            s0.load(tfile);
+            fill_interior(x0, s0.take((size_t)mpi::width_x * mpi::width_t * 2), mpi::width_x, mpi::width_t, 2);
+        }
+        BiCG::max_iter = max_iter;
+        BiCG::tol = tol;
+        CG::max_iter = max_iter;
+        CG::tol = tol;
+        double t0 = now();
+        int itb = bi_cgstab(U, rhs, x0, xb, m0, false);
+        double t1 = now();
+        D_dagger_phi(U, rhs, ddag, m0);  /* Methods::CG (src/methods.cpp:42-58) */
+        double t2 = now();
+        int itc = conjugate_gradient(U, ddag, xc, m0, false);
+        double t3 = now();
+        dump("x_bicg.bin", interior(xb, mpi::width_x, mpi::width_t, 2));
+        dump("x_cg.bin", interior(xc, mpi::width_x, mpi::width_t, 2));
+        std::ofstream m(g_out + "/krylov.txt");
+        m.precision(17);
+        m << "bicg_iterations " << itb << "\nbicg_s " << (t1 - t0) << "\ncg_iterations " << itc << "\ncg_s "
+          << (t3 - t2) << "\n";
         return 0;
     }
     std::cerr << "unknown mode " << mode << "\n";

@@ -36,6 +36,9 @@ CASES = [
     # 64x64, 2 levels, SAP 4x4, Nv = 10, restart 20, beta = 2, 500 sweeps, m0 = -0.18
     dict(name="solve_64x64_l2", Nx=64, Nt=64, levels=2, m0=-0.18,
          rows=[[0, 16, 16, 10, 16, 16]], beta=2.0, sweeps=500, seed=2024, m=20, modes=("solve",)),
+    # the comparison solvers of src/conjugate_gradient.cpp (BiCGstab on D, CG on D^dagger D)
+    dict(name="krylov_32x32", Nx=32, Nt=32, levels=2, m0=-0.15,
+         rows=[[0, 8, 8, 6, 4, 4]], beta=2.0, sweeps=30, seed=12, m=20, modes=("krylov",)),
 ]
 
 OPS_OUT = ["Dphi", "Ddagphi"]
@@ -110,12 +113,25 @@ def make_case(c, work):
         run([harness, "solve", str(L), repr(c["m0"]), pfile, conf, rhsf, "-", sd, "0", str(c["m"]), "50", "1e-10"])
         meta = dict(line.split() for line in open(os.path.join(sd, "solve.txt")))
         out["ref_iters_V_stock"] = int(meta["iterations"])
+    if "krylov" in c["modes"]:
+        kd = os.path.join(work, "krylov")
+        os.makedirs(kd)
+        run([harness, "krylov", str(L), repr(c["m0"]), pfile, conf, rhsf, "-", kd, "10000", "1e-10"])
+        out["ref_x_bicg"] = rd(os.path.join(kd, "x_bicg.bin"))
+        out["ref_x_cg"] = rd(os.path.join(kd, "x_cg.bin"))
+        meta = dict(line.split() for line in open(os.path.join(kd, "krylov.txt")))
+        out["ref_iters_bicg"] = int(meta["bicg_iterations"])
+        out["ref_iters_cg"] = int(meta["cg_iterations"])
     return out
 
 
 def main():
+    """python tests/golden/make_golden.py [case names]  (default: every case)"""
     pyoracle.build()
+    want = set(sys.argv[1:])
     for c in CASES:
+        if want and c["name"] not in want:
+            continue
         work = tempfile.mkdtemp(prefix="golden_")
         try:
             out = make_case(c, work)

@@ -113,3 +113,19 @@ def test_galerkin_identity(golden):
         lhs = o.level_op(l + 1, vc)
         rhs = o.restrict(l, o.level_op(l, o.prolong(l, vc)))
         assert rel(lhs, rhs) < 1e-12
+
+
+def test_krylov_comparison_solvers(golden):
+    """bi_cgstab and conjugate_gradient on D^dagger D (src/conjugate_gradient.cpp) against the
+    reference's own run: same iteration counts, same iterates to rounding."""
+    z = golden("krylov_32x32")
+    o = po.Oracle(int(z["Nx"]), int(z["Nt"]), int(z["levels"]), float(z["m0"]), z["rows"],
+                  po.links_from_theta(z["theta"]))
+    xb, itb = o.bicgstab(z["rhs"])
+    assert itb == int(z["ref_iters_bicg"])
+    assert rel(xb, z["ref_x_bicg"]) < 1e-12
+    xc, itc = o.cg_normal(o.dirac(z["rhs"], True))  # Methods::CG solves with D^dagger rhs
+    assert itc == int(z["ref_iters_cg"])
+    assert rel(xc, z["ref_x_cg"]) < 1e-12
+    for x in (xb, xc):
+        assert np.linalg.norm(o.dirac(x) - z["rhs"]) / np.linalg.norm(z["rhs"]) < 1e-9
