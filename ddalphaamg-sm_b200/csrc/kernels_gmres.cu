@@ -69,7 +69,8 @@ struct GmresK {
 // shared memory and the five partials of a site are summed in a fixed order.
 template <int NI>
 __device__ void apply_own(const GmresK& k, const double2* __restrict__ in, double2* __restrict__ out,
-                          const double2* __restrict__ bsub, int s0, int s1, double2* __restrict__ part) {
+                          const double2* __restrict__ bsub, int s0, int s1, double2* __restrict__ part,
+                          double scale = 1.0) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int dof = k.dof, Nt = k.Nt, Nx = k.Nx;
     const int ntask = (s1 - s0) * 5;
@@ -127,7 +128,7 @@ __device__ void apply_own(const GmresK& k, const double2* __restrict__ in, doubl
     for (int e = threadIdx.x; e < (s1 - s0) * dof; e += blockDim.x) {
         const int sl = e / dof, i = e - sl * dof;
         const double2* pp = part + sl * 5 * dof + i;
-        double2 o = pp[0] - pp[dof] - pp[2 * dof] - pp[3 * dof] - pp[4 * dof];
+        double2 o = scale * (pp[0] - pp[dof] - pp[2 * dof] - pp[3 * dof] - pp[4 * dof]);
         const long ge = (long)(s0 + sl) * dof + i;
         if (bsub) o = bsub[ge] - o;
         out[ge] = o;
@@ -170,6 +171,11 @@ __device__ double2 reduce_slot0(const GmresK& k, const double2* __restrict__ par
     return *tmp;
 }
 
+// The Krylov basis is stored unnormalised: slot i of V holds u_i with v_i = sc[i] u_i (sc in shared
+// memory, identical in every CTA).  The second Gram-Schmidt pass writes u_{j+1} straight into its
+// slot before the norm's grid barrier, so that barrier also publishes it to the neighbours'
+// operator application, and no normalisation pass or extra barrier is needed: three grid
+// barriers per Arnoldi step, plus one per restart for the Hessenberg columns.
 template <int NI>
 __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
     extern __shared__ double2 sh[];
@@ -180,7 +186,8 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
     double2* cn = gm + (m + 1);   // m
     double2* sn = cn + m;         // m
     double2* eta = sn + m;        // m
-    double2* part = eta + m;      // sites per CTA x 5 x dof: per-direction partial products
+    double* sc = reinterpret_cast<double*>(eta + m);  // m+1 scale factors (m+1 double2 reserved)
+    double2* part = eta + m + (m + 1);  // sites per CTA x 5 x dof: per-direction partial products
     __shared__ int s_flag;
     __shared__ double2 s_sum;
     const unsigned G = gridDim.x;
@@ -192,16 +199,17 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
     double2* pA = k.partial;
     double2* pB = pA + (long)G * k.P;
     double2* pC = pB + (long)G * k.P;
+    double2* u0 = k.V;  // the residual lands in slot 0
 
     // x = x0 = b
     for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) k.x[e] = k.b[e];
     if (!grid_barrier(k.bar, k.status, G)) return;
-    apply_own<NI>(k, k.x, k.w, k.b, s0, s1, part);  // w = r = b - D x
+    apply_own<NI>(k, k.x, u0, k.b, s0, s1, part);  // u_0 = r = b - D x
     __syncthreads();
     {
         double rr = 0.0, bb = 0.0;
         for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-            rr += cnorm2(k.w[e]);
+            rr += cnorm2(u0[e]);
             bb += cnorm2(k.b[e]);
         }
         __shared__ double2 red[33];
@@ -223,33 +231,39 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
         converged = true;
     }
     for (int kk = 0; kk < k.restarts && !converged; kk++) {
-        const double inv = 1.0 / err;
-        for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) k.V[e] = inv * k.w[e];
-        if (threadIdx.x == 0) gm[0] = make_double2(err, 0.0);
-        if (!grid_barrier(k.bar, k.status, G)) return;
+        if (threadIdx.x == 0) {
+            gm[0] = make_double2(err, 0.0);
+            sc[0] = 1.0 / err;  // v_0 = r / ||r||
+        }
+        __syncthreads();
         for (int j = 0; j < m; j++) {
-            const double2* vj = k.V + (long)j * n;
-            apply_own<NI>(k, vj, k.w, nullptr, s0, s1, part);
+            // w = D v_j = sc_j D u_j (u_j of the neighbours was published by the last barrier)
+            apply_own<NI>(k, k.V + (long)j * n, k.w, nullptr, s0, s1, part, sc[j]);
             __syncthreads();
-            partial_dots(k, k.w, j + 1, pA, e0, e1, n);
+            partial_dots(k, k.w, j + 1, pA, e0, e1, n);  // (u_i, w)
             if (!grid_barrier(k.bar, k.status, G)) return;
             reduce_partials(k, pA, j + 1, h);
+            for (int i = threadIdx.x; i <= j; i += blockDim.x) h[i] = sc[i] * h[i];  // h_i = (v_i, w)
+            __syncthreads();
             // w -= V h ; reorthogonalise
             for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
                 double2 a = k.w[e];
-                for (int i = 0; i <= j; i++) a = a - cmul(h[i], k.V[(long)i * n + e]);
+                for (int i = 0; i <= j; i++) a = a - cmul(sc[i] * h[i], k.V[(long)i * n + e]);
                 k.w[e] = a;
             }
             __syncthreads();
             partial_dots(k, k.w, j + 1, pB, e0, e1, n);
             if (!grid_barrier(k.bar, k.status, G)) return;
             reduce_partials(k, pB, j + 1, h2);
+            for (int i = threadIdx.x; i <= j; i += blockDim.x) h2[i] = sc[i] * h2[i];
+            __syncthreads();
             {
+                double2* un = k.V + (long)(j + 1) * n;  // u_{j+1}, unnormalised
                 double ss = 0.0;
                 for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
                     double2 a = k.w[e];
-                    for (int i = 0; i <= j; i++) a = a - cmul(h2[i], k.V[(long)i * n + e]);
-                    k.w[e] = a;
+                    for (int i = 0; i <= j; i++) a = a - cmul(sc[i] * h2[i], k.V[(long)i * n + e]);
+                    un[e] = a;
                     ss += cnorm2(a);
                 }
                 __shared__ double2 red2[33];
@@ -257,14 +271,10 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
                 if (threadIdx.x == 0) pC[(long)blockIdx.x * k.P] = t;
             }
             for (int i = threadIdx.x; i <= j; i += blockDim.x) h[i] = h[i] + h2[i];
-            if (!grid_barrier(k.bar, k.status, G)) return;
+            if (!grid_barrier(k.bar, k.status, G)) return;  // also publishes u_{j+1}
             const double hn = sqrt(reduce_slot0(k, pC, &s_sum).x);
-            if (hn > 0) {
-                const double ih = 1.0 / hn;
-                double2* vn = k.V + (long)(j + 1) * n;
-                for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) vn[e] = ih * k.w[e];
-            }
             if (threadIdx.x == 0) {  // FGMRES::rotation (src/fgmres.cpp:99-115) on column j
+                sc[j + 1] = hn > 0 ? 1.0 / hn : 0.0;
                 h[j + 1] = make_double2(hn, 0.0);
                 for (int i = 0; i < j; i++) {
                     double2 tmp = cmulc(cn[i], h[i]) + cmulc(sn[i], h[i + 1]);
@@ -283,13 +293,12 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
             __syncthreads();
             if (blockIdx.x == 0)
                 for (int i = threadIdx.x; i <= j; i += blockDim.x) k.H[(long)j * (m + 1) + i] = h[i];
-            const bool brk = s_flag != 0;
-            if (!grid_barrier(k.bar, k.status, G)) return;  // V_{j+1} and H column j visible
-            if (brk) {
+            if (s_flag) {  // identical in every CTA
                 maxIt = j + 1;
                 break;
             }
         }
+        if (!grid_barrier(k.bar, k.status, G)) return;  // the Hessenberg columns of block 0 visible
         // solve_upper_triangular (src/fgmres.cpp:118-128), column-oriented
         for (int i = threadIdx.x; i < maxIt; i += blockDim.x) eta[i] = gm[i];
         __syncthreads();
@@ -299,17 +308,19 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
             for (int q = threadIdx.x; q < i; q += blockDim.x) eta[q] = eta[q] - cmul(k.H[(long)i * (m + 1) + q], eta[i]);
             __syncthreads();
         }
+        for (int i = threadIdx.x; i < maxIt; i += blockDim.x) eta[i] = sc[i] * eta[i];  // x += sum eta_i v_i
+        __syncthreads();
         for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
             double2 a = k.x[e];
             for (int jj = 0; jj < maxIt; jj++) a = cfma(eta[jj], k.V[(long)jj * n + e], a);
             k.x[e] = a;
         }
         if (!grid_barrier(k.bar, k.status, G)) return;
-        apply_own<NI>(k, k.x, k.w, k.b, s0, s1, part);
+        apply_own<NI>(k, k.x, u0, k.b, s0, s1, part);  // new residual into slot 0
         __syncthreads();
         {
             double rr = 0.0;
-            for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) rr += cnorm2(k.w[e]);
+            for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) rr += cnorm2(u0[e]);
             __shared__ double2 red3[33];
             double2 t = block_sum(make_double2(rr, 0.0), red3);
             if (threadIdx.x == 0) pC[(long)blockIdx.x * k.P] = t;
@@ -329,7 +340,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
 int coarse_gmres_grid(long sites, int sms) { return (int)std::min<long>(sms, std::max<long>(1, (sites + 1) / 2)); }
 static size_t coarse_gmres_smem(long sites, int grid, int m, int dof) {
     const long spc = (sites + grid - 1) / grid;
-    return sizeof(double2) * ((size_t)6 * (m + 1) + (size_t)spc * 5 * dof);
+    return sizeof(double2) * ((size_t)7 * (m + 1) + (size_t)spc * 5 * dof);
 }
 
 void coarse_gmres_prepare(CoarseGmresWork& w, int n, int m, int dof, int device) {
