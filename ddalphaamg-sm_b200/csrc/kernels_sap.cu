@@ -43,6 +43,18 @@ __device__ __forceinline__ float2 level0_hop(const float2* __restrict__ U, int N
     return 0.5f * cmul(coef, u);
 }
 
+// warp sums of N values with one interleaved butterfly (N independent shuffle chains)
+template <int N> __device__ __forceinline__ void warp_sum_n(double2 (&v)[N]) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int g = 0; g < N; g++) {
+            v[g].x += __shfl_xor_sync(0xffffffffu, v[g].x, o);
+            v[g].y += __shfl_xor_sync(0xffffffffu, v[g].y, o);
+        }
+}
+constexpr int kGsBatch = 6;  // Gram-Schmidt coefficients per interleaved butterfly (restart length 5: all)
+
 struct SapKParams {
     int m, restarts;
     double tol, m0;
@@ -55,16 +67,18 @@ struct SapKParams {
 
 
 // Shared memory of one CTA: RB right-hand sides of one Schwarz block.  Vectors are stored
-// [element][rhs] so that the RB values a link element multiplies sit side by side.
+// [rhs][element], so a warp's Gram-Schmidt loads and stores of one right-hand side are
+// contiguous (no bank conflicts); the operator's operand reads are broadcasts either way.
 template <typename V, int RB> struct SapSmem {
-    V* basis;      // (m+1) x NE x RB
-    V* op;         // NE x RB: operand of D_B
+    V* basis;      // (m+1) x RB x NE
+    V* op;         // RB x NE: operand of D_B
     double2* red;  // 2 buffers x warps x RB*(kSapMaxM+1): reductions
     double2* H;    // RB x (m+1) x m, H[r][i*m + j]
     double2* gm;   // RB x (m+1)
     double2* cn;   // RB x m
     double2* sn;   // RB x m
     double2* eta;  // RB x m
+    double2* tot;  // RB x (kSapMaxM+1): CTA totals of the Gram-Schmidt coefficients
     int* flag;     // RB: the Arnoldi estimate met tol
     __device__ SapSmem(unsigned char* raw, int m, int NE, int nw) {
         double2* d = reinterpret_cast<double2*>(raw);
@@ -74,12 +88,14 @@ template <typename V, int RB> struct SapSmem {
         cn = gm + RB * (m + 1);
         sn = cn + RB * m;
         eta = sn + RB * m;
-        flag = reinterpret_cast<int*>(eta + RB * m);
+        tot = eta + RB * m;
+        flag = reinterpret_cast<int*>(tot + RB * (kSapMaxM + 1));
         basis = reinterpret_cast<V*>(flag + ((RB + 3) / 4) * 4);
         op = basis + (size_t)(m + 1) * NE * RB;
     }
     static size_t bytes(int m, int NE, int nw) {
-        return sizeof(double2) * ((size_t)2 * nw * RB * (kSapMaxM + 1) + (size_t)RB * ((m + 1) * m + (m + 1) + 3 * m)) +
+        return sizeof(double2) * ((size_t)2 * nw * RB * (kSapMaxM + 1) +
+                                  (size_t)RB * ((m + 1) * m + (m + 1) + 3 * m + kSapMaxM + 1)) +
                sizeof(int) * ((RB + 3) / 4) * 4 + sizeof(V) * (size_t)(m + 2) * NE * RB;
     }
 };
@@ -155,10 +171,18 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __r
         v = warp_sum(v);
         if (lane == 0) sm.red[((size_t)rbuf * nw + wid) * SL + slot] = v;
     };
-    auto total = [&](int buf, int slot) {
-        double2 t = make_double2(0.0, 0.0);
-        for (int ww = 0; ww < nw; ww++) t += sm.red[((size_t)buf * nw + ww) * SL + slot];
-        return t;
+    auto total = [&](int buf, int slot) {  // four independent load/add chains over the warps
+        const double2* pr = sm.red + (size_t)buf * nw * SL + slot;
+        double2 t0 = make_double2(0.0, 0.0), t1 = t0, t2 = t0, t3 = t0;
+        int ww = 0;
+        for (; ww + 4 <= nw; ww += 4) {
+            t0 += pr[(ww + 0) * SL];
+            t1 += pr[(ww + 1) * SL];
+            t2 += pr[(ww + 2) * SL];
+            t3 += pr[(ww + 3) * SL];
+        }
+        for (; ww < nw; ww++) t0 += pr[ww * SL];
+        return (t0 + t1) + (t2 + t3);
     };
 
     // w = D_B op for all RB vectors (op in shared memory, fully written before the call)
@@ -180,7 +204,7 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __r
                     const int kk = nbk[q][d];
                     if (kk < 0) continue;
                     const V* M = L + ((long)n * 5 + d) * dof * dof + i;
-                    const V* o = op + (size_t)kk * dof * RB;
+                    const V* o = op + (size_t)kk * dof;  // vector r at o[r * NE + j]
                     int j = 0;
                     for (; j + CH <= dof; j += CH) {  // CH link loads in flight
                         V mv[CH];
@@ -189,7 +213,7 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __r
 #pragma unroll
                         for (int u = 0; u < CH; u++)
 #pragma unroll
-                            for (int r = 0; r < RB; r++) acc[r][u & 1] = cfma(mv[u], o[(j + u) * RB + r], acc[r][u & 1]);
+                            for (int r = 0; r < RB; r++) acc[r][u & 1] = cfma(mv[u], o[(size_t)r * NE + j + u], acc[r][u & 1]);
                     }
                     for (; j + 8 <= dof; j += 8) {  // 8 link loads in flight
                         V mv[8];
@@ -198,12 +222,12 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __r
 #pragma unroll
                         for (int u = 0; u < 8; u++)
 #pragma unroll
-                            for (int r = 0; r < RB; r++) acc[r][u & 1] = cfma(mv[u], o[(j + u) * RB + r], acc[r][u & 1]);
+                            for (int r = 0; r < RB; r++) acc[r][u & 1] = cfma(mv[u], o[(size_t)r * NE + j + u], acc[r][u & 1]);
                     }
                     for (; j < dof; j++) {
                         const V mv = __ldg(M + (long)j * dof);
 #pragma unroll
-                        for (int r = 0; r < RB; r++) acc[r][0] = cfma(mv, o[j * RB + r], acc[r][0]);
+                        for (int r = 0; r < RB; r++) acc[r][0] = cfma(mv, o[(size_t)r * NE + j], acc[r][0]);
                     }
                 }
             } else {
@@ -214,13 +238,13 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __r
                     const V h0 = hop[q][DENSE ? 0 : (d - 1) * 2], h1 = hop[q][DENSE ? 0 : (d - 1) * 2 + 1];
 #pragma unroll
                     for (int r = 0; r < RB; r++) {
-                        acc[r][0] = cfma(h0, op[(kk * 2) * RB + r], acc[r][0]);
-                        acc[r][1] = cfma(h1, op[(kk * 2 + 1) * RB + r], acc[r][1]);
+                        acc[r][0] = cfma(h0, op[(size_t)r * NE + kk * 2], acc[r][0]);
+                        acc[r][1] = cfma(h1, op[(size_t)r * NE + kk * 2 + 1], acc[r][1]);
                     }
                 }
             }
 #pragma unroll
-            for (int r = 0; r < RB; r++) w[q][r] = mm * op[(k * dof + i) * RB + r] - (acc[r][0] + acc[r][1]);
+            for (int r = 0; r < RB; r++) w[q][r] = mm * op[(size_t)r * NE + k * dof + i] - (acc[r][0] + acc[r][1]);
         }
     };
     auto store_op = [&](V (&v)[EPT][RB]) {
@@ -228,7 +252,7 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __r
         for (int q = 0; q < EPT; q++)
             if (ev[q])
 #pragma unroll
-                for (int r = 0; r < RB; r++) sm.op[(size_t)sidx(q) * RB + r] = v[q][r];
+                for (int r = 0; r < RB; r++) sm.op[(size_t)r * NE + sidx(q)] = v[q][r];
     };
 
     // x = x0 = b; r = b - D_B x
@@ -276,7 +300,7 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __r
             const R inv = R(1.0 / err[r]);
 #pragma unroll
             for (int q = 0; q < EPT; q++)
-                if (ev[q]) sm.basis[(size_t)sidx(q) * RB + r] = inv * w[q][r];
+                if (ev[q]) sm.basis[(size_t)r * NE + sidx(q)] = inv * w[q][r];
             if (threadIdx.x == 0) sm.gm[r * (m + 1)] = make_double2(err[r], 0.0);
         }
         for (int j = 0; j < m; j++) {
@@ -286,37 +310,60 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __r
             if (!anyarn) break;
             __syncthreads();
             apply(sm.basis + (size_t)j * NE * RB);  // w = D_B V_j
-            // classical Gram-Schmidt coefficients <w, V_i>, i <= j, in one reduction
+            // classical Gram-Schmidt coefficients <w, V_i>, i <= j, in one reduction: the warp sums of up
+            // to kGsBatch coefficients share one interleaved butterfly, and the CTA totals are formed
+            // once (a thread per coefficient) instead of by every thread that needs them
             const int dbuf = rbuf;
 #pragma unroll
             for (int r = 0; r < RB; r++) {
                 if (!arn[r]) continue;
-                for (int i = 0; i <= j; i++) {
-                    double2 s = make_double2(0.0, 0.0);
+                for (int i0 = 0; i0 <= j; i0 += kGsBatch) {
+                    double2 sv[kGsBatch];
 #pragma unroll
-                    for (int q = 0; q < EPT; q++)
-                        if (ev[q]) s = cfmac(to_d(sm.basis[((size_t)i * NE + sidx(q)) * RB + r]), to_d(w[q][r]), s);
-                    partial(s, r * (kSapMaxM + 1) + i);
+                    for (int g2 = 0; g2 < kGsBatch; g2++) {
+                        sv[g2] = make_double2(0.0, 0.0);
+                        if (i0 + g2 <= j)
+#pragma unroll
+                            for (int q = 0; q < EPT; q++)
+                                if (ev[q])
+                                    sv[g2] = cfmac(to_d(sm.basis[((size_t)(i0 + g2) * RB + r) * NE + sidx(q)]),
+                                                   to_d(w[q][r]), sv[g2]);
+                    }
+                    warp_sum_n<kGsBatch>(sv);
+                    if (lane == 0)
+#pragma unroll
+                        for (int g2 = 0; g2 < kGsBatch; g2++)
+                            if (i0 + g2 <= j) sm.red[((size_t)rbuf * nw + wid) * SL + r * (kSapMaxM + 1) + i0 + g2] = sv[g2];
                 }
             }
             __syncthreads();
+            for (int t = threadIdx.x; t < RB * (j + 1); t += blockDim.x) {
+                const int r = t / (j + 1), slot = r * (kSapMaxM + 1) + (t - r * (j + 1));
+                sm.tot[slot] = total(dbuf, slot);
+            }
+            __syncthreads();
             rbuf ^= 1;
+            double2 wn[RB];
 #pragma unroll
             for (int r = 0; r < RB; r++) {
                 double ww = 0.0;
                 if (arn[r]) {
                     for (int i = 0; i <= j; i++) {
-                        const V h = from_d<V>(total(dbuf, r * (kSapMaxM + 1) + i));
+                        const V h = from_d<V>(sm.tot[r * (kSapMaxM + 1) + i]);
 #pragma unroll
                         for (int q = 0; q < EPT; q++)
-                            if (ev[q]) w[q][r] = w[q][r] - cmul(h, sm.basis[((size_t)i * NE + sidx(q)) * RB + r]);
+                            if (ev[q]) w[q][r] = w[q][r] - cmul(h, sm.basis[((size_t)i * RB + r) * NE + sidx(q)]);
                     }
 #pragma unroll
                     for (int q = 0; q < EPT; q++)
                         if (ev[q]) ww += (double)cnorm2(w[q][r]);
                 }
-                partial(make_double2(ww, 0.0), r);
+                wn[r] = make_double2(ww, 0.0);
             }
+            warp_sum_n<RB>(wn);
+            if (lane == 0)
+#pragma unroll
+                for (int r = 0; r < RB; r++) sm.red[((size_t)rbuf * nw + wid) * SL + r] = wn[r];
             __syncthreads();
             double hn[RB];
 #pragma unroll
@@ -326,7 +373,7 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __r
                     const R inv = R(1.0 / hn[r]);
 #pragma unroll
                     for (int q = 0; q < EPT; q++)
-                        if (ev[q]) sm.basis[((size_t)(j + 1) * NE + sidx(q)) * RB + r] = inv * w[q][r];
+                        if (ev[q]) sm.basis[((size_t)(j + 1) * RB + r) * NE + sidx(q)] = inv * w[q][r];
                 }
             }
             rbuf ^= 1;
@@ -336,7 +383,7 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __r
                 double2* cn = sm.cn + r * m;
                 double2* sn = sm.sn + r * m;
                 double2* gm = sm.gm + r * (m + 1);
-                for (int i = 0; i <= j; i++) H[i * m + j] = total(dbuf, r * (kSapMaxM + 1) + i);
+                for (int i = 0; i <= j; i++) H[i * m + j] = sm.tot[r * (kSapMaxM + 1) + i];
                 H[(j + 1) * m + j] = make_double2(hn[r], 0.0);
                 for (int i = 0; i < j; i++) {  // FGMRES::rotation (src/fgmres.cpp:99-115)
                     double2 hij = H[i * m + j], hi1 = H[(i + 1) * m + j];
@@ -382,7 +429,7 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __r
                 if (!ev[q]) continue;
                 V a = x[q][r];
                 for (int jj = 0; jj < maxIt[r]; jj++)
-                    a = cfma(from_d<V>(sm.eta[r * m + jj]), sm.basis[((size_t)jj * NE + sidx(q)) * RB + r], a);
+                    a = cfma(from_d<V>(sm.eta[r * m + jj]), sm.basis[((size_t)jj * RB + r) * NE + sidx(q)], a);
                 x[q][r] = a;
             }
         }
@@ -885,7 +932,7 @@ static void launch_sap_k(cudaStream_t s, int threads, const Geom& g, const V* L,
 static int pick_rb(int nrhs, int ept, int m, int NE, int threads, size_t vbytes) {
     auto fits = [&](int rb) {
         const size_t smem = sizeof(double2) * ((size_t)2 * (threads / 32) * rb * (kSapMaxM + 1) +
-                                               (size_t)rb * ((m + 1) * m + (m + 1) + 3 * m)) +
+                                               (size_t)rb * ((m + 1) * m + (m + 1) + 3 * m + kSapMaxM + 1)) +
                             16 + vbytes * (size_t)(m + 2) * NE * rb;
         return smem <= 227 * 1024 && ept * rb * (int)(vbytes / 8) <= 8;  // register budget
     };
@@ -906,7 +953,7 @@ static bool rb_admissible(int rb, int nrhs, int m, int NE, size_t vbytes) {
     if (rb == 1) return true;
     if (rb > nrhs || ept != 1 || (threads > 512 && rb > 2)) return false;
     const size_t smem = sizeof(double2) * ((size_t)2 * (threads / 32) * rb * (kSapMaxM + 1) +
-                                           (size_t)rb * ((m + 1) * m + (m + 1) + 3 * m)) +
+                                           (size_t)rb * ((m + 1) * m + (m + 1) + 3 * m + kSapMaxM + 1)) +
                         16 + vbytes * (size_t)(m + 2) * NE * rb;
     return smem <= 227 * 1024 && rb * (int)(vbytes / 8) <= 8;  // shared memory and register budget
 }
