@@ -681,9 +681,19 @@ def profile_case(name):
     """One small invocation of a hot kernel for an ncu capture (no timing, no JSON line):
     sap-l1   the bench workload's FP64 solve (level-1 sap_block_kernel sweeps inside);
     tc-apply one batched FP32 level-1 SAP sweep pair on 512x512 with 64 right-hand sides
-             (tc_block_apply_kernel, the tensor-core block operator)."""
+             (tc_block_apply_kernel, the tensor-core block operator);
+    krylov   20 BiCGstab iterations on a 1024x1024 field (bicg_* kernels, 11 fields of 32 MiB)."""
     import ddamg
 
+    if name == "krylov":
+        N = 1024
+        th, _ = ddamg.gauge_metropolis(N, N, 4.0, 10, 3)
+        s = ddamg.Solver(ddamg.default_params(N, N, 2, -0.07, [[0, 128, 128, 4, 128, 128]]))
+        s.load_gauge(np.exp(1j * th))
+        _, info = s.bi_cgstab(ddamg.gaussian_field(2 * N * N, 77), max_iter=20)
+        print("krylov: BiCGstab iterations", info.iterations)
+        s.close()
+        return 0
     if name == "sap-l1":
         w = WORKLOAD
         U, b, _, _ = make_inputs()
@@ -718,7 +728,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the 1024x1024 and 512x512 batched lines")
-    ap.add_argument("--profile-case", choices=["sap-l1", "tc-apply"],
+    ap.add_argument("--profile-case", choices=["sap-l1", "tc-apply", "krylov"],
                     help="run one small case of a hot kernel for an ncu capture and exit")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
