@@ -190,6 +190,16 @@ def level_geoms():
     return gs
 
 
+def max_over_ranks(value, dist, device):
+    """The slowest rank's figure: every rank contributes its own, all receive the maximum (replicas
+    run the same workload, so the job takes as long as the slowest)."""
+    import torch
+
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---------------------------------------------------------------- reference arm
 def run_reference_arm(args, rank, world):
     if rank != 0:
@@ -312,9 +322,7 @@ def run_ours(args, rank, world, local_rank):
     step_ms = [starts[k].elapsed_time(ends[k]) for k in range(args.steps)]
     total_ms = sum(step_ms)
     if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{local_rank}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = max_over_ranks(total_ms, dist, f"cuda:{local_rank}")
     ms_per_step = total_ms / args.steps
     clocks = clk.summary()
     x = x_dev.cpu().numpy().view(np.complex128)
@@ -388,9 +396,7 @@ def run_ours(args, rank, world, local_rank):
             e2e_ms.append(1e3 * (t1 - t0))
     e2e = statistics.median(e2e_ms)
     if dist:
-        t = torch.tensor([e2e], device=f"cuda:{local_rank}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e = float(t.item())
+        e2e = max_over_ranks(e2e, dist, f"cuda:{local_rank}")
     # ---- secondary: mixed precision on the same workload, D_W bandwidth
     sec = {}
     if rank == 0:
