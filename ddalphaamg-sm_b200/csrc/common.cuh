@@ -81,6 +81,23 @@ DDAMG_HD float2 cdiv(float2 a, float2 b) {
     }
 }
 
+// ---------------------------------------------------------------- 256-bit site accesses
+// One 32-byte access for the two spin components of an FP64 fine-lattice site (ld.global.nc.v4.f64 /
+// st.global.v4.f64, sm_100).  The address must be 32-byte aligned: device buffers from cudaMalloc and
+// site offsets (32 bytes each) keep it; callers that take outside pointers check first.
+__device__ __forceinline__ void ld2w(const double2* __restrict__ p, double2& a, double2& b) {
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y) : "l"(p));
+}
+// the same through the coherent path, for a field the kernel also writes
+__device__ __forceinline__ void ld2wc(const double2* p, double2& a, double2& b) {
+    asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y) : "l"(p)
+                 : "memory");
+}
+__device__ __forceinline__ void st2w(double2* p, double2 a, double2 b) {
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y)
+                 : "memory");
+}
+
 // ---------------------------------------------------------------- warp / block reductions
 __device__ __forceinline__ double2 warp_sum(double2 v) {
 #pragma unroll

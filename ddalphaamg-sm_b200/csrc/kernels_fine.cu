@@ -21,11 +21,13 @@ __device__ __forceinline__ void st2(double2* p, double2 a, double2 b) {
 __device__ __forceinline__ void st2(float2* p, float2 a, float2 b) {
     *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
 }
+__device__ __forceinline__ void ld2w(const float2* __restrict__ p, float2& a, float2& b) { ld2(p, a, b); }
+__device__ __forceinline__ void st2w(float2* p, float2 a, float2 b) { st2(p, a, b); }
 
 // D_phi / D_dagger_phi, src/dirac_operator.cpp:24-85, written with the spin projections
 // (1 -/+ sigma_mu) factored: each hop is one link multiply.  sigma_0 = sigma_x acts along t
 // (mu = 0), sigma_1 = sigma_y along x (mu = 1); the t-wrap hop carries the antiperiodic sign.
-template <typename V, bool DAG, bool RESID>
+template <typename V, bool DAG, bool RESID, bool W = false>
 __global__ void __launch_bounds__(256) wilson_kernel(const V* __restrict__ U, const V* __restrict__ in,
                                                      V* __restrict__ out, const V* __restrict__ b, int Nx, int Nt,
                                                      typename RealOf<V>::R m0, long stride) {
@@ -41,17 +43,25 @@ __global__ void __launch_bounds__(256) wilson_kernel(const V* __restrict__ U, co
     const int r0 = x * Nt + tp, l0 = x * Nt + tm, r1 = xp * Nt + t, l1 = xm * Nt + t;
     const R sr = (t == Nt - 1) ? R(-1) : R(1), sl = (t == 0) ? R(-1) : R(1);
 
-    V u0, u1, ul0, ul1, dummy;
-    ld2(U + 2 * n, u0, u1);
+    V u0, u1, ul0, ul1;
+    V p0, p1, a0, a1, c0, c1, e0, e1, g0, g1;
+    if (W) {
+        ld2w(U + 2 * n, u0, u1);
+        ld2w(in + 2 * n, p0, p1);
+        ld2w(in + 2 * r0, a0, a1);
+        ld2w(in + 2 * r1, c0, c1);
+        ld2w(in + 2 * l0, e0, e1);
+        ld2w(in + 2 * l1, g0, g1);
+    } else {
+        ld2(U + 2 * n, u0, u1);
+        ld2(in + 2 * n, p0, p1);
+        ld2(in + 2 * r0, a0, a1);
+        ld2(in + 2 * r1, c0, c1);
+        ld2(in + 2 * l0, e0, e1);
+        ld2(in + 2 * l1, g0, g1);
+    }
     ul0 = __ldg(U + 2 * l0);
     ul1 = __ldg(U + 2 * l1 + 1);
-    (void)dummy;
-    V p0, p1, a0, a1, c0, c1, e0, e1, g0, g1;
-    ld2(in + 2 * n, p0, p1);
-    ld2(in + 2 * r0, a0, a1);
-    ld2(in + 2 * r1, c0, c1);
-    ld2(in + 2 * l0, e0, e1);
-    ld2(in + 2 * l1, g0, g1);
     V s0, s1;
     if (!DAG) {
         V a = sr * cmul(u0, a0 - a1);             // +t: (1 - sigma_x)
@@ -73,11 +83,13 @@ __global__ void __launch_bounds__(256) wilson_kernel(const V* __restrict__ U, co
     V o1 = mm * p1 - h * s1;
     if (RESID) {
         V b0, b1;
-        ld2(b + ro + 2 * n, b0, b1);
+        if (W) ld2w(b + ro + 2 * n, b0, b1);
+        else ld2(b + ro + 2 * n, b0, b1);
         o0 = b0 - o0;
         o1 = b1 - o1;
     }
-    st2(out + 2 * n, o0, o1);
+    if (W) st2w(out + 2 * n, o0, o1);
+    else st2(out + 2 * n, o0, o1);
 }
 
 template <typename V>
@@ -86,6 +98,20 @@ void launch_wilson(cudaStream_t s, const V* U, const V* in, V* out, const V* b, 
     typedef typename RealOf<V>::R R;
     dim3 grid(ceil_div((long)Nx * Nt, 256), nrhs);
     long stride = 2L * Nx * Nt;
+    // FP64 sites are 32 bytes: one 256-bit access per site when every field starts on a 32-byte
+    // boundary (sites and right-hand sides then stay on one)
+    auto a32 = [](const void* p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 31) == 0; };
+    const bool wide = sizeof(V) == 16 && a32(U) && a32(in) && a32(out) && a32(b);
+    if (wide) {
+        if (dagger) {
+            if (b) DDAMG_LAUNCH((wilson_kernel<V, true, true, true>), grid, 256, 0, s, U, in, out, b, Nx, Nt, (R)m0, stride);
+            else DDAMG_LAUNCH((wilson_kernel<V, true, false, true>), grid, 256, 0, s, U, in, out, b, Nx, Nt, (R)m0, stride);
+        } else {
+            if (b) DDAMG_LAUNCH((wilson_kernel<V, false, true, true>), grid, 256, 0, s, U, in, out, b, Nx, Nt, (R)m0, stride);
+            else DDAMG_LAUNCH((wilson_kernel<V, false, false, true>), grid, 256, 0, s, U, in, out, b, Nx, Nt, (R)m0, stride);
+        }
+        return;
+    }
     if (dagger) {
         if (b) DDAMG_LAUNCH((wilson_kernel<V, true, true>), grid, 256, 0, s, U, in, out, b, Nx, Nt, (R)m0, stride);
         else DDAMG_LAUNCH((wilson_kernel<V, true, false>), grid, 256, 0, s, U, in, out, b, Nx, Nt, (R)m0, stride);

@@ -40,7 +40,8 @@ __device__ __forceinline__ void wilson_at(const double2* __restrict__ U, int Nx,
     const int xp = (x + 1 == Nx) ? 0 : x + 1, xm = (x == 0) ? Nx - 1 : x - 1;
     const int r0 = x * Nt + tp, l0 = x * Nt + tm, r1 = xp * Nt + t, l1 = xm * Nt + t;
     const double sr = (t == Nt - 1) ? -1.0 : 1.0, sl = (t == 0) ? -1.0 : 1.0;
-    const double2 u0 = __ldg(U + 2 * n), u1 = __ldg(U + 2 * n + 1);
+    double2 u0, u1;
+    ld2w(U + 2 * n, u0, u1);
     const double2 ul0 = __ldg(U + 2 * l0), ul1 = __ldg(U + 2 * l1 + 1);
     double2 p0, p1, a0, a1, c0, c1, e0, e1, g0, g1;
     fld(n, p0, p1);
@@ -141,11 +142,13 @@ __global__ void __launch_bounds__(256) bicg_dir_kernel(KrylovVecs k) {
     const double2 omega = st->omega;
     const double2 beta = it ? cdiv(cmul(st->alpha, st->rho), cmul(omega, st->rho_prev)) : make_double2(0.0, 0.0);
     auto dir = [&](int m, double2& a, double2& c) {
-        a = __ldg(k.r + 2 * m);
-        c = __ldg(k.r + 2 * m + 1);
+        ld2w(k.r + 2 * m, a, c);
         if (it) {
-            a = a + cmul(beta, __ldg(dp + 2 * m) - cmul(omega, __ldg(Adp + 2 * m)));
-            c = c + cmul(beta, __ldg(dp + 2 * m + 1) - cmul(omega, __ldg(Adp + 2 * m + 1)));
+            double2 d0, d1, A0, A1;
+            ld2w(dp + 2 * m, d0, d1);
+            ld2w(Adp + 2 * m, A0, A1);
+            a = a + cmul(beta, d0 - cmul(omega, A0));
+            c = c + cmul(beta, d1 - cmul(omega, A1));
         }
     };
     double2 q[1] = {make_double2(0.0, 0.0)};
@@ -153,11 +156,11 @@ __global__ void __launch_bounds__(256) bicg_dir_kernel(KrylovVecs k) {
         double2 o0, o1, d0, d1;
         wilson_at<false>(k.U, k.Nx, k.Nt, k.m0, n, dir, o0, o1);
         dir(n, d0, d1);
-        dn[2 * n] = d0;
-        dn[2 * n + 1] = d1;
-        Adn[2 * n] = o0;
-        Adn[2 * n + 1] = o1;
-        q[0] = cfmac(__ldg(k.rt + 2 * n), o0, cfmac(__ldg(k.rt + 2 * n + 1), o1, q[0]));  // sum A d conj(r~)
+        st2w(dn + 2 * n, d0, d1);
+        st2w(Adn + 2 * n, o0, o1);
+        double2 t0, t1;
+        ld2w(k.rt + 2 * n, t0, t1);
+        q[0] = cfmac(t0, o0, cfmac(t1, o1, q[0]));  // sum A d conj(r~)
     }
     __shared__ double2 tot[1];
     if (reduce_last<1>(q, k.part, &k.st->ticket, tot) && threadIdx.x == 0) k.st->alpha = cdiv(st->rho, tot[0]);
@@ -172,18 +175,19 @@ __global__ void __launch_bounds__(256) bicg_s_kernel(KrylovVecs k) {
     const double2* Ad = k.Ad[it & 1];
     const double2 alpha = st->alpha;
     auto sv = [&](int m, double2& a, double2& c) {
-        a = __ldg(k.r + 2 * m) - cmul(alpha, __ldg(Ad + 2 * m));
-        c = __ldg(k.r + 2 * m + 1) - cmul(alpha, __ldg(Ad + 2 * m + 1));
+        double2 r0, r1, A0, A1;
+        ld2w(k.r + 2 * m, r0, r1);
+        ld2w(Ad + 2 * m, A0, A1);
+        a = r0 - cmul(alpha, A0);
+        c = r1 - cmul(alpha, A1);
     };
     double2 q[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < sites; n += gridDim.x * blockDim.x) {
         double2 t0, t1, s0, s1;
         wilson_at<false>(k.U, k.Nx, k.Nt, k.m0, n, sv, t0, t1);
         sv(n, s0, s1);
-        k.s[2 * n] = s0;
-        k.s[2 * n + 1] = s1;
-        k.t[2 * n] = t0;
-        k.t[2 * n + 1] = t1;
+        st2w(k.s + 2 * n, s0, s1);
+        st2w(k.t + 2 * n, t0, t1);
         q[0] = cfmac(t0, s0, cfmac(t1, s1, q[0]));  // sum s conj(t)
         q[1] = cfmac(t0, t0, cfmac(t1, t1, q[1]));
         q[2] = cfmac(s0, s0, cfmac(s1, s1, q[2]));
@@ -212,17 +216,20 @@ __global__ void __launch_bounds__(256) bicg_update_kernel(KrylovVecs k) {
     const double2 alpha = st->alpha, omega = st->omega;
     double2 q[1] = {make_double2(0.0, 0.0)};
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < sites; n += gridDim.x * blockDim.x) {
-        for (int c = 0; c < 2; c++) {
-            const int e = 2 * n + c;
-            if (done == 1) {
-                k.x[e] = k.x[e] + cmul(alpha, d[e]);
-            } else {
-                const double2 s = k.s[e];
-                const double2 r = s - cmul(omega, k.t[e]);
-                k.r[e] = r;
-                k.x[e] = (k.x[e] + cmul(alpha, d[e])) + cmul(omega, s);
-                q[0] = cfmac(k.rt[e], r, q[0]);
-            }
+        double2 x0, x1, d0, d1;
+        ld2wc(k.x + 2 * n, x0, x1);
+        ld2w(d + 2 * n, d0, d1);
+        if (done == 1) {
+            st2w(k.x + 2 * n, x0 + cmul(alpha, d0), x1 + cmul(alpha, d1));
+        } else {
+            double2 s0, s1, t0, t1, q0, q1;
+            ld2w(k.s + 2 * n, s0, s1);
+            ld2w(k.t + 2 * n, t0, t1);
+            ld2w(k.rt + 2 * n, q0, q1);
+            const double2 r0 = s0 - cmul(omega, t0), r1 = s1 - cmul(omega, t1);
+            st2w(k.r + 2 * n, r0, r1);
+            st2w(k.x + 2 * n, (x0 + cmul(alpha, d0)) + cmul(omega, s0), (x1 + cmul(alpha, d1)) + cmul(omega, s1));
+            q[0] = cfmac(q0, r0, cfmac(q1, r1, q[0]));
         }
     }
     __shared__ double2 tot[1];
@@ -262,7 +269,7 @@ __global__ void __launch_bounds__(256) cg_init_b_kernel(KrylovVecs k) {
     double2 q[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < sites; n += gridDim.x * blockDim.x) {
         double2 o0, o1;
-        wilson_at<true>(k.U, k.Nx, k.Nt, k.m0, n, [&](int m, double2& a, double2& c) { a = __ldg(k.y + 2 * m); c = __ldg(k.y + 2 * m + 1); },
+        wilson_at<true>(k.U, k.Nx, k.Nt, k.m0, n, [&](int m, double2& a, double2& c) { ld2w(k.y + 2 * m, a, c); },
                         o0, o1);
         const double2 p0 = k.b[2 * n], p1 = k.b[2 * n + 1];
         const double2 r0 = p0 - o0, r1 = p1 - o1;
@@ -292,24 +299,24 @@ __global__ void __launch_bounds__(256) cg_y_kernel(KrylovVecs k) {
     double2* dn = k.d[it & 1];
     const double2 beta = st->beta;
     auto dir = [&](int m, double2& a, double2& c) {
-        a = cmul(__ldg(dp + 2 * m), beta) + __ldg(k.r + 2 * m);
-        c = cmul(__ldg(dp + 2 * m + 1), beta) + __ldg(k.r + 2 * m + 1);
+        double2 d0, d1, r0, r1;
+        ld2w(dp + 2 * m, d0, d1);
+        ld2w(k.r + 2 * m, r0, r1);
+        a = cmul(d0, beta) + r0;
+        c = cmul(d1, beta) + r1;
     };
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < sites; n += gridDim.x * blockDim.x) {
         double2 o0, o1;
         if (it == 0) {
             wilson_at<false>(k.U, k.Nx, k.Nt, k.m0, n,
-                             [&](int m, double2& a, double2& c) { a = __ldg(dn + 2 * m); c = __ldg(dn + 2 * m + 1); },
-                             o0, o1);
+                             [&](int m, double2& a, double2& c) { ld2w(dn + 2 * m, a, c); }, o0, o1);
         } else {
             wilson_at<false>(k.U, k.Nx, k.Nt, k.m0, n, dir, o0, o1);
             double2 d0, d1;
             dir(n, d0, d1);
-            dn[2 * n] = d0;
-            dn[2 * n + 1] = d1;
+            st2w(dn + 2 * n, d0, d1);
         }
-        k.y[2 * n] = o0;
-        k.y[2 * n + 1] = o1;
+        st2w(k.y + 2 * n, o0, o1);
     }
 }
 // A d = D^dagger y; alpha = (r, r) / (d, A d)
@@ -322,11 +329,12 @@ __global__ void __launch_bounds__(256) cg_ad_kernel(KrylovVecs k) {
     double2 q[1] = {make_double2(0.0, 0.0)};
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < sites; n += gridDim.x * blockDim.x) {
         double2 o0, o1;
-        wilson_at<true>(k.U, k.Nx, k.Nt, k.m0, n, [&](int m, double2& a, double2& c) { a = __ldg(k.y + 2 * m); c = __ldg(k.y + 2 * m + 1); },
+        wilson_at<true>(k.U, k.Nx, k.Nt, k.m0, n, [&](int m, double2& a, double2& c) { ld2w(k.y + 2 * m, a, c); },
                         o0, o1);
-        k.Ad[0][2 * n] = o0;
-        k.Ad[0][2 * n + 1] = o1;
-        q[0] = cfmac(o0, d[2 * n], cfmac(o1, d[2 * n + 1], q[0]));  // sum d conj(A d)
+        st2w(k.Ad[0] + 2 * n, o0, o1);
+        double2 d0, d1;
+        ld2w(d + 2 * n, d0, d1);
+        q[0] = cfmac(o0, d0, cfmac(o1, d1, q[0]));  // sum d conj(A d)
     }
     __shared__ double2 tot[1];
     if (reduce_last<1>(q, k.part, &k.st->ticket, tot) && threadIdx.x == 0) k.st->alpha = cdiv(st->rnorm2, tot[0]);
@@ -341,13 +349,16 @@ __global__ void __launch_bounds__(256) cg_update_kernel(KrylovVecs k) {
     const double2 alpha = st->alpha;
     double2 q[1] = {make_double2(0.0, 0.0)};
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < sites; n += gridDim.x * blockDim.x) {
-        for (int c = 0; c < 2; c++) {
-            const int e = 2 * n + c;
-            k.x[e] = k.x[e] + cmul(alpha, d[e]);
-            const double2 r = k.r[e] - cmul(alpha, k.Ad[0][e]);
-            k.r[e] = r;
-            q[0] = cfmac(r, r, q[0]);
-        }
+        double2 x0, x1, d0, d1, r0, r1, A0, A1;
+        ld2wc(k.x + 2 * n, x0, x1);
+        ld2w(d + 2 * n, d0, d1);
+        ld2wc(k.r + 2 * n, r0, r1);
+        ld2w(k.Ad[0] + 2 * n, A0, A1);
+        st2w(k.x + 2 * n, x0 + cmul(alpha, d0), x1 + cmul(alpha, d1));
+        r0 = r0 - cmul(alpha, A0);
+        r1 = r1 - cmul(alpha, A1);
+        st2w(k.r + 2 * n, r0, r1);
+        q[0] = cfmac(r0, r0, cfmac(r1, r1, q[0]));
     }
     __shared__ double2 tot[1];
     if (reduce_last<1>(q, k.part, &k.st->ticket, tot) && threadIdx.x == 0) {
