@@ -154,6 +154,8 @@ void launch_krylov_init(cudaStream_t s, int solver, const KrylovWork& w, const d
                         double tol, int max_iter);
 void launch_krylov_iterations(cudaStream_t s, int solver, const KrylovWork& w, const double2* U, int Nx, int Nt,
                               double m0, double tol, int max_iter, int count);
+// one-thread kernel for the body of a graph while node: condition = (the solve is still running)
+void launch_krylov_continue(cudaStream_t s, cudaGraphConditionalHandle hc, const KrylovWork& w);
 
 // ------------------------------------------------------------ coarsest GMRES (kernels_gmres.cu)
 struct CoarseGmresWork {

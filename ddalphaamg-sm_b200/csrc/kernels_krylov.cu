@@ -380,6 +380,11 @@ __global__ void __launch_bounds__(256) cg_update_kernel(KrylovVecs k) {
     }
 }
 
+// sets the condition of the solve graph's while node: run another body while the solve is going
+__global__ void krylov_continue_kernel(cudaGraphConditionalHandle hc, const KrylovState* st) {
+    cudaGraphSetConditional(hc, st->done < 2 ? 1u : 0u);
+}
+
 // ---------------------------------------------------------------- host side
 // a few CTAs per SM with grid-stride loops: enough warps to keep HBM busy, few partial sums for
 // the last CTA to add
@@ -438,6 +443,10 @@ void launch_krylov_iterations(cudaStream_t s, int solver, const KrylovWork& w, c
             DDAMG_LAUNCH(cg_update_kernel, G, 256, 0, s, k);
         }
     }
+}
+
+void launch_krylov_continue(cudaStream_t s, cudaGraphConditionalHandle hc, const KrylovWork& w) {
+    DDAMG_LAUNCH(krylov_continue_kernel, 1, 1, 0, s, hc, w.st);
 }
 
 }  // namespace ddamg

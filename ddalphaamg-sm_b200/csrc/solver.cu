@@ -1537,11 +1537,56 @@ static void krylov_alloc(ddamg_handle* h) {
 }
 
 // bi_cgstab (solver 0) or conjugate_gradient on D^dagger D (solver 1), src/conjugate_gradient.cpp.
-// Iterations are queued in batches of kKrylovBatch (replayed from a CUDA graph when cuda_graphs is
-// set); the next batch is queued before the device's done word of the current one is read, so
-// the GPU never waits for the host.  info->iterations follows the reference's count; the true
-// residual is recomputed for the system the solver iterates on.
+// With cuda_graphs set the whole iteration runs on the device: one graph whose while node repeats a
+// body of kKrylovBody iterations and a one-thread kernel that keeps the loop going while the done
+// word is clear (the device sets it at convergence or at max_iter, so the loop is bounded).
+// Otherwise (or if the graph cannot be built) iterations are queued in batches of kKrylovBatch and
+// the next batch is queued before the done word of the current one is read.  info->iterations
+// follows the reference's count; the true residual is recomputed for the system the solver
+// iterates on.
 constexpr int kKrylovBatch = 16;
+constexpr int kKrylovBody = 4;
+
+// the device-driven solve graph; nullptr if this driver or runtime cannot build it
+static cudaGraphExec_t krylov_while_graph(ddamg_handle* h, int solver, const KrylovWork& w, const Geom& g,
+                                          double tol, int max_iter) {
+    cudaStream_t s = h->s;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const long long l0 = g_launches;
+    bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess;
+    cudaGraphConditionalHandle hc{};
+    ok = ok && cudaGraphConditionalHandleCreate(&hc, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = hc;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    ok = ok && cudaGraphAddNode(&node, graph, nullptr, 0, &np) == cudaSuccess;
+    if (ok && cudaStreamBeginCaptureToGraph(s, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+        try {
+            launch_krylov_iterations(s, solver, w, h->lv[0].d.U, g.Nx, g.Nt, h->p.m0, tol, max_iter, kKrylovBody);
+            launch_krylov_continue(s, hc, w);
+        } catch (...) {
+            ok = false;
+        }
+        cudaGraph_t body = nullptr;
+        if (cudaStreamEndCapture(s, &body) != cudaSuccess) ok = false;
+    } else {
+        ok = false;
+    }
+    ok = ok && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    g_launches = l0;  // recorded, not run; counted after the solve
+    if (!ok) {
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        return nullptr;
+    }
+    return exec;
+}
 static ddamg_status krylov_run(ddamg_handle* h, int solver, const double* b, const double* x0, double* x,
                                int max_iter, double tol, ddamg_solve_info* info) {
     if (!h->gauge) throw ParamFailure{"no gauge field loaded"};
@@ -1571,9 +1616,18 @@ static ddamg_status krylov_run(ddamg_handle* h, int solver, const double* b, con
         if (x0) DDAMG_CUDA_TRY(cudaMemcpyAsync(w.x, x0, sizeof(double2) * n, cudaMemcpyHostToDevice, s));
         else DDAMG_CUDA_TRY(cudaMemsetAsync(w.x, 0, sizeof(double2) * n, s));
     }
+    cudaGraphExec_t wexec = (h->p.cuda_graphs && !h->prof) ? krylov_while_graph(h, solver, w, g, tol, max_iter)
+                                                          : nullptr;
+    {
+        const std::string note = std::string(solver == 0 ? "bicgstab" : "cg_normal") +
+                                 (wexec ? ": device loop (graph while node, " + std::to_string(kKrylovBody) +
+                                              " iterations per body)\n"
+                                        : ": host-queued batches of " + std::to_string(kKrylovBatch) + " iterations\n");
+        if (h->tune_log.find(note) == std::string::npos) h->tune_log += note;
+    }
     cudaGraphExec_t exec = nullptr;
     long long graph_kernels = 0;
-    if (h->p.cuda_graphs && !h->prof) {  // one batch of iterations as a graph
+    if (!wexec && h->p.cuda_graphs && !h->prof) {  // one batch of iterations as a graph
         cudaGraph_t graph = nullptr;
         const long long l0 = g_launches;
         bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed) == cudaSuccess;
@@ -1603,6 +1657,10 @@ static ddamg_status krylov_run(ddamg_handle* h, int solver, const double* b, con
         DDAMG_CUDA_TRY(cudaEventRecord(h->ev0, s));
         launch_krylov_init(s, solver, w, U, g.Nx, g.Nt, h->p.m0, tol, max_iter);
         long launched = 0;
+        if (wexec) {  // the whole iteration on the device
+            DDAMG_CUDA_TRY(cudaGraphLaunch(wexec, s));
+            launched = max_iter;
+        }
         auto enqueue = [&](int slot) {
             if (exec) {
                 DDAMG_CUDA_TRY(cudaGraphLaunch(exec, s));
@@ -1614,11 +1672,13 @@ static ddamg_status krylov_run(ddamg_handle* h, int solver, const double* b, con
             DDAMG_CUDA_TRY(cudaEventRecord(evb[slot], s));
             launched += kKrylovBatch;
         };
-        enqueue(0);
-        for (int i = 0;; i++) {
-            if (launched < max_iter) enqueue((i + 1) & 1);
-            DDAMG_CUDA_TRY(cudaEventSynchronize(evb[i & 1]));
-            if (hd[i & 1] >= 2) break;
+        if (!wexec) {
+            enqueue(0);
+            for (int i = 0;; i++) {
+                if (launched < max_iter) enqueue((i + 1) & 1);
+                DDAMG_CUDA_TRY(cudaEventSynchronize(evb[i & 1]));
+                if (hd[i & 1] >= 2) break;
+            }
         }
         DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, s));
         // true residual of the iterated system: b - D x (BiCGstab), phi - D^dagger D x (CG)
@@ -1636,6 +1696,7 @@ static ddamg_status krylov_run(ddamg_handle* h, int solver, const double* b, con
         DDAMG_CUDA_TRY(cudaMemcpyAsync(nn, h->dn, sizeof(nn), cudaMemcpyDeviceToHost, s));
         DDAMG_CUDA_TRY(cudaMemcpyAsync(x, w.x, sizeof(double2) * n, cudaMemcpyDeviceToHost, s));
         sync(h);
+        if (wexec) g_launches += (long long)(st.k / kKrylovBody + 1) * (3 * kKrylovBody + 1);
         float ms = 0;
         DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
         const double rel = nn[1] > 0 ? std::sqrt(nn[0] / nn[1]) : 0.0;
@@ -1657,10 +1718,12 @@ static ddamg_status krylov_run(ddamg_handle* h, int solver, const double* b, con
         for (cudaEvent_t e : evb)
             if (e) cudaEventDestroy(e);
         if (exec) cudaGraphExecDestroy(exec);
+        if (wexec) cudaGraphExecDestroy(wexec);
         throw;
     }
     for (cudaEvent_t e : evb) cudaEventDestroy(e);
     if (exec) cudaGraphExecDestroy(exec);
+    if (wexec) cudaGraphExecDestroy(wexec);
     return result;
 }
 }  // namespace ddamg

@@ -82,6 +82,25 @@ def test_repeated_solves_are_deterministic(case):
     x1, i1 = s.bi_cgstab(b)
     x2, i2 = s.bi_cgstab(b)
     assert i1.iterations == i2.iterations and np.array_equal(x1, x2)
+    # with cuda_graphs (the default) the iteration runs as a device-side graph loop
+    assert "bicgstab: device loop" in s.autotune_report()
+
+
+def test_host_batched_path_matches_device_loop(golden):
+    z = golden("krylov_32x32")
+    Nx, Nt, L = int(z["Nx"]), int(z["Nt"]), int(z["levels"])
+    U = po.links_from_theta(z["theta"])
+    out = []
+    for graphs in (1, 0):
+        s = ddamg.Solver(ddamg.default_params(Nx, Nt, L, float(z["m0"]), z["rows"], cuda_graphs=graphs))
+        s.load_gauge(U)
+        out.append((s.bi_cgstab(z["rhs"]), s.conjugate_gradient(z["rhs"], max_iter=50), s.autotune_report()))
+        s.close()
+    (xa, ia), (ca, ja), ra = out[0]
+    (xb, ib), (cb, jb), rb = out[1]
+    assert "device loop" in ra and "host-queued" in rb
+    assert ia.iterations == ib.iterations and np.array_equal(xa, xb)
+    assert ja.iterations == jb.iterations == 50 and np.array_equal(ca, cb)
 
 
 def test_zero_rhs(case):
