@@ -688,9 +688,27 @@ def profile_case(name):
     sap-l1   the bench workload's FP64 solve (level-1 sap_block_kernel sweeps inside);
     tc-apply one batched FP32 level-1 SAP sweep pair on 512x512 with 64 right-hand sides
              (tc_block_apply_kernel, the tensor-core block operator);
-    krylov   20 BiCGstab iterations on a 1024x1024 field (bicg_* kernels, 11 fields of 32 MiB)."""
+    krylov   20 BiCGstab iterations on a 1024x1024 field (bicg_* kernels, 11 fields of 32 MiB);
+    dw       D_W and D_W^dagger on a 1024x1024 field, FP64 then FP32 (wilson_kernel, 32 + 32 MiB in/out)."""
     import ddamg
 
+    if name == "dw":
+        import torch
+
+        N = 1024
+        th, _ = ddamg.gauge_metropolis(N, N, 4.0, 10, 3)
+        s = ddamg.Solver(ddamg.default_params(N, N, 2, -0.07, [[0, 128, 128, 4, 128, 128]], precision=ddamg.PREC_MIXED))
+        s.load_gauge(np.exp(1j * th))
+        for dt, fn in ((torch.float64, s.L.ddamg_apply_dirac_device), (torch.float32, s.L.ddamg_apply_dirac_f32_device)):
+            x = torch.randn(4 * N * N, dtype=dt, device="cuda")
+            y = torch.empty_like(x)
+            for dag in (0, 1):
+                for _ in range(2):
+                    ddamg.check(fn(s.h, dag, x.data_ptr(), y.data_ptr(), 1))
+        torch.cuda.synchronize()
+        print("dw: 8 applications (FP64 D, D^dagger, FP32 D, D^dagger; 2 each) on 1024x1024")
+        s.close()
+        return 0
     if name == "krylov":
         N = 1024
         th, _ = ddamg.gauge_metropolis(N, N, 4.0, 10, 3)
@@ -734,7 +752,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the 1024x1024 and 512x512 batched lines")
-    ap.add_argument("--profile-case", choices=["sap-l1", "tc-apply", "krylov"],
+    ap.add_argument("--profile-case", choices=["sap-l1", "tc-apply", "krylov", "dw"],
                     help="run one small case of a hot kernel for an ncu capture and exit")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
