@@ -471,6 +471,34 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+LAST_TUNE = {}  # autotuner report of the last timed_solves handle
+
+
+def tensor_figure(report, level, R, flop):
+    """Tensor-pipe figure of the tcgen05 block operator from the autotuner's timing of the chosen tile shape
+    (one application, all blocks of a colour, CUDA events): achieved TF32 TFLOP/s against half the measured
+    dense bf16 rate (TF32 issues at half the bf16 rate on these tensor cores)."""
+    import re
+
+    for line in report.splitlines():
+        if line.startswith(f"level {level} rhs {R}:"):
+            m = re.search(r"\[rhs/cta (\d+) stages (\d+) chains (\d+): ([0-9.]+) us \*\]", line)
+            if not m:
+                return None
+            us = float(m.group(4))
+            try:
+                bf16 = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))["bf16_tflops"]
+                kind = "half the measured dense bf16 rate (MEASURED_PEAKS.json)"
+            except Exception:
+                bf16, kind = 1590.0, "half the fallback dense bf16 rate"
+            ach = flop / (us * 1e-6) / 1e12
+            return {"kernel": f"tc_block_apply_kernel, level {level}, {R} right-hand sides", "bound": "tensor",
+                    "tile": {"rhs_per_cta": int(m.group(1)), "ring_stages": int(m.group(2)), "chains": int(m.group(3))},
+                    "flop_per_application": flop, "us_per_application": us, "achieved_tflops": ach,
+                    "peak_tflops": bf16 / 2, "frac": ach / (bf16 / 2), "peak_kind": kind}
+    return None
+
+
 def timed_solves(ddamg, torch, dev, p, U, b_dev, R, reps=2):
     """setup + solve of R right-hand sides on one handle; returns (setup_ms, solve_ms, infos, x) of the
     last of `reps` repetitions, times from the library's own events (device time)."""
@@ -480,6 +508,7 @@ def timed_solves(ddamg, torch, dev, p, U, b_dev, R, reps=2):
     for _ in range(reps):
         s.setUpPhase(seed=5)
         infos = s.solve_device(b_dev.data_ptr(), x.data_ptr(), R)
+    LAST_TUNE["report"] = s.autotune_report()
     s.close()
     xs = x.cpu().numpy().view(np.complex128)
     return 1e3 * infos[0].setup_seconds, 1e3 * infos[0].solve_seconds, infos, xs
@@ -554,8 +583,12 @@ def batched_512(ddamg, torch, dev):
     s64, t64, i64, x64 = timed_solves(ddamg, torch, dev, p(ddamg.PREC_DOUBLE, 1), U, b_dev[:2 * n], 1)
     sB, tB, iB, xB = timed_solves(ddamg, torch, dev, p(ddamg.PREC_DOUBLE, R), U, b_dev, R, reps=1)
     sb, tb, ib, xb = timed_solves(ddamg, torch, dev, p(ddamg.PREC_MIXED, R), U, b_dev, R)
+    # one level-1 block-operator application: 128 blocks x 64 in-block (site, hop) tiles x 64x64 real
+    # matrix (2 dof, dof = 32) x R right-hand sides, 2 flops per multiply-add
+    tens = tensor_figure(LAST_TUNE.get("report", ""), 1, R, 128 * 64 * 64 * 64 * R * 2)
     errs = rel_errs(xb, xB, n)
     out = {
+        "tensor_pipe": tens,
         "workload": f"512x512 beta=3 (1000 sweeps, acceptance {acc:.3f}), m0=-0.10, 3 levels Nv=16, FGMRES(30) "
                     "V-cycle to 1e-10",
         "fp64_single": {"setup_ms": s64, "solve_ms": t64, "iterations": i64[0].iterations},
