@@ -1164,6 +1164,35 @@ ddamg_status ddamg_read_binary(const char* path, int Nx, int Nt, double* out) {
     }
     return DDAMG_OK;
 }
+ddamg_status ddamg_from_halo(const double* halo, int Nx, int Nt, int dof, double* compact) {
+    if (!halo || !compact || Nx <= 0 || Nt <= 0 || dof <= 0) {
+        set_error("ddamg_from_halo: bad argument");
+        return DDAMG_ERR_BAD_PARAM;
+    }
+    for (int x = 1; x <= Nx; x++)
+        for (int t = 1; t <= Nt; t++)
+            for (int d = 0; d < dof; d++) {
+                const long h = ((long)x * (Nt + 2) + t) * dof + d, c = ((long)(x - 1) * Nt + (t - 1)) * dof + d;
+                compact[2 * c] = halo[2 * h];
+                compact[2 * c + 1] = halo[2 * h + 1];
+            }
+    return DDAMG_OK;
+}
+ddamg_status ddamg_to_halo(const double* compact, int Nx, int Nt, int dof, double* halo) {
+    if (!halo || !compact || Nx <= 0 || Nt <= 0 || dof <= 0) {
+        set_error("ddamg_to_halo: bad argument");
+        return DDAMG_ERR_BAD_PARAM;
+    }
+    std::fill(halo, halo + 2L * (Nx + 2) * (Nt + 2) * dof, 0.0);
+    for (int x = 1; x <= Nx; x++)
+        for (int t = 1; t <= Nt; t++)
+            for (int d = 0; d < dof; d++) {
+                const long h = ((long)x * (Nt + 2) + t) * dof + d, c = ((long)(x - 1) * Nt + (t - 1)) * dof + d;
+                halo[2 * h] = compact[2 * c];
+                halo[2 * h + 1] = compact[2 * c + 1];
+            }
+    return DDAMG_OK;
+}
 ddamg_status ddamg_write_binary(const char* path, int Nx, int Nt, const double* field) {
     if (!path || !field || Nx <= 0 || Nt <= 0) return DDAMG_ERR_BAD_PARAM;
     std::ofstream f(path, std::ios::binary);

@@ -14,7 +14,7 @@ from . import _lib
 from ._lib import CYCLE_K, CYCLE_V, PREC_DOUBLE, PREC_MIXED, DDAMGError, Params, SolveInfo, check
 
 __all__ = ["Solver", "Params", "SolveInfo", "DDAMGError", "default_params", "read_parameters", "read_binary",
-           "write_binary", "gauge_metropolis", "gaussian_field", "PREC_DOUBLE", "PREC_MIXED", "CYCLE_V", "CYCLE_K"]
+           "write_binary", "from_halo", "to_halo", "gauge_metropolis", "gaussian_field", "PREC_DOUBLE", "PREC_MIXED", "CYCLE_V", "CYCLE_K"]
 
 
 def _dp(a):
@@ -57,6 +57,22 @@ def read_binary(path, Nx, Nt):
 def write_binary(path, Nx, Nt, field):
     f = _c(field)
     check(_lib.load().ddamg_write_binary(path.encode(), Nx, Nt, _dp(f)))
+
+
+def from_halo(halo, Nx, Nt, dof):
+    """The reference's halo spinor layout (x, t in 1..N of an (Nx+2) x (Nt+2) grid) -> compact [site][dof]."""
+    halo = _c(halo)
+    out = np.empty(Nx * Nt * dof, dtype=np.complex128)
+    check(_lib.load().ddamg_from_halo(_dp(halo), Nx, Nt, dof, _dp(out)))
+    return out
+
+
+def to_halo(compact, Nx, Nt, dof):
+    """compact [site][dof] -> the reference's halo spinor layout (halo sites zero)."""
+    compact = _c(compact)
+    out = np.empty((Nx + 2) * (Nt + 2) * dof, dtype=np.complex128)
+    check(_lib.load().ddamg_to_halo(_dp(compact), Nx, Nt, dof, _dp(out)))
+    return out
 
 
 def gauge_metropolis(Nx, Nt, beta, sweeps, seed, delta=1.0, device=0):

@@ -85,6 +85,8 @@ SIGNATURES = {
     "ddamg_link_derivative": (_st, [_h, _dp, _dp, _dp]),
     "ddamg_gauge_metropolis": (_st, [_i, _i, ctypes.c_double, _i, ctypes.c_uint64, ctypes.c_double, _dp, _dp, _i]),
     "ddamg_gaussian_field": (_st, [ctypes.c_int64, ctypes.c_uint64, _dp]),
+    "ddamg_from_halo": (_st, [_dp, _i, _i, _i, _dp]),
+    "ddamg_to_halo": (_st, [_dp, _i, _i, _i, _dp]),
 }
 
 _lib = None

@@ -127,6 +127,11 @@ ddamg_status ddamg_autotune_report(ddamg_t* h, char* buf, int len);
 ddamg_status ddamg_read_binary(const char* path, int Nx, int Nt, double* out);
 /* writer of the same format (the reference has none; its inputs come from HMC) */
 ddamg_status ddamg_write_binary(const char* path, int Nx, int Nt, const double* field);
+/* layout converters for callers holding the reference's spinors (struct spinor, include/variables.h:201-238,
+ * indexed by idx, include/utils.h:46-52): halo[(x*(Nt+2)+t)*dof + d] for x in 1..Nx, t in 1..Nt
+ * <-> compact[((x-1)*Nt + (t-1))*dof + d], complex interleaved; to_halo zeroes the halo sites */
+ddamg_status ddamg_from_halo(const double* halo, int Nx, int Nt, int dof, double* compact);
+ddamg_status ddamg_to_halo(const double* compact, int Nx, int Nt, int dof, double* halo);
 /* gauge links U_mu(x) (spinor U of src/main.cpp:74-78), [site][mu] complex */
 ddamg_status ddamg_load_gauge(ddamg_t* h, const double* U);
 

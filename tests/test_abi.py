@@ -93,3 +93,24 @@ def test_null_handle_and_bad_args_rejected():
     assert L.ddamg_load_gauge(None, None) == _lib.ERR_BAD_PARAM
     assert L.ddamg_params_default(None) == _lib.ERR_BAD_PARAM
     assert L.ddamg_gauge_metropolis(3, 4, 1.0, 1, 1, 1.0, None, None, 0) == _lib.ERR_BAD_PARAM
+
+
+def test_halo_layout_round_trip():
+    """ddamg_from_halo / ddamg_to_halo follow the reference's spinor indexing idx(x, t, mu) =
+    (x*(Nt+2)+t)*DOF + mu for x, t >= 1 (include/utils.h:46-52)."""
+    import ddamg
+
+    Nx, Nt, dof = 5, 7, 4
+    rng = np.random.default_rng(3)
+    halo = rng.standard_normal((Nx + 2) * (Nt + 2) * dof) + 1j * rng.standard_normal((Nx + 2) * (Nt + 2) * dof)
+    c = ddamg.from_halo(halo, Nx, Nt, dof)
+    for x in range(1, Nx + 1):
+        for t in range(1, Nt + 1):
+            for d in range(dof):
+                assert c[((x - 1) * Nt + (t - 1)) * dof + d] == halo[(x * (Nt + 2) + t) * dof + d]
+    h2 = ddamg.to_halo(c, Nx, Nt, dof)
+    inner = np.zeros((Nx + 2, Nt + 2), dtype=bool)
+    inner[1:-1, 1:-1] = True
+    mask = np.repeat(inner.reshape(-1), dof)
+    assert np.array_equal(h2[mask], halo[mask]) and not h2[~mask].any()
+    assert ddamg._lib.load().ddamg_from_halo(None, Nx, Nt, dof, None) == _lib.ERR_BAD_PARAM
