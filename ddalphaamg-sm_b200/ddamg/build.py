@@ -3,7 +3,8 @@
     python -m ddamg.build            (from ddalphaamg-sm_b200/)
     python ddalphaamg-sm_b200/ddamg/build.py
 
-Objects go to ddalphaamg-sm_b200/_build/, the library to ddalphaamg-sm_b200/ddamg/libddamg.so.
+Objects go to ddalphaamg-sm_b200/_build/, the library to ddalphaamg-sm_b200/ddamg/libddamg.so and the
+command-line driver (driver/ddamg_main.cpp, the reference's main against the C ABI) to ddamg/ddamg_main.
 Sources are recompiled when they (or a header) are newer than their object.
 """
 import concurrent.futures as cf
@@ -55,6 +56,16 @@ def build(verbose=False, extra=()):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    # the command-line driver (driver/ddamg_main.cpp): plain C++ against the C ABI, next to the library
+    drv_src = os.path.join(ROOT, "driver", "ddamg_main.cpp")
+    drv = os.path.join(PKG, "ddamg_main")
+    if os.path.exists(drv_src) and (not os.path.exists(drv) or
+                                    os.path.getmtime(drv) < max(os.path.getmtime(drv_src), os.path.getmtime(LIB))):
+        cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-I" + os.path.join(REPO, "include"), drv_src,
+               "-o", drv, "-L" + PKG, "-lddamg", "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"driver build failed:\n{r.stdout}\n{r.stderr}")
     if verbose:
         print("built", LIB)
     return LIB
