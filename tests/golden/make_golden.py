@@ -36,6 +36,14 @@ CASES = [
     # 64x64, 2 levels, SAP 4x4, Nv = 10, restart 20, beta = 2, 500 sweeps, m0 = -0.18
     dict(name="solve_64x64_l2", Nx=64, Nt=64, levels=2, m0=-0.18,
          rows=[[0, 16, 16, 10, 16, 16]], beta=2.0, sweeps=500, seed=2024, m=20, modes=("solve",)),
+    # iteration spread over setup seeds (the same injected random vectors in both codes): configs[0]
+    # 64x64 and the bench's 256x256 3-level workload
+    dict(name="seeds_64x64_l2", Nx=64, Nt=64, levels=2, m0=-0.18,
+         rows=[[0, 16, 16, 10, 16, 16]], beta=2.0, sweeps=500, seed=2024, m=20, modes=("seeds",),
+         setup_seeds=list(range(1, 9))),
+    dict(name="seeds_256x256_l3", Nx=256, Nt=256, levels=3, m0=-0.10,
+         rows=[[0, 64, 64, 12, 64, 64], [1, 16, 16, 12, 16, 16]], beta=3.0, sweeps=1000, seed=2025, rhs_seed=77,
+         m=30, modes=("seeds",), setup_seeds=[1, 2, 3, 4]),
     # the comparison solvers of src/conjugate_gradient.cpp (BiCGstab on D, CG on D^dagger D)
     dict(name="krylov_32x32", Nx=32, Nt=32, levels=2, m0=-0.15,
          rows=[[0, 8, 8, 6, 4, 4]], beta=2.0, sweeps=30, seed=12, m=20, modes=("krylov",)),
@@ -66,7 +74,7 @@ def make_case(c, work):
     nrnd = o.setup_random_count()
     rnd = pyoracle.uniform(nrnd, c["seed"] + 1)
     probes = [pyoracle.gaussian(sizes[l], c["seed"] + 100 + l) for l in range(L)]
-    rhs = pyoracle.gaussian(Nx * Nt * 2, c["seed"] + 7)
+    rhs = pyoracle.gaussian(Nx * Nt * 2, c.get("rhs_seed", c["seed"] + 7))
 
     pfile = os.path.join(work, "params")
     with open(pfile, "w") as f:
@@ -82,6 +90,7 @@ def make_case(c, work):
     np.concatenate(probes).tofile(pf)
 
     out = dict(Nx=Nx, Nt=Nt, levels=L, m0=c["m0"], rows=np.array(c["rows"], dtype=np.int32), theta=theta,
+               rhs_seed=c.get("rhs_seed", c["seed"] + 7),
                beta=c["beta"], sweeps=c["sweeps"], seed=c["seed"], rnd_count=nrnd, rhs=rhs, fgmres_m=c["m"],
                acceptance=acc)
     # the setup's random stream is pyoracle.uniform(rnd_count, seed + 1); it is regenerated, not stored
@@ -113,6 +122,24 @@ def make_case(c, work):
         run([harness, "solve", str(L), repr(c["m0"]), pfile, conf, rhsf, "-", sd, "0", str(c["m"]), "50", "1e-10"])
         meta = dict(line.split() for line in open(os.path.join(sd, "solve.txt")))
         out["ref_iters_V_stock"] = int(meta["iterations"])
+    if "seeds" in c["modes"]:
+        # V-cycle FGMRES iterations of the reference for each injected setup; the field and right-hand
+        # side are regenerated by the tests from the stored seeds (theta is kept only for the smaller case)
+        its = []
+        for sd in c["setup_seeds"]:
+            kd = os.path.join(work, f"seed{sd}")
+            os.makedirs(kd)
+            tfs = os.path.join(work, f"tvec_{sd}.bin")
+            pyoracle.uniform(nrnd, sd).tofile(tfs)
+            run([harness, "solve", str(L), repr(c["m0"]), pfile, conf, rhsf, tfs, kd, "0", str(c["m"]), "50", "1e-10"])
+            meta = dict(line.split() for line in open(os.path.join(kd, "solve.txt")))
+            its.append(int(meta["iterations"]))
+        out["setup_seeds"] = np.array(c["setup_seeds"], dtype=np.int64)
+        out["ref_iters_V_seeds"] = np.array(its, dtype=np.int64)
+        if Nx * Nt > 64 * 64:
+            del out["theta"], out["rhs"]
+            for l in range(L):
+                del out[f"probe_{l}"]
     if "krylov" in c["modes"]:
         kd = os.path.join(work, "krylov")
         os.makedirs(kd)
@@ -140,7 +167,7 @@ def main():
         path = os.path.join(HERE, c["name"] + ".npz")
         np.savez_compressed(path, **out)
         print(f"{c['name']}: {os.path.getsize(path) / 1024:.0f} KiB, keys={len(out)}",
-              {k: int(v) for k, v in out.items() if k.endswith("_iters") or k.startswith("ref_iters")})
+              {k: np.asarray(v).tolist() for k, v in out.items() if k.endswith("_iters") or k.startswith("ref_iters")})
 
 
 if __name__ == "__main__":

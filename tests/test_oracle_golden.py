@@ -129,3 +129,17 @@ def test_krylov_comparison_solvers(golden):
     assert rel(xc, z["ref_x_cg"]) < 1e-12
     for x in (xb, xc):
         assert np.linalg.norm(o.dirac(x) - z["rhs"]) / np.linalg.norm(z["rhs"]) < 1e-9
+
+
+def test_iterations_per_setup_seed_64(golden):
+    """The oracle, given the same injected setup vectors, takes the reference's V-cycle iteration count
+    for every seed of configs[0] (64x64, 2 levels)."""
+    z = golden("seeds_64x64_l2")
+    o = po.Oracle(int(z["Nx"]), int(z["Nt"]), int(z["levels"]), float(z["m0"]), z["rows"],
+                  po.links_from_theta(z["theta"]))
+    its = []
+    for sd in z["setup_seeds"][:4]:
+        o.setup(po.uniform(int(z["rnd_count"]), int(sd)))
+        _, it = o.solve(z["rhs"], cycle=0, m=int(z["fgmres_m"]))
+        its.append(it)
+    assert its == [int(v) for v in z["ref_iters_V_seeds"][:4]]
