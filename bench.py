@@ -474,7 +474,7 @@ def run_ours(args, rank, world, local_rank):
 LAST_TUNE = {}  # autotuner report of the last timed_solves handle
 
 
-def tensor_figure(report, level, R, flop):
+def tensor_figure(report, level, R, flop, hbm_bytes=None):
     """Tensor-pipe figure of the tcgen05 block operator from the autotuner's timing of the chosen tile shape
     (one application, all blocks of a colour, CUDA events): achieved TF32 TFLOP/s against half the measured
     dense bf16 rate (TF32 issues at half the bf16 rate on these tensor cores)."""
@@ -492,10 +492,16 @@ def tensor_figure(report, level, R, flop):
             except Exception:
                 bf16, kind = 1590.0, "half the fallback dense bf16 rate"
             ach = flop / (us * 1e-6) / 1e12
-            return {"kernel": f"tc_block_apply_kernel, level {level}, {R} right-hand sides", "bound": "tensor",
-                    "tile": {"rhs_per_cta": int(m.group(1)), "ring_stages": int(m.group(2)), "chains": int(m.group(3))},
-                    "flop_per_application": flop, "us_per_application": us, "achieved_tflops": ach,
-                    "peak_tflops": bf16 / 2, "frac": ach / (bf16 / 2), "peak_kind": kind}
+            out = {"kernel": f"tc_block_apply_kernel, level {level}, {R} right-hand sides", "bound": "tensor",
+                   "tile": {"rhs_per_cta": int(m.group(1)), "ring_stages": int(m.group(2)), "chains": int(m.group(3))},
+                   "flop_per_application": flop, "us_per_application": us, "achieved_tflops": ach,
+                   "peak_tflops": bf16 / 2, "frac": ach / (bf16 / 2), "peak_kind": kind}
+            if hbm_bytes:  # the same application against HBM: embedded link tiles, vector tiles in, output out
+                hbm, hkind = peaks()
+                gbs = hbm_bytes / (us * 1e-6) / 1e9
+                out.update({"hbm_bytes_per_application": hbm_bytes, "hbm_gbs": gbs, "hbm_frac": gbs / hbm,
+                            "hbm_peak_kind": hkind})
+            return out
     return None
 
 
@@ -585,7 +591,10 @@ def batched_512(ddamg, torch, dev):
     sb, tb, ib, xb = timed_solves(ddamg, torch, dev, p(ddamg.PREC_MIXED, R), U, b_dev, R)
     # one level-1 block-operator application: 128 blocks x 64 in-block (site, hop) tiles x 64x64 real
     # matrix (2 dof, dof = 32) x R right-hand sides, 2 flops per multiply-add
-    tens = tensor_figure(LAST_TUNE.get("report", ""), 1, R, 128 * 64 * 64 * 64 * R * 2)
+    # HBM bytes of the same application: 128 x 64 embedded link tiles of 16 KB, and the colour's vector
+    # tiles read and output tiles written (2048 sites x R x 2 dof x 4 B each way)
+    tens = tensor_figure(LAST_TUNE.get("report", ""), 1, R, 128 * 64 * 64 * 64 * R * 2,
+                         128 * 64 * 16384 + 2 * 2048 * R * 64 * 4)
     errs = rel_errs(xb, xB, n)
     out = {
         "tensor_pipe": tens,
