@@ -91,6 +91,8 @@ struct ddamg_handle {
     std::vector<ddamg::CoarseGmresWork> cg_lane;    // lanes 1..: concurrent coarsest solves of a batch
     std::vector<cudaStream_t> lane_s;
     std::vector<cudaEvent_t> lane_ev;
+    std::vector<cudaStream_t> setup_s;  // extra streams of the setup's grouped coarse smoothing
+    std::vector<cudaEvent_t> setup_ev;
     cudaEvent_t fork_ev = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_setup_s = 0;
@@ -870,6 +872,70 @@ static long setup_random_count(const ddamg_handle* h) {
     return n;
 }
 
+// The setup's smoothing at a coarse level: SAP with right-hand side 0 on every test vector
+// (src/amg.cpp:49-52).  The vectors are independent, so groups of the CUDA-core sweep's tuned width
+// run their sweeps and residual updates on separate streams, and one group's CTAs fill the SMs that
+// the last wave of another group's sweep leaves idle.  With v = 0 the reference's test
+// ||r|| < tol ||v|| never passes, so every vector takes exactly nu iterations and no norms are
+// needed, as in sap_t.  Returns false (nothing done) where the single-stream path applies.
+template <typename V>
+static bool sap_setup_split(ddamg_handle* h, int l, const V* v, V* x, int nu, int nrhs) {
+    if (l == 0 || h->prof || nrhs < 2) return false;
+    LevelData& D = h->lv[l];
+    const Geom& g = D.g;
+    const long n = g.size();
+    V* r = B<V>(D).r;
+    SapArgs a{h->p.sap_gmres_restart_length, h->p.sap_gmres_restarts, h->p.sap_gmres_tolerance, h->p.m0, D.red,
+              D.nred, D.done};
+    DDAMG_CUDA_TRY(cudaMemsetAsync(D.done, 0, sizeof(int) * nrhs, h->s));
+    level_op<V>(h, l, x, r, v, nrhs);  // r = v - D x for every vector
+    const int rb = rb_for<V>(h, l, r, a, nrhs);  // tuned on first use on red sweeps (times into scratch, syncs)
+    const int G = nrhs / rb;
+    // the groups of one Schwarz block share its links through L2 only while they run side by side,
+    // which one launch guarantees (block-major CTA order) and separate streams do not: split only when
+    // one colour's links fit in L2 (128x128 sites at dof 32, 671 MB per colour, lost 38 % of its setup)
+    const double colour_link_bytes = 0.5 * (double)g.sites * 5 * g.dof * g.dof * sizeof(V);
+    if (G < 2 || G * rb != nrhs || colour_link_bytes > 100e6) {  // one stream: the plain sweep loop
+        for (int it = 0; it < nu; it++)
+            for (int colour = 0; colour < 2; colour++) {
+                a.blocks = colour == 0 ? D.red : D.black;
+                a.nblocks = colour == 0 ? D.nred : D.nblack;
+                launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs, rb);
+                if (!(colour == 1 && it == nu - 1)) level_op<V>(h, l, x, r, v, nrhs);
+            }
+        return true;
+    }
+    while ((int)h->setup_s.size() < G - 1) {
+        cudaStream_t q;
+        cudaEvent_t e;
+        DDAMG_CUDA_TRY(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+        DDAMG_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        h->setup_s.push_back(q);
+        h->setup_ev.push_back(e);
+    }
+    DDAMG_CUDA_TRY(cudaEventRecord(h->fork_ev, h->s));
+    for (int k = 1; k < G; k++) DDAMG_CUDA_TRY(cudaStreamWaitEvent(h->setup_s[k - 1], h->fork_ev, 0));
+    for (int k = 0; k < G; k++) {
+        cudaStream_t st = k == 0 ? h->s : h->setup_s[k - 1];
+        const long off = (long)k * rb * n;
+        SapArgs ak = a;
+        ak.done = D.done + k * rb;
+        for (int it = 0; it < nu; it++)
+            for (int colour = 0; colour < 2; colour++) {
+                ak.blocks = colour == 0 ? D.red : D.black;
+                ak.nblocks = colour == 0 ? D.nred : D.nblack;
+                launch_sap_sweep_coarse<V>(st, g, B<V>(D).links, r + off, x + off, ak, rb, rb);
+                if (!(colour == 1 && it == nu - 1))
+                    launch_coarse_op<V>(st, B<V>(D).links, x + off, r + off, v + off, g.Nx, g.Nt, g.dof, h->p.m0, rb);
+            }
+    }
+    for (int k = 1; k < G; k++) {
+        DDAMG_CUDA_TRY(cudaEventRecord(h->setup_ev[k - 1], h->setup_s[k - 1]));
+        DDAMG_CUDA_TRY(cudaStreamWaitEvent(h->s, h->setup_ev[k - 1], 0));
+    }
+    return true;
+}
+
 // AlgebraicMG::setUpPhase (src/amg.cpp:4-56).  rnd: device stream of random complex values
 // (or null with a seed: drawn on the device with the same counter RNG as the oracle).
 static void setup(ddamg_handle* h, const double2* rnd_host, uint64_t seed) {
@@ -899,7 +965,8 @@ static void setup(ddamg_handle* h, const double2* rnd_host, uint64_t seed) {
         const int nv = D.g.ntest;
         // SAP(rhs = 0, tvec, nu = SAP_test_vectors_iterations) on all test vectors at once
         DDAMG_CUDA_TRY(cudaMemsetAsync(D.d.eta, 0, sizeof(double2) * n * nv, s));
-        sap_t<double2>(h, l, D.d.eta, D.d.tv, h->p.sap_test_vectors_iterations, 1e-10, false, nv, false);
+        if (!sap_setup_split<double2>(h, l, D.d.eta, D.d.tv, h->p.sap_test_vectors_iterations, nv))
+            sap_t<double2>(h, l, D.d.eta, D.d.tv, h->p.sap_test_vectors_iterations, 1e-10, false, nv, false);
         {
             ProfScope ps(h, 3, l);
             launch_orthonormalize(s, D.g, D.d.tv);
@@ -1088,6 +1155,8 @@ ddamg_status ddamg_destroy(ddamg_t* h) {
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : h->lane_ev) cudaEventDestroy(e);
     for (cudaStream_t q : h->lane_s) cudaStreamDestroy(q);
+    for (cudaStream_t q : h->setup_s) cudaStreamDestroy(q);
+    for (cudaEvent_t e : h->setup_ev) cudaEventDestroy(e);
     if (h->fork_ev) cudaEventDestroy(h->fork_ev);
     if (h->hpin) cudaFreeHost(h->hpin);
     if (h->hpin2) cudaFreeHost(h->hpin2);
