@@ -92,6 +92,90 @@ __global__ void __launch_bounds__(256) wilson_kernel(const V* __restrict__ U, co
     else st2(out + 2 * n, o0, o1);
 }
 
+// FP32 D_W with the two sites (x, t0), (x, t0 + 1), t0 even, per thread: the pair's psi, its links
+// and its output are each one 32-byte access (ld.global.nc.v8.f32 / st.global.v8.f32), so every warp
+// instruction covers 1 KB of contiguous memory; the t-neighbours inside the pair come from registers.
+__device__ __forceinline__ void ld8f(const float2* __restrict__ p, float2& a, float2& b, float2& c, float2& d) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(b.x), "=f"(b.y), "=f"(c.x), "=f"(c.y), "=f"(d.x), "=f"(d.y)
+        : "l"(p));
+}
+__device__ __forceinline__ void st8f(float2* p, float2 a, float2 b, float2 c, float2 d) {
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(a.x), "f"(a.y), "f"(b.x),
+                 "f"(b.y), "f"(c.x), "f"(c.y), "f"(d.x), "f"(d.y)
+                 : "memory");
+}
+// one site of D_phi / D_dagger_phi from its links and neighbours (the arithmetic of wilson_kernel)
+template <bool DAG>
+__device__ __forceinline__ void wilson_site(float2 u0, float2 u1, float2 ul0, float2 ul1, float2 p0, float2 p1,
+                                            float2 a0, float2 a1, float2 c0, float2 c1, float2 e0, float2 e1,
+                                            float2 g0, float2 g1, float sr, float sl, float mm, float2& o0,
+                                            float2& o1) {
+    float2 s0, s1;
+    if (!DAG) {
+        float2 a = sr * cmul(u0, a0 - a1);      // +t: (1 - sigma_x)
+        float2 c = cmul(u1, c0 + imul(c1));    // +x: (1 - sigma_y)
+        float2 e = sl * cmulc(ul0, e0 + e1);   // -t: (1 + sigma_x)
+        float2 g = cmulc(ul1, g0 - imul(g1));  // -x: (1 + sigma_y)
+        s0 = a + c + e + g;
+        s1 = -a - imul(c) + e + imul(g);
+    } else {
+        float2 a = sl * cmulc(ul0, e0 - e1);   // -t: (1 - sigma_x)
+        float2 c = cmulc(ul1, g0 + imul(g1));  // -x: (1 - sigma_y)
+        float2 e = sr * cmul(u0, a0 + a1);     // +t: (1 + sigma_x)
+        float2 g = cmul(u1, c0 - imul(c1));    // +x: (1 + sigma_y)
+        s0 = a + c + e + g;
+        s1 = -a - imul(c) + e + imul(g);
+    }
+    o0 = mm * p0 - 0.5f * s0;
+    o1 = mm * p1 - 0.5f * s1;
+}
+template <bool DAG, bool RESID>
+__global__ void __launch_bounds__(256) wilson_pair_kernel(const float2* __restrict__ U, const float2* __restrict__ in,
+                                                          float2* __restrict__ out, const float2* __restrict__ b,
+                                                          int Nx, int Nt, float m0, long stride) {
+    const int n0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (n0 >= Nx * Nt) return;
+    const long ro = (long)blockIdx.y * stride;
+    in += ro;
+    out += ro;
+    const int x = n0 / Nt, t0 = n0 - x * Nt;
+    const int xp = (x + 1 == Nx) ? 0 : x + 1, xm = (x == 0) ? Nx - 1 : x - 1;
+    const int tm = (t0 == 0) ? Nt - 1 : t0 - 1, tp = (t0 + 2 == Nt) ? 0 : t0 + 2;
+    float2 pa0, pa1, pb0, pb1;  // own sites t0 (a) and t0 + 1 (b), spins 0, 1
+    float2 ca0, ca1, cb0, cb1;  // x + 1
+    float2 ga0, ga1, gb0, gb1;  // x - 1
+    float2 e0, e1, f0, f1;      // t0 - 1 and t0 + 2
+    ld8f(in + 2 * n0, pa0, pa1, pb0, pb1);
+    ld8f(in + 2 * (xp * Nt + t0), ca0, ca1, cb0, cb1);
+    ld8f(in + 2 * (xm * Nt + t0), ga0, ga1, gb0, gb1);
+    ld2(in + 2 * (x * Nt + tm), e0, e1);
+    ld2(in + 2 * (x * Nt + tp), f0, f1);
+    float2 u0a, u1a, u0b, u1b, w0a, w1a, w0b, w1b;  // links of the pair, and of the pair at x - 1
+    ld8f(U + 2 * n0, u0a, u1a, u0b, u1b);
+    ld8f(U + 2 * (xm * Nt + t0), w0a, w1a, w0b, w1b);
+    const float2 ul0 = __ldg(U + 2 * (x * Nt + tm));
+    (void)w0a;
+    (void)w0b;
+    const float mm = m0 + 2.f;
+    float2 oa0, oa1, ob0, ob1;
+    // site t0: +t neighbour t0 + 1, -t neighbour t0 - 1 (the t-wrap sign when t0 = 0)
+    wilson_site<DAG>(u0a, u1a, ul0, w1a, pa0, pa1, pb0, pb1, ca0, ca1, e0, e1, ga0, ga1, 1.f, t0 == 0 ? -1.f : 1.f,
+                     mm, oa0, oa1);
+    // site t0 + 1: +t neighbour t0 + 2 (the sign when t0 + 1 = Nt - 1), -t neighbour t0
+    wilson_site<DAG>(u0b, u1b, u0a, w1b, pb0, pb1, f0, f1, cb0, cb1, pa0, pa1, gb0, gb1, t0 + 2 == Nt ? -1.f : 1.f,
+                     1.f, mm, ob0, ob1);
+    if (RESID) {
+        float2 b0, b1, b2, b3;
+        ld8f(b + ro + 2 * n0, b0, b1, b2, b3);
+        oa0 = b0 - oa0;
+        oa1 = b1 - oa1;
+        ob0 = b2 - ob0;
+        ob1 = b3 - ob1;
+    }
+    st8f(out + 2 * n0, oa0, oa1, ob0, ob1);
+}
+
 template <typename V>
 void launch_wilson(cudaStream_t s, const V* U, const V* in, V* out, const V* b, int Nx, int Nt, double m0,
                    int dagger, int nrhs) {
@@ -102,6 +186,22 @@ void launch_wilson(cudaStream_t s, const V* U, const V* in, V* out, const V* b, 
     // boundary (sites and right-hand sides then stay on one)
     auto a32 = [](const void* p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 31) == 0; };
     const bool wide = sizeof(V) == 16 && a32(U) && a32(in) && a32(out) && a32(b);
+    if (sizeof(V) == 8 && Nt % 2 == 0 && a32(U) && a32(in) && a32(out) && a32(b)) {
+        // FP32: two sites per thread (t0 even), a pair of sites is 32 bytes
+        const float2* Uf = reinterpret_cast<const float2*>(U);
+        const float2* inf = reinterpret_cast<const float2*>(in);
+        float2* outf = reinterpret_cast<float2*>(out);
+        const float2* bf = reinterpret_cast<const float2*>(b);
+        dim3 pg(ceil_div((long)Nx * Nt / 2, 256), nrhs);
+        if (dagger) {
+            if (b) DDAMG_LAUNCH((wilson_pair_kernel<true, true>), pg, 256, 0, s, Uf, inf, outf, bf, Nx, Nt, (float)m0, stride);
+            else DDAMG_LAUNCH((wilson_pair_kernel<true, false>), pg, 256, 0, s, Uf, inf, outf, bf, Nx, Nt, (float)m0, stride);
+        } else {
+            if (b) DDAMG_LAUNCH((wilson_pair_kernel<false, true>), pg, 256, 0, s, Uf, inf, outf, bf, Nx, Nt, (float)m0, stride);
+            else DDAMG_LAUNCH((wilson_pair_kernel<false, false>), pg, 256, 0, s, Uf, inf, outf, bf, Nx, Nt, (float)m0, stride);
+        }
+        return;
+    }
     if (wide) {
         if (dagger) {
             if (b) DDAMG_LAUNCH((wilson_kernel<V, true, true, true>), grid, 256, 0, s, U, in, out, b, Nx, Nt, (R)m0, stride);
