@@ -167,19 +167,6 @@ def sap_sweep_bytes(level_geom, fp_bytes, nvec=1):
     return links + vecs
 
 
-def setup_groups(report, level, nv, geom):
-    """Stream groups of the setup's smoothing at a coarse level: nv / (tuned vectors per CTA) when that
-    divides, is at least 2 and one colour's FP64 links fit in 100 MB (the library's rule), else 1."""
-    import re
-
-    m = re.search(rf"level {level} rhs {nv} fp64 CUDA-core sweep:.*?\[rhs/cta (\d+): [0-9.e+-]+ us \*\]", report)
-    if not m:
-        return 1
-    rb = int(m.group(1))
-    colour_links = 0.5 * geom["sites"] * 5 * geom["dof"] ** 2 * 16
-    return nv // rb if (nv % rb == 0 and nv // rb >= 2 and colour_links <= 100e6) else 1
-
-
 def sap_l2_bytes(level):
     """Link bytes one single-vector SAP colour sweep of a coarse level streams from L2: every block
     solve applies its block operator 1 + restarts x (m + 1) = 31 times (GMRES(5) x 5 at tol 1e-3 does
@@ -351,23 +338,23 @@ def run_ours(args, rank, world, local_rank):
     roof = None
     if best and best[0] == 0:
         g = level_geoms()[best[1]]
-        # per step: 2 x (setup SAP iterations) x G setup sweeps over nv / G test vectors each (G stream groups
-        # of the tuned width where one colour's links fit in L2, else 1), the rest over one vector
+        # per step: 2 x (setup SAP iterations) setup sweeps over the level's nv test vectors, the rest over one
+        # vector (with per-launch events on, the library runs the setup's smoothing as one launch per colour
+        # instead of its stream groups, so this pass has the single-launch mix)
         nv = w["rows"][best[1]][3] if best[1] < len(w["rows"]) else 1
-        G = setup_groups(s.autotune_report(), best[1], nv, g) if best[1] >= 1 else 1
-        n_setup = min(best[3], args.steps * 2 * s.params.sap_test_vectors_iterations * G) if best[1] >= 1 else 0
+        n_setup = min(best[3], args.steps * 2 * s.params.sap_test_vectors_iterations) if best[1] >= 1 else 0
         n_solve = best[3] - n_setup
-        bytes_per = (n_setup * sap_sweep_bytes(g, 8, nv // G) + n_solve * sap_sweep_bytes(g, 8, 1)) / best[3]
+        bytes_per = (n_setup * sap_sweep_bytes(g, 8, nv) + n_solve * sap_sweep_bytes(g, 8, 1)) / best[3]
         avg_ms = best[2] / best[3]
         ach = bytes_per / (avg_ms * 1e-3) / 1e9
-        tr_setup = profile_figure("traffic_bytes_per_launch", f"level{best[1]}", "setup")
+        tr_setup = profile_figure("traffic_bytes_per_launch", f"level{best[1]}", "setup12")
         tr_solve = profile_figure("traffic_bytes_per_launch", f"level{best[1]}", "solve")
         traffic = ((n_setup * tr_setup + n_solve * tr_solve) / best[3]) if (tr_setup and tr_solve) else None
         roof = {"kernel": f"{kinds[0]} level {best[1]}", "bound": "hbm", "achieved": ach, "peak": hbm,
                 "unit": "GB/s", "frac": ach / hbm, "traffic": traffic,
                 "traffic_source": "ncu dram bytes of one setup and one solve sweep (profiles/sap_sweep_l1_256x256.txt), "
                                   "weighted by the launches of each kind",
-                "launch_mix": {"setup_sweeps": n_setup, "setup_vectors_per_sweep": nv // G, "solve_sweeps": n_solve},
+                "launch_mix": {"setup_sweeps": n_setup, "setup_vectors_per_sweep": nv, "solve_sweeps": n_solve},
                 "peak_kind": peak_kind, "algorithmic_bytes_per_launch": bytes_per, "avg_launch_ms": avg_ms,
                 "launches": best[3], "share_of_step": best[2] / total_ms if total_ms else None,
                 "measured": "CUDA events around every launch of the kind on the library's stream, in a second "
