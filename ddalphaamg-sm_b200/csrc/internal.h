@@ -157,6 +157,11 @@ void launch_krylov_iterations(cudaStream_t s, int solver, const KrylovWork& w, c
 // one-thread kernel for the body of a graph while node: condition = (the solve is still running)
 void launch_krylov_continue(cudaStream_t s, cudaGraphConditionalHandle hc, const KrylovWork& w);
 
+// ------------------------------------------------------------ HMC (kernels_hmc.cu)
+void launch_gauge_force(cudaStream_t s, const double* th, double* F, int Nx, int Nt, double beta);
+void launch_hmc_momentum(cudaStream_t s, double* p, const double* Fg, const double* Ff, double eps, long nlinks);
+void launch_hmc_theta(cudaStream_t s, double* th, const double* p, double eps, long nlinks);
+
 // ------------------------------------------------------------ coarsest GMRES (kernels_gmres.cu)
 struct CoarseGmresWork {
     double2* V = nullptr;      // (m+1) x n

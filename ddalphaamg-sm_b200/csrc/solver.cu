@@ -3,6 +3,8 @@
 // All device work is issued on the handle's stream; data-dependent branches that would
 // otherwise need a host round trip (SAP early exit) are device-side flags.
 #include <algorithm>
+#include <chrono>
+#include <cmath>
 #include <cstring>
 #include <fstream>
 #include <functional>
@@ -1842,6 +1844,182 @@ ddamg_status ddamg_cg_normal(ddamg_t* h, const double* phi, double* x, int max_i
     if (!phi || !x) throw ParamFailure{"null vector"};
     return krylov_run(h, 1, phi, nullptr, x, max_iter, tol, info);
     API_END
+}
+
+// ------------------------------------------------------------------ HMC
+namespace ddamg {
+constexpr uint64_t kStreamHmc = 0x484D43ull;
+static const double kPi = 3.14159265358979323846;
+
+static double host_gauge_action(const std::vector<double>& th, int Nx, int Nt, double beta, double* plaq_mean) {
+    double s = 0.0, c = 0.0;
+    for (int x = 0; x < Nx; x++)
+        for (int t = 0; t < Nt; t++) {
+            const int n = x * Nt + t, ntp = x * Nt + (t + 1) % Nt, nxp = ((x + 1) % Nx) * Nt + t;
+            const double P = th[2 * n] + th[2 * ntp + 1] - th[2 * nxp] - th[2 * n + 1];
+            s += 1.0 - std::cos(P);
+            c += std::cos(P);
+        }
+    if (plaq_mean) *plaq_mean = c / ((double)Nx * Nt);
+    return beta * s;
+}
+
+// HMC state on the device for one call: angles, momenta, the two force fields, the CG solution and D X
+struct HmcBuffers {
+    double *th = nullptr, *p = nullptr, *Fg = nullptr, *Ff = nullptr;
+    double2 *X = nullptr, *Y = nullptr, *tmp = nullptr;
+};
+
+// dS/dtheta at the angles in B.th for phi (host): U = exp(i theta) into the handle, X = (D^dagger D)^-1 phi by
+// CG (X also returned on the host), Y = D X, Ff = link derivative(psi = X, lambda = Y), Fg = gauge force
+static int hmc_force(ddamg_handle* h, HmcBuffers& B, const std::vector<double>& phi, std::vector<double>& X,
+                     double beta, double cg_tol) {
+    const Geom& g = h->lv[0].g;
+    const long nl = 2L * g.sites;
+    launch_theta_to_links(h->s, B.th, h->lv[0].d.U, nl);
+    ddamg_solve_info info{};
+    const ddamg_status st = krylov_run(h, 1, phi.data(), nullptr, X.data(), 100000, cg_tol, &info);
+    if (st != DDAMG_OK) throw ParamFailure{"HMC force: the CG solve did not converge (" + std::string(ddamg_last_error()) +
+                                           ")"};
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(B.X, X.data(), sizeof(double2) * g.size(), cudaMemcpyHostToDevice, h->s));
+    launch_wilson<double2>(h->s, h->lv[0].d.U, B.X, B.Y, nullptr, g.Nx, g.Nt, h->p.m0, 0, 1);
+    launch_link_derivative(h->s, h->lv[0].d.U, B.X, B.Y, B.Ff, g.Nx, g.Nt);
+    launch_gauge_force(h->s, B.th, B.Fg, g.Nx, g.Nt, beta);
+    return info.iterations;
+}
+
+static HmcBuffers hmc_alloc(ddamg_handle* h) {
+    const Geom& g = h->lv[0].g;
+    const long nl = 2L * g.sites, n = g.size();
+    HmcBuffers B;
+    DDAMG_CUDA_TRY(cudaMalloc(&B.th, sizeof(double) * nl));
+    DDAMG_CUDA_TRY(cudaMalloc(&B.p, sizeof(double) * nl));
+    DDAMG_CUDA_TRY(cudaMalloc(&B.Fg, sizeof(double) * nl));
+    DDAMG_CUDA_TRY(cudaMalloc(&B.Ff, sizeof(double) * nl));
+    DDAMG_CUDA_TRY(cudaMalloc(&B.X, sizeof(double2) * n));
+    DDAMG_CUDA_TRY(cudaMalloc(&B.Y, sizeof(double2) * n));
+    DDAMG_CUDA_TRY(cudaMalloc(&B.tmp, sizeof(double2) * n));
+    return B;
+}
+static void hmc_free(HmcBuffers& B) {
+    for (void* q : {(void*)B.th, (void*)B.p, (void*)B.Fg, (void*)B.Ff, (void*)B.X, (void*)B.Y, (void*)B.tmp})
+        if (q) cudaFree(q);
+    B = HmcBuffers{};
+}
+}  // namespace ddamg
+
+ddamg_status ddamg_hmc_force(ddamg_t* h, const double* theta, const double* phi, double beta, double cg_tol,
+                             double* force) {
+    CHECK_HANDLE(h);
+    if (!theta || !phi || !force || !(cg_tol > 0)) {
+        set_error("ddamg_hmc_force: bad argument");
+        return DDAMG_ERR_BAD_PARAM;
+    }
+    HmcBuffers B;
+    API_BEGIN
+    if (!h->gauge) throw ParamFailure{"load a gauge field first (it sets up the fine-level storage)"};
+    const Geom& g = h->lv[0].g;
+    const long nl = 2L * g.sites, n = g.size();
+    B = hmc_alloc(h);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(B.th, theta, sizeof(double) * nl, cudaMemcpyHostToDevice, h->s));
+    std::vector<double> ph(phi, phi + 2 * n), X(2 * n);
+    hmc_force(h, B, ph, X, beta, cg_tol);
+    DDAMG_CUDA_TRY(cudaMemsetAsync(B.p, 0, sizeof(double) * nl, h->s));
+    launch_hmc_momentum(h->s, B.p, B.Fg, B.Ff, -1.0, nl);  // p = Fg + 2 Ff
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(force, B.p, sizeof(double) * nl, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    h->setup_done = false;
+    hmc_free(B);
+    return DDAMG_OK;
+    }
+    catch (const ParamFailure& e) {
+        hmc_free(B);
+        set_error(e.msg);
+        return DDAMG_ERR_BAD_PARAM;
+    }
+    catch (const CudaFailure&) {
+        hmc_free(B);
+        return DDAMG_ERR_CUDA;
+    }
+}
+
+ddamg_status ddamg_hmc_trajectory(ddamg_t* h, double* theta, double beta, int md_steps, double tau, uint64_t seed,
+                                  double cg_tol, ddamg_hmc_info* info) {
+    CHECK_HANDLE(h);
+    if (!theta || md_steps < 1 || !(tau > 0) || !(cg_tol > 0)) {
+        set_error("ddamg_hmc_trajectory: bad argument");
+        return DDAMG_ERR_BAD_PARAM;
+    }
+    HmcBuffers B;
+    API_BEGIN
+    if (!h->gauge) throw ParamFailure{"load a gauge field first (it sets up the fine-level storage)"};
+    const auto t0 = std::chrono::steady_clock::now();
+    const Geom& g = h->lv[0].g;
+    const long V = g.sites, nl = 2L * V, n = g.size();
+    B = hmc_alloc(h);
+    std::vector<double> th0(theta, theta + nl), p(nl), eta(2 * n), phi(2 * n), X(2 * n), th1(nl), p1(nl);
+    // momenta ~ N(0, 1) per link and eta complex Gaussian with E|eta|^2 = 1, from the counter RNG
+    ddamg_gaussian_field(V, rng64(seed, kStreamHmc, 1), p.data());
+    for (double& v : p) v *= std::sqrt(2.0);
+    ddamg_gaussian_field(n, rng64(seed, kStreamHmc, 2), eta.data());
+    double pp = 0.0, ee = 0.0;
+    for (double v : p) pp += v * v;
+    for (double v : eta) ee += v * v;
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(B.th, th0.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, h->s));
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(B.p, p.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, h->s));
+    // phi = D^dagger eta at the starting field; then S_f(start) = phi^dagger (D^dagger D)^-1 phi = |eta|^2
+    launch_theta_to_links(h->s, B.th, h->lv[0].d.U, nl);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(B.tmp, eta.data(), sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    launch_wilson<double2>(h->s, h->lv[0].d.U, B.tmp, B.Y, nullptr, g.Nx, g.Nt, h->p.m0, 1, 1);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(phi.data(), B.Y, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    const double H0 = 0.5 * pp + host_gauge_action(th0, g.Nx, g.Nt, beta, nullptr) + ee;
+    // leapfrog: half step in p, md_steps full steps in theta, half step at the end
+    const double eps = tau / md_steps;
+    int cg = hmc_force(h, B, phi, X, beta, cg_tol);
+    launch_hmc_momentum(h->s, B.p, B.Fg, B.Ff, 0.5 * eps, nl);
+    for (int k = 1; k <= md_steps; k++) {
+        launch_hmc_theta(h->s, B.th, B.p, eps, nl);
+        cg += hmc_force(h, B, phi, X, beta, cg_tol);
+        launch_hmc_momentum(h->s, B.p, B.Fg, B.Ff, k < md_steps ? eps : 0.5 * eps, nl);
+    }
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(th1.data(), B.th, sizeof(double) * nl, cudaMemcpyDeviceToHost, h->s));
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(p1.data(), B.p, sizeof(double) * nl, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    double pp1 = 0.0, sf1 = 0.0;
+    for (double v : p1) pp1 += v * v;
+    for (long i = 0; i < 2 * n; i++) sf1 += phi[i] * X[i];  // Re(phi^dagger X), X solved at the end field
+    const double H1 = 0.5 * pp1 + host_gauge_action(th1, g.Nx, g.Nt, beta, nullptr) + sf1;
+    const double dH = H1 - H0;
+    const double u = u01(rng64(seed, kStreamHmc, 3));
+    const bool acc = std::isfinite(dH) && (dH <= 0.0 || u < std::exp(-dH));
+    std::vector<double>& out = acc ? th1 : th0;
+    for (long i = 0; i < nl; i++) theta[i] = out[i] - 2.0 * kPi * std::floor((out[i] + kPi) / (2.0 * kPi));
+    // the handle's gauge field becomes the returned one
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(B.th, theta, sizeof(double) * nl, cudaMemcpyHostToDevice, h->s));
+    launch_theta_to_links(h->s, B.th, h->lv[0].d.U, nl);
+    sync(h);
+    h->setup_done = false;
+    if (info) {
+        info->accepted = acc ? 1 : 0;
+        info->dH = dH;
+        std::vector<double> tv(theta, theta + nl);
+        host_gauge_action(tv, g.Nx, g.Nt, beta, &info->plaquette);
+        info->cg_iterations = cg;
+        info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    hmc_free(B);
+    return DDAMG_OK;
+    }
+    catch (const ParamFailure& e) {
+        hmc_free(B);
+        set_error(e.msg);
+        return DDAMG_ERR_BAD_PARAM;
+    }
+    catch (const CudaFailure&) {
+        hmc_free(B);
+        return DDAMG_ERR_CUDA;
+    }
 }
 
 ddamg_status ddamg_link_derivative(ddamg_t* h, const double* psi, const double* lambda, double* out) {

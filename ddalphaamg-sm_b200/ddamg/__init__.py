@@ -276,6 +276,27 @@ class Solver:
         """Methods::CG (src/methods.cpp:42-58): D^dagger b, then conjugate_gradient; x solves D x = b."""
         return self.conjugate_gradient(self.D_dagger_phi(b), max_iter=max_iter, tol=tol)
 
+    def hmc_trajectory(self, theta, beta, md_steps=20, tau=1.0, seed=0, cg_tol=1e-10):
+        """One HMC trajectory of the two-flavour Schwinger model from theta ([site][mu], updated in place);
+        returns HmcInfo (accepted, dH, plaquette, cg_iterations, seconds).  The handle's gauge field becomes
+        the returned one; run setUpPhase again before solving."""
+        th = np.ascontiguousarray(theta, dtype=np.float64)
+        info = _lib.HmcInfo()
+        check(self.L.ddamg_hmc_trajectory(self.h, th.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), beta, md_steps,
+                                          tau, seed, cg_tol, ctypes.byref(info)))
+        if th is not theta:
+            theta[...] = th
+        return info
+
+    def hmc_force(self, theta, phi, beta, cg_tol=1e-12):
+        """dS/dtheta of beta sum_P (1 - cos theta_P) + phi^dagger (D^dagger D)^-1 phi at theta ([site][mu])."""
+        th = np.ascontiguousarray(theta, dtype=np.float64)
+        phi = _c(phi)
+        out = np.empty(2 * self.Nx * self.Nt)
+        check(self.L.ddamg_hmc_force(self.h, th.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _dp(phi), beta, cg_tol,
+                                     out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
     def gradient(self, eta, b):
         """dL/dtheta_mu(x) for L = Re(eta^dagger D^-1 b); returns ([site][mu] float64, infos)."""
         eta, b = _c(eta), _c(b)

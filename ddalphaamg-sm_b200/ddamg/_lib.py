@@ -41,6 +41,11 @@ _vp = ctypes.c_void_p
 _h = ctypes.c_void_p
 _st = ctypes.c_int
 _i = ctypes.c_int
+class HmcInfo(ctypes.Structure):
+    _fields_ = [("accepted", ctypes.c_int), ("dH", ctypes.c_double), ("plaquette", ctypes.c_double),
+                ("cg_iterations", ctypes.c_int), ("seconds", ctypes.c_double)]
+
+
 SIGNATURES = {
     "ddamg_params_default": (_st, [ctypes.POINTER(Params)]),
     "ddamg_parse_params_file": (_st, [ctypes.c_char_p, _i, ctypes.POINTER(Params)]),
@@ -86,6 +91,9 @@ SIGNATURES = {
     "ddamg_gauge_metropolis": (_st, [_i, _i, ctypes.c_double, _i, ctypes.c_uint64, ctypes.c_double, _dp, _dp, _i]),
     "ddamg_gaussian_field": (_st, [ctypes.c_int64, ctypes.c_uint64, _dp]),
     "ddamg_from_halo": (_st, [_dp, _i, _i, _i, _dp]),
+    "ddamg_hmc_trajectory": (_st, [_h, _dp, ctypes.c_double, _i, ctypes.c_double, ctypes.c_uint64, ctypes.c_double,
+                                   ctypes.POINTER(HmcInfo)]),
+    "ddamg_hmc_force": (_st, [_h, _dp, _dp, ctypes.c_double, ctypes.c_double, _dp]),
     "ddamg_to_halo": (_st, [_dp, _i, _i, _i, _dp]),
 }
 

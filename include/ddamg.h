@@ -229,6 +229,27 @@ ddamg_status ddamg_gradient(ddamg_t* h, const double* eta, const double* b, doub
 /* the link-derivative kernel alone, given psi = D^-1 b and lambda = D^-dagger eta */
 ddamg_status ddamg_link_derivative(ddamg_t* h, const double* psi, const double* lambda, double* dL_dtheta);
 
+/* ------------------------------------------------------------------ HMC (no reference counterpart: the
+ * reference reads HMC configurations generated elsewhere) */
+typedef struct {
+    int accepted;         /* the trajectory's end point was accepted */
+    double dH;            /* H(end) - H(start) */
+    double plaquette;     /* mean cos(theta_P) of the returned field */
+    int cg_iterations;    /* CG iterations over all force evaluations and the final action */
+    double seconds;       /* wall time of the trajectory */
+} ddamg_hmc_info;
+/* one HMC trajectory of the two-flavour Schwinger model, S = beta sum_P (1 - cos theta_P) +
+ * phi^dagger (D^dagger D)^-1 phi with phi = D^dagger eta: Gaussian momenta and eta from seed, leapfrog
+ * with md_steps steps of tau / md_steps, forces from the gauge plaquettes and the link derivative of
+ * the CG solution (ddamg_cg_normal to cg_tol), Metropolis accept/reject.  theta: [site][mu] in/out
+ * (unchanged when rejected); the handle's gauge field becomes the returned one and its multigrid
+ * setup must be redone before the next solve. */
+ddamg_status ddamg_hmc_trajectory(ddamg_t* h, double* theta, double beta, int md_steps, double tau, uint64_t seed,
+                                  double cg_tol, ddamg_hmc_info* info);
+/* dS/dtheta_mu(x) of that action at theta for a given phi: force[site*2 + mu] (the integrator's force) */
+ddamg_status ddamg_hmc_force(ddamg_t* h, const double* theta, const double* phi, double beta, double cg_tol,
+                             double* force);
+
 /* ------------------------------------------------------------------ inputs (no reference counterpart) */
 /* U(1) Metropolis of S = beta sum_P (1 - cos theta_P), hot start theta ~ U[-pi, pi), on the
  * device; theta: [site][mu]; *acceptance: acceptance rate of the last sweep (may be NULL) */
