@@ -1908,6 +1908,25 @@ static void hmc_free(HmcBuffers& B) {
 }
 }  // namespace ddamg
 
+namespace ddamg {
+// after a failed trajectory or force evaluation: the handle's links back to the caller's (unchanged)
+// angles, best effort, and the device buffers freed
+static void hmc_restore(ddamg_handle* h, HmcBuffers& B, const double* theta) {
+    if (B.th) {
+        const long nl = 2L * h->lv[0].g.sites;
+        if (cudaMemcpyAsync(B.th, theta, sizeof(double) * nl, cudaMemcpyHostToDevice, h->s) == cudaSuccess) {
+            try {
+                launch_theta_to_links(h->s, B.th, h->lv[0].d.U, nl);
+            } catch (...) {
+            }
+            cudaStreamSynchronize(h->s);
+        }
+    }
+    h->setup_done = false;
+    hmc_free(B);
+}
+}  // namespace ddamg
+
 ddamg_status ddamg_hmc_force(ddamg_t* h, const double* theta, const double* phi, double beta, double cg_tol,
                              double* force) {
     CHECK_HANDLE(h);
@@ -1933,11 +1952,13 @@ ddamg_status ddamg_hmc_force(ddamg_t* h, const double* theta, const double* phi,
     return DDAMG_OK;
     }
     catch (const ParamFailure& e) {
+        h->setup_done = false;
         hmc_free(B);
         set_error(e.msg);
         return DDAMG_ERR_BAD_PARAM;
     }
     catch (const CudaFailure&) {
+        h->setup_done = false;
         hmc_free(B);
         return DDAMG_ERR_CUDA;
     }
@@ -2012,12 +2033,12 @@ ddamg_status ddamg_hmc_trajectory(ddamg_t* h, double* theta, double beta, int md
     return DDAMG_OK;
     }
     catch (const ParamFailure& e) {
-        hmc_free(B);
+        hmc_restore(h, B, theta);
         set_error(e.msg);
         return DDAMG_ERR_BAD_PARAM;
     }
     catch (const CudaFailure&) {
-        hmc_free(B);
+        hmc_restore(h, B, theta);
         return DDAMG_ERR_CUDA;
     }
 }

@@ -242,8 +242,8 @@ typedef struct {
  * phi^dagger (D^dagger D)^-1 phi with phi = D^dagger eta: Gaussian momenta and eta from seed, leapfrog
  * with md_steps steps of tau / md_steps, forces from the gauge plaquettes and the link derivative of
  * the CG solution (ddamg_cg_normal to cg_tol), Metropolis accept/reject.  theta: [site][mu] in/out
- * (unchanged when rejected); the handle's gauge field becomes the returned one and its multigrid
- * setup must be redone before the next solve. */
+ * (unchanged when rejected or on an error); the handle's gauge field becomes the returned one and its
+ * multigrid setup must be redone before the next solve. */
 ddamg_status ddamg_hmc_trajectory(ddamg_t* h, double* theta, double beta, int md_steps, double tau, uint64_t seed,
                                   double cg_tol, ddamg_hmc_info* info);
 /* dS/dtheta_mu(x) of that action at theta for a given phi: force[site*2 + mu] (the integrator's force) */
