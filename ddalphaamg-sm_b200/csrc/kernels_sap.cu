@@ -310,65 +310,93 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __r
             if (!anyarn) break;
             __syncthreads();
             apply(sm.basis + (size_t)j * NE * RB);  // w = D_B V_j
-            // classical Gram-Schmidt coefficients <w, V_i>, i <= j, in one reduction: the warp sums of up
-            // to kGsBatch coefficients share one interleaved butterfly, and the CTA totals are formed
-            // once (a thread per coefficient) instead of by every thread that needs them
+            // classical Gram-Schmidt coefficients <w, V_i>, i <= j, and ||w||^2 (slot j + 1) in one
+            // reduction: the warp sums of up to kGsBatch values share one interleaved butterfly, and the
+            // CTA totals are formed once (a thread per value) instead of by every thread that needs them
             const int dbuf = rbuf;
 #pragma unroll
             for (int r = 0; r < RB; r++) {
                 if (!arn[r]) continue;
-                for (int i0 = 0; i0 <= j; i0 += kGsBatch) {
+                for (int i0 = 0; i0 <= j + 1; i0 += kGsBatch) {
                     double2 sv[kGsBatch];
 #pragma unroll
                     for (int g2 = 0; g2 < kGsBatch; g2++) {
                         sv[g2] = make_double2(0.0, 0.0);
-                        if (i0 + g2 <= j)
+                        if (i0 + g2 <= j) {
 #pragma unroll
                             for (int q = 0; q < EPT; q++)
                                 if (ev[q])
                                     sv[g2] = cfmac(to_d(sm.basis[((size_t)(i0 + g2) * RB + r) * NE + sidx(q)]),
                                                    to_d(w[q][r]), sv[g2]);
+                        } else if (i0 + g2 == j + 1) {
+#pragma unroll
+                            for (int q = 0; q < EPT; q++)
+                                if (ev[q]) sv[g2].x += (double)cnorm2(w[q][r]);
+                        }
                     }
                     warp_sum_n<kGsBatch>(sv);
                     if (lane == 0)
 #pragma unroll
                         for (int g2 = 0; g2 < kGsBatch; g2++)
-                            if (i0 + g2 <= j) sm.red[((size_t)rbuf * nw + wid) * SL + r * (kSapMaxM + 1) + i0 + g2] = sv[g2];
+                            if (i0 + g2 <= j + 1) sm.red[((size_t)rbuf * nw + wid) * SL + r * (kSapMaxM + 1) + i0 + g2] = sv[g2];
                 }
             }
             __syncthreads();
-            for (int t = threadIdx.x; t < RB * (j + 1); t += blockDim.x) {
-                const int r = t / (j + 1), slot = r * (kSapMaxM + 1) + (t - r * (j + 1));
+            for (int t = threadIdx.x; t < RB * (j + 2); t += blockDim.x) {
+                const int r = t / (j + 2), slot = r * (kSapMaxM + 1) + (t - r * (j + 2));
                 sm.tot[slot] = total(dbuf, slot);
             }
             __syncthreads();
             rbuf ^= 1;
-            double2 wn[RB];
+            // ||w - V h||^2 = ||w||^2 - sum |h_i|^2 for orthonormal V: no second reduction, unless the
+            // difference cancels below 1e-4 of ||w||^2 (1e-2 for an FP32 basis, whose orthogonality holds
+            // to ~1e-6); then the norm of the updated w is reduced as is
+            constexpr double kCancel = sizeof(R) == 8 ? 1e-4 : 1e-2;
+            double hn[RB];
+            bool reduce_norm = false;
 #pragma unroll
             for (int r = 0; r < RB; r++) {
-                double ww = 0.0;
-                if (arn[r]) {
-                    for (int i = 0; i <= j; i++) {
-                        const V h = from_d<V>(sm.tot[r * (kSapMaxM + 1) + i]);
+                hn[r] = 0.0;
+                if (!arn[r]) continue;
+                const double w2 = sm.tot[r * (kSapMaxM + 1) + j + 1].x;
+                double hh = 0.0;
+                for (int i = 0; i <= j; i++) hh += cnorm2(sm.tot[r * (kSapMaxM + 1) + i]);
+                const double d = w2 - hh;
+                if (d > kCancel * w2) hn[r] = sqrt(d);
+                else reduce_norm = true;  // identical in every thread: the totals are shared
+            }
 #pragma unroll
-                        for (int q = 0; q < EPT; q++)
-                            if (ev[q]) w[q][r] = w[q][r] - cmul(h, sm.basis[((size_t)i * RB + r) * NE + sidx(q)]);
-                    }
+            for (int r = 0; r < RB; r++) {
+                if (!arn[r]) continue;
+                for (int i = 0; i <= j; i++) {
+                    const V h = from_d<V>(sm.tot[r * (kSapMaxM + 1) + i]);
 #pragma unroll
                     for (int q = 0; q < EPT; q++)
-                        if (ev[q]) ww += (double)cnorm2(w[q][r]);
+                        if (ev[q]) w[q][r] = w[q][r] - cmul(h, sm.basis[((size_t)i * RB + r) * NE + sidx(q)]);
                 }
-                wn[r] = make_double2(ww, 0.0);
             }
-            warp_sum_n<RB>(wn);
-            if (lane == 0)
+            if (reduce_norm) {
+                double2 wn[RB];
 #pragma unroll
-                for (int r = 0; r < RB; r++) sm.red[((size_t)rbuf * nw + wid) * SL + r] = wn[r];
-            __syncthreads();
-            double hn[RB];
+                for (int r = 0; r < RB; r++) {
+                    double ww = 0.0;
+                    if (arn[r])
+#pragma unroll
+                        for (int q = 0; q < EPT; q++)
+                            if (ev[q]) ww += (double)cnorm2(w[q][r]);
+                    wn[r] = make_double2(ww, 0.0);
+                }
+                warp_sum_n<RB>(wn);
+                if (lane == 0)
+#pragma unroll
+                    for (int r = 0; r < RB; r++) sm.red[((size_t)rbuf * nw + wid) * SL + r] = wn[r];
+                __syncthreads();
+#pragma unroll
+                for (int r = 0; r < RB; r++) hn[r] = sqrt(total(rbuf, r).x);
+                rbuf ^= 1;
+            }
 #pragma unroll
             for (int r = 0; r < RB; r++) {
-                hn[r] = sqrt(total(rbuf, r).x);
                 if (arn[r] && hn[r] > 0) {
                     const R inv = R(1.0 / hn[r]);
 #pragma unroll
@@ -376,7 +404,6 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block_kernel(Geom g, const V* __r
                         if (ev[q]) sm.basis[((size_t)(j + 1) * RB + r) * NE + sidx(q)] = inv * w[q][r];
                 }
             }
-            rbuf ^= 1;
             if (threadIdx.x < RB && arn[threadIdx.x]) {  // thread r: Hessenberg column j of RHS r
                 const int r = threadIdx.x;
                 double2* H = sm.H + r * (m + 1) * m;
