@@ -39,6 +39,22 @@ REF_BIN = os.path.join(REPO, "oracle", "_ref", "ref_harness_256x256")
 L2_FLUSH_BYTES = 512 << 20
 
 
+def bench_config(world):
+    """The config dict both arms print (identical, so the two lines describe the same run)."""
+    return {"workload": WORKLOAD_NAME, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "l2": f"flushed between steps ({L2_FLUSH_BYTES >> 20} MiB write)"}
+
+
+def mpi_note():
+    """Whether this host has an MPI launcher for the reference's stock multi-rank build."""
+    import shutil
+
+    m = shutil.which("mpirun") or shutil.which("mpiexec")
+    if m:
+        return {"mpirun": m, "note": "an MPI launcher exists, but the timed reference is the single-rank build"}
+    return {"mpirun": None, "note": "no MPI on this host: the reference runs as one rank on 1 core"}
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -234,11 +250,13 @@ def run_reference_arm(args, rank, world):
     line = {
         "impl": "reference", "metric": "time_to_solution", "value": v, "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": {"workload": WORKLOAD_NAME},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": bench_config(world),
+        "concurrency": {"processes_at_once": par_n, "note": "each step is one full solve in its own single-core "
+                                                             "process; value is the median per-solve time"},
         "iterations": timed[0]["iterations"], "rel_residual": timed[0]["relres"],
         "setup_ms": statistics.median(1e3 * r["setup_s"] for r in timed),
         "solve_ms": statistics.median(1e3 * r["solve_s"] for r in timed),
-        "cpu_baseline": {"value": v, "unit": "ms", "cores": 1, "kind": "reference",
+        "cpu_baseline": {"value": v, "unit": "ms", "cores": 1, "kind": "reference", "mpi": mpi_note(),
                          "sample": f"{n} full 256x256 solves of the reference's own code (single rank, MPI stand-in), "
                                    f"run {par_n} at a time as separate single-core processes; first {args.warmup} "
                                    f"discarded; median of {args.steps}; wall {wall:.0f} s"},
@@ -442,7 +460,7 @@ def run_ours(args, rank, world, local_rank):
         if p.returncode == 0:
             r = read_reference(out)
             tts = 1e3 * (r["setup_s"] + r["solve_s"])
-            cpu = {"value": tts, "unit": "ms", "cores": 1, "kind": "reference",
+            cpu = {"value": tts, "unit": "ms", "cores": 1, "kind": "reference", "mpi": mpi_note(),
                    "sample": "one full 256x256 solve (setup + FGMRES(30) V-cycle) of the reference's own code, single "
                              "rank via the MPI stand-in; its stock mt19937 setup",
                    "iterations": r["iterations"], "setup_ms": 1e3 * r["setup_s"], "solve_ms": 1e3 * r["solve_s"]}
@@ -453,9 +471,8 @@ def run_ours(args, rank, world, local_rank):
             "metric": "time_to_solution", "value": ms_per_step, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "l2": f"flushed between steps ({L2_FLUSH_BYTES >> 20} MiB write)",
-                       "metropolis_acceptance": acc, "plaquette": plaq},
+            "config": bench_config(world),
+            "inputs": {"metropolis_acceptance": acc, "plaquette": plaq},
             "iterations": infos[-1].iterations, "rel_residual": infos[-1].rel_residual,
             "setup_ms": 1e3 * infos[-1].setup_seconds, "solve_ms": 1e3 * infos[-1].solve_seconds,
             "rel_err_vs_reference_solution": err_vs_ref,
@@ -522,6 +539,19 @@ def timed_solves(ddamg, torch, dev, p, U, b_dev, R, reps=2):
     return 1e3 * infos[0].setup_seconds, 1e3 * infos[0].solve_seconds, infos, xs
 
 
+def oracle_residuals(N, m0, U, b, xs):
+    """True relative residuals ||b_r - D x_r|| / ||b_r|| of the GPU solutions x_r under the oracle's CPU D_phi
+    (the checker, src/dirac_operator.cpp:24-54), for every right-hand side stored back to back."""
+    import pyoracle as po
+
+    n = 2 * N * N
+    out = []
+    for r in range(len(xs) // n):
+        br = b[r * n:(r + 1) * n]
+        out.append(float(np.linalg.norm(po.dirac(N, N, m0, U, xs[r * n:(r + 1) * n]) - br) / np.linalg.norm(br)))
+    return out
+
+
 def rel_errs(xs, ref, n):
     return [float(np.linalg.norm(xs[r * n:(r + 1) * n] - ref[r * n:(r + 1) * n]) / np.linalg.norm(ref[r * n:(r + 1) * n]))
             for r in range(len(xs) // n)]
@@ -549,7 +579,12 @@ def mixed_1024(ddamg, torch, dev, R=16):
     sb, tb, ib, xb = timed_solves(ddamg, torch, dev, p(ddamg.PREC_MIXED, R), U, b_dev, R)
     assert np.linalg.norm(xB64[:n] - x64) / np.linalg.norm(x64) < 1e-8
     errs = rel_errs(xb, xB64, n)
+    ores = {"fp64_single": max(oracle_residuals(N, -0.07, U, b[:n], x64)),
+            "fp64_batched_max": max(oracle_residuals(N, -0.07, U, b, xB64)),
+            "mixed_single": max(oracle_residuals(N, -0.07, U, b[:n], xm)),
+            "mixed_batched_max": max(oracle_residuals(N, -0.07, U, b, xb))}
     return {
+        "oracle_true_rel_residual": ores,
         "workload": f"1024x1024 beta=4 (2000 sweeps, acceptance {acc:.3f}), m0=-0.07, 3 levels Nv=16, "
                     f"FGMRES(30) V-cycle to 1e-10; {R} Gaussian RHS",
         "fp64_single": {"setup_ms": s64, "solve_ms": t64, "iterations": i64[0].iterations,
@@ -599,6 +634,9 @@ def batched_512(ddamg, torch, dev):
                          128 * 64 * 16384 + 2 * 2048 * R * 64 * 4)
     errs = rel_errs(xb, xB, n)
     out = {
+        "oracle_true_rel_residual": {"fp64_single": max(oracle_residuals(N, -0.10, U, b[:n], x64)),
+                                     "fp64_batched_max": max(oracle_residuals(N, -0.10, U, b, xB)),
+                                     "mixed_batched_64_max": max(oracle_residuals(N, -0.10, U, b, xb))},
         "tensor_pipe": tens,
         "workload": f"512x512 beta=3 (1000 sweeps, acceptance {acc:.3f}), m0=-0.10, 3 levels Nv=16, FGMRES(30) "
                     "V-cycle to 1e-10",
@@ -612,13 +650,16 @@ def batched_512(ddamg, torch, dev):
     }
     # 8 configurations x 8 RHS: one handle per configuration, all set up and solved concurrently
     C, RC = 8, 8
-    handles, bufs = [], []
+    handles, bufs, fields = [], [], []
     for c in range(C):
         thc, _ = ddamg.gauge_metropolis(N, N, 3.0, 1000, 600 + c, device=dev)
         h = ddamg.Solver(p(ddamg.PREC_MIXED, RC))
-        h.load_gauge(np.exp(1j * thc))
-        bc = torch.from_numpy(ddamg.gaussian_field(n * RC, 700 + c).view(np.float64).copy()).to(f"cuda:{dev}")
+        Uc = np.exp(1j * thc)
+        h.load_gauge(Uc)
+        bh = ddamg.gaussian_field(n * RC, 700 + c)
+        bc = torch.from_numpy(bh.view(np.float64).copy()).to(f"cuda:{dev}")
         bufs.append((bc, torch.zeros_like(bc)))
+        fields.append((Uc, bh))
         handles.append(h)
     res = [None] * C
 
@@ -639,7 +680,10 @@ def batched_512(ddamg, torch, dev):
         torch.cuda.synchronize()
         walls.append(1e3 * (time.perf_counter() - t0))
     its = [i.iterations for r in res for i in r]
+    ores8 = max(max(oracle_residuals(N, -0.10, fields[c][0], fields[c][1],
+                                     bufs[c][1].cpu().numpy().view(np.complex128))) for c in range(C))
     out["mixed_8configs_x_8rhs"] = {
+        "oracle_true_rel_residual_max": ores8,
         "wall_ms": walls[-1], "time_to_solution_ms_per_rhs": walls[-1] / (C * RC),
         "iterations": sorted(set(its)), "max_rel_residual": max(i.rel_residual for r in res for i in r),
         "speedup_per_rhs_time_to_solution_vs_fp64_single": (s64 + t64) / (walls[-1] / (C * RC)),

@@ -178,6 +178,12 @@ struct ParamFailure {
     std::string msg;
 };
 struct TimeoutFailure {};
+struct NanFailure {  // a NaN / Inf in an input or an iterate -> DDAMG_ERR_NAN
+    std::string msg;
+};
+struct NotConvergedFailure {  // an inner solve that a call depends on missed its tolerance -> DDAMG_NOT_CONVERGED
+    std::string msg;
+};
 
 // launch bookkeeping: every kernel launch in the library goes through this counter
 extern std::atomic<long long> g_launches;  // kernels launched by the library (all handles)

@@ -173,6 +173,7 @@ struct CoarseGmresWork {
     int* status = nullptr;     // [0] error flag, [1] iterations
     int grid = 0;
     int block = 256;
+    long long spin_limit = 0;  // polls before a grid barrier gives up (<= 0: the default, 2^24)
 };
 void coarse_gmres_prepare(CoarseGmresWork& w, int n, int m, int dof, int device);
 // x = GMRES(m) x restarts solution of D x = b from x0 = b; returns on the stream

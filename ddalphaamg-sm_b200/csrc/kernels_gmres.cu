@@ -10,11 +10,13 @@
 
 namespace ddamg {
 
-constexpr long long kSpinLimit = 1LL << 24;  // ~1-2 s of polling before a barrier gives up
+constexpr long long kSpinLimit = 1LL << 24;  // default: ~1-2 s of polling before a barrier gives up
 
 // Bounded grid barrier: arrive on bar[0], wait for the generation bar[1] to move.  On timeout
 // (or when another CTA already failed) it sets status[0] and returns false; callers return.
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status, unsigned nblocks) {
+// Every CTA of the cooperative grid is resident, so a CTA that gives up only makes the others
+// leave at their next wait: the kernel always ends.
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status, unsigned nblocks, long long limit) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -35,7 +37,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status, unsigne
                     good = 0;
                     break;
                 }
-                if (++spins > kSpinLimit) {
+                if (++spins > limit) {
                     atomicExch(status, 1);
                     good = 0;
                     break;
@@ -62,6 +64,7 @@ struct GmresK {
     int* status;
     int Nx, Nt, dof, m, restarts, P;
     double m0, tol;
+    long long spin_limit;
 };
 
 // out = [b -] D in on this CTA's sites.  The CTA's (site, direction) pairs are spread over its
@@ -203,7 +206,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
 
     // x = x0 = b
     for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) k.x[e] = k.b[e];
-    if (!grid_barrier(k.bar, k.status, G)) return;
+    if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;
     apply_own<NI>(k, k.x, u0, k.b, s0, s1, part);  // u_0 = r = b - D x
     __syncthreads();
     {
@@ -216,7 +219,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
         double2 t = block_sum(make_double2(rr, bb), red);
         if (threadIdx.x == 0) pC[(long)blockIdx.x * k.P] = t;
     }
-    if (!grid_barrier(k.bar, k.status, G)) return;
+    if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;
     double err, norm_b;
     {
         const double2 t = reduce_slot0(k, pC, &s_sum);
@@ -241,7 +244,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
             apply_own<NI>(k, k.V + (long)j * n, k.w, nullptr, s0, s1, part, sc[j]);
             __syncthreads();
             partial_dots(k, k.w, j + 1, pA, e0, e1, n);  // (u_i, w)
-            if (!grid_barrier(k.bar, k.status, G)) return;
+            if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;
             reduce_partials(k, pA, j + 1, h);
             for (int i = threadIdx.x; i <= j; i += blockDim.x) h[i] = sc[i] * h[i];  // h_i = (v_i, w)
             __syncthreads();
@@ -253,7 +256,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
             }
             __syncthreads();
             partial_dots(k, k.w, j + 1, pB, e0, e1, n);
-            if (!grid_barrier(k.bar, k.status, G)) return;
+            if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;
             reduce_partials(k, pB, j + 1, h2);
             for (int i = threadIdx.x; i <= j; i += blockDim.x) h2[i] = sc[i] * h2[i];
             __syncthreads();
@@ -271,7 +274,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
                 if (threadIdx.x == 0) pC[(long)blockIdx.x * k.P] = t;
             }
             for (int i = threadIdx.x; i <= j; i += blockDim.x) h[i] = h[i] + h2[i];
-            if (!grid_barrier(k.bar, k.status, G)) return;  // also publishes u_{j+1}
+            if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;  // also publishes u_{j+1}
             const double hn = sqrt(reduce_slot0(k, pC, &s_sum).x);
             if (threadIdx.x == 0) {  // FGMRES::rotation (src/fgmres.cpp:99-115) on column j
                 sc[j + 1] = hn > 0 ? 1.0 / hn : 0.0;
@@ -298,7 +301,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
                 break;
             }
         }
-        if (!grid_barrier(k.bar, k.status, G)) return;  // the Hessenberg columns of block 0 visible
+        if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;  // the Hessenberg columns of block 0 visible
         // solve_upper_triangular (src/fgmres.cpp:118-128), column-oriented
         for (int i = threadIdx.x; i < maxIt; i += blockDim.x) eta[i] = gm[i];
         __syncthreads();
@@ -315,7 +318,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
             for (int jj = 0; jj < maxIt; jj++) a = cfma(eta[jj], k.V[(long)jj * n + e], a);
             k.x[e] = a;
         }
-        if (!grid_barrier(k.bar, k.status, G)) return;
+        if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;
         apply_own<NI>(k, k.x, u0, k.b, s0, s1, part);  // new residual into slot 0
         __syncthreads();
         {
@@ -325,7 +328,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
             double2 t = block_sum(make_double2(rr, 0.0), red3);
             if (threadIdx.x == 0) pC[(long)blockIdx.x * k.P] = t;
         }
-        if (!grid_barrier(k.bar, k.status, G)) return;
+        if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;
         err = sqrt(reduce_slot0(k, pC, &s_sum).x);
         if (err < k.tol * norm_b) {
             iters = kk * m + maxIt;
@@ -384,6 +387,7 @@ void launch_coarse_gmres(cudaStream_t s, const CoarseGmresWork& w, const double2
     k.P = m + 2;
     k.m0 = m0;
     k.tol = tol;
+    k.spin_limit = w.spin_limit > 0 ? w.spin_limit : kSpinLimit;
     DDAMG_CUDA_TRY(cudaMemsetAsync(w.bar, 0, 2 * sizeof(unsigned), s));
     DDAMG_CUDA_TRY(cudaMemsetAsync(w.status, 0, 2 * sizeof(int), s));
     size_t smem = coarse_gmres_smem((long)Nx * Nt, w.grid, m, dof);

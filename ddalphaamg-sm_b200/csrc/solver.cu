@@ -58,6 +58,15 @@ struct LevelData {
     std::map<int, int> rb_choice; // 2 * batch width + fp32 -> right-hand sides per CTA (CUDA cores)
 };
 constexpr int kTcMinRhs = 8;  // fewer right-hand sides leave too little link reuse for the tensor cores
+// A Schwarz-block layout of the fine level other than the parameters file's: the block counts of
+// SAP_fine_level as FGMRES_SAP and Methods::SAP build it (include/sap.h:185-233), with its red and
+// black block lists on the device
+struct SapLayout {
+    Geom g;
+    int* red = nullptr;
+    int* black = nullptr;
+    int nred = 0, nblack = 0;
+};
 template <typename V> LevelBufs<V>& B(LevelData& L);
 template <> LevelBufs<double2>& B<double2>(LevelData& L) { return L.d; }
 template <> LevelBufs<float2>& B<float2>(LevelData& L) { return L.f; }
@@ -120,6 +129,8 @@ struct ddamg_handle {
     bool graphs_off = false;  // a capture failed: launch directly from then on
     double prof_ms[kProfKinds][DDAMG_MAX_LEVELS] = {};
     long long prof_n[kProfKinds][DDAMG_MAX_LEVELS] = {};
+    // fine-level Schwarz layouts by block counts (FGMRES_SAP, stand-alone fine SAP), made on first use
+    std::map<std::pair<int, int>, ddamg::SapLayout> fine_sap;
 };
 
 namespace ddamg {
@@ -366,6 +377,7 @@ static void allocate(ddamg_handle* h) {
     h->cg.H = dalloc_t<double2>(h, (size_t)(cm + 1) * cm);
     h->cg.bar = dalloc_t<unsigned>(h, 2);
     h->cg.status = dalloc_t<int>(h, 2);
+    h->cg.spin_limit = p.coarse_barrier_polls;
     // extra lanes so the coarsest solves of a batch run side by side (each a cooperative grid)
     const int lanes = std::min(p.max_rhs, 8);
     DDAMG_CUDA_TRY(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
@@ -442,9 +454,10 @@ template <typename V> static int rb_for(ddamg_handle* h, int l, const V* r, cons
 // SAP_C::SAP (src/sap.cpp:81-165) on nrhs independent vectors; returns the reference's value
 // for rhs 0 when want_iters (one host sync), else nu.
 template <typename V>
-static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, bool x_zero, int nrhs, bool want_iters) {
+static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, bool x_zero, int nrhs, bool want_iters,
+                 const SapLayout* lay = nullptr) {
     LevelData& D = h->lv[l];
-    const Geom& g = D.g;
+    const Geom& g = lay ? lay->g : D.g;  // the block layout of the sweeps (the operator is the level's)
     const long n = g.size();
     V* r = B<V>(D).r;
     DDAMG_CUDA_TRY(cudaMemsetAsync(D.done, 0, sizeof(int) * nrhs, h->s));
@@ -456,8 +469,8 @@ static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, b
               D.done};
     for (int it = 0; it < nu; it++) {
         for (int colour = 0; colour < 2; colour++) {
-            a.blocks = colour == 0 ? D.red : D.black;
-            a.nblocks = colour == 0 ? D.nred : D.nblack;
+            a.blocks = colour == 0 ? (lay ? lay->red : D.red) : (lay ? lay->black : D.black);
+            a.nblocks = colour == 0 ? (lay ? lay->nred : D.nred) : (lay ? lay->nblack : D.nblack);
             {
                 ProfScope ps(h, 0, l);
                 if (l == 0) launch_sap_sweep_fine<V>(h->s, g, B<V>(D).U, r, x, a, nrhs);
@@ -1043,6 +1056,14 @@ using namespace ddamg;
         set_error("a bounded device-side wait gave up (grid barrier timeout)");                  \
         return DDAMG_ERR_DEVICE_TIMEOUT;                                                         \
     }                                                                                            \
+    catch (const NanFailure& e) {                                                                \
+        set_error(e.msg);                                                                        \
+        return DDAMG_ERR_NAN;                                                                    \
+    }                                                                                            \
+    catch (const NotConvergedFailure& e) {                                                       \
+        set_error(e.msg);                                                                        \
+        return DDAMG_NOT_CONVERGED;                                                              \
+    }                                                                                            \
     catch (const std::exception& e) {                                                            \
         set_error(e.what());                                                                     \
         return DDAMG_ERR_STATE;                                                                  \
@@ -1092,6 +1113,7 @@ ddamg_status ddamg_params_default(ddamg_params* p) {
     p->device = 0;
     p->tensor_cores = 1;
     p->cuda_graphs = 1;
+    p->coarse_barrier_polls = 1 << 24;
     return DDAMG_OK;
 }
 
@@ -1624,6 +1646,205 @@ ddamg_status ddamg_gmres_plain(ddamg_t* h, const double* b, double* x, int m, in
     API_END
 }
 
+// ------------------------------------------------------------------ stand-alone multigrid, FGMRES_SAP
+namespace ddamg {
+static void check_finite(const double* a, long count, const char* what) {
+    for (long i = 0; i < count; i++)
+        if (!std::isfinite(a[i])) throw NanFailure{std::string("non-finite value in ") + what};
+}
+
+// the fine-level Schwarz layout of sap_x x sap_t blocks (counts), made on first use
+static const SapLayout& fine_layout(ddamg_handle* h, int sx, int st) {
+    const auto key = std::make_pair(sx, st);
+    auto it = h->fine_sap.find(key);
+    if (it != h->fine_sap.end()) return it->second;
+    const Geom& g0 = h->lv[0].g;
+    if (sx < 1 || st < 1 || g0.Nx % sx || g0.Nt % st) bad("SAP block counts must divide the lattice");
+    const int nb = sx * st;
+    // the reference fills RedBlocks[block/2] (src/sap.cpp:30-37): an odd count > 1 overruns it
+    if (nb > 1 && nb % 2) bad("the number of SAP blocks must be even (or 1)");
+    SapLayout L;
+    L.g = g0;
+    L.g.sap_x = sx;
+    L.g.sap_t = st;
+    L.g.sel_x = g0.Nx / sx;
+    L.g.sel_t = g0.Nt / st;
+    const int S = L.g.sel_x * L.g.sel_t, NE = 2 * S;
+    // blocks of up to 256 sites run one per warp; larger ones one per CTA with the Krylov basis in
+    // shared memory
+    if (S > 256 && (NE > 4096 || sap_smem_bytes(h->p.sap_gmres_restart_length, NE, true) > 227 * 1024))
+        bad("SAP block of " + std::to_string(S) + " sites too large (its Krylov basis does not fit in shared memory)");
+    std::vector<int> red, black;
+    for (int b = 0; b < nb; b++) {  // red iff (bx + bt) even (src/sap.cpp:27-38); one block is both
+        const int bx = b / st, bt = b % st;
+        if (nb == 1) {
+            red.push_back(b);
+            black.push_back(b);
+        } else if ((bx + bt) % 2 == 0) red.push_back(b);
+        else black.push_back(b);
+    }
+    L.red = dalloc_t<int>(h, red.size());
+    L.black = dalloc_t<int>(h, black.size());
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(L.red, red.data(), red.size() * sizeof(int), cudaMemcpyHostToDevice, h->s));
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(L.black, black.data(), black.size() * sizeof(int), cudaMemcpyHostToDevice, h->s));
+    L.nred = (int)red.size();
+    L.nblack = (int)black.size();
+    sync(h);
+    return h->fine_sap[key] = L;
+}
+
+// FGMRES_SAP::preconditioner (include/sap.h:269-280): out = 0, one SAP iteration over the layout's
+// blocks in the level-0 working precision (one iteration ends before SAP's convergence test matters)
+static void fine_sap_prec(ddamg_handle* h, const SapLayout& lay, const double2* in, double2* out, int R) {
+    LevelData& D = h->lv[0];
+    const long n = D.g.size() * R;
+    if (D.fp32) {
+        launch_convert<double2, float2>(h->s, in, D.f.eta, n);
+        DDAMG_CUDA_TRY(cudaMemsetAsync(D.f.psi, 0, sizeof(float2) * n, h->s));
+        sap_t<float2>(h, 0, D.f.eta, D.f.psi, 1, 0.0, true, R, false, &lay);
+        launch_convert<float2, double2>(h->s, D.f.psi, out, n);
+    } else {
+        DDAMG_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double2) * n, h->s));
+        sap_t<double2>(h, 0, in, out, 1, 0.0, true, R, false, &lay);
+    }
+}
+}  // namespace ddamg
+
+ddamg_status ddamg_set_coarse_barrier_polls(ddamg_t* h, int polls) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    h->p.coarse_barrier_polls = polls;
+    h->cg.spin_limit = polls;
+    for (auto& w : h->cg_lane) w.spin_limit = polls;
+    // captured V-cycle graphs hold the old limit in their kernel parameters: capture again
+    for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second.exec);
+    h->graphs.clear();
+    h->graph_warm.clear();
+    API_END
+}
+
+ddamg_status ddamg_apply_multilevel(ddamg_t* h, const double* rhs, double* x, int max_cycles, double tol,
+                                    int* cycles, double* rel_residual) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    need_setup(h);
+    if (!rhs || !x || max_cycles < 0 || !(tol > 0)) throw ParamFailure{"ddamg_apply_multilevel: bad argument"};
+    LevelData& D = h->lv[0];
+    const Geom& g0 = D.g;
+    const long n = g0.size();
+    check_finite(rhs, 2 * n, "the right-hand side");
+    check_finite(x, 2 * n, "the initial guess");
+    cudaStream_t s = h->s;
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(h->ob, rhs, sizeof(double2) * n, cudaMemcpyHostToDevice, s));
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(h->ox, x, sizeof(double2) * n, cudaMemcpyHostToDevice, s));
+    double* hn = reinterpret_cast<double*>(h->hpin);
+    launch_norm2<double2>(s, h->ob, n, n, 1, h->dpart, h->dn);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(hn, h->dn, sizeof(double), cudaMemcpyDeviceToHost, s));
+    sync(h);
+    const double norm = std::sqrt(hn[0]);
+    int ran = 0;
+    double err = 0.0;
+    bool conv = false;
+    if (norm == 0.0) {  // the zero right-hand side: x = 0 (the reference would run max_cycles cycles)
+        DDAMG_CUDA_TRY(cudaMemsetAsync(h->ox, 0, sizeof(double2) * n, s));
+        conv = true;
+    }
+    for (int i = 0; i < max_cycles && !conv; i++) {
+        if (!D.fp32) {
+            cycle(h, 0, h->ob, h->ox, false, h->p.cycle, 1);  // v_cycle / k_cycle(0, rhs, out): out is the iterate
+        } else {
+            // the FP32 cycle acts on the FP64 residual from zero; its result corrects the FP64 iterate
+            launch_wilson<double2>(s, D.d.U, h->ox, h->orr, h->ob, g0.Nx, g0.Nt, h->p.m0, 0, 1);
+            outer_prec(h, h->orr, h->ow, 1);
+            launch_add<double2>(s, h->ow, h->ox, n);
+        }
+        // r = rhs - D out with the level-0 operator, ||r|| (src/amg.cpp:186-199)
+        launch_wilson<double2>(s, D.d.U, h->ox, h->orr, h->ob, g0.Nx, g0.Nt, h->p.m0, 0, 1);
+        launch_norm2<double2>(s, h->orr, n, n, 1, h->dpart, h->dn);
+        DDAMG_CUDA_TRY(cudaMemcpyAsync(hn, h->dn, sizeof(double), cudaMemcpyDeviceToHost, s));
+        sync(h);
+        err = std::sqrt(hn[0]);
+        ran = i + 1;
+        if (!std::isfinite(err)) throw NanFailure{"non-finite residual in the multigrid iteration"};
+        if (err < tol * norm) conv = true;
+    }
+    check_coarse_status(h, nullptr);
+    check_tc_status(h);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(x, h->ox, sizeof(double2) * n, cudaMemcpyDeviceToHost, s));
+    sync(h);
+    if (cycles) *cycles = ran;
+    if (rel_residual) *rel_residual = norm > 0 ? err / norm : 0.0;
+    if (!conv) {
+        set_error("no convergence within max_cycles cycles");
+        return DDAMG_NOT_CONVERGED;
+    }
+    API_END
+}
+
+ddamg_status ddamg_fgmres_sap(ddamg_t* h, const double* b, double* x, int blocks_x, int blocks_t, int m,
+                              int restarts, double tol, ddamg_solve_info* info) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (!h->gauge) throw ParamFailure{"no gauge field loaded"};
+    if (!b || !x || m < 1 || restarts < 1 || !(tol > 0)) throw ParamFailure{"ddamg_fgmres_sap: bad argument"};
+    const Geom& g0 = h->lv[0].g;
+    const long n = g0.size();
+    check_finite(b, 2 * n, "the right-hand side");
+    const SapLayout& lay = fine_layout(h, blocks_x, blocks_t);
+    // the outer FGMRES basis: the handle's when it is long enough, else a temporary one
+    const bool own = m <= h->p.fgmres_restart_length;
+    double2* Vb = own ? h->oV : dalloc_t<double2>(h, (size_t)(m + 1) * n);
+    double2* Z = own ? h->oZ : dalloc_t<double2>(h, (size_t)m * n);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(h->ob, b, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    std::function<void(const double2*, double2*, int)> A = [h, &g0](const double2* in, double2* out, int R) {
+        launch_wilson<double2>(h->s, h->lv[0].d.U, in, out, nullptr, g0.Nx, g0.Nt, h->p.m0, 0, R);
+    };
+    std::function<void(const double2*, double2*, int, int)> M = [h, &lay](const double2* in, double2* out, int R,
+                                                                          int) { fine_sap_prec(h, lay, in, out, R); };
+    Krylov<double2> K{Vb, Z, h->ow, h->orr};
+    double rel = 0;
+    int it = 0;
+    DDAMG_CUDA_TRY(cudaEventRecord(h->ev0, h->s));
+    fgmres_host<double2>(h, n, 1, m, restarts, tol, A, &M, h->ob, nullptr, true, h->ox, K, &it, &rel);
+    DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, h->s));
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(x, h->ox, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    float ms = 0;
+    DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    if (!own)
+        for (void* q : {(void*)Vb, (void*)Z}) {
+            cudaFree(q);
+            h->allocs.erase(std::find(h->allocs.begin(), h->allocs.end(), q));
+        }
+    if (info) {
+        info->iterations = it;
+        info->converged = rel < tol;
+        info->rel_residual = rel;
+        info->setup_seconds = 0;
+        info->solve_seconds = ms * 1e-3;
+    }
+    if (!(rel < tol)) return DDAMG_NOT_CONVERGED;
+    API_END
+}
+
+ddamg_status ddamg_sap_fine(ddamg_t* h, const double* v, double* x, int blocks_x, int blocks_t, int nu, double tol,
+                            int* iters) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    if (!h->gauge) throw ParamFailure{"no gauge field loaded"};
+    if (!v || !x || nu < 0) throw ParamFailure{"ddamg_sap_fine: bad argument"};
+    LevelData& D = h->lv[0];
+    const long n = D.g.size();
+    const SapLayout& lay = fine_layout(h, blocks_x, blocks_t);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.eta, v, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(D.d.psi, x, sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+    const int it = sap_t<double2>(h, 0, D.d.eta, D.d.psi, nu, tol, false, 1, true, &lay);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(x, D.d.psi, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    if (iters) *iters = it;
+    API_END
+}
+
 // ------------------------------------------------------------------ comparison solvers
 namespace ddamg {
 static void krylov_alloc(ddamg_handle* h) {
@@ -1879,8 +2100,10 @@ static int hmc_force(ddamg_handle* h, HmcBuffers& B, const std::vector<double>& 
     launch_theta_to_links(h->s, B.th, h->lv[0].d.U, nl);
     ddamg_solve_info info{};
     const ddamg_status st = krylov_run(h, 1, phi.data(), nullptr, X.data(), 100000, cg_tol, &info);
-    if (st != DDAMG_OK) throw ParamFailure{"HMC force: the CG solve did not converge (" + std::string(ddamg_last_error()) +
-                                           ")"};
+    if (st == DDAMG_NOT_CONVERGED)
+        throw NotConvergedFailure{"HMC force: the CG solve did not converge (" + std::string(ddamg_last_error()) + ")"};
+    if (st == DDAMG_ERR_NAN) throw NanFailure{"HMC force: " + std::string(ddamg_last_error())};
+    if (st != DDAMG_OK) throw ParamFailure{"HMC force: the CG solve failed (" + std::string(ddamg_last_error()) + ")"};
     DDAMG_CUDA_TRY(cudaMemcpyAsync(B.X, X.data(), sizeof(double2) * g.size(), cudaMemcpyHostToDevice, h->s));
     launch_wilson<double2>(h->s, h->lv[0].d.U, B.X, B.Y, nullptr, g.Nx, g.Nt, h->p.m0, 0, 1);
     launch_link_derivative(h->s, h->lv[0].d.U, B.X, B.Y, B.Ff, g.Nx, g.Nt);
@@ -1888,10 +2111,10 @@ static int hmc_force(ddamg_handle* h, HmcBuffers& B, const std::vector<double>& 
     return info.iterations;
 }
 
-static HmcBuffers hmc_alloc(ddamg_handle* h) {
+// the buffers are filled in place, so after a failure part way through hmc_free releases what was allocated
+static void hmc_alloc(ddamg_handle* h, HmcBuffers& B) {
     const Geom& g = h->lv[0].g;
     const long nl = 2L * g.sites, n = g.size();
-    HmcBuffers B;
     DDAMG_CUDA_TRY(cudaMalloc(&B.th, sizeof(double) * nl));
     DDAMG_CUDA_TRY(cudaMalloc(&B.p, sizeof(double) * nl));
     DDAMG_CUDA_TRY(cudaMalloc(&B.Fg, sizeof(double) * nl));
@@ -1899,31 +2122,55 @@ static HmcBuffers hmc_alloc(ddamg_handle* h) {
     DDAMG_CUDA_TRY(cudaMalloc(&B.X, sizeof(double2) * n));
     DDAMG_CUDA_TRY(cudaMalloc(&B.Y, sizeof(double2) * n));
     DDAMG_CUDA_TRY(cudaMalloc(&B.tmp, sizeof(double2) * n));
-    return B;
 }
 static void hmc_free(HmcBuffers& B) {
     for (void* q : {(void*)B.th, (void*)B.p, (void*)B.Fg, (void*)B.Ff, (void*)B.X, (void*)B.Y, (void*)B.tmp})
         if (q) cudaFree(q);
     B = HmcBuffers{};
 }
-}  // namespace ddamg
 
-namespace ddamg {
-// after a failed trajectory or force evaluation: the handle's links back to the caller's (unchanged)
-// angles, best effort, and the device buffers freed
-static void hmc_restore(ddamg_handle* h, HmcBuffers& B, const double* theta) {
-    if (B.th) {
+// after a failed trajectory: the handle's links back to the caller's starting angles (best effort), the
+// device buffers freed; the multigrid setup no longer matches the links the trajectory left behind
+static void hmc_restore(ddamg_handle* h, HmcBuffers& B, const std::vector<double>& theta0) {
+    if (B.th && !theta0.empty()) {
         const long nl = 2L * h->lv[0].g.sites;
-        if (cudaMemcpyAsync(B.th, theta, sizeof(double) * nl, cudaMemcpyHostToDevice, h->s) == cudaSuccess) {
+        if (cudaMemcpyAsync(B.th, theta0.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, h->s) == cudaSuccess) {
             try {
                 launch_theta_to_links(h->s, B.th, h->lv[0].d.U, nl);
             } catch (...) {
             }
-            cudaStreamSynchronize(h->s);
         }
+        cudaStreamSynchronize(h->s);
     }
     h->setup_done = false;
     hmc_free(B);
+}
+
+// the HMC entry points map their failures to status codes themselves, because the device buffers and
+// the handle's links must be put right on every path
+static ddamg_status hmc_guard(const std::function<ddamg_status()>& body, const std::function<void()>& cleanup) {
+    try {
+        return body();
+    } catch (const ParamFailure& e) {
+        cleanup();
+        set_error(e.msg);
+        return DDAMG_ERR_BAD_PARAM;
+    } catch (const NotConvergedFailure& e) {
+        cleanup();
+        set_error(e.msg);
+        return DDAMG_NOT_CONVERGED;
+    } catch (const NanFailure& e) {
+        cleanup();
+        set_error(e.msg);
+        return DDAMG_ERR_NAN;
+    } catch (const CudaFailure&) {
+        cleanup();
+        return DDAMG_ERR_CUDA;
+    } catch (const std::exception& e) {
+        cleanup();
+        set_error(e.what());
+        return DDAMG_ERR_STATE;
+    }
 }
 }  // namespace ddamg
 
@@ -1935,33 +2182,37 @@ ddamg_status ddamg_hmc_force(ddamg_t* h, const double* theta, const double* phi,
         return DDAMG_ERR_BAD_PARAM;
     }
     HmcBuffers B;
-    API_BEGIN
-    if (!h->gauge) throw ParamFailure{"load a gauge field first (it sets up the fine-level storage)"};
-    const Geom& g = h->lv[0].g;
-    const long nl = 2L * g.sites, n = g.size();
-    B = hmc_alloc(h);
-    DDAMG_CUDA_TRY(cudaMemcpyAsync(B.th, theta, sizeof(double) * nl, cudaMemcpyHostToDevice, h->s));
-    std::vector<double> ph(phi, phi + 2 * n), X(2 * n);
-    hmc_force(h, B, ph, X, beta, cg_tol);
-    DDAMG_CUDA_TRY(cudaMemsetAsync(B.p, 0, sizeof(double) * nl, h->s));
-    launch_hmc_momentum(h->s, B.p, B.Fg, B.Ff, -1.0, nl);  // p = Fg + 2 Ff
-    DDAMG_CUDA_TRY(cudaMemcpyAsync(force, B.p, sizeof(double) * nl, cudaMemcpyDeviceToHost, h->s));
-    sync(h);
-    h->setup_done = false;
-    hmc_free(B);
-    return DDAMG_OK;
-    }
-    catch (const ParamFailure& e) {
-        h->setup_done = false;
+    bool saved = false;
+    // the force needs the links of theta in the handle for the CG: the handle's own links are kept in
+    // B.tmp (2 complex per site, the size of a fine vector) and put back on every path, so the handle's
+    // gauge field and multigrid setup are unchanged afterwards
+    auto restore_links = [&]() {
+        if (saved)
+            cudaMemcpyAsync(h->lv[0].d.U, B.tmp, sizeof(double2) * 2 * h->lv[0].g.sites, cudaMemcpyDeviceToDevice, h->s);
+        cudaStreamSynchronize(h->s);
         hmc_free(B);
-        set_error(e.msg);
-        return DDAMG_ERR_BAD_PARAM;
-    }
-    catch (const CudaFailure&) {
-        h->setup_done = false;
-        hmc_free(B);
-        return DDAMG_ERR_CUDA;
-    }
+    };
+    return hmc_guard(
+        [&]() -> ddamg_status {
+            if (!h->gauge) throw ParamFailure{"load a gauge field first (it sets up the fine-level storage)"};
+            const Geom& g = h->lv[0].g;
+            const long nl = 2L * g.sites, n = g.size();
+            hmc_alloc(h, B);
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(B.tmp, h->lv[0].d.U, sizeof(double2) * nl, cudaMemcpyDeviceToDevice, h->s));
+            saved = true;
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(B.th, theta, sizeof(double) * nl, cudaMemcpyHostToDevice, h->s));
+            std::vector<double> ph(phi, phi + 2 * n), X(2 * n);
+            hmc_force(h, B, ph, X, beta, cg_tol);
+            DDAMG_CUDA_TRY(cudaMemsetAsync(B.p, 0, sizeof(double) * nl, h->s));
+            launch_hmc_momentum(h->s, B.p, B.Fg, B.Ff, -1.0, nl);  // p = Fg + 2 Ff
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(force, B.p, sizeof(double) * nl, cudaMemcpyDeviceToHost, h->s));
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(h->lv[0].d.U, B.tmp, sizeof(double2) * nl, cudaMemcpyDeviceToDevice, h->s));
+            saved = false;
+            sync(h);
+            hmc_free(B);
+            return DDAMG_OK;
+        },
+        restore_links);
 }
 
 ddamg_status ddamg_hmc_trajectory(ddamg_t* h, double* theta, double beta, int md_steps, double tau, uint64_t seed,
@@ -1972,75 +2223,70 @@ ddamg_status ddamg_hmc_trajectory(ddamg_t* h, double* theta, double beta, int md
         return DDAMG_ERR_BAD_PARAM;
     }
     HmcBuffers B;
-    API_BEGIN
-    if (!h->gauge) throw ParamFailure{"load a gauge field first (it sets up the fine-level storage)"};
-    const auto t0 = std::chrono::steady_clock::now();
-    const Geom& g = h->lv[0].g;
-    const long V = g.sites, nl = 2L * V, n = g.size();
-    B = hmc_alloc(h);
-    std::vector<double> th0(theta, theta + nl), p(nl), eta(2 * n), phi(2 * n), X(2 * n), th1(nl), p1(nl);
-    // momenta ~ N(0, 1) per link and eta complex Gaussian with E|eta|^2 = 1, from the counter RNG
-    ddamg_gaussian_field(V, rng64(seed, kStreamHmc, 1), p.data());
-    for (double& v : p) v *= std::sqrt(2.0);
-    ddamg_gaussian_field(n, rng64(seed, kStreamHmc, 2), eta.data());
-    double pp = 0.0, ee = 0.0;
-    for (double v : p) pp += v * v;
-    for (double v : eta) ee += v * v;
-    DDAMG_CUDA_TRY(cudaMemcpyAsync(B.th, th0.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, h->s));
-    DDAMG_CUDA_TRY(cudaMemcpyAsync(B.p, p.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, h->s));
-    // phi = D^dagger eta at the starting field; then S_f(start) = phi^dagger (D^dagger D)^-1 phi = |eta|^2
-    launch_theta_to_links(h->s, B.th, h->lv[0].d.U, nl);
-    DDAMG_CUDA_TRY(cudaMemcpyAsync(B.tmp, eta.data(), sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
-    launch_wilson<double2>(h->s, h->lv[0].d.U, B.tmp, B.Y, nullptr, g.Nx, g.Nt, h->p.m0, 1, 1);
-    DDAMG_CUDA_TRY(cudaMemcpyAsync(phi.data(), B.Y, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
-    sync(h);
-    const double H0 = 0.5 * pp + host_gauge_action(th0, g.Nx, g.Nt, beta, nullptr) + ee;
-    // leapfrog: half step in p, md_steps full steps in theta, half step at the end
-    const double eps = tau / md_steps;
-    int cg = hmc_force(h, B, phi, X, beta, cg_tol);
-    launch_hmc_momentum(h->s, B.p, B.Fg, B.Ff, 0.5 * eps, nl);
-    for (int k = 1; k <= md_steps; k++) {
-        launch_hmc_theta(h->s, B.th, B.p, eps, nl);
-        cg += hmc_force(h, B, phi, X, beta, cg_tol);
-        launch_hmc_momentum(h->s, B.p, B.Fg, B.Ff, k < md_steps ? eps : 0.5 * eps, nl);
-    }
-    DDAMG_CUDA_TRY(cudaMemcpyAsync(th1.data(), B.th, sizeof(double) * nl, cudaMemcpyDeviceToHost, h->s));
-    DDAMG_CUDA_TRY(cudaMemcpyAsync(p1.data(), B.p, sizeof(double) * nl, cudaMemcpyDeviceToHost, h->s));
-    sync(h);
-    double pp1 = 0.0, sf1 = 0.0;
-    for (double v : p1) pp1 += v * v;
-    for (long i = 0; i < 2 * n; i++) sf1 += phi[i] * X[i];  // Re(phi^dagger X), X solved at the end field
-    const double H1 = 0.5 * pp1 + host_gauge_action(th1, g.Nx, g.Nt, beta, nullptr) + sf1;
-    const double dH = H1 - H0;
-    const double u = u01(rng64(seed, kStreamHmc, 3));
-    const bool acc = std::isfinite(dH) && (dH <= 0.0 || u < std::exp(-dH));
-    std::vector<double>& out = acc ? th1 : th0;
-    for (long i = 0; i < nl; i++) theta[i] = out[i] - 2.0 * kPi * std::floor((out[i] + kPi) / (2.0 * kPi));
-    // the handle's gauge field becomes the returned one
-    DDAMG_CUDA_TRY(cudaMemcpyAsync(B.th, theta, sizeof(double) * nl, cudaMemcpyHostToDevice, h->s));
-    launch_theta_to_links(h->s, B.th, h->lv[0].d.U, nl);
-    sync(h);
-    h->setup_done = false;
-    if (info) {
-        info->accepted = acc ? 1 : 0;
-        info->dH = dH;
-        std::vector<double> tv(theta, theta + nl);
-        host_gauge_action(tv, g.Nx, g.Nt, beta, &info->plaquette);
-        info->cg_iterations = cg;
-        info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    }
-    hmc_free(B);
-    return DDAMG_OK;
-    }
-    catch (const ParamFailure& e) {
-        hmc_restore(h, B, theta);
-        set_error(e.msg);
-        return DDAMG_ERR_BAD_PARAM;
-    }
-    catch (const CudaFailure&) {
-        hmc_restore(h, B, theta);
-        return DDAMG_ERR_CUDA;
-    }
+    std::vector<double> th0;  // the caller's angles: theta is written only once the trajectory has succeeded
+    return hmc_guard(
+        [&]() -> ddamg_status {
+            if (!h->gauge) throw ParamFailure{"load a gauge field first (it sets up the fine-level storage)"};
+            const auto t0 = std::chrono::steady_clock::now();
+            const Geom& g = h->lv[0].g;
+            const long V = g.sites, nl = 2L * V, n = g.size();
+            th0.assign(theta, theta + nl);
+            hmc_alloc(h, B);
+            std::vector<double> p(nl), eta(2 * n), phi(2 * n), X(2 * n), th1(nl), p1(nl), thw(nl);
+            // momenta ~ N(0, 1) per link and eta complex Gaussian with E|eta|^2 = 1, from the counter RNG
+            ddamg_gaussian_field(V, rng64(seed, kStreamHmc, 1), p.data());
+            for (double& v : p) v *= std::sqrt(2.0);
+            ddamg_gaussian_field(n, rng64(seed, kStreamHmc, 2), eta.data());
+            double pp = 0.0, ee = 0.0;
+            for (double v : p) pp += v * v;
+            for (double v : eta) ee += v * v;
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(B.th, th0.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, h->s));
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(B.p, p.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, h->s));
+            // phi = D^dagger eta at the starting field; then S_f(start) = phi^dagger (D^dagger D)^-1 phi = |eta|^2
+            launch_theta_to_links(h->s, B.th, h->lv[0].d.U, nl);
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(B.tmp, eta.data(), sizeof(double2) * n, cudaMemcpyHostToDevice, h->s));
+            launch_wilson<double2>(h->s, h->lv[0].d.U, B.tmp, B.Y, nullptr, g.Nx, g.Nt, h->p.m0, 1, 1);
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(phi.data(), B.Y, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
+            sync(h);
+            const double H0 = 0.5 * pp + host_gauge_action(th0, g.Nx, g.Nt, beta, nullptr) + ee;
+            // leapfrog: half step in p, md_steps full steps in theta, half step at the end
+            const double eps = tau / md_steps;
+            int cg = hmc_force(h, B, phi, X, beta, cg_tol);
+            launch_hmc_momentum(h->s, B.p, B.Fg, B.Ff, 0.5 * eps, nl);
+            for (int k = 1; k <= md_steps; k++) {
+                launch_hmc_theta(h->s, B.th, B.p, eps, nl);
+                cg += hmc_force(h, B, phi, X, beta, cg_tol);
+                launch_hmc_momentum(h->s, B.p, B.Fg, B.Ff, k < md_steps ? eps : 0.5 * eps, nl);
+            }
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(th1.data(), B.th, sizeof(double) * nl, cudaMemcpyDeviceToHost, h->s));
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(p1.data(), B.p, sizeof(double) * nl, cudaMemcpyDeviceToHost, h->s));
+            sync(h);
+            double pp1 = 0.0, sf1 = 0.0;
+            for (double v : p1) pp1 += v * v;
+            for (long i = 0; i < 2 * n; i++) sf1 += phi[i] * X[i];  // Re(phi^dagger X), X solved at the end field
+            const double H1 = 0.5 * pp1 + host_gauge_action(th1, g.Nx, g.Nt, beta, nullptr) + sf1;
+            const double dH = H1 - H0;
+            const double u = u01(rng64(seed, kStreamHmc, 3));
+            const bool acc = std::isfinite(dH) && (dH <= 0.0 || u < std::exp(-dH));
+            const std::vector<double>& out = acc ? th1 : th0;
+            for (long i = 0; i < nl; i++) thw[i] = out[i] - 2.0 * kPi * std::floor((out[i] + kPi) / (2.0 * kPi));
+            // the handle's gauge field becomes the returned one
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(B.th, thw.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, h->s));
+            launch_theta_to_links(h->s, B.th, h->lv[0].d.U, nl);
+            sync(h);
+            h->setup_done = false;
+            std::copy(thw.begin(), thw.end(), theta);  // every step has succeeded
+            if (info) {
+                info->accepted = acc ? 1 : 0;
+                info->dH = dH;
+                host_gauge_action(thw, g.Nx, g.Nt, beta, &info->plaquette);
+                info->cg_iterations = cg;
+                info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            }
+            hmc_free(B);
+            return DDAMG_OK;
+        },
+        [&]() { hmc_restore(h, B, th0); });
 }
 
 ddamg_status ddamg_link_derivative(ddamg_t* h, const double* psi, const double* lambda, double* out) {

@@ -228,6 +228,40 @@ class Solver:
         check(self.L.ddamg_kcycle(self.h, _dp(eta), _dp(psi)))
         return psi
 
+    def applyMultilevel(self, rhs, x0=None, max_cycles=100, tol=1e-10, allow_not_converged=False):
+        """AlgebraicMG::applyMultilevel (src/amg.cpp:177-243): cycles of the handle's kind on the iterate
+        until ||rhs - D x|| < tol ||rhs||; returns (x, cycles run, relative residual)."""
+        rhs = _c(rhs)
+        x = np.zeros_like(rhs) if x0 is None else np.array(x0, dtype=np.complex128)
+        n = ctypes.c_int(0)
+        rel = ctypes.c_double(0)
+        check(self.L.ddamg_apply_multilevel(self.h, _dp(rhs), _dp(x), max_cycles, tol, ctypes.byref(n),
+                                            ctypes.byref(rel)),
+              allow=(_lib.NOT_CONVERGED,) if allow_not_converged else ())
+        return x, n.value, rel.value
+
+    def fgmres_sap(self, b, blocks_x=4, blocks_t=4, m=20, restarts=50, tol=1e-10, allow_not_converged=False):
+        """FGMRES_SAP (include/sap.h:236-333): FGMRES(m) on D_W preconditioned by one fine-level SAP
+        iteration over blocks_x x blocks_t Schwarz blocks (counts); returns (x, SolveInfo)."""
+        b = _c(b)
+        x = np.empty_like(b)
+        info = SolveInfo()
+        check(self.L.ddamg_fgmres_sap(self.h, _dp(b), _dp(x), blocks_x, blocks_t, m, restarts, tol, ctypes.byref(info)),
+              allow=(_lib.NOT_CONVERGED,) if allow_not_converged else ())
+        return x, info
+
+    def SAP_fine(self, v, blocks_x, blocks_t, x0=None, nu=2, tol=1e-10):
+        """SAP_C::SAP of SAP_fine_level over blocks_x x blocks_t blocks (Methods::SAP); returns (x, iterations)."""
+        v = _c(v)
+        x = np.zeros_like(v) if x0 is None else np.array(x0, dtype=np.complex128)
+        it = ctypes.c_int(0)
+        check(self.L.ddamg_sap_fine(self.h, _dp(v), _dp(x), blocks_x, blocks_t, nu, tol, ctypes.byref(it)))
+        return x, it.value
+
+    def set_coarse_barrier_polls(self, polls):
+        """Polls after which a grid barrier of the coarsest-level GMRES gives up (DEVICE_TIMEOUT)."""
+        check(self.L.ddamg_set_coarse_barrier_polls(self.h, int(polls)))
+
     def solve(self, b, nrhs=1, allow_not_converged=False):
         """FGMRES_AMG_{v,k}_cycle::fgmres from x0 = 0; returns (x, [SolveInfo])."""
         b = _c(b)

@@ -26,7 +26,7 @@ class Params(ctypes.Structure):
         ("fgmres_restarts", ctypes.c_int), ("fgmres_tolerance", ctypes.c_double),
         ("smoother_tolerance", ctypes.c_double), ("cycle", ctypes.c_int), ("precision", ctypes.c_int),
         ("max_rhs", ctypes.c_int), ("device", ctypes.c_int), ("tensor_cores", ctypes.c_int),
-        ("cuda_graphs", ctypes.c_int),
+        ("cuda_graphs", ctypes.c_int), ("coarse_barrier_polls", ctypes.c_int),
     ]
 
 
@@ -79,6 +79,10 @@ SIGNATURES = {
     "ddamg_coarse_solve": (_st, [_h, _dp, _dp, ctypes.POINTER(_i)]),
     "ddamg_coarse_gmres_noalloc": (_st, [_vp, _vp, _vp, _i, _i, _i, ctypes.c_double, _i, _i, ctypes.c_double, _vp,
                                          ctypes.POINTER(_i)]),
+    "ddamg_set_coarse_barrier_polls": (_st, [_h, _i]),
+    "ddamg_apply_multilevel": (_st, [_h, _dp, _dp, _i, ctypes.c_double, ctypes.POINTER(_i), _dp]),
+    "ddamg_fgmres_sap": (_st, [_h, _dp, _dp, _i, _i, _i, _i, ctypes.c_double, ctypes.POINTER(SolveInfo)]),
+    "ddamg_sap_fine": (_st, [_h, _dp, _dp, _i, _i, _i, ctypes.c_double, ctypes.POINTER(_i)]),
     "ddamg_vcycle": (_st, [_h, _dp, _dp]),
     "ddamg_kcycle": (_st, [_h, _dp, _dp]),
     "ddamg_solve": (_st, [_h, _dp, _dp, _i, ctypes.POINTER(SolveInfo)]),

@@ -81,6 +81,10 @@ typedef struct {
      * (ddamg_profile) is on and for the K-cycle, whose inner FGMRES is host driven.  No reference
      * counterpart. */
     int cuda_graphs;
+    /* polls (64 ns sleeps apart) after which a grid barrier of the coarsest-level GMRES kernel gives up
+     * and the solve returns DDAMG_ERR_DEVICE_TIMEOUT; default 2^24 (about 1-2 s); <= 0 also means the
+     * default.  The reference's MPI collectives wait without a bound. */
+    int coarse_barrier_polls;
 } ddamg_params;
 
 typedef struct {
@@ -187,19 +191,33 @@ ddamg_status ddamg_coarse_solve(ddamg_t* h, const double* b, double* x, int* ite
  * 5*dof*dof complex per site), b and x (sites*dof complex); stream may be 0.  Scratch comes from
  * one fixed 32 MiB array of complex doubles compiled into the library: the solve must fit in
  * (m+2)*n + (m+1)*m + 3*G*(m+2) + 2 <= 2097152 complex values (n = Nx*Nt*dof, G = min(SMs,
- * (sites+1)/2)) or the call returns DDAMG_ERR_BAD_PARAM; e.g. m = 400 allows n up to about 4,600.
- * The array is device memory of every GPU that runs this code, held until the process exits.
- * The first call on a device looks the array's address up (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  All calls share the one array and it
- * keeps the last call's contents (its barrier and status words are cleared at each call): calls
- * that overlap on the GPU, on any stream, race and give wrong results.  Waits for completion;
+ * (sites+1)/2)) or the call returns DDAMG_ERR_BAD_PARAM; e.g. m = 400 with G = 148 allows n up to
+ * about 4,370.  The array is device memory of every GPU that runs this code, held until the process
+ * exits.  The first call on a device looks the array's address up (cudaGetSymbolAddress) with that
+ * device current.  All calls share the one array and it keeps the last call's contents (its barrier
+ * and status words are cleared at each call): calls that overlap on the GPU, on any stream, race and
+ * give wrong results.  The call synchronizes its stream before it returns (it reads the solve's
+ * status words), so it must not be made while that stream is being captured into a graph;
  * *iterations gets the GMRES iteration count. */
 ddamg_status ddamg_coarse_gmres_noalloc(const void* links, const void* b, void* x, int Nx, int Nt, int dof,
                                         double m0, int m, int restarts, double tol, void* stream,
                                         int* iterations);
+/* changes coarse_barrier_polls of a live handle (launches made after the call use it; V-cycle graphs
+ * captured earlier are dropped and captured again).  No reference counterpart. */
+ddamg_status ddamg_set_coarse_barrier_polls(ddamg_t* h, int polls);
 /* one cycle from psi = 0: AlgebraicMG::v_cycle / k_cycle (src/amg.cpp:64-174) */
 ddamg_status ddamg_vcycle(ddamg_t* h, const double* eta, double* psi);
 ddamg_status ddamg_kcycle(ddamg_t* h, const double* eta, double* psi);
+/* stand-alone multigrid, AlgebraicMG::applyMultilevel (src/amg.cpp:177-243) as Methods::Vcycle /
+ * Kcycle drive it (src/methods.cpp:106-127): up to max_cycles cycles of the handle's kind (V or K) on
+ * the iterate x (initial guess in, result out), each followed by the true residual with the FP64
+ * operator, until ||rhs - D x|| < tol ||rhs||.  In FP64 each cycle acts on x itself as the reference's
+ * does; in mixed precision each cycle runs on the FP64 residual from zero and its result is added to x.
+ * *cycles gets the cycles run (the reference only prints it), *rel_residual the last relative residual
+ * (either may be NULL); DDAMG_NOT_CONVERGED if max_cycles were not enough.  A zero rhs gives x = 0 after
+ * 0 cycles (the reference would iterate max_cycles times). */
+ddamg_status ddamg_apply_multilevel(ddamg_t* h, const double* rhs, double* x, int max_cycles, double tol,
+                                    int* cycles, double* rel_residual);
 /* FGMRES_AMG_v_cycle / _k_cycle::fgmres (include/amg.h:147-270, src/fgmres.cpp:5-97) from
  * x0 = 0 for nrhs right-hand sides; info may be NULL or point to nrhs entries */
 ddamg_status ddamg_solve(ddamg_t* h, const double* b, double* x, int nrhs, ddamg_solve_info* info);
@@ -207,6 +225,21 @@ ddamg_status ddamg_solve_device(ddamg_t* h, const void* b, void* x, int nrhs, dd
 /* FGMRES_fine_level (include/fgmres.h:153-236): unpreconditioned GMRES(m) on D_W */
 ddamg_status ddamg_gmres_plain(ddamg_t* h, const double* b, double* x, int m, int restarts, double tol,
                                ddamg_solve_info* info);
+/* FGMRES_SAP (include/sap.h:236-333) as Methods::FGMRES_sap runs it (src/methods.cpp:83-104): FGMRES(m) x
+ * restarts on D_W from x0 = 0 to tol, preconditioned by one fine-level SAP iteration from zero over
+ * sap_x x sap_t Schwarz blocks (block COUNTS; the reference fixes 4 x 4, SAPV::sap_block_x/t,
+ * include/variables.h:131-132), each block solved by GMRES(sap_gmres_restart_length) x
+ * sap_gmres_restarts to sap_gmres_tolerance.  The blocks must divide the lattice, their number must be
+ * even (or 1), and a block may hold at most 256 sites, or more if its Krylov basis fits in one CTA's
+ * shared memory (about 1000 sites at restart length 5).  The SAP runs in the handle's level-0
+ * precision (FP32 in mixed mode), the outer FGMRES in FP64.  info may be NULL. */
+ddamg_status ddamg_fgmres_sap(ddamg_t* h, const double* b, double* x, int sap_x, int sap_t, int m, int restarts,
+                              double tol, ddamg_solve_info* info);
+/* SAP_C::SAP of SAP_fine_level (src/sap.cpp:81-165) over sap_x x sap_t fine-level blocks, as Methods::SAP
+ * runs it (src/methods.cpp:60-80): x is the initial guess on entry and the result on exit; FP64;
+ * *iters gets SAP's return value (same block limits as ddamg_fgmres_sap) */
+ddamg_status ddamg_sap_fine(ddamg_t* h, const double* v, double* x, int sap_x, int sap_t, int nu, double tol,
+                            int* iters);
 
 /* bi_cgstab (src/conjugate_gradient.cpp:87-176, driven as Methods::BiCG, src/methods.cpp:3-19):
  * BiCGstab on D_W from x0 (NULL: zero) until ||s|| < tol ||b||; info->iterations is the
@@ -246,7 +279,9 @@ typedef struct {
  * multigrid setup must be redone before the next solve. */
 ddamg_status ddamg_hmc_trajectory(ddamg_t* h, double* theta, double beta, int md_steps, double tau, uint64_t seed,
                                   double cg_tol, ddamg_hmc_info* info);
-/* dS/dtheta_mu(x) of that action at theta for a given phi: force[site*2 + mu] (the integrator's force) */
+/* dS/dtheta_mu(x) of that action at theta for a given phi: force[site*2 + mu] (the integrator's force).
+ * The handle's gauge field and multigrid setup are the same afterwards as before, on success and on
+ * error; DDAMG_NOT_CONVERGED if the CG solve misses cg_tol within 100000 iterations. */
 ddamg_status ddamg_hmc_force(ddamg_t* h, const double* theta, const double* phi, double beta, double cg_tol,
                              double* force);
 

@@ -856,6 +856,177 @@ int orc_gmres_plain(const orc_mg* mg, int m, int restarts, double tol, const dou
     return it;
 }
 
+/* ------------------------------------------------------------------ stand-alone multigrid */
+/* AlgebraicMG::applyMultilevel, src/amg.cpp:177-243 (driven by Methods::Vcycle / Kcycle,
+ * src/methods.cpp:106-127): `it` cycles applied to the same iterate (out is the initial guess on
+ * entry), each followed by the true residual ||rhs - D out|| with the level-0 operator; stops
+ * once it is below tol ||rhs||.  Returns the cycles run (the reference only prints them) and the
+ * last relative residual. */
+int orc_apply_multilevel(const orc_mg* mg, int cycle, int it, double tol, const double* rhsp, double* outp,
+                         double* rel_residual) {
+    const cplx* rhs = (const cplx*)rhsp;
+    cplx* out = (cplx*)outp;
+    long n = (long)mg->lv[0].sites * mg->lv[0].dof;
+    cplx* Dx = (cplx*)calloc(n, sizeof(cplx));
+    cplx* r = (cplx*)calloc(n, sizeof(cplx));
+    double norm = sqrt(creal(vdot(rhs, rhs, n)));
+    double err = 0.0;
+    int ran = it;
+    for (int i = 0; i < it; i++) {
+        if (cycle == 0) vcycle(mg, 0, rhs, out);
+        else kcycle(mg, 0, rhs, out);
+        level_op(mg, 0, out, Dx);
+        for (long q = 0; q < n; q++) r[q] = rhs[q] - Dx[q];
+        err = sqrt(creal(vdot(r, r, n)));
+        if (err < tol * norm) {
+            ran = i + 1;
+            break;
+        }
+    }
+    if (rel_residual) *rel_residual = norm > 0 ? err / norm : 0.0;
+    free(Dx);
+    free(r);
+    return ran;
+}
+
+/* ------------------------------------------------------------------ FGMRES with SAP */
+/* The fine-level SAP of SAP_fine_level (include/sap.h:185-233) with its own block counts: the
+ * block operator is SAP_fine_level::D_B (src/sap.cpp:169-218), the global operator D_phi. */
+typedef struct {
+    const orc_mg* mg;
+    int sap_x, sap_t, sel_x, sel_t;
+    int block;
+} fblk;
+
+/* SAP_fine_level::D_B, src/sap.cpp:169-218: the Wilson stencil on one block, neighbours outside
+ * the block read as zero.  The rsign/lsign factors there only touch hops that leave the block, so
+ * they never act; block vectors are [local site][spin]. */
+static void d_block_fine(const void* vctx, const cplx* v, cplx* out) {
+    const fblk* f = (const fblk*)vctx;
+    const orc_mg* mg = f->mg;
+    const cplx* U = mg->U;
+    int Nx = mg->Nx, Nt = mg->Nt, ex = f->sel_x, et = f->sel_t;
+    int bx = f->block / f->sap_t, bt = f->block % f->sap_t;
+    double m0 = mg->m0;
+    for (int mx = 0; mx < ex; mx++)
+        for (int mt = 0; mt < et; mt++) {
+            int m = mx * et + mt;
+            int gx = bx * ex + mx, gt = bt * et + mt;
+            int n = gx * Nt + gt;
+            int l0 = nbr_bwd(Nx, Nt, gx, gt, 0), l1 = nbr_bwd(Nx, Nt, gx, gt, 1);
+            cplx z = 0;
+            cplx r00 = mt + 1 < et ? v[2 * (m + 1)] : z, r01 = mt + 1 < et ? v[2 * (m + 1) + 1] : z;
+            cplx r10 = mx + 1 < ex ? v[2 * (m + et)] : z, r11 = mx + 1 < ex ? v[2 * (m + et) + 1] : z;
+            cplx l00 = mt > 0 ? v[2 * (m - 1)] : z, l01 = mt > 0 ? v[2 * (m - 1) + 1] : z;
+            cplx l10 = mx > 0 ? v[2 * (m - et)] : z, l11 = mx > 0 ? v[2 * (m - et) + 1] : z;
+            cplx rs0 = rsign(Nt, gt, 0), ls0 = lsign(gt, 0), rs1 = 1.0, ls1 = 1.0;
+            out[2 * m] = (m0 + 2) * v[2 * m] - 0.5 * (U[2 * n] * rs0 * (r00 - r01) + U[2 * n + 1] * rs1 * (r10 + I * r11) +
+                                                      conj(U[2 * l0]) * ls0 * (l00 + l01) +
+                                                      conj(U[2 * l1 + 1]) * ls1 * (l10 - I * l11));
+            out[2 * m + 1] = (m0 + 2) * v[2 * m + 1] -
+                             0.5 * (U[2 * n] * rs0 * (-r00 + r01) + U[2 * n + 1] * rs1 * (-I * r10 + r11) +
+                                    conj(U[2 * l0]) * ls0 * (l00 + l01) + conj(U[2 * l1 + 1]) * ls1 * (I * l10 + l11));
+        }
+}
+
+/* one colour sweep of SAP_C::SAP (src/sap.cpp:48-77, 104-139) with the fine block operator */
+static void sap_fine_colour(const fblk* base, int red, const cplx* r, cplx* x) {
+    const orc_mg* mg = base->mg;
+    int nb = base->sap_x * base->sap_t, ex = base->sel_x, et = base->sel_t, Nt = mg->Nt;
+    long nv = (long)ex * et * 2;
+    cplx* rb = (cplx*)malloc(sizeof(cplx) * nv);
+    cplx* eb = (cplx*)malloc(sizeof(cplx) * nv);
+    for (int blk = 0; blk < nb; blk++) {
+        int bx = blk / base->sap_t, bt = blk % base->sap_t;
+        int is_red = ((bx + bt) % 2) == 0;
+        if (nb == 1) is_red = 1; /* single block: RedBlocks = BlackBlocks = {0} */
+        if (nb > 1 && is_red != red) continue;
+        for (int mx = 0; mx < ex; mx++)
+            for (int mt = 0; mt < et; mt++)
+                for (int d = 0; d < 2; d++) rb[(mx * et + mt) * 2 + d] = r[((bx * ex + mx) * Nt + bt * et + mt) * 2 + d];
+        fblk f = *base;
+        f.block = blk;
+        fgmres(nv, mg->k.sap_gmres_m, mg->k.sap_gmres_restarts, mg->k.sap_gmres_tol, d_block_fine, &f, NULL, NULL, rb,
+               rb, eb);
+        for (int mx = 0; mx < ex; mx++)
+            for (int mt = 0; mt < et; mt++)
+                for (int d = 0; d < 2; d++) x[((bx * ex + mx) * Nt + bt * et + mt) * 2 + d] += eb[(mx * et + mt) * 2 + d];
+    }
+    free(rb);
+    free(eb);
+}
+
+/* SAP_C::SAP (src/sap.cpp:81-165) for SAP_fine_level: funcGlobal = D_phi */
+static int sap_fine(const fblk* f, const cplx* v, cplx* x, int nu, double tol) {
+    const orc_mg* mg = f->mg;
+    long n = (long)mg->Nx * mg->Nt * 2;
+    cplx* r = (cplx*)malloc(sizeof(cplx) * n);
+    cplx* Dx = (cplx*)malloc(sizeof(cplx) * n);
+    double v_norm = sqrt(creal(vdot(v, v, n)));
+    int ret = nu;
+    orc_dirac(mg, 0, (const double*)x, (double*)Dx);
+    for (long i = 0; i < n; i++) r[i] = v[i] - Dx[i];
+    for (int it = 0; it < nu; it++) {
+        sap_fine_colour(f, 1, r, x);
+        orc_dirac(mg, 0, (const double*)x, (double*)Dx);
+        for (long i = 0; i < n; i++) r[i] = v[i] - Dx[i];
+        sap_fine_colour(f, 0, r, x);
+        orc_dirac(mg, 0, (const double*)x, (double*)Dx);
+        for (long i = 0; i < n; i++) r[i] = v[i] - Dx[i];
+        double err = sqrt(creal(vdot(r, r, n)));
+        if (err < tol * v_norm) {
+            ret = it;
+            break;
+        }
+    }
+    free(r);
+    free(Dx);
+    return ret;
+}
+
+/* FGMRES_SAP::preconditioner (include/sap.h:269-280): out = 0, then one SAP iteration at the
+ * SAP tolerance (SAPV::sap_tolerance = 1e-10, src/variables.cpp:104) */
+static void fgmres_sap_prec(const void* v, const cplx* in, cplx* out) {
+    const fblk* f = (const fblk*)v;
+    long n = (long)f->mg->Nx * f->mg->Nt * 2;
+    memset(out, 0, sizeof(cplx) * n);
+    sap_fine(f, in, out, 1, 1e-10);
+}
+static void op_dirac_mg(const void* v, const cplx* in, cplx* out) {
+    orc_dirac(((const fblk*)v)->mg, 0, (const double*)in, (double*)out);
+}
+/* FGMRES_SAP (include/sap.h:236-333) as Methods::FGMRES_sap runs it (src/methods.cpp:83-104):
+ * FGMRES(m) x restarts on D_phi from x0 = 0 with the SAP preconditioner over sap_x x sap_t blocks
+ * (block COUNTS; the reference uses SAPV::sap_block_x = sap_block_t = 4, include/variables.h:131-132).
+ * Returns the FGMRES iteration count, or -1 if the blocks do not divide the lattice. */
+int orc_fgmres_sap(const orc_mg* mg, int sap_x, int sap_t, int m, int restarts, double tol, const double* b, double* x) {
+    if (sap_x < 1 || sap_t < 1 || mg->Nx % sap_x || mg->Nt % sap_t) return -1;
+    fblk f = {mg, sap_x, sap_t, mg->Nx / sap_x, mg->Nt / sap_t, 0};
+    long n = (long)mg->Nx * mg->Nt * 2;
+    cplx* x0 = (cplx*)calloc(n, sizeof(cplx));
+    int it = fgmres(n, m, restarts, tol, op_dirac_mg, &f, fgmres_sap_prec, &f, (const cplx*)b, x0, (cplx*)x);
+    free(x0);
+    return it;
+}
+/* SAP_C::SAP with SAP_fine_level over sap_x x sap_t blocks (Methods::SAP, src/methods.cpp:60-80):
+ * x is the initial guess on entry; returns SAP's value */
+int orc_sap_fine(const orc_mg* mg, int sap_x, int sap_t, const double* v, double* x, int nu, double tol) {
+    if (sap_x < 1 || sap_t < 1 || mg->Nx % sap_x || mg->Nt % sap_t) return -1;
+    fblk f = {mg, sap_x, sap_t, mg->Nx / sap_x, mg->Nt / sap_t, 0};
+    return sap_fine(&f, (const cplx*)v, (cplx*)x, nu, tol);
+}
+
+/* D_phi / D_dagger_phi without a hierarchy (for residual checks of large lattices) */
+void orc_dirac_plain(int Nx, int Nt, double m0, const double* U, int dagger, const double* in, double* out) {
+    orc_mg mg;
+    memset(&mg, 0, sizeof(mg));
+    mg.Nx = Nx;
+    mg.Nt = Nt;
+    mg.m0 = m0;
+    mg.U = (cplx*)U;
+    orc_dirac(&mg, dagger, in, out);
+}
+
 /* ------------------------------------------------------------------ comparison solvers */
 /* bi_cgstab, src/conjugate_gradient.cpp:87-176: BiCGstab on D_phi from x0, ||s|| < tol ||phi||;
  * returns k+1 at convergence, max_iter otherwise (as the reference). */

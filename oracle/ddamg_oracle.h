@@ -82,6 +82,20 @@ int orc_solve(const orc_mg* mg, int cycle, int m, int restarts, double tol, cons
 /* plain GMRES(m) on D_W with no preconditioner (FGMRES_fine_level, include/fgmres.h:153-236) */
 int orc_gmres_plain(const orc_mg* mg, int m, int restarts, double tol, const double* b, double* x);
 
+/* stand-alone multigrid, AlgebraicMG::applyMultilevel (src/amg.cpp:177-243): up to `it` cycles
+ * (cycle 0 = V, 1 = K) on the iterate out (initial guess on entry) until the true residual is below
+ * tol ||rhs||; returns the cycles run, *rel_residual the last relative residual */
+int orc_apply_multilevel(const orc_mg* mg, int cycle, int it, double tol, const double* rhs, double* out,
+                         double* rel_residual);
+/* FGMRES_SAP (include/sap.h:236-333, Methods::FGMRES_sap src/methods.cpp:83-104): FGMRES(m) on D_W
+ * from x0 = 0, preconditioned by one fine-level SAP iteration over sap_x x sap_t blocks (counts) */
+int orc_fgmres_sap(const orc_mg* mg, int sap_x, int sap_t, int m, int restarts, double tol, const double* b,
+                   double* x);
+/* SAP_C::SAP with SAP_fine_level over sap_x x sap_t blocks (Methods::SAP, src/methods.cpp:60-80) */
+int orc_sap_fine(const orc_mg* mg, int sap_x, int sap_t, const double* v, double* x, int nu, double tol);
+/* D_phi / D_dagger_phi without a hierarchy: U [site][mu] */
+void orc_dirac_plain(int Nx, int Nt, double m0, const double* U, int dagger, const double* in, double* out);
+
 /* comparison solvers (src/conjugate_gradient.cpp): BiCGstab on D_W from x0, returning k+1 or
  * max_iter; CG on D^dagger D x = phi from x0 = phi, returning k+1 or 0 */
 int orc_bicgstab(const orc_mg* mg, const double* phi, const double* x0, double* x, int max_iter, double tol);

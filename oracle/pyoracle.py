@@ -80,6 +80,16 @@ def lib():
         L.orc_gmres_plain.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _c_dp, _c_dp]
         L.orc_gmres_plain.restype = ctypes.c_int
         L.orc_link_gradient.argtypes = [ctypes.c_void_p, _c_dp, _c_dp, _c_dp]
+        L.orc_apply_multilevel.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _c_dp, _c_dp,
+                                           _c_dp]
+        L.orc_apply_multilevel.restype = ctypes.c_int
+        L.orc_fgmres_sap.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_double, _c_dp, _c_dp]
+        L.orc_fgmres_sap.restype = ctypes.c_int
+        L.orc_sap_fine.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _c_dp, _c_dp, ctypes.c_int,
+                                   ctypes.c_double]
+        L.orc_sap_fine.restype = ctypes.c_int
+        L.orc_dirac_plain.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, _c_dp, ctypes.c_int, _c_dp, _c_dp]
         L.orc_bicgstab.argtypes = [ctypes.c_void_p, _c_dp, _c_dp, _c_dp, ctypes.c_int, ctypes.c_double]
         L.orc_bicgstab.restype = ctypes.c_int
         L.orc_cg_normal.argtypes = [ctypes.c_void_p, _c_dp, _c_dp, ctypes.c_int, ctypes.c_double]
@@ -116,6 +126,15 @@ def default_constants():
 
 
 # ---------------------------------------------------------------- inputs
+def dirac(Nx, Nt, m0, U, phi, dagger=False):
+    """D_phi / D_dagger_phi (src/dirac_operator.cpp:24-85) without building a hierarchy."""
+    U = np.ascontiguousarray(U, dtype=np.complex128)
+    phi = np.ascontiguousarray(phi, dtype=np.complex128)
+    out = np.zeros_like(phi)
+    lib().orc_dirac_plain(Nx, Nt, m0, _p(U), int(bool(dagger)), _p(phi), _p(out))
+    return out
+
+
 def metropolis(Nx, Nt, beta, sweeps, seed, delta=1.0):
     th = np.zeros(2 * Nx * Nt)
     acc = lib().orc_metropolis(Nx, Nt, beta, sweeps, seed, delta, _p(th))
@@ -307,6 +326,28 @@ class Oracle:
         phi = np.ascontiguousarray(phi, dtype=np.complex128)
         x = self._out(phi.size)
         it = lib().orc_cg_normal(self.h, _p(phi), _p(x), max_iter, tol)
+        return x, it
+
+    def apply_multilevel(self, rhs, cycle=0, it=100, tol=1e-10, x0=None):
+        """AlgebraicMG::applyMultilevel (src/amg.cpp:177-243); returns (x, cycles run, rel. residual)."""
+        rhs = np.ascontiguousarray(rhs, dtype=np.complex128)
+        x = self._out(rhs.size) if x0 is None else np.array(x0, dtype=np.complex128)
+        rel = ctypes.c_double(0)
+        n = lib().orc_apply_multilevel(self.h, cycle, it, tol, _p(rhs), _p(x), ctypes.byref(rel))
+        return x, n, rel.value
+
+    def fgmres_sap(self, b, sap_x=4, sap_t=4, m=20, restarts=50, tol=1e-10):
+        """FGMRES_SAP (include/sap.h:236-333); returns (x, iterations)."""
+        b = np.ascontiguousarray(b, dtype=np.complex128)
+        x = self._out(b.size)
+        it = lib().orc_fgmres_sap(self.h, sap_x, sap_t, m, restarts, tol, _p(b), _p(x))
+        return x, it
+
+    def sap_fine(self, v, sap_x, sap_t, x0=None, nu=2, tol=1e-10):
+        """SAP_C::SAP of SAP_fine_level over sap_x x sap_t blocks; returns (x, SAP's value)."""
+        v = np.ascontiguousarray(v, dtype=np.complex128)
+        x = self._out(v.size) if x0 is None else np.array(x0, dtype=np.complex128)
+        it = lib().orc_sap_fine(self.h, sap_x, sap_t, _p(v), _p(x), nu, tol)
         return x, it
 
     def link_gradient(self, psi, lam):

@@ -12,6 +12,10 @@
  *                     <cycle:0=V,1=K> <fgmres_m> <fgmres_restarts> <tol>
  *   ref_harness krylov <levels> <m0> <params> <conf.bin> <rhs.bin> <x0.bin|-> <outdir> <max_iter> <tol>
  *                     (bi_cgstab from x0, then Methods::CG: conjugate_gradient on D^dagger rhs)
+ *   ref_harness multilevel <levels> <m0> <params> <conf.bin> <rhs.bin> <tvec.bin> <outdir> <cycle> <it> <tol>
+ *                     (AlgebraicMG::applyMultilevel after the injected setup; prints its cycle count)
+ *   ref_harness fgmres_sap <levels> <m0> <params> <conf.bin> <rhs.bin> - <outdir> <m> <restarts> <tol>
+ *   ref_harness sapfine <levels> <m0> <params> <conf.bin> <rhs.bin> - <outdir> <xblocks> <tblocks> <nu>
  *
  * conf.bin / rhs.bin use the reference binary record format (src/io.cpp:32-44).
  * probe.bin / tvec.bin / outputs are raw little-endian complex128 arrays
@@ -280,6 +284,58 @@ int main(int argc, char** argv) {
         m.precision(17);
         m << "iterations " << iters << "\nsetup_s " << (t1 - t0) << "\nsolve_s " << (t2 - t1) << "\nrelres "
           << std::sqrt(nr / nb) << "\n";
+        return 0;
+    }
+    if (mode == "multilevel") {
+        /* AlgebraicMG::applyMultilevel (src/amg.cpp:177-243) after an injected setup; it prints the
+         * cycle count itself ("V-cycle converged in N cycles"), which the caller reads from stdout */
+        if (argc < 12) {
+            std::cerr << "multilevel needs cycle it tol\n";
+            return 2;
+        }
+        AMGV::cycle = std::atoi(argv[9]);
+        const int it = std::atoi(argv[10]);
+        const double tol = std::atof(argv[11]);
+        spinor rhs(mpi::maxSizeH), x(mpi::maxSizeH);
+        read_binary(vfile, rhs);
+        AlgebraicMG amg(U, m0, AMGV::nu1, AMGV::nu2);
+        Stream rnd;
+        rnd.load(tfile);
+        setup_injected(amg, rnd);
+        amg.applyMultilevel(it, rhs, x, tol, true);
+        dump("x.bin", interior(x, mpi::width_x, mpi::width_t, 2));
+        return 0;
+    }
+    if (mode == "fgmres_sap") {
+        /* FGMRES_SAP (include/sap.h:236-333) as Methods::FGMRES_sap builds it (src/methods.cpp:83-104) */
+        if (argc < 12) {
+            std::cerr << "fgmres_sap needs m restarts tol\n";
+            return 2;
+        }
+        const int len = std::atoi(argv[9]), restarts = std::atoi(argv[10]);
+        const double tol = std::atof(argv[11]);
+        spinor rhs(mpi::maxSizeH), x0(mpi::maxSizeH), x(mpi::maxSizeH);
+        read_binary(vfile, rhs);
+        FGMRES_SAP fs(LV::Ntot, LV::dof, mpi::maxSizeH, 1, 1, mpi::width_x, mpi::width_t, len, restarts, tol, U, m0);
+        const int iters = fs.fgmres(rhs, x0, x, false);
+        dump("x.bin", interior(x, mpi::width_x, mpi::width_t, 2));
+        std::ofstream(g_out + "/fgmres_sap.txt") << "iterations " << iters << "\n";
+        return 0;
+    }
+    if (mode == "sapfine") {
+        /* Methods::SAP (src/methods.cpp:60-80): SAP_fine_level over xblocks x tblocks, from x = 0 */
+        if (argc < 12) {
+            std::cerr << "sapfine needs xblocks tblocks nu\n";
+            return 2;
+        }
+        const int xb = std::atoi(argv[9]), tb = std::atoi(argv[10]), nu = std::atoi(argv[11]);
+        spinor rhs(mpi::maxSizeH), x(mpi::maxSizeH);
+        read_binary(vfile, rhs);
+        SAP_fine_level sap(mpi::width_x, mpi::width_t, xb, tb, 2, 1);
+        sap.set_params(U, m0);
+        const int it = sap.SAP(rhs, x, nu, 1e-10, false);
+        dump("x.bin", interior(x, mpi::width_x, mpi::width_t, 2));
+        std::ofstream(g_out + "/sapfine.txt") << "iterations " << it << "\n";
         return 0;
     }
     if (mode == "krylov") {

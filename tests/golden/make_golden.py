@@ -44,6 +44,20 @@ CASES = [
     dict(name="seeds_256x256_l3", Nx=256, Nt=256, levels=3, m0=-0.10,
          rows=[[0, 64, 64, 12, 64, 64], [1, 16, 16, 12, 16, 16]], beta=3.0, sweeps=1000, seed=2025, rhs_seed=77,
          m=30, modes=("seeds",), setup_seeds=[1, 2, 3, 4]),
+    # the bench's 256x256 3-level workload: the reference's V-cycle FGMRES(30) solution from
+    # the injected setup stream, for the solution-level check at the bench size
+    dict(name="solve_256x256_l3", Nx=256, Nt=256, levels=3, m0=-0.10,
+         rows=[[0, 64, 64, 12, 64, 64], [1, 16, 16, 12, 16, 16]], beta=3.0, sweeps=1000, seed=2025, rhs_seed=77,
+         m=30, modes=("solve_v",)),
+    # stand-alone multigrid (AlgebraicMG::applyMultilevel), FGMRES with the SAP preconditioner
+    # (FGMRES_SAP) and the fine-level SAP of SAP_fine_level (Methods::SAP) on the inputs of ops_32x32_l2 and
+    # ops_16x32_l3, and FGMRES_SAP on configs[0]'s 64x64 field
+    dict(name="multilevel_32x32_l2", Nx=32, Nt=32, levels=2, m0=-0.15,
+         rows=[[0, 8, 8, 6, 4, 4]], beta=2.0, sweeps=30, seed=12, m=20, modes=("multilevel", "fgmres_sap", "sapfine")),
+    dict(name="multilevel_16x32_l3", Nx=16, Nt=32, levels=3, m0=-0.10,
+         rows=[[0, 4, 8, 4, 2, 4], [1, 2, 4, 6, 2, 2]], beta=2.0, sweeps=20, seed=11, m=20, modes=("multilevel",)),
+    dict(name="fgmres_sap_64x64", Nx=64, Nt=64, levels=2, m0=-0.18,
+         rows=[[0, 16, 16, 10, 16, 16]], beta=2.0, sweeps=500, seed=2024, m=20, modes=("fgmres_sap",)),
     # the comparison solvers of src/conjugate_gradient.cpp (BiCGstab on D, CG on D^dagger D)
     dict(name="krylov_32x32", Nx=32, Nt=32, levels=2, m0=-0.15,
          rows=[[0, 8, 8, 6, 4, 4]], beta=2.0, sweeps=30, seed=12, m=20, modes=("krylov",)),
@@ -122,6 +136,48 @@ def make_case(c, work):
         run([harness, "solve", str(L), repr(c["m0"]), pfile, conf, rhsf, "-", sd, "0", str(c["m"]), "50", "1e-10"])
         meta = dict(line.split() for line in open(os.path.join(sd, "solve.txt")))
         out["ref_iters_V_stock"] = int(meta["iterations"])
+    if "solve_v" in c["modes"]:
+        # V-cycle FGMRES from the injected setup stream; the field and right-hand side are regenerated by the
+        # tests from their seeds, so only the solution and its iteration count are stored
+        sd = os.path.join(work, "solveV")
+        os.makedirs(sd)
+        run([harness, "solve", str(L), repr(c["m0"]), pfile, conf, rhsf, tf, sd, "0", str(c["m"]), "50", "1e-10"])
+        out["ref_x_V"] = rd(os.path.join(sd, "x.bin"))
+        meta = dict(line.split() for line in open(os.path.join(sd, "solve.txt")))
+        out["ref_iters_V"] = int(meta["iterations"])
+        out["ref_relres_V"] = float(meta["relres"])
+        del out["theta"], out["rhs"]
+        for l in range(L):
+            del out[f"probe_{l}"]
+    if "multilevel" in c["modes"]:
+        # applyMultilevel prints "V-cycle converged in N cycles" (or K-cycle); its solution goes to x.bin
+        import re
+        for cyc, tag in ((0, "V"), (1, "K")):
+            md = os.path.join(work, f"ml{tag}")
+            os.makedirs(md)
+            txt = run([harness, "multilevel", str(L), repr(c["m0"]), pfile, conf, rhsf, tf, md, str(cyc), "100",
+                       "1e-10"])
+            m = re.search(r"cycle converged in (\d+) cycles", txt)
+            if not m:
+                raise RuntimeError("applyMultilevel did not report convergence:\n" + txt[-500:])
+            out[f"ref_x_ml_{tag}"] = rd(os.path.join(md, "x.bin"))
+            out[f"ref_cycles_ml_{tag}"] = int(m.group(1))
+    if "fgmres_sap" in c["modes"]:
+        fd = os.path.join(work, "fsap")
+        os.makedirs(fd)
+        run([harness, "fgmres_sap", str(L), repr(c["m0"]), pfile, conf, rhsf, "-", fd, str(c["m"]), "50", "1e-10"])
+        out["ref_x_fsap"] = rd(os.path.join(fd, "x.bin"))
+        out["ref_iters_fsap"] = int(open(os.path.join(fd, "fgmres_sap.txt")).read().split()[1])
+    if "sapfine" in c["modes"]:
+        # SAP_fine_level over 4 x 8 blocks, 3 iterations from x = 0 on the right-hand side
+        fd = os.path.join(work, "sapfine")
+        os.makedirs(fd)
+        run([harness, "sapfine", str(L), repr(c["m0"]), pfile, conf, rhsf, "-", fd, "4", "8", "3"])
+        out["ref_x_sapfine_4x8"] = rd(os.path.join(fd, "x.bin"))
+        out["ref_iters_sapfine_4x8"] = int(open(os.path.join(fd, "sapfine.txt")).read().split()[1])
+    if not ({"ops", "solve", "seeds", "solve_v"} & set(c["modes"])):
+        for l in range(L):  # the probes feed only the "ops" mode
+            del out[f"probe_{l}"]
     if "seeds" in c["modes"]:
         # V-cycle FGMRES iterations of the reference for each injected setup; the field and right-hand
         # side are regenerated by the tests from the stored seeds (theta is kept only for the smaller case)

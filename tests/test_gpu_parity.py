@@ -6,7 +6,8 @@ Tolerances (relative 2-norm of the difference):
     same arithmetic, different summation order;
   * setup products (test vectors, coarse links), SAP, cycles: 1e-9 — the same algorithm, with
     rounding differences amplified through 4 smoothing iterations and Krylov solves;
-  * solutions: within the solver tolerance scaled by the conditioning (stated per test).
+  * solutions: 1e-9 against the reference's FP64 solution (the gate the solver is built to), with
+    the true residual below 1e-10 under the oracle's operator and the iteration count within 10 %.
 """
 import numpy as np
 import pytest
@@ -137,10 +138,12 @@ def test_cycles(golden):
     for name in OPS:
         z = golden(name)
         s, o = make_pair(z)
-        assert rel(s.v_cycle(z["probe_0"]), o.vcycle(z["probe_0"])) < 1e-8, name
+        ev = rel(s.v_cycle(z["probe_0"]), o.vcycle(z["probe_0"]))
         s.close()
         s, o = make_pair(z, cycle=ddamg.CYCLE_K)
-        assert rel(s.k_cycle(z["probe_0"]), o.kcycle(z["probe_0"])) < 1e-8, name
+        ek = rel(s.k_cycle(z["probe_0"]), o.kcycle(z["probe_0"]))
+        print(f"{name}: V-cycle rel diff {ev:.2e}, K-cycle {ek:.2e}")
+        assert ev < 1e-9 and ek < 1e-9, name
         s.close()
 
 
@@ -157,8 +160,10 @@ def test_solve_fp64(golden, name, cycle, tag):
     assert rel(o.dirac(x), z["rhs"]) < 1e-10
     # iteration count within +-10% of the reference's (at least +-1)
     assert abs(info[0].iterations - ref_it) <= max(1, int(0.1 * ref_it)), (info[0].iterations, ref_it)
-    # same solution as the reference to the accuracy the 1e-10 residual allows
-    assert rel(x, z[f"ref_x_{tag}"]) < 1e-8
+    # the reference's FP64 solution to 1e-9
+    e = rel(x, z[f"ref_x_{tag}"])
+    print(f"{name} {tag}: iterations {info[0].iterations} (reference {ref_it}), rel diff to the reference {e:.2e}")
+    assert e < 1e-9
     s.close()
 
 
@@ -169,7 +174,9 @@ def test_solve_mixed(golden, name):
     x, info = s.solve(z["rhs"])
     assert info[0].converged == 1 and info[0].rel_residual < 1e-10
     assert rel(o.dirac(x), z["rhs"]) < 1e-10
-    assert rel(x, z["ref_x_V"]) < 1e-8
+    e = rel(x, z["ref_x_V"])
+    print(f"{name} mixed: rel diff to the reference's FP64 solution {e:.2e}")
+    assert e < 1e-9
     s.close()
 
 
@@ -253,3 +260,49 @@ def test_solve_batched_with_zero_rhs(golden):
     assert np.all(x[:n] == 0) and info[0].iterations == 0
     assert info[1].converged == 1 and rel(o.dirac(x[n:]), z["rhs"]) < 1e-10
     s.close()
+
+
+def test_solve_bench_workload_matches_reference(golden):
+    """The bench workload (256x256 FP64, 3 levels, FGMRES(30) V-cycle): with the reference's setup stream
+    injected, the GPU solve takes the reference's iteration count and lands within 1e-9 of its solution."""
+    z = golden("solve_256x256_l3")
+    Nx, Nt, L = int(z["Nx"]), int(z["Nt"]), int(z["levels"])
+    theta, _ = po.metropolis(Nx, Nt, float(z["beta"]), int(z["sweeps"]), int(z["seed"]))
+    U = po.links_from_theta(theta)
+    b = po.gaussian(2 * Nx * Nt, int(z["rhs_seed"]))
+    s = ddamg.Solver(ddamg.default_params(Nx, Nt, L, float(z["m0"]), z["rows"], fgmres_restart_length=int(z["fgmres_m"])))
+    s.load_gauge(U)
+    s.setUpPhase(vectors=po.uniform(int(z["rnd_count"]), int(z["seed"]) + 1))
+    x, info = s.solve(b)
+    s.close()
+    ref_it = int(z["ref_iters_V"])
+    res = rel(po.dirac(Nx, Nt, float(z["m0"]), U, x), b)
+    e = rel(x, z["ref_x_V"])
+    print(f"256x256: iterations {info[0].iterations} (reference {ref_it}), residual {res:.2e}, rel diff {e:.2e}")
+    assert info[0].converged == 1 and res < 1e-10
+    assert abs(info[0].iterations - ref_it) <= max(1, ref_it // 10)
+    assert e < 1e-9
+
+
+@pytest.mark.parametrize("cycle", [ddamg.CYCLE_V, ddamg.CYCLE_K])
+def test_solve_batched_tensor_cores_vs_oracle(golden, cycle):
+    """The batched mixed solve whose coarse SAP runs on the tensor cores (8 right-hand sides, TF32 block
+    operator): every solution within 1e-9 of the oracle's FP64 solve of the same system (solved to 1e-13),
+    true residual below 1e-10 under the oracle's operator."""
+    z = golden("ops_16x32_l3")
+    R = 8
+    s, o = make_pair(z, precision=ddamg.PREC_MIXED, cycle=cycle, max_rhs=R)
+    n = z["rhs"].size
+    bs = [po.gaussian(n, 600 + r) for r in range(R)]
+    x, infos = s.solve(np.concatenate(bs), nrhs=R)
+    assert "level 1 rhs 8:" in s.autotune_report()  # the tensor-core sweep ran (the autotuner timed it)
+    s.close()
+    worst = 0.0
+    for r in range(R):
+        xr = x[r * n:(r + 1) * n]
+        xo, _ = o.solve(bs[r], cycle=int(cycle), m=20, tol=1e-13)
+        assert infos[r].converged == 1
+        assert rel(o.dirac(xr), bs[r]) < 1e-10
+        worst = max(worst, rel(xr, xo))
+    print(f"tensor-core batched mixed solve, cycle {int(cycle)}: max rel diff to the FP64 oracle {worst:.2e}")
+    assert worst < 1e-9

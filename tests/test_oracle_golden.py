@@ -143,3 +143,59 @@ def test_iterations_per_setup_seed_64(golden):
         _, it = o.solve(z["rhs"], cycle=0, m=int(z["fgmres_m"]))
         its.append(it)
     assert its == [int(v) for v in z["ref_iters_V_seeds"][:4]]
+
+
+@pytest.mark.parametrize("name", ["multilevel_32x32_l2", "multilevel_16x32_l3"])
+@pytest.mark.parametrize("cycle,tag", [(0, "V"), (1, "K")])
+def test_apply_multilevel(golden, name, cycle, tag):
+    """AlgebraicMG::applyMultilevel (src/amg.cpp:177-243): same cycle count, same iterate bit for bit."""
+    z = golden(name)
+    o = make_oracle(z)
+    x, n, relres = o.apply_multilevel(z["rhs"], cycle=cycle, it=100, tol=1e-10)
+    assert n == int(z[f"ref_cycles_ml_{tag}"])
+    assert relres < 1e-10
+    assert rel(x, z[f"ref_x_ml_{tag}"]) < TOL
+
+
+@pytest.mark.parametrize("name", ["multilevel_32x32_l2", "fgmres_sap_64x64"])
+def test_fgmres_sap(golden, name):
+    """FGMRES_SAP (include/sap.h:236-333) with the reference's 4 x 4 SAP blocks."""
+    z = golden(name)
+    Nx, Nt = int(z["Nx"]), int(z["Nt"])
+    o = po.Oracle(Nx, Nt, int(z["levels"]), float(z["m0"]), z["rows"], po.links_from_theta(z["theta"]))
+    x, it = o.fgmres_sap(z["rhs"], 4, 4, m=int(z["fgmres_m"]), restarts=50, tol=1e-10)
+    assert it == int(z["ref_iters_fsap"])
+    assert rel(x, z["ref_x_fsap"]) < TOL
+    assert rel(po.dirac(Nx, Nt, float(z["m0"]), po.links_from_theta(z["theta"]), x), z["rhs"]) < 1e-10
+
+
+def test_sap_fine(golden):
+    """SAP_C::SAP of SAP_fine_level (Methods::SAP) over 4 x 8 blocks, 3 iterations from zero."""
+    z = golden("multilevel_32x32_l2")
+    o = po.Oracle(int(z["Nx"]), int(z["Nt"]), int(z["levels"]), float(z["m0"]), z["rows"],
+                  po.links_from_theta(z["theta"]))
+    x, it = o.sap_fine(z["rhs"], 4, 8, nu=3)
+    assert it == int(z["ref_iters_sapfine_4x8"])
+    assert rel(x, z["ref_x_sapfine_4x8"]) < TOL
+
+
+def test_dirac_plain_matches_hierarchy(golden):
+    z = golden("ops_16x32_l3")
+    U = po.links_from_theta(z["theta"])
+    o = make_oracle(z)
+    for dag in (False, True):
+        assert np.array_equal(po.dirac(int(z["Nx"]), int(z["Nt"]), float(z["m0"]), U, z["probe_0"], dag),
+                              o.dirac(z["probe_0"], dag))
+
+
+def test_solve_256_fixture_regenerates(golden):
+    """The bench workload's fixture stores only the reference's solution: its field and right-hand side come
+    back from their seeds, and the reference's solution has the residual the reference reported."""
+    z = golden("solve_256x256_l3")
+    Nx, Nt = int(z["Nx"]), int(z["Nt"])
+    th, _ = po.metropolis(Nx, Nt, float(z["beta"]), int(z["sweeps"]), int(z["seed"]))
+    U = po.links_from_theta(th)
+    b = po.gaussian(2 * Nx * Nt, int(z["rhs_seed"]))
+    r = rel(po.dirac(Nx, Nt, float(z["m0"]), U, z["ref_x_V"]), b)
+    assert r < 1e-10
+    assert abs(r - float(z["ref_relres_V"])) < 1e-3 * r
