@@ -96,11 +96,17 @@ struct SapArgs {
 template <typename V>
 void launch_sap_sweep_fine(cudaStream_t s, const Geom& g, const V* U, const V* r, V* x, const SapArgs& a,
                            int nrhs);
-// rb: right-hand sides per CTA (0: a default from the batch width and the block size)
+// variant = rb * 4 + kernel: rb right-hand sides per CTA, kernel 0 the block solver with the
+// single-thread Hessenberg update (sap_block_kernel), 1 the latency-trimmed block solver
+// (sap_block2_kernel); 0 lets the launcher choose from the batch width and the block size
 template <typename V>
 void launch_sap_sweep_coarse(cudaStream_t s, const Geom& g, const V* links, const V* r, V* x, const SapArgs& a,
-                             int nrhs, int rb = 0);
-// autotuner of rb: times one sweep per candidate (1, 2, 4, 8) into the scratch field xs; us[4]
+                             int nrhs, int variant = 0);
+// the autotuner's candidate variants
+constexpr int kSapVariantCount = 6;
+constexpr int kSapVariants[kSapVariantCount] = {4 * 1 + 0, 4 * 1 + 1, 4 * 2 + 1, 4 * 4 + 0, 4 * 4 + 1, 4 * 8 + 0};
+// autotuner of the variant: times one sweep per admissible candidate into the scratch field xs;
+// us[kSapVariantCount]; returns the fastest variant
 template <typename V>
 int tune_sap_rb(cudaStream_t s, const Geom& g, const V* links, const V* r, V* xs, const SapArgs& a, int nrhs,
                 double* us);

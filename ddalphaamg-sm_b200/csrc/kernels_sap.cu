@@ -5,6 +5,7 @@
 // operator (Level::SAP_level_l::D_local, src/level.cpp:607-653: neighbours outside the block
 // read as zero, no boundary sign) streams the level's links.
 #include "internal.h"
+#include "sap_common.cuh"
 
 namespace ddamg {
 
@@ -43,28 +44,7 @@ __device__ __forceinline__ float2 level0_hop(const float2* __restrict__ U, int N
     return 0.5f * cmul(coef, u);
 }
 
-// warp sums of N values with one interleaved butterfly (N independent shuffle chains)
-template <int N> __device__ __forceinline__ void warp_sum_n(double2 (&v)[N]) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-        for (int g = 0; g < N; g++) {
-            v[g].x += __shfl_xor_sync(0xffffffffu, v[g].x, o);
-            v[g].y += __shfl_xor_sync(0xffffffffu, v[g].y, o);
-        }
-}
 constexpr int kGsBatch = 6;  // Gram-Schmidt coefficients per interleaved butterfly (restart length 5: all)
-
-struct SapKParams {
-    int m, restarts;
-    double tol, m0;
-    const int* blocks;
-    int nblocks;
-    const int* done;
-    int nrhs;     // vectors in the sweep
-    int ngroups;  // CTAs per Schwarz block: ceil(nrhs / RB)
-};
-
 
 // Shared memory of one CTA: RB right-hand sides of one Schwarz block.  Vectors are stored
 // [rhs][element], so a warp's Gram-Schmidt loads and stores of one right-hand side are
@@ -985,9 +965,17 @@ static bool rb_admissible(int rb, int nrhs, int m, int NE, size_t vbytes) {
     return smem <= 227 * 1024 && rb * (int)(vbytes / 8) <= 8;  // shared memory and register budget
 }
 
+// A coarse sweep variant is rb * 4 + kernel: rb right-hand sides per CTA and kernel 0 = sap_block_kernel,
+// 1 = sap_block2_kernel; variant 0 lets the launcher choose.
+static bool variant_admissible(int variant, int nrhs, int m, int NE, size_t vbytes) {
+    const int rb = variant / 4, kern = variant % 4;
+    if (rb < 1 || kern > 1 || !rb_admissible(rb, nrhs, m, NE, vbytes)) return false;
+    return kern == 0 || sap2_fits(rb, m, NE, vbytes);
+}
+
 template <typename V, bool DENSE>
 static void launch_sap(cudaStream_t s, const Geom& g, const V* L, const V* r, V* x, const SapArgs& a, int nrhs,
-                       int rb_req = 0) {
+                       int variant = 0) {
     if (a.m > kSapMaxM) throw ParamFailure{"SAP block GMRES restart length above 8 is not supported"};
     const int NE = g.sel_x * g.sel_t * g.dof;
     const int threads = std::min(1024, ((NE + 31) / 32) * 32);
@@ -995,8 +983,17 @@ static void launch_sap(cudaStream_t s, const Geom& g, const V* L, const V* r, V*
     SapKParams p{a.m, a.restarts, a.tol, a.m0, a.blocks, a.nblocks, a.done, nrhs, 1};
     // level 0 keeps one vector per CTA: its links are 32 B per site, so there is nothing to share,
     // and a wider CTA would only cost shared memory and occupancy
-    int rb = DENSE ? pick_rb(nrhs, ept, a.m, NE, threads, sizeof(V)) : 1;
-    if (DENSE && rb_req > 0 && rb_admissible(rb_req, nrhs, a.m, NE, sizeof(V))) rb = rb_req;
+    int rb = DENSE ? pick_rb(nrhs, ept, a.m, NE, threads, sizeof(V)) : 1, kern = 0;
+    if (DENSE && variant > 0 && variant_admissible(variant, nrhs, a.m, NE, sizeof(V))) {
+        rb = variant / 4;
+        kern = variant % 4;
+    }
+    if (DENSE && kern == 1) {
+        if (rb == 4) launch_sap2<V, 4>(s, g, L, r, x, p);
+        else if (rb == 2) launch_sap2<V, 2>(s, g, L, r, x, p);
+        else launch_sap2<V, 1>(s, g, L, r, x, p);
+        return;
+    }
     // blocks of at most 384 unknowns: a 384-thread bound leaves 168 registers per thread, enough to
     // keep 12 link loads in flight per right-hand side group
     if (DENSE && ept == 1 && threads <= 384 && (rb == 1 || rb == 4)) {
@@ -1040,29 +1037,35 @@ void launch_sap_sweep_fine(cudaStream_t s, const Geom& g, const V* U, const V* r
 }
 template <typename V>
 void launch_sap_sweep_coarse(cudaStream_t s, const Geom& g, const V* links, const V* r, V* x, const SapArgs& a,
-                             int nrhs, int rb) {
-    launch_sap<V, true>(s, g, links, r, x, a, nrhs, rb);
+                             int nrhs, int variant) {
+    launch_sap<V, true>(s, g, links, r, x, a, nrhs, variant);
 }
 
-// Autotuner for the CUDA-core coarse sweep: times one sweep per admissible count of right-hand sides
-// per CTA (1, 2, 4, 8), accumulating into the scratch field xs (its contents do not matter), and
-// returns the fastest; us[i] gets the time of candidate i (negative: not admissible).  Synchronises.
+// Autotuner for the CUDA-core coarse sweep: times one sweep per admissible variant (rb 1, 2, 4, 8
+// right-hand sides per CTA, each with the kernels that take it), accumulating into the scratch field xs
+// (its contents do not matter), and returns the fastest variant; us[i] gets the time of
+// kSapVariants[i] (negative: not admissible).  Synchronises.
 template <typename V>
 int tune_sap_rb(cudaStream_t s, const Geom& g, const V* links, const V* r, V* xs, const SapArgs& a, int nrhs,
                 double* us) {
-    static const int cand[4] = {1, 2, 4, 8};
     const int NE = g.sel_x * g.sel_t * g.dof;
     cudaEvent_t e0, e1;
     DDAMG_CUDA_TRY(cudaEventCreate(&e0));
     DDAMG_CUDA_TRY(cudaEventCreate(&e1));
     int best = 0;
     double best_us = -1;
-    for (int i = 0; i < 4; i++) {
+    // where sap_block2_kernel takes the shape, only its variants compete: they give bit-identical results
+    // for every right-hand side whatever their width, so two handles agree whichever one the timing picks
+    bool new_ok = false;
+    for (int i = 0; i < kSapVariantCount; i++)
+        new_ok |= kSapVariants[i] % 4 == 1 && variant_admissible(kSapVariants[i], nrhs, a.m, NE, sizeof(V));
+    for (int i = 0; i < kSapVariantCount; i++) {
         us[i] = -1;
-        if (!rb_admissible(cand[i], nrhs, a.m, NE, sizeof(V))) continue;
-        launch_sap<V, true>(s, g, links, r, xs, a, nrhs, cand[i]);  // warm-up
+        const int v = kSapVariants[i];
+        if (!variant_admissible(v, nrhs, a.m, NE, sizeof(V)) || (new_ok && v % 4 == 0)) continue;
+        launch_sap<V, true>(s, g, links, r, xs, a, nrhs, v);  // warm-up
         DDAMG_CUDA_TRY(cudaEventRecord(e0, s));
-        launch_sap<V, true>(s, g, links, r, xs, a, nrhs, cand[i]);
+        launch_sap<V, true>(s, g, links, r, xs, a, nrhs, v);
         DDAMG_CUDA_TRY(cudaEventRecord(e1, s));
         DDAMG_CUDA_TRY(cudaEventSynchronize(e1));
         float ms = 0;
@@ -1070,12 +1073,12 @@ int tune_sap_rb(cudaStream_t s, const Geom& g, const V* links, const V* r, V* xs
         us[i] = 1e3 * ms;
         if (best_us < 0 || us[i] < best_us) {
             best_us = us[i];
-            best = cand[i];
+            best = v;
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    return best > 0 ? best : 1;
+    return best > 0 ? best : 4;
 }
 template int tune_sap_rb<double2>(cudaStream_t, const Geom&, const double2*, const double2*, double2*,
                                   const SapArgs&, int, double*);

@@ -1,0 +1,537 @@
+// Coarse-level SAP colour sweep with the block GMRES control trimmed for latency
+// (SAP_C::SAP inner loops, src/sap.cpp:48-77 and 104-139; FGMRES::fgmres with the identity
+// preconditioner, src/fgmres.cpp:5-128, x0 = r_B as src/sap.cpp:65; block operator
+// Level::SAP_level_l::D_local, src/level.cpp:607-653).
+#include "internal.h"
+#include "sap_common.cuh"
+
+namespace ddamg {
+
+// ---------------------------------------------------------------- coarse levels, restart length M
+// The block solve of sap_block_kernel (RB right-hand sides of one Schwarz block per CTA, one block
+// element per thread) restructured around what its phase timing showed (cycles per Arnoldi step at
+// 256x256 level 1, FP64, one right-hand side: block-operator application 9.1 K, Gram-Schmidt warp
+// butterfly 2.6 K, totals and update 1.9 K, Givens 1.9 K, barrier waits 3.5 K):
+//  * the multi-value warp sums halve the value set at each of the first levels (a double2 costs four
+//    32-bit shuffles per level, so six coefficients cost 120 shuffles as a plain butterfly, 36 here);
+//  * every warp forms the CTA totals itself from the warps' partial sums (a quarter of the warps per
+//    lane group, then two butterfly levels; the same order in every warp, so all threads hold
+//    bit-identical totals): one CTA barrier per reduction;
+//  * warp 0 forms Hessenberg column j, the Givens rotation and the break flag after its own update;
+//    the flag is read after the next step's first barrier, where the reference reads it;
+//  * norms and the rotation use one reciprocal square root (1/sqrt(x) with 1 ulp error) instead of a
+//    square root and divisions, and the triangular solve at a restart end multiplies by reciprocal
+//    diagonal entries formed with the rotation, so no FP64 division sits on the critical path;
+//  * the shared memory the Krylov basis leaves free caches the first `ncache` in-block link matrices
+//    (self terms first), filled by the first block-operator application: later applications stream
+//    only the rest from L2.
+// The arithmetic is the single-vector FGMRES::fgmres of the reference (src/fgmres.cpp:5-128) with
+// classical Gram-Schmidt; rounding differs from the reference's order at the ulp level.
+
+// sum over the warp of 8 double2 values by recursive halving: afterwards every lane l holds the warp
+// total of value ((l >> 2) & 7).  The values are separate arguments, so the lane-dependent selections
+// stay register selects.
+__device__ __forceinline__ double2 xor_shfl2(double2 a, int o) {
+    return make_double2(__shfl_xor_sync(0xffffffffu, a.x, o), __shfl_xor_sync(0xffffffffu, a.y, o));
+}
+__device__ __forceinline__ double2 sel2(bool c, double2 a, double2 b) {
+    return make_double2(c ? a.x : b.x, c ? a.y : b.y);
+}
+__device__ __forceinline__ double2 warp_sum8(double2 v0, double2 v1, double2 v2, double2 v3, double2 v4, double2 v5,
+                                             double2 v6, double2 v7) {
+    const int lane = threadIdx.x & 31;
+    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+    // level 16: lanes with bit 4 keep values 4-7, the others 0-3
+    const double2 a0 = sel2(h16, v4, v0) + xor_shfl2(sel2(h16, v0, v4), 16);
+    const double2 a1 = sel2(h16, v5, v1) + xor_shfl2(sel2(h16, v1, v5), 16);
+    const double2 a2 = sel2(h16, v6, v2) + xor_shfl2(sel2(h16, v2, v6), 16);
+    const double2 a3 = sel2(h16, v7, v3) + xor_shfl2(sel2(h16, v3, v7), 16);
+    // level 8: bit 3 keeps the upper pair
+    const double2 c0 = sel2(h8, a2, a0) + xor_shfl2(sel2(h8, a0, a2), 8);
+    const double2 c1 = sel2(h8, a3, a1) + xor_shfl2(sel2(h8, a1, a3), 8);
+    // level 4: bit 2 keeps the odd value
+    double2 d = sel2(h4, c1, c0) + xor_shfl2(sel2(h4, c0, c1), 4);
+    d = d + xor_shfl2(d, 2);
+    d = d + xor_shfl2(d, 1);
+    return d;
+}
+
+// the warp totals of sv[0..cnt) into row[0..cnt) (row: this warp's partial-sum slots of one rhs)
+__device__ __forceinline__ void warp_partial(const double2 (&sv)[8], double2* row, int cnt) {
+    const int lane = threadIdx.x & 31;
+    const double2 t = warp_sum8(sv[0], sv[1], sv[2], sv[3], sv[4], sv[5], sv[6], sv[7]);
+    const int s = (lane >> 2) & 7;
+    if ((lane & 3) == 0 && s < cnt) row[s] = t;
+}
+// CTA totals t[0..cnt) of the partial sums col[w * stride + s] of warps w < nwe (nwe <= 16), formed by the
+// calling warp: lane group g = lane / 8 sums warps g, g+4, g+8, g+12 of slot lane % 8 in that order, two
+// butterfly levels finish, and the totals are broadcast through the warp's scratch tw[8]; identical in
+// every warp
+__device__ __forceinline__ void cta_totals(const double2* col, int stride, int nwe, int cnt, double2* tw,
+                                           double2 (&t)[8]) {
+    const int lane = threadIdx.x & 31, s = lane & 7;
+    double2 v = make_double2(0.0, 0.0);
+    if (s < cnt)
+        for (int ww = lane >> 3; ww < nwe; ww += 4) v = v + col[(size_t)ww * stride + s];
+    v = v + xor_shfl2(v, 8);
+    v = v + xor_shfl2(v, 16);
+    __syncwarp();  // this warp's previous reads of tw are done
+    if (lane < 8) tw[lane] = v;
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 8; q++) t[q] = q < cnt ? tw[q] : make_double2(0.0, 0.0);
+}
+
+template <typename V, int RB, int M> struct Sap2Smem {
+    static constexpr int kSlots = 8;  // per rhs: the Gram-Schmidt coefficients and the new norm (M + 2 <= 8)
+    V* basis;       // (M+1) x RB x NE
+    V* op;          // RB x NE: operand of the residual applications
+    double2* red;   // 2 buffers x nwe x RB*kSlots: warp partial sums
+    double2* tw;    // nwe x kSlots: per-warp broadcast of one rhs' totals
+    double2* H;     // RB x (M+1) x M, H[r][i*M + j]
+    double2* gm;    // RB x (M+1)
+    double2* cn;    // RB x M
+    double2* sn;    // RB x M
+    double2* dinv;  // RB x M: 1 / H[q][q] once column q is rotated
+    double2* ct;    // RB x kSlots: step j's totals of rhs r for warp 0's lanes (slot j+1: the new norm)
+    int* flag;      // RB x M: break flag of step j
+    V* cache;       // ncache x dof x dof link matrices
+    __device__ Sap2Smem(unsigned char* raw, int NE, int nwe) {
+        double2* d = reinterpret_cast<double2*>(raw);
+        red = d;
+        tw = red + (size_t)2 * nwe * RB * kSlots;
+        H = tw + (size_t)nwe * kSlots;
+        gm = H + RB * (M + 1) * M;
+        cn = gm + RB * (M + 1);
+        sn = cn + RB * M;
+        dinv = sn + RB * M;
+        ct = dinv + RB * M;
+        flag = reinterpret_cast<int*>(ct + RB * kSlots);
+        basis = reinterpret_cast<V*>(reinterpret_cast<double2*>(flag) + (RB * M + 3) / 4);
+        op = basis + (size_t)(M + 1) * NE * RB;
+        cache = op + (size_t)NE * RB;
+    }
+    static size_t bytes(int NE, int nwe) {  // without the link cache
+        return sizeof(double2) * ((size_t)2 * nwe * RB * kSlots + (size_t)nwe * kSlots +
+                                  (size_t)RB * ((M + 1) * M + (M + 1) + 3 * M + kSlots) + (RB * M + 3) / 4) +
+               sizeof(V) * (size_t)(M + 2) * NE * RB;
+    }
+};
+
+template <typename V, int RB, int M, int CH, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __restrict__ L, const V* __restrict__ rg,
+                                                           V* __restrict__ xg, SapKParams p, int ncache) {
+    typedef typename RealOf<V>::R R;
+    typedef Sap2Smem<V, RB, M> SM;
+    constexpr int KS = SM::kSlots;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int et = g.sel_t, ex = g.sel_x, S = ex * et, dof = g.dof, NE = S * dof;
+    const int nwe = (NE + 31) >> 5;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int kb = blockIdx.x / p.ngroups, r0 = (blockIdx.x - kb * p.ngroups) * RB;
+    constexpr int SL = RB * KS;  // partial-sum slots per warp
+    bool act[RB];
+    bool any = false;
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+        act[r] = (r0 + r < p.nrhs) && !(p.done && p.done[r0 + r]);
+        any |= act[r];
+    }
+    if (!any) return;
+    SM sm(smraw, NE, nwe);
+    const int blk = p.blocks[kb];
+    const int bx = blk / g.sap_t, bt = blk - bx * g.sap_t;
+    const R mm = R(p.m0) + R(2);
+    int rbuf = 0;
+
+    const int e = threadIdx.x;
+    const bool ev = e < NE;
+    const int k = ev ? e / dof : 0, i = ev ? e - k * dof : 0;
+    const int kx = k / et, kt = k - kx * et;
+    const int n = (bx * ex + kx) * g.Nt + bt * et + kt;
+    int nbk[5], cslot[5];
+    nbk[0] = k;
+    nbk[1] = (kt + 1 < et) ? k + 1 : -1;
+    nbk[2] = (kx + 1 < ex) ? k + et : -1;
+    nbk[3] = (kt > 0) ? k - 1 : -1;
+    nbk[4] = (kx > 0) ? k - et : -1;
+    {  // cache slots of the in-block matrices: self terms, then +t, +x, -t, -x hops
+        const int b1 = S, b2 = b1 + ex * (et - 1), b3 = b2 + (ex - 1) * et, b4 = b3 + ex * (et - 1);
+        cslot[0] = k;
+        cslot[1] = b1 + kx * (et - 1) + kt;
+        cslot[2] = b2 + kx * et + kt;
+        cslot[3] = b3 + kx * (et - 1) + kt - 1;
+        cslot[4] = b4 + (kx - 1) * et + kt;
+    }
+    const int dd2 = dof * dof;
+    V b[RB], x[RB], w[RB];
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+        b[r] = (ev && act[r]) ? rg[(long)(r0 + r) * g.size() + (long)n * dof + i] : czero<V>();
+        x[r] = b[r];
+    }
+
+    // w = D_B op for the RB vectors op[r * NE + .]; fill: keep the cached matrices while loading them
+    auto apply = [&](const V* op, bool fill) {
+        V acc[RB][2];
+#pragma unroll
+        for (int r = 0; r < RB; r++) acc[r][0] = acc[r][1] = czero<V>();
+        if (!ev) {
+#pragma unroll
+            for (int r = 0; r < RB; r++) w[r] = czero<V>();
+            return;
+        }
+#pragma unroll
+        for (int d = 0; d < 5; d++) {
+            const int kk = nbk[d];
+            if (kk < 0) continue;
+            const V* o = op + (size_t)kk * dof;
+            const bool cached = cslot[d] < ncache;
+            V* Mc = sm.cache + (size_t)cslot[d] * dd2 + i;
+            if (cached && !fill) {
+                for (int j = 0; j < dof; j += 2) {  // dof is even
+                    const V m0 = Mc[(size_t)j * dof], m1 = Mc[(size_t)(j + 1) * dof];
+#pragma unroll
+                    for (int r = 0; r < RB; r++) {
+                        acc[r][0] = cfma(m0, o[(size_t)r * NE + j], acc[r][0]);
+                        acc[r][1] = cfma(m1, o[(size_t)r * NE + j + 1], acc[r][1]);
+                    }
+                }
+                continue;
+            }
+            const V* Mt = L + ((long)n * 5 + d) * dd2 + i;
+            int j = 0;
+            for (; j + CH <= dof; j += CH) {  // CH link loads in flight
+                V mv[CH];
+#pragma unroll
+                for (int u = 0; u < CH; u++) mv[u] = __ldg(Mt + (long)(j + u) * dof);
+                if (cached)
+#pragma unroll
+                    for (int u = 0; u < CH; u++) Mc[(size_t)(j + u) * dof] = mv[u];
+#pragma unroll
+                for (int u = 0; u < CH; u++)
+#pragma unroll
+                    for (int r = 0; r < RB; r++) acc[r][u & 1] = cfma(mv[u], o[(size_t)r * NE + j + u], acc[r][u & 1]);
+            }
+            for (; j < dof; j++) {
+                const V mv = __ldg(Mt + (long)j * dof);
+                if (cached) Mc[(size_t)j * dof] = mv;
+#pragma unroll
+                for (int r = 0; r < RB; r++) acc[r][0] = cfma(mv, o[(size_t)r * NE + j], acc[r][0]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RB; r++) w[r] = mm * op[(size_t)r * NE + e] - (acc[r][0] + acc[r][1]);
+    };
+    // this warp's partial sums of rhs r: the warp totals of sv[0..cnt) into slots 0..cnt of buffer rbuf
+#define SAP2_PARTIAL(sv, r, cnt) warp_partial(sv, sm.red + ((size_t)rbuf * nwe + wid) * SL + (r) * KS, cnt)
+    // CTA totals of slots 0..cnt of rhs r in buffer buf (every warp forms them itself)
+#define SAP2_TOTALS(buf, r, cnt, t) \
+    cta_totals(sm.red + (size_t)(buf) * nwe * SL + (r) * KS, SL, nwe, cnt, sm.tw + (size_t)wid * KS, t)
+
+    // x = x0 = b; r = b - D_B x (this application fills the link cache)
+#pragma unroll
+    for (int r = 0; r < RB; r++)
+        if (ev) sm.op[(size_t)r * NE + e] = x[r];
+    __syncthreads();
+    apply(sm.op, true);
+    double norm_b[RB], err[RB];
+    bool fin[RB];  // converged, inactive, or a zero right-hand side
+    int maxIt[RB];
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+        w[r] = b[r] - w[r];
+        double2 sv[KS];
+#pragma unroll
+        for (int q = 0; q < KS; q++) sv[q] = make_double2(0.0, 0.0);
+        if (ev) {
+            sv[0].x = (double)cnorm2(b[r]);
+            sv[1].x = (double)cnorm2(w[r]);
+        }
+        SAP2_PARTIAL(sv, r, 2);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+        double2 t[KS];
+        SAP2_TOTALS(rbuf, r, 2, t);
+        norm_b[r] = sqrt(t[0].x);
+        err[r] = sqrt(t[1].x);
+        // a zero block right-hand side has the zero solution (the reference would divide by zero)
+        fin[r] = !act[r] || norm_b[r] == 0.0;
+        maxIt[r] = M;
+    }
+    rbuf ^= 1;
+    for (int kr = 0; kr < p.restarts; kr++) {
+        bool arn[RB], anyarn = false;
+#pragma unroll
+        for (int r = 0; r < RB; r++) {
+            arn[r] = !fin[r];
+            anyarn |= arn[r];
+        }
+        if (!anyarn) break;
+#pragma unroll
+        for (int r = 0; r < RB; r++) {  // V_0 = r / beta
+            if (!arn[r]) continue;
+            const R inv = R(1.0 / err[r]);
+            if (ev) sm.basis[(size_t)r * NE + e] = inv * w[r];
+            if (wid == 0 && lane == 0) sm.gm[r * (M + 1)] = make_double2(err[r], 0.0);
+        }
+        for (int j = 0; j < M; j++) {
+            __syncthreads();  // v_j complete; warp 0's step j-1 (flags, Hessenberg) visible
+            if (j > 0) {
+                anyarn = false;
+#pragma unroll
+                for (int r = 0; r < RB; r++) {
+                    if (arn[r] && sm.flag[r * M + j - 1]) {
+                        maxIt[r] = j;  // not reset at the next restart (src/fgmres.cpp:14,56)
+                        arn[r] = false;
+                    }
+                    anyarn |= arn[r];
+                }
+                if (!anyarn) break;
+            }
+            apply(sm.basis + (size_t)j * NE * RB, false);  // w = D_B V_j
+            // classical Gram-Schmidt coefficients <w, V_i>, i <= j, and ||w||^2 (slot j + 1)
+#pragma unroll
+            for (int r = 0; r < RB; r++) {
+                if (!arn[r]) continue;
+                // (selects, not a store to sv[j + 1], which would put sv in local memory)
+                const double nw = ev ? (double)cnorm2(w[r]) : 0.0;
+                double2 sv[KS];
+#pragma unroll
+                for (int q = 0; q < KS; q++) {
+                    sv[q] = make_double2(0.0, 0.0);
+                    if (q <= M && ev && q <= j)
+                        sv[q] = cfmac(to_d(sm.basis[((size_t)q * RB + r) * NE + e]), to_d(w[r]), sv[q]);
+                    sv[q].x += (q == j + 1) ? nw : 0.0;
+                }
+                SAP2_PARTIAL(sv, r, j + 2);
+            }
+            __syncthreads();  // partial sums visible
+            const int dbuf = rbuf;
+            rbuf ^= 1;
+            // ||w - V h||^2 = ||w||^2 - sum |h_i|^2 for orthonormal V: no second reduction, unless the
+            // difference cancels below 1e-4 of ||w||^2 (1e-2 for an FP32 basis, whose orthogonality holds
+            // to ~1e-6); then the norm of the updated w is reduced as is
+            constexpr double kCancel = sizeof(R) == 8 ? 1e-4 : 1e-2;
+            double hn[RB], ihn[RB];
+            bool reduce_norm = false;
+#pragma unroll
+            for (int r = 0; r < RB; r++) {
+                hn[r] = 0.0;
+                ihn[r] = 0.0;
+                if (!arn[r]) continue;
+                double2 t[KS];
+                SAP2_TOTALS(dbuf, r, j + 2, t);
+                double w2 = 0.0, hh = 0.0;
+#pragma unroll
+                for (int q = 0; q <= M; q++) {
+                    if (q <= j) hh += cnorm2(t[q]);
+                    else if (q == j + 1) w2 = t[q].x;
+                }
+                const double dd = w2 - hh;
+                if (dd > kCancel * w2) {
+                    ihn[r] = rsqrt(dd);
+                    hn[r] = dd * ihn[r];
+                } else {
+                    reduce_norm = true;  // identical in every thread: the totals are
+                }
+                if (ev) {
+#pragma unroll
+                    for (int q = 0; q <= M; q++)
+                        if (q <= j) w[r] = w[r] - cmul(from_d<V>(t[q]), sm.basis[((size_t)q * RB + r) * NE + e]);
+                }
+                if (wid == 0 && lane == 0)
+#pragma unroll
+                    for (int q = 0; q <= M; q++)
+                        if (q <= j) sm.ct[r * KS + q] = t[q];
+            }
+            if (reduce_norm) {
+#pragma unroll
+                for (int r = 0; r < RB; r++) {
+                    double2 sv[KS];
+#pragma unroll
+                    for (int q = 0; q < KS; q++) sv[q] = make_double2(0.0, 0.0);
+                    if (arn[r] && ev) sv[0].x = (double)cnorm2(w[r]);
+                    SAP2_PARTIAL(sv, r, 1);
+                }
+                __syncthreads();
+#pragma unroll
+                for (int r = 0; r < RB; r++) {
+                    double2 t[KS];
+                    SAP2_TOTALS(rbuf, r, 1, t);
+                    if (arn[r] && t[0].x > 0) {
+                        ihn[r] = rsqrt(t[0].x);
+                        hn[r] = t[0].x * ihn[r];
+                    }
+                }
+                rbuf ^= 1;
+            }
+#pragma unroll
+            for (int r = 0; r < RB; r++) {
+                if (arn[r] && hn[r] > 0 && ev) sm.basis[((size_t)(j + 1) * RB + r) * NE + e] = R(ihn[r]) * w[r];
+                if (wid == 0 && lane == 0) sm.ct[r * KS + j + 1] = make_double2(hn[r], 0.0);
+            }
+            if (wid == 0) {
+                __syncwarp();
+                bool a = false;
+                double nbr = 0.0;
+#pragma unroll
+                for (int r = 0; r < RB; r++)
+                    if (r == lane) {
+                        a = arn[r];
+                        nbr = norm_b[r];
+                    }
+                if (lane < RB && a) {  // lane r: Hessenberg column j of rhs r
+                    const int r = lane;
+                    double2* H = sm.H + r * (M + 1) * M;
+                    double2* cn = sm.cn + r * M;
+                    double2* sn = sm.sn + r * M;
+                    double2* gm = sm.gm + r * (M + 1);
+                    const double2* ct = sm.ct + r * KS;
+                    double2 hc[M + 1];
+#pragma unroll
+                    for (int q = 0; q <= M; q++) hc[q] = (q <= j + 1) ? ct[q] : make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int q = 0; q < M; q++) {  // FGMRES::rotation (src/fgmres.cpp:99-115)
+                        if (q >= j) break;
+                        const double2 tmp = cmulc(cn[q], hc[q]) + cmulc(sn[q], hc[q + 1]);
+                        hc[q + 1] = cmul(cn[q], hc[q + 1]) - cmul(sn[q], hc[q]);
+                        hc[q] = tmp;
+                    }
+                    double2 hjj = make_double2(0.0, 0.0), hj1 = hjj;
+#pragma unroll
+                    for (int q = 0; q < M; q++)
+                        if (q == j) {
+                            hjj = hc[q];
+                            hj1 = hc[q + 1];
+                        }
+                    const double iden = rsqrt(cnorm2(hjj) + cnorm2(hj1));
+                    const double2 s_j = make_double2(hj1.x * iden, hj1.y * iden);
+                    const double2 c_j = make_double2(hjj.x * iden, hjj.y * iden);
+                    sn[j] = s_j;
+                    cn[j] = c_j;
+                    const double2 hd = cmulc(c_j, hjj) + cmulc(s_j, hj1);
+#pragma unroll
+                    for (int q = 0; q < M; q++) {
+                        if (q > j) break;
+                        H[q * M + j] = (q == j) ? hd : hc[q];
+                    }
+                    const double id2 = 1.0 / cnorm2(hd);
+                    sm.dinv[r * M + j] = make_double2(hd.x * id2, -hd.y * id2);
+                    const double2 gj = gm[j];
+                    const double2 g1 = -cmul(s_j, gj);
+                    gm[j + 1] = g1;
+                    gm[j] = cmulc(c_j, gj);
+                    const double thr = p.tol * nbr;
+                    sm.flag[r * M + j] = (cnorm2(g1) < thr * thr) ? 1 : 0;
+                }
+            }
+        }
+        __syncthreads();  // the last step's Hessenberg column and rotations visible
+        // solve_upper_triangular (src/fgmres.cpp:118-128), repeated by every thread; x += sum eta_j V_j
+#pragma unroll
+        for (int r = 0; r < RB; r++) {
+            if (fin[r]) continue;
+            const double2* H = sm.H + r * (M + 1) * M;
+            const double2* gmr = sm.gm + r * (M + 1);
+            const double2* di = sm.dinv + r * M;
+            double2 eta[M];
+#pragma unroll
+            for (int q = M - 1; q >= 0; q--) {
+                eta[q] = make_double2(0.0, 0.0);
+                if (q >= maxIt[r]) continue;
+                double2 t = gmr[q];
+#pragma unroll
+                for (int jj = q + 1; jj < M; jj++)
+                    if (jj < maxIt[r]) t = t - cmul(H[q * M + jj], eta[jj]);
+                eta[q] = cmul(t, di[q]);
+            }
+            if (ev) {
+                V a = x[r];
+#pragma unroll
+                for (int jj = 0; jj < M; jj++)
+                    if (jj < maxIt[r]) a = cfma(from_d<V>(eta[jj]), sm.basis[((size_t)jj * RB + r) * NE + e], a);
+                x[r] = a;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RB; r++)
+            if (ev) sm.op[(size_t)r * NE + e] = x[r];
+        __syncthreads();
+        apply(sm.op, false);
+#pragma unroll
+        for (int r = 0; r < RB; r++) {
+            w[r] = b[r] - w[r];
+            double2 sv[KS];
+#pragma unroll
+            for (int q = 0; q < KS; q++) sv[q] = make_double2(0.0, 0.0);
+            if (ev) sv[0].x = (double)cnorm2(w[r]);
+            SAP2_PARTIAL(sv, r, 1);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < RB; r++) {
+            double2 t[KS];
+            SAP2_TOTALS(rbuf, r, 1, t);
+            err[r] = sqrt(t[0].x);
+            if (!fin[r] && err[r] < p.tol * norm_b[r]) fin[r] = true;
+        }
+        rbuf ^= 1;
+    }
+    // x_B += e  (src/sap.cpp:106-113)
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+        if (!act[r] || norm_b[r] == 0.0 || !ev) continue;
+        V* o = xg + (long)(r0 + r) * g.size() + (long)n * dof + i;
+        *o = *o + x[r];
+    }
+#undef SAP2_PARTIAL
+#undef SAP2_TOTALS
+}
+
+// the kernel takes blocks of at most 512 unknowns at restart length 5 with 1, 2 or 4 right-hand sides
+// per CTA, where its shared memory (without the link cache) fits
+constexpr int kSap2M = 5;
+template <typename V> static size_t sap2_base_bytes(int rb, int NE) {
+    const int nwe = (NE + 31) / 32;
+    return rb == 1 ? Sap2Smem<V, 1, kSap2M>::bytes(NE, nwe)
+                   : rb == 2 ? Sap2Smem<V, 2, kSap2M>::bytes(NE, nwe) : Sap2Smem<V, 4, kSap2M>::bytes(NE, nwe);
+}
+bool sap2_fits(int rb, int m, int NE, size_t vbytes) {
+    if (m != kSap2M || NE > 512 || !(rb == 1 || rb == 2 || rb == 4)) return false;
+    const size_t smem = vbytes == 16 ? sap2_base_bytes<double2>(rb, NE) : sap2_base_bytes<float2>(rb, NE);
+    return smem <= 227 * 1024;
+}
+template <typename V, int RB, int CH, int MAXT>
+static void launch_sap2_k(cudaStream_t s, const Geom& g, const V* L, const V* r, V* x, SapKParams p) {
+    const int ex = g.sel_x, et = g.sel_t, S = ex * et, NE = S * g.dof;
+    const int nwe = (NE + 31) / 32;
+    p.ngroups = (p.nrhs + RB - 1) / RB;
+    const size_t base = Sap2Smem<V, RB, kSap2M>::bytes(NE, nwe);
+    // link matrices in the rest of the 227 KB: at most the block's in-block (site, hop) pairs
+    const int inblock = S + 2 * ex * (et - 1) + 2 * (ex - 1) * et;
+    const size_t mat = sizeof(V) * (size_t)g.dof * g.dof;
+    const int ncache = (int)std::min<size_t>(inblock, (227 * 1024 - base) / mat);
+    const size_t smem = base + (size_t)ncache * mat;
+    DDAMG_CUDA_TRY(cudaFuncSetAttribute(sap_block2_kernel<V, RB, kSap2M, CH, MAXT>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DDAMG_LAUNCH((sap_block2_kernel<V, RB, kSap2M, CH, MAXT>), dim3(p.nblocks * p.ngroups), 32 * nwe, smem, s, g, L, r,
+                 x, p, ncache);
+}
+template <typename V, int RB>
+void launch_sap2(cudaStream_t s, const Geom& g, const V* L, const V* r, V* x, SapKParams p) {
+    const int NE = g.sel_x * g.sel_t * g.dof;
+    if (NE <= 384) launch_sap2_k<V, RB, 12, 384>(s, g, L, r, x, p);
+    else launch_sap2_k<V, RB, 8, 512>(s, g, L, r, x, p);
+}
+
+template void launch_sap2<double2, 1>(cudaStream_t, const Geom&, const double2*, const double2*, double2*, SapKParams);
+template void launch_sap2<double2, 2>(cudaStream_t, const Geom&, const double2*, const double2*, double2*, SapKParams);
+template void launch_sap2<double2, 4>(cudaStream_t, const Geom&, const double2*, const double2*, double2*, SapKParams);
+template void launch_sap2<float2, 1>(cudaStream_t, const Geom&, const float2*, const float2*, float2*, SapKParams);
+template void launch_sap2<float2, 2>(cudaStream_t, const Geom&, const float2*, const float2*, float2*, SapKParams);
+template void launch_sap2<float2, 4>(cudaStream_t, const Geom&, const float2*, const float2*, float2*, SapKParams);
+
+}  // namespace ddamg

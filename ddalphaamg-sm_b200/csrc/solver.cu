@@ -432,30 +432,34 @@ static int tc_shape_for(ddamg_handle* h, int l, const float2* r, const SapArgs& 
     return best;
 }
 
-// right-hand sides per CTA of the CUDA-core coarse sweep for this batch width and precision: tuned
-// on first use (one timed sweep per candidate into the level's scratch field t; syncs), then cached
+// the variant (right-hand sides per CTA and block-solver kernel) of the CUDA-core coarse sweep for this
+// batch width and precision: tuned on first use (one timed sweep per candidate into the level's scratch
+// field t; syncs), then cached
 template <typename V> static int rb_for(ddamg_handle* h, int l, const V* r, const SapArgs& a, int nrhs) {
     LevelData& D = h->lv[l];
     const int key = nrhs * 2 + (std::is_same<V, float2>::value ? 1 : 0);
     auto it = D.rb_choice.find(key);
     if (it != D.rb_choice.end()) return it->second;
-    double us[4];
+    double us[kSapVariantCount];
     const int best = tune_sap_rb<V>(h->s, D.g, B<V>(D).links, r, B<V>(D).t, a, nrhs, us);
     D.rb_choice[key] = best;
     std::ostringstream o;
     o << "level " << l << " rhs " << nrhs << (key & 1 ? " fp32" : " fp64") << " CUDA-core sweep:";
-    static const int cand[4] = {1, 2, 4, 8};
-    for (int i = 0; i < 4; i++)
-        if (us[i] >= 0) o << " [rhs/cta " << cand[i] << ": " << us[i] << " us" << (cand[i] == best ? " *" : "") << "]";
+    static const char* kname[2] = {"block", "block2"};
+    for (int i = 0; i < kSapVariantCount; i++)
+        if (us[i] >= 0)
+            o << " [rhs/cta " << kSapVariants[i] / 4 << " " << kname[kSapVariants[i] % 4] << ": " << us[i] << " us"
+              << (kSapVariants[i] == best ? " *" : "") << "]";
     h->tune_log += o.str() + "\n";
     return best;
 }
 
 // SAP_C::SAP (src/sap.cpp:81-165) on nrhs independent vectors; returns the reference's value
-// for rhs 0 when want_iters (one host sync), else nu.
+// for rhs 0 when want_iters (one host sync), else nu.  lay: a fine-level block layout other than the
+// level's; allow_tc: batched FP32 coarse sweeps may use the tensor-core block operator.
 template <typename V>
 static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, bool x_zero, int nrhs, bool want_iters,
-                 const SapLayout* lay = nullptr) {
+                 const SapLayout* lay = nullptr, bool allow_tc = true) {
     LevelData& D = h->lv[l];
     const Geom& g = lay ? lay->g : D.g;  // the block layout of the sweeps (the operator is the level's)
     const long n = g.size();
@@ -474,12 +478,11 @@ static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, b
             {
                 ProfScope ps(h, 0, l);
                 if (l == 0) launch_sap_sweep_fine<V>(h->s, g, B<V>(D).U, r, x, a, nrhs);
-                else if (std::is_same<V, float2>::value && D.tc && nrhs >= kTcMinRhs)
+                else if (std::is_same<V, float2>::value && D.tc && allow_tc && nrhs >= kTcMinRhs)
                     launch_sap_sweep_tc(h->s, g, D.tcw, reinterpret_cast<const float2*>(r),
                                         reinterpret_cast<float2*>(x), a, nrhs,
                                         tc_shape_for(h, l, reinterpret_cast<const float2*>(r), a, nrhs));
-                else launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs,
-                                                 nrhs > 1 ? rb_for<V>(h, l, r, a, nrhs) : 1);
+                else launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs, rb_for<V>(h, l, r, a, nrhs));
             }
             // the residual after the last black sweep only feeds the convergence test
             const bool last = (colour == 1 && it == nu - 1);
@@ -904,7 +907,8 @@ static bool sap_setup_split(ddamg_handle* h, int l, const V* v, V* x, int nu, in
               D.nred, D.done};
     DDAMG_CUDA_TRY(cudaMemsetAsync(D.done, 0, sizeof(int) * nrhs, h->s));
     level_op<V>(h, l, x, r, v, nrhs);  // r = v - D x for every vector
-    const int rb = rb_for<V>(h, l, r, a, nrhs);  // tuned on first use on red sweeps (times into scratch, syncs)
+    const int var = rb_for<V>(h, l, r, a, nrhs);  // tuned on first use on red sweeps (times into scratch, syncs)
+    const int rb = var / 4;
     const int G = nrhs / rb;
     // the groups of one Schwarz block share its links through L2 only while they run side by side,
     // which one launch guarantees (block-major CTA order) and separate streams do not: split only when
@@ -915,7 +919,7 @@ static bool sap_setup_split(ddamg_handle* h, int l, const V* v, V* x, int nu, in
             for (int colour = 0; colour < 2; colour++) {
                 a.blocks = colour == 0 ? D.red : D.black;
                 a.nblocks = colour == 0 ? D.nred : D.nblack;
-                launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs, rb);
+                launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs, var);
                 if (!(colour == 1 && it == nu - 1)) level_op<V>(h, l, x, r, v, nrhs);
             }
         return true;
@@ -939,7 +943,7 @@ static bool sap_setup_split(ddamg_handle* h, int l, const V* v, V* x, int nu, in
             for (int colour = 0; colour < 2; colour++) {
                 ak.blocks = colour == 0 ? D.red : D.black;
                 ak.nblocks = colour == 0 ? D.nred : D.nblack;
-                launch_sap_sweep_coarse<V>(st, g, B<V>(D).links, r + off, x + off, ak, rb, rb);
+                launch_sap_sweep_coarse<V>(st, g, B<V>(D).links, r + off, x + off, ak, rb, var);
                 if (!(colour == 1 && it == nu - 1))
                     launch_coarse_op<V>(st, B<V>(D).links, x + off, r + off, v + off, g.Nx, g.Nt, g.dof, h->p.m0, rb);
             }
@@ -978,10 +982,27 @@ static void setup(ddamg_handle* h, const double2* rnd_host, uint64_t seed) {
         LevelData& D = h->lv[l];
         const long n = D.g.size();
         const int nv = D.g.ntest;
+        const int nu = h->p.sap_test_vectors_iterations;
         // SAP(rhs = 0, tvec, nu = SAP_test_vectors_iterations) on all test vectors at once
-        DDAMG_CUDA_TRY(cudaMemsetAsync(D.d.eta, 0, sizeof(double2) * n * nv, s));
-        if (!sap_setup_split<double2>(h, l, D.d.eta, D.d.tv, h->p.sap_test_vectors_iterations, nv))
-            sap_t<double2>(h, l, D.d.eta, D.d.tv, h->p.sap_test_vectors_iterations, 1e-10, false, nv, false);
+        // (src/amg.cpp:45-52), in the level's working precision: in mixed precision the smoother is FP32
+        // (its operator converted from this level's FP64 links, built just before by level l-1), and the
+        // smoothed vectors are promoted to FP64 for the orthonormalisation and the coarse links
+        if (D.fp32) {
+            if (l > 0) {
+                launch_convert<double2, float2>(s, D.d.links, D.f.links, (long)D.g.sites * 5 * D.g.dof * D.g.dof);
+                if (D.tc) launch_pack_tc_links(s, D.g, D.f.links, D.tcw.tiles);
+            }
+            launch_convert<double2, float2>(s, D.d.tv, D.f.tv, n * nv);
+            DDAMG_CUDA_TRY(cudaMemsetAsync(D.f.eta, 0, sizeof(float2) * n * nv, s));
+            // CUDA cores only: TF32 block operators would coarsen the test vectors
+            if (!sap_setup_split<float2>(h, l, D.f.eta, D.f.tv, nu, nv))
+                sap_t<float2>(h, l, D.f.eta, D.f.tv, nu, 1e-10, false, nv, false, nullptr, false);
+            launch_convert<float2, double2>(s, D.f.tv, D.d.tv, n * nv);
+        } else {
+            DDAMG_CUDA_TRY(cudaMemsetAsync(D.d.eta, 0, sizeof(double2) * n * nv, s));
+            if (!sap_setup_split<double2>(h, l, D.d.eta, D.d.tv, nu, nv))
+                sap_t<double2>(h, l, D.d.eta, D.d.tv, nu, 1e-10, false, nv, false);
+        }
         {
             ProfScope ps(h, 3, l);
             launch_orthonormalize(s, D.g, D.d.tv);
