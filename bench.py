@@ -183,11 +183,36 @@ def sap_sweep_bytes(level_geom, fp_bytes, nvec=1):
     return links + vecs
 
 
+def sap_sweep_flop(level):
+    """FP64 flops of one single-vector SAP colour sweep of a coarse level: 31 block-operator applications per
+    block solve, each a dof x dof complex matrix-vector product (8 flops per complex multiply-add) per in-block
+    (site, hop) pair."""
+    return sap_l2_bytes(level) // 16 * 8
+
+
+def fp64_peak_tflops(torch, dev, N=4096):
+    """The FP64 rate this GPU reaches in cuBLAS DGEMM (the denominator of the FP64-pipe fraction)."""
+    a = torch.randn(N, N, dtype=torch.float64, device=f"cuda:{dev}")
+    b = torch.randn(N, N, dtype=torch.float64, device=f"cuda:{dev}")
+    torch.matmul(a, b)
+    best = None
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    return 2.0 * N ** 3 / (best * 1e-3) / 1e12
+
+
 def sap_l2_bytes(level):
-    """Link bytes one single-vector SAP colour sweep of a coarse level streams from L2: every block
+    """Link bytes one single-vector SAP colour sweep of a coarse level reads on chip: every block
     solve applies its block operator 1 + restarts x (m + 1) = 31 times (GMRES(5) x 5 at tol 1e-3 does
     not stop early at these levels), and each application reads the links of the block's in-block
-    hops (self, and +-t / +-x only where the neighbour is in the block) once."""
+    hops (self, and +-t / +-x only where the neighbour is in the block) once, from L2 or, for the matrices
+    the kernel keeps there, from shared memory."""
     w = WORKLOAD
     r_prev, r = w["rows"][level - 1], w["rows"][level]
     Lx, Lt = r_prev[1], r_prev[2]  # level sites
@@ -351,7 +376,7 @@ def run_ours(args, rank, world, local_rank):
             ms, cnt = s.profile_query(kind, l)
             if cnt and (best is None or ms > best[2]):
                 best = (kind, l, ms, cnt)
-    kinds = {0: "sap_block_kernel (SAP colour sweep)", 1: "coarse_gmres_kernel", 2: "level operator"}
+    kinds = {0: "SAP colour sweep (sap_block2_kernel)", 1: "coarse_gmres_kernel", 2: "level operator"}
     hbm, peak_kind = peaks()
     roof = None
     if best and best[0] == 0:
@@ -384,12 +409,19 @@ def run_ours(args, rank, world, local_rank):
             ms1, cnt1 = s.profile_query(0, best[1])
             s.profile(False)
             l2b = sap_l2_bytes(best[1])
-            roof["l2"] = {"kernel": f"sap_block_kernel level {best[1]}, one right-hand side (the solve's sweeps)",
-                          "avg_launch_ms": ms1 / cnt1, "l2_bytes_per_launch": l2b,
-                          "achieved_gbs": l2b / (ms1 / cnt1 * 1e-3) / 1e9,
+            flop = sap_sweep_flop(best[1])
+            t1 = ms1 / cnt1 * 1e-3
+            f64 = fp64_peak_tflops(torch, local_rank)
+            roof["l2"] = {"kernel": f"sap_block2_kernel level {best[1]}, one right-hand side (the solve's sweeps)",
+                          "avg_launch_ms": ms1 / cnt1, "onchip_link_bytes_per_launch": l2b,
+                          "achieved_gbs": l2b / t1 / 1e9,
                           "ncu_lts_throughput_pct": profile_figure("lts_throughput_pct", f"level{best[1]}"),
-                          "note": "31 block-operator applications per block solve, each streaming the block's "
-                                  "in-block links from L2; HBM sees them once per sweep"}
+                          "fp64": {"flop_per_launch": flop, "achieved_tflops": flop / t1 / 1e12,
+                                   "peak_tflops": f64, "frac": flop / t1 / 1e12 / f64,
+                                   "peak_kind": "measured here: cuBLAS DGEMM 4096^3, best of 5"},
+                          "note": "31 block-operator applications per block solve, each reading the block's "
+                                  "in-block links once, part from shared memory (the matrices the Krylov basis "
+                                  "leaves room for) and the rest from L2; HBM sees them once per sweep"}
     elif best:
         roof = {"kernel": kinds[best[0]] + f" level {best[1]}", "bound": "hbm", "achieved": None, "peak": hbm,
                 "unit": "GB/s", "frac": None, "traffic": None, "avg_launch_ms": best[2] / best[3]}
@@ -773,7 +805,8 @@ def dw_bandwidth(ddamg, torch, dev):
 
 def profile_case(name):
     """One small invocation of a hot kernel for an ncu capture (no timing, no JSON line):
-    sap-l1   the bench workload's FP64 solve (level-1 sap_block_kernel sweeps inside);
+    sap-l1   the bench workload's FP64 setup and solve, then, between cudaProfilerStart and Stop, one
+             single-vector and one 12-vector level-1 SAP iteration (sap_block2_kernel sweeps);
     tc-apply one batched FP32 level-1 SAP sweep pair on 512x512 with 64 right-hand sides
              (tc_block_apply_kernel, the tensor-core block operator);
     krylov   20 BiCGstab iterations on a 1024x1024 field (bicg_* kernels, 11 fields of 32 MiB);
@@ -807,6 +840,8 @@ def profile_case(name):
         s.close()
         return 0
     if name == "sap-l1":
+        import torch
+
         w = WORKLOAD
         U, b, _, _ = make_inputs()
         p = ddamg.default_params(w["Nx"], w["Nt"], w["levels"], w["m0"], w["rows"],
@@ -814,7 +849,19 @@ def profile_case(name):
         s = ddamg.Solver(p)
         s.load_gauge(U)
         s.setUpPhase(seed=w["setup_seed"])
-        x, info = s.solve(b)
+        x, info = s.solve(b)  # tunes the sweep variants
+        v1 = ddamg.gaussian_field(s.size(1), 21)
+        v12 = ddamg.gaussian_field(s.size(1) * 12, 22)
+        s.SAP(1, v1, nu=1, tol=0)
+        s.SAP_batched(1, v12, 12, nu=1, tol=0)
+        torch.cuda.synchronize()
+        # the captured region (ncu --profile-from-start off): a single-vector red + black sweep pair (the
+        # solve's kind) and a 12-vector pair (the setup's kind, one launch per colour)
+        torch.cuda.profiler.start()
+        s.SAP(1, v1, nu=1, tol=0)
+        s.SAP_batched(1, v12, 12, nu=1, tol=0)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
         print("sap-l1: iterations", info[0].iterations)
     else:
         N, R = 512, 64
