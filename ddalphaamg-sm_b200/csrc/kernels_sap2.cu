@@ -14,8 +14,9 @@ namespace ddamg {
 // butterfly 2.6 K, totals and update 1.9 K, Givens 1.9 K, barrier waits 3.5 K):
 //  * the multi-value warp sums halve the value set at each of the first levels (a double2 costs four
 //    32-bit shuffles per level, so six coefficients cost 120 shuffles as a plain butterfly, 36 here);
-//  * every warp forms the CTA totals itself from the warps' partial sums (a quarter of the warps per
-//    lane group, then two butterfly levels; the same order in every warp, so all threads hold
+//  * the coefficients of all RB right-hand sides share one packed warp reduction (groups of eight), and
+//    every warp forms the CTA totals of all of them at once from the warps' partial sums (a lane per
+//    slot, then a butterfly over the lane groups; the same order in every warp, so all threads hold
 //    bit-identical totals): one CTA barrier per reduction;
 //  * warp 0 forms Hessenberg column j, the Givens rotation and the break flag after its own update;
 //    the flag is read after the next step's first barrier, where the reference reads it;
@@ -56,30 +57,48 @@ __device__ __forceinline__ double2 warp_sum8(double2 v0, double2 v1, double2 v2,
     return d;
 }
 
-// the warp totals of sv[0..cnt) into row[0..cnt) (row: this warp's partial-sum slots of one rhs)
-__device__ __forceinline__ void warp_partial(const double2 (&sv)[8], double2* row, int cnt) {
+// the warp sums of the RB x NV values val(r, q) (all right-hand sides packed into groups of eight, each
+// value formed when its group is reduced) into this warp's partial-sum slots row[r * KS + q]
+template <int RB, int NV, int KS, typename F>
+__device__ __forceinline__ void warp_partials(F&& val, double2* row) {
     const int lane = threadIdx.x & 31;
-    const double2 t = warp_sum8(sv[0], sv[1], sv[2], sv[3], sv[4], sv[5], sv[6], sv[7]);
-    const int s = (lane >> 2) & 7;
-    if ((lane & 3) == 0 && s < cnt) row[s] = t;
-}
-// CTA totals t[0..cnt) of the partial sums col[w * stride + s] of warps w < nwe (nwe <= 16), formed by the
-// calling warp: lane group g = lane / 8 sums warps g, g+4, g+8, g+12 of slot lane % 8 in that order, two
-// butterfly levels finish, and the totals are broadcast through the warp's scratch tw[8]; identical in
-// every warp
-__device__ __forceinline__ void cta_totals(const double2* col, int stride, int nwe, int cnt, double2* tw,
-                                           double2 (&t)[8]) {
-    const int lane = threadIdx.x & 31, s = lane & 7;
-    double2 v = make_double2(0.0, 0.0);
-    if (s < cnt)
-        for (int ww = lane >> 3; ww < nwe; ww += 4) v = v + col[(size_t)ww * stride + s];
-    v = v + xor_shfl2(v, 8);
-    v = v + xor_shfl2(v, 16);
-    __syncwarp();  // this warp's previous reads of tw are done
-    if (lane < 8) tw[lane] = v;
-    __syncwarp();
+    constexpr int NF = RB * NV, NG = (NF + 7) / 8;
 #pragma unroll
-    for (int q = 0; q < 8; q++) t[q] = q < cnt ? tw[q] : make_double2(0.0, 0.0);
+    for (int gi = 0; gi < NG; gi++) {
+        double2 v[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) {
+            const int f = gi * 8 + t;
+            v[t] = f < NF ? val(f / NV, f % NV) : make_double2(0.0, 0.0);
+        }
+        const double2 tot = warp_sum8(v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]);
+        const int f = gi * 8 + ((lane >> 2) & 7);
+        if ((lane & 3) == 0 && f < NF) row[(f / NV) * KS + f % NV] = tot;
+    }
+}
+// CTA totals of the RB x KS slots of the warps' partial sums (warp w's at col + w * stride; slot q of each
+// rhs only for q < cnt), formed by the calling warp and broadcast through its scratch tw[RB * KS]: lane l
+// sums slot l % (RB*KS) over every (32 / (RB*KS))-th warp in two chains, and a butterfly over the lane
+// groups finishes; the same order in every warp, so all threads hold bit-identical totals
+template <int RB, int KS>
+__device__ __forceinline__ void cta_totals(const double2* col, int stride, int nwe, int cnt, double2* tw) {
+    constexpr int ST = RB * KS, NGR = 32 / ST;
+    const int lane = threadIdx.x & 31, slot = lane % ST, g = lane / ST;
+    double2 v0 = make_double2(0.0, 0.0), v1 = v0;
+    if (slot % KS < cnt) {
+        int ww = g;
+        for (; ww + NGR < nwe; ww += 2 * NGR) {
+            v0 = v0 + col[(size_t)ww * stride + slot];
+            v1 = v1 + col[(size_t)(ww + NGR) * stride + slot];
+        }
+        if (ww < nwe) v0 = v0 + col[(size_t)ww * stride + slot];
+    }
+    double2 v = v0 + v1;
+#pragma unroll
+    for (int o = ST; o < 32; o <<= 1) v = v + xor_shfl2(v, o);
+    __syncwarp();  // this warp's previous reads of tw are done
+    if (lane < ST) tw[lane] = v;
+    __syncwarp();
 }
 
 template <typename V, int RB, int M> struct Sap2Smem {
@@ -87,7 +106,7 @@ template <typename V, int RB, int M> struct Sap2Smem {
     V* basis;       // (M+1) x RB x NE
     V* op;          // RB x NE: operand of the residual applications
     double2* red;   // 2 buffers x nwe x RB*kSlots: warp partial sums
-    double2* tw;    // nwe x kSlots: per-warp broadcast of one rhs' totals
+    double2* tw;    // nwe x RB*kSlots: per-warp broadcast of the totals
     double2* H;     // RB x (M+1) x M, H[r][i*M + j]
     double2* gm;    // RB x (M+1)
     double2* cn;    // RB x M
@@ -100,7 +119,7 @@ template <typename V, int RB, int M> struct Sap2Smem {
         double2* d = reinterpret_cast<double2*>(raw);
         red = d;
         tw = red + (size_t)2 * nwe * RB * kSlots;
-        H = tw + (size_t)nwe * kSlots;
+        H = tw + (size_t)nwe * RB * kSlots;
         gm = H + RB * (M + 1) * M;
         cn = gm + RB * (M + 1);
         sn = cn + RB * M;
@@ -112,7 +131,7 @@ template <typename V, int RB, int M> struct Sap2Smem {
         cache = op + (size_t)NE * RB;
     }
     static size_t bytes(int NE, int nwe) {  // without the link cache
-        return sizeof(double2) * ((size_t)2 * nwe * RB * kSlots + (size_t)nwe * kSlots +
+        return sizeof(double2) * ((size_t)2 * nwe * RB * kSlots + (size_t)nwe * RB * kSlots +
                                   (size_t)RB * ((M + 1) * M + (M + 1) + 3 * M + kSlots) + (RB * M + 3) / 4) +
                sizeof(V) * (size_t)(M + 2) * NE * RB;
     }
@@ -223,11 +242,14 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
 #pragma unroll
         for (int r = 0; r < RB; r++) w[r] = mm * op[(size_t)r * NE + e] - (acc[r][0] + acc[r][1]);
     };
-    // this warp's partial sums of rhs r: the warp totals of sv[0..cnt) into slots 0..cnt of buffer rbuf
-#define SAP2_PARTIAL(sv, r, cnt) warp_partial(sv, sm.red + ((size_t)rbuf * nwe + wid) * SL + (r) * KS, cnt)
-    // CTA totals of slots 0..cnt of rhs r in buffer buf (every warp forms them itself)
-#define SAP2_TOTALS(buf, r, cnt, t) \
-    cta_totals(sm.red + (size_t)(buf) * nwe * SL + (r) * KS, SL, nwe, cnt, sm.tw + (size_t)wid * KS, t)
+    constexpr int NV = M + 1;  // values per rhs in a reduction: the dots and the new norm
+    // this warp's partial sums of all right-hand sides (sv[r][q]) into buffer rbuf
+#define SAP2_PARTIAL(val) warp_partials<RB, NV, KS>(val, sm.red + ((size_t)rbuf * nwe + wid) * SL)
+    // CTA totals of slots 0..cnt of every rhs in buffer buf (every warp forms them itself); then
+    // SAP2_TOT(r, q) is total q of rhs r
+#define SAP2_TOTALS(buf, cnt) cta_totals<RB, KS>(sm.red + (size_t)(buf) * nwe * SL, SL, nwe, cnt, twp)
+#define SAP2_TOT(r, q) twp[(r) * KS + (q)]
+    double2* const twp = sm.tw + (size_t)wid * SL;  // this warp's copy of the totals
 
     // x = x0 = b; r = b - D_B x (this application fills the link cache)
 #pragma unroll
@@ -239,24 +261,16 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
     bool fin[RB];  // converged, inactive, or a zero right-hand side
     int maxIt[RB];
 #pragma unroll
-    for (int r = 0; r < RB; r++) {
-        w[r] = b[r] - w[r];
-        double2 sv[KS];
-#pragma unroll
-        for (int q = 0; q < KS; q++) sv[q] = make_double2(0.0, 0.0);
-        if (ev) {
-            sv[0].x = (double)cnorm2(b[r]);
-            sv[1].x = (double)cnorm2(w[r]);
-        }
-        SAP2_PARTIAL(sv, r, 2);
-    }
+    for (int r = 0; r < RB; r++) w[r] = b[r] - w[r];
+    SAP2_PARTIAL([&](int r, int q) {  // ||b||^2, ||r||^2
+        return make_double2(ev && q < 2 ? (double)cnorm2(q == 0 ? b[r] : w[r]) : 0.0, 0.0);
+    });
     __syncthreads();
+    SAP2_TOTALS(rbuf, 2);
 #pragma unroll
     for (int r = 0; r < RB; r++) {
-        double2 t[KS];
-        SAP2_TOTALS(rbuf, r, 2, t);
-        norm_b[r] = sqrt(t[0].x);
-        err[r] = sqrt(t[1].x);
+        norm_b[r] = sqrt(SAP2_TOT(r, 0).x);
+        err[r] = sqrt(SAP2_TOT(r, 1).x);
         // a zero block right-hand side has the zero solution (the reference would divide by zero)
         fin[r] = !act[r] || norm_b[r] == 0.0;
         maxIt[r] = M;
@@ -293,21 +307,15 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
             }
             apply(sm.basis + (size_t)j * NE * RB, false);  // w = D_B V_j
             // classical Gram-Schmidt coefficients <w, V_i>, i <= j, and ||w||^2 (slot j + 1)
-#pragma unroll
-            for (int r = 0; r < RB; r++) {
-                if (!arn[r]) continue;
-                // (selects, not a store to sv[j + 1], which would put sv in local memory)
-                const double nw = ev ? (double)cnorm2(w[r]) : 0.0;
-                double2 sv[KS];
-#pragma unroll
-                for (int q = 0; q < KS; q++) {
-                    sv[q] = make_double2(0.0, 0.0);
-                    if (q <= M && ev && q <= j)
-                        sv[q] = cfmac(to_d(sm.basis[((size_t)q * RB + r) * NE + e]), to_d(w[r]), sv[q]);
-                    sv[q].x += (q == j + 1) ? nw : 0.0;
+            // (selects on j, not a store at index j + 1, which would put the values in local memory)
+            SAP2_PARTIAL([&](int r, int q) {
+                double2 v = make_double2(0.0, 0.0);
+                if (arn[r] && ev) {
+                    if (q <= j) v = cfmac(to_d(sm.basis[((size_t)q * RB + r) * NE + e]), to_d(w[r]), v);
+                    v.x += (q == j + 1) ? (double)cnorm2(w[r]) : 0.0;
                 }
-                SAP2_PARTIAL(sv, r, j + 2);
-            }
+                return v;
+            });
             __syncthreads();  // partial sums visible
             const int dbuf = rbuf;
             rbuf ^= 1;
@@ -317,13 +325,15 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
             constexpr double kCancel = sizeof(R) == 8 ? 1e-4 : 1e-2;
             double hn[RB], ihn[RB];
             bool reduce_norm = false;
+            SAP2_TOTALS(dbuf, j + 2);
 #pragma unroll
             for (int r = 0; r < RB; r++) {
                 hn[r] = 0.0;
                 ihn[r] = 0.0;
                 if (!arn[r]) continue;
-                double2 t[KS];
-                SAP2_TOTALS(dbuf, r, j + 2, t);
+                double2 t[NV];
+#pragma unroll
+                for (int q = 0; q < NV; q++) t[q] = q <= j + 1 ? SAP2_TOT(r, q) : make_double2(0.0, 0.0);
                 double w2 = 0.0, hh = 0.0;
 #pragma unroll
                 for (int q = 0; q <= M; q++) {
@@ -348,22 +358,17 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
                         if (q <= j) sm.ct[r * KS + q] = t[q];
             }
             if (reduce_norm) {
-#pragma unroll
-                for (int r = 0; r < RB; r++) {
-                    double2 sv[KS];
-#pragma unroll
-                    for (int q = 0; q < KS; q++) sv[q] = make_double2(0.0, 0.0);
-                    if (arn[r] && ev) sv[0].x = (double)cnorm2(w[r]);
-                    SAP2_PARTIAL(sv, r, 1);
-                }
+                SAP2_PARTIAL([&](int r, int q) {
+                    return make_double2(arn[r] && ev && q == 0 ? (double)cnorm2(w[r]) : 0.0, 0.0);
+                });
                 __syncthreads();
+                SAP2_TOTALS(rbuf, 1);
 #pragma unroll
                 for (int r = 0; r < RB; r++) {
-                    double2 t[KS];
-                    SAP2_TOTALS(rbuf, r, 1, t);
-                    if (arn[r] && t[0].x > 0) {
-                        ihn[r] = rsqrt(t[0].x);
-                        hn[r] = t[0].x * ihn[r];
+                    const double t0 = SAP2_TOT(r, 0).x;
+                    if (arn[r] && t0 > 0) {
+                        ihn[r] = rsqrt(t0);
+                        hn[r] = t0 * ihn[r];
                     }
                 }
                 rbuf ^= 1;
@@ -462,20 +467,13 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
         __syncthreads();
         apply(sm.op, false);
 #pragma unroll
-        for (int r = 0; r < RB; r++) {
-            w[r] = b[r] - w[r];
-            double2 sv[KS];
-#pragma unroll
-            for (int q = 0; q < KS; q++) sv[q] = make_double2(0.0, 0.0);
-            if (ev) sv[0].x = (double)cnorm2(w[r]);
-            SAP2_PARTIAL(sv, r, 1);
-        }
+        for (int r = 0; r < RB; r++) w[r] = b[r] - w[r];
+        SAP2_PARTIAL([&](int r, int q) { return make_double2(ev && q == 0 ? (double)cnorm2(w[r]) : 0.0, 0.0); });
         __syncthreads();
+        SAP2_TOTALS(rbuf, 1);
 #pragma unroll
         for (int r = 0; r < RB; r++) {
-            double2 t[KS];
-            SAP2_TOTALS(rbuf, r, 1, t);
-            err[r] = sqrt(t[0].x);
+            err[r] = sqrt(SAP2_TOT(r, 0).x);
             if (!fin[r] && err[r] < p.tol * norm_b[r]) fin[r] = true;
         }
         rbuf ^= 1;
@@ -489,6 +487,7 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
     }
 #undef SAP2_PARTIAL
 #undef SAP2_TOTALS
+#undef SAP2_TOT
 }
 
 // the kernel takes blocks of at most 512 unknowns at restart length 5 with 1, 2 or 4 right-hand sides
