@@ -178,7 +178,7 @@ struct CoarseGmresWork {
     unsigned* bar = nullptr;   // barrier counter + generation
     int* status = nullptr;     // [0] error flag, [1] iterations
     int grid = 0;
-    int block = 256;
+    int block = 0;             // threads per CTA (set by coarse_gmres_prepare)
     long long spin_limit = 0;  // polls before a grid barrier gives up (<= 0: the default, 2^24)
 };
 void coarse_gmres_prepare(CoarseGmresWork& w, int n, int m, int dof, int device);

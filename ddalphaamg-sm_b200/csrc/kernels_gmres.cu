@@ -77,6 +77,7 @@ __device__ void apply_own(const GmresK& k, const double2* __restrict__ in, doubl
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int dof = k.dof, Nt = k.Nt, Nx = k.Nx;
     const int ntask = (s1 - s0) * 5;
+    constexpr int CB = NI == 1 ? 16 : 4;  // column loads in flight per lane
     for (int task = wid; task < ntask; task += nw) {
         const int sl = task / 5, d = task - sl * 5;
         const int n = s0 + sl;
@@ -101,10 +102,10 @@ __device__ void apply_own(const GmresK& k, const double2* __restrict__ in, doubl
 #pragma unroll
         for (int jq = 0; jq < NI; jq++) {
             const int jn = min(32, dof - 32 * jq);
-            for (int j0 = 0; j0 < jn; j0 += 8) {  // 8 column loads in flight per lane
-                double2 mv[8][NI];
+            for (int j0 = 0; j0 < jn; j0 += CB) {
+                double2 mv[CB][NI];
 #pragma unroll
-                for (int u = 0; u < 8; u++)
+                for (int u = 0; u < CB; u++)
 #pragma unroll
                     for (int q = 0; q < NI; q++) {
                         const int i = lane + 32 * q;
@@ -112,7 +113,7 @@ __device__ void apply_own(const GmresK& k, const double2* __restrict__ in, doubl
                                                             : make_double2(0.0, 0.0);
                     }
 #pragma unroll
-                for (int u = 0; u < 8; u++) {
+                for (int u = 0; u < CB; u++) {
                     if (j0 + u >= jn) break;
                     const double2 vj = make_double2(__shfl_sync(0xffffffffu, vd[jq].x, j0 + u),
                                                     __shfl_sync(0xffffffffu, vd[jq].y, j0 + u));
@@ -150,6 +151,18 @@ __device__ void partial_dots(const GmresK& k, const double2* __restrict__ w, int
         if (lane == 0) part[(long)blockIdx.x * k.P + i] = s;
     }
 }
+// the same with slot cnt = ||w||^2: the Gram-Schmidt coefficients and the norm in one reduction
+__device__ void partial_dots_norm(const GmresK& k, const double2* __restrict__ w, int cnt, double2* __restrict__ part,
+                                  long e0, long e1, long n) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = wid; i <= cnt; i += nw) {
+        const double2* vi = i < cnt ? k.V + (long)i * n : w;
+        double2 s = make_double2(0.0, 0.0);
+        for (long e = e0 + lane; e < e1; e += 32) s = cfmac(vi[e], w[e], s);
+        s = warp_sum(s);
+        if (lane == 0) part[(long)blockIdx.x * k.P + i] = s;
+    }
+}
 // h[i] = sum_blk partial[blk*P + i]: one warp per coefficient, lanes stride over the CTAs' partials,
 // a shuffle tree finishes; every CTA runs the identical order, so all CTAs hold identical sums
 __device__ void reduce_partials(const GmresK& k, const double2* __restrict__ part, int cnt, double2* h) {
@@ -174,13 +187,19 @@ __device__ double2 reduce_slot0(const GmresK& k, const double2* __restrict__ par
     return *tmp;
 }
 
+constexpr int kHs = 48;
+// threads per CTA: 16 warps, so the (site, direction) matrix products of a CTA's two sites stream at once
+constexpr int kCoarseThreads = 512;  // Hessenberg columns every CTA keeps for its own triangular solve
+
 // The Krylov basis is stored unnormalised: slot i of V holds u_i with v_i = sc[i] u_i (sc in shared
-// memory, identical in every CTA).  The second Gram-Schmidt pass writes u_{j+1} straight into its
-// slot before the norm's grid barrier, so that barrier also publishes it to the neighbours'
-// operator application, and no normalisation pass or extra barrier is needed: three grid
-// barriers per Arnoldi step, plus one per restart for the Hessenberg columns.
+// memory, identical in every CTA).  An Arnoldi step reduces the Gram-Schmidt coefficients and ||w||^2
+// together (one grid barrier), forms ||w - V h||^2 = ||w||^2 - sum |h_i|^2, writes u_{j+1} and
+// publishes it with a second barrier; only where that difference cancels below 1e-4 of ||w||^2 (so that
+// it would lose digits) does it run a second Gram-Schmidt pass (classical Gram-Schmidt twice, whose norm
+// barrier publishes u_{j+1}), as the SAP block solvers do.  Every CTA keeps the rotated Hessenberg triangle of the first kHs columns, so the
+// triangular solve at a restart end needs no barrier.
 template <int NI>
-__global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
+__global__ void __launch_bounds__(kCoarseThreads) coarse_gmres_kernel(GmresK k) {
     extern __shared__ double2 sh[];
     const int m = k.m;
     double2* h = sh;              // m+1
@@ -190,7 +209,8 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
     double2* sn = cn + m;         // m
     double2* eta = sn + m;        // m
     double* sc = reinterpret_cast<double*>(eta + m);  // m+1 scale factors (m+1 double2 reserved)
-    double2* part = eta + m + (m + 1);  // sites per CTA x 5 x dof: per-direction partial products
+    double2* hs = eta + m + (m + 1);    // kHs (kHs + 1) / 2: the rotated Hessenberg triangle of the first kHs columns
+    double2* part = hs + kHs * (kHs + 1) / 2;  // sites per CTA x 5 x dof: per-direction partial products
     __shared__ int s_flag;
     __shared__ double2 s_sum;
     const unsigned G = gridDim.x;
@@ -243,39 +263,57 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
             // w = D v_j = sc_j D u_j (u_j of the neighbours was published by the last barrier)
             apply_own<NI>(k, k.V + (long)j * n, k.w, nullptr, s0, s1, part, sc[j]);
             __syncthreads();
-            partial_dots(k, k.w, j + 1, pA, e0, e1, n);  // (u_i, w)
+            // (u_i, w) for i <= j and ||w||^2 in one reduction
+            partial_dots_norm(k, k.w, j + 1, pA, e0, e1, n);
             if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;
-            reduce_partials(k, pA, j + 1, h);
+            reduce_partials(k, pA, j + 2, h);
             for (int i = threadIdx.x; i <= j; i += blockDim.x) h[i] = sc[i] * h[i];  // h_i = (v_i, w)
             __syncthreads();
-            // w -= V h ; reorthogonalise
-            for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-                double2 a = k.w[e];
-                for (int i = 0; i <= j; i++) a = a - cmul(sc[i] * h[i], k.V[(long)i * n + e]);
-                k.w[e] = a;
-            }
-            __syncthreads();
-            partial_dots(k, k.w, j + 1, pB, e0, e1, n);
-            if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;
-            reduce_partials(k, pB, j + 1, h2);
-            for (int i = threadIdx.x; i <= j; i += blockDim.x) h2[i] = sc[i] * h2[i];
-            __syncthreads();
-            {
-                double2* un = k.V + (long)(j + 1) * n;  // u_{j+1}, unnormalised
-                double ss = 0.0;
+            // ||w - V h||^2 = ||w||^2 - sum |h_i|^2; a second Gram-Schmidt pass only where that difference
+            // cancels below 1e-4 of ||w||^2 (identical in every CTA)
+            double hh = 0.0;
+            for (int i = 0; i <= j; i++) hh += cnorm2(h[i]);
+            const double w2 = h[j + 1].x, d2 = w2 - hh;
+            const bool reorth = !(d2 > 1e-4 * w2);
+            double2* un = k.V + (long)(j + 1) * n;  // u_{j+1}, unnormalised
+            double hn;
+            if (!reorth) {
                 for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
                     double2 a = k.w[e];
-                    for (int i = 0; i <= j; i++) a = a - cmul(sc[i] * h2[i], k.V[(long)i * n + e]);
+                    for (int i = 0; i <= j; i++) a = a - cmul(sc[i] * h[i], k.V[(long)i * n + e]);
                     un[e] = a;
-                    ss += cnorm2(a);
                 }
-                __shared__ double2 red2[33];
-                double2 t = block_sum(make_double2(ss, 0.0), red2);
-                if (threadIdx.x == 0) pC[(long)blockIdx.x * k.P] = t;
+                hn = sqrt(d2);
+                if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;  // publishes u_{j+1}
+            } else {
+                // w -= V h ; reorthogonalise
+                for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+                    double2 a = k.w[e];
+                    for (int i = 0; i <= j; i++) a = a - cmul(sc[i] * h[i], k.V[(long)i * n + e]);
+                    k.w[e] = a;
+                }
+                __syncthreads();
+                partial_dots(k, k.w, j + 1, pB, e0, e1, n);
+                if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;
+                reduce_partials(k, pB, j + 1, h2);
+                for (int i = threadIdx.x; i <= j; i += blockDim.x) h2[i] = sc[i] * h2[i];
+                __syncthreads();
+                {
+                    double ss = 0.0;
+                    for (long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+                        double2 a = k.w[e];
+                        for (int i = 0; i <= j; i++) a = a - cmul(sc[i] * h2[i], k.V[(long)i * n + e]);
+                        un[e] = a;
+                        ss += cnorm2(a);
+                    }
+                    __shared__ double2 red2[33];
+                    double2 t = block_sum(make_double2(ss, 0.0), red2);
+                    if (threadIdx.x == 0) pC[(long)blockIdx.x * k.P] = t;
+                }
+                for (int i = threadIdx.x; i <= j; i += blockDim.x) h[i] = h[i] + h2[i];
+                if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;  // also publishes u_{j+1}
+                hn = sqrt(reduce_slot0(k, pC, &s_sum).x);
             }
-            for (int i = threadIdx.x; i <= j; i += blockDim.x) h[i] = h[i] + h2[i];
-            if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;  // also publishes u_{j+1}
-            const double hn = sqrt(reduce_slot0(k, pC, &s_sum).x);
             if (threadIdx.x == 0) {  // FGMRES::rotation (src/fgmres.cpp:99-115) on column j
                 sc[j + 1] = hn > 0 ? 1.0 / hn : 0.0;
                 h[j + 1] = make_double2(hn, 0.0);
@@ -294,6 +332,8 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
                 s_flag = (sqrt(cnorm2(gm[j + 1])) < k.tol * norm_b) ? 1 : 0;
             }
             __syncthreads();
+            if (j < kHs)  // this CTA's own copy of the rotated column (identical in every CTA)
+                for (int i = threadIdx.x; i <= j; i += blockDim.x) hs[j * (j + 1) / 2 + i] = h[i];
             if (blockIdx.x == 0)
                 for (int i = threadIdx.x; i <= j; i += blockDim.x) k.H[(long)j * (m + 1) + i] = h[i];
             if (s_flag) {  // identical in every CTA
@@ -301,15 +341,25 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
                 break;
             }
         }
-        if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;  // the Hessenberg columns of block 0 visible
-        // solve_upper_triangular (src/fgmres.cpp:118-128), column-oriented
-        for (int i = threadIdx.x; i < maxIt; i += blockDim.x) eta[i] = gm[i];
-        __syncthreads();
-        for (int i = maxIt - 1; i >= 0; i--) {
-            if (threadIdx.x == 0) eta[i] = cdiv(eta[i], k.H[(long)i * (m + 1) + i]);
+        // solve_upper_triangular (src/fgmres.cpp:118-128)
+        if (maxIt <= kHs) {  // from this CTA's own triangle, by one thread, in the reference's row order
             __syncthreads();
-            for (int q = threadIdx.x; q < i; q += blockDim.x) eta[q] = eta[q] - cmul(k.H[(long)i * (m + 1) + q], eta[i]);
+            if (threadIdx.x == 0)
+                for (int i = maxIt - 1; i >= 0; i--) {
+                    double2 e = gm[i];
+                    for (int q = i + 1; q < maxIt; q++) e = e - cmul(hs[q * (q + 1) / 2 + i], eta[q]);
+                    eta[i] = cdiv(e, hs[i * (i + 1) / 2 + i]);
+                }
+        } else {  // column-oriented from block 0's columns in global memory
+            if (!grid_barrier(k.bar, k.status, G, k.spin_limit)) return;  // the Hessenberg columns visible
+            for (int i = threadIdx.x; i < maxIt; i += blockDim.x) eta[i] = gm[i];
             __syncthreads();
+            for (int i = maxIt - 1; i >= 0; i--) {
+                if (threadIdx.x == 0) eta[i] = cdiv(eta[i], k.H[(long)i * (m + 1) + i]);
+                __syncthreads();
+                for (int q = threadIdx.x; q < i; q += blockDim.x) eta[q] = eta[q] - cmul(k.H[(long)i * (m + 1) + q], eta[i]);
+                __syncthreads();
+            }
         }
         for (int i = threadIdx.x; i < maxIt; i += blockDim.x) eta[i] = sc[i] * eta[i];  // x += sum eta_i v_i
         __syncthreads();
@@ -343,7 +393,7 @@ __global__ void __launch_bounds__(256) coarse_gmres_kernel(GmresK k) {
 int coarse_gmres_grid(long sites, int sms) { return (int)std::min<long>(sms, std::max<long>(1, (sites + 1) / 2)); }
 static size_t coarse_gmres_smem(long sites, int grid, int m, int dof) {
     const long spc = (sites + grid - 1) / grid;
-    return sizeof(double2) * ((size_t)7 * (m + 1) + (size_t)spc * 5 * dof);
+    return sizeof(double2) * ((size_t)7 * (m + 1) + (size_t)kHs * (kHs + 1) / 2 + (size_t)spc * 5 * dof);
 }
 
 void coarse_gmres_prepare(CoarseGmresWork& w, int n, int m, int dof, int device) {
@@ -356,15 +406,15 @@ void coarse_gmres_prepare(CoarseGmresWork& w, int n, int m, int dof, int device)
     if (dof <= 32) {
         DDAMG_CUDA_TRY(cudaFuncSetAttribute(coarse_gmres_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem));
-        DDAMG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_gmres_kernel<1>, 256, smem));
+        DDAMG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_gmres_kernel<1>, kCoarseThreads, smem));
     } else {
         DDAMG_CUDA_TRY(cudaFuncSetAttribute(coarse_gmres_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem));
-        DDAMG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_gmres_kernel<2>, 256, smem));
+        DDAMG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_gmres_kernel<2>, kCoarseThreads, smem));
     }
     if (per_sm < 1) throw ParamFailure{"coarsest GMRES kernel cannot be resident"};
     w.grid = grid;
-    w.block = 256;
+    w.block = kCoarseThreads;
 }
 
 void launch_coarse_gmres(cudaStream_t s, const CoarseGmresWork& w, const double2* links, const double2* b,
