@@ -901,6 +901,196 @@ __global__ void __launch_bounds__(128, (sizeof(V) == 8 || SPL == 1) ? 4 : 1) sap
             }
 }
 
+// The register kernel for blocks of at most 16 sites with two (block, rhs) tasks per warp, one per
+// half-warp, so that no lane idles (one task per warp would leave lanes 16-31 without a site).  The
+// halves run the block GMRES in lockstep: each keeps its own Arnoldi / restart state, and the loops
+// continue while either half is still working; a half that has finished computes values it never uses.
+// Every reduction is a butterfly over the half (xor 8, 4, 2, 1), which adds in the order the 32-lane
+// butterfly of sap_fine_reg_kernel does after its first level (which adds the idle lanes' zeros), so each
+// task's results are bit-identical to that kernel's.
+template <typename V, int M>
+__global__ void __launch_bounds__(128, 4) sap_fine_pair_kernel(Geom g, const V* __restrict__ U, const V* __restrict__ rg,
+                                                              V* __restrict__ xg, SapKParams p, size_t tbytes) {
+    typedef typename RealOf<V>::R R;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, half = lane >> 4, l16 = lane & 15;
+    const int task = (blockIdx.x * 4 + wib) * 2 + half;
+    const int ntask = p.nblocks * p.nrhs;
+    const int kb = task / p.nrhs, rhs = task - kb * p.nrhs;  // block-major
+    const bool valid = task < ntask && !(p.done && p.done[rhs]);
+    const int et = g.sel_t, ex = g.sel_x, S = ex * et;
+    // per task: Hessenberg matrix, rotations and triangular solve (lane 0 of the half), stencil operand
+    V* H = reinterpret_cast<V*>(smraw + (size_t)(wib * 2 + half) * tbytes);  // (M+1) x M
+    V* gm = H + (M + 1) * M;
+    V* cn = gm + (M + 1);
+    V* sn = cn + M;
+    V* eta = sn + M;
+    V* op = eta + M;
+    const int blk = valid ? p.blocks[kb] : 0;
+    const int bx = blk / g.sap_t, bt = blk - bx * g.sap_t;
+    const long ro = (long)(valid ? rhs : 0) * g.size();
+    const R mm = R(p.m0) + R(2), half_ = R(0.5);
+    const bool sv = valid && l16 < S;
+    const int k = sv ? l16 : 0, kx = k / et, kt = k - kx * et;
+    const int nsite = (bx * ex + kx) * g.Nt + bt * et + kt;
+    const V u0 = sv ? __ldg(U + 2 * nsite) : czero<V>();
+    const V u1 = sv ? __ldg(U + 2 * nsite + 1) : czero<V>();
+    const V ul0 = (sv && kt > 0) ? conjc(__ldg(U + 2 * (nsite - 1))) : czero<V>();
+    const V ul1 = (sv && kx > 0) ? conjc(__ldg(U + 2 * (nsite - g.Nt) + 1)) : czero<V>();
+    V b[2], x[2], w[2];
+    V Vb[M + 1][2];
+#pragma unroll
+    for (int a = 0; a < 2; a++) {
+        b[a] = sv ? rg[ro + (long)nsite * 2 + a] : czero<V>();
+        x[a] = b[a];
+    }
+    // w = D_B v through the half's operand buffer (the stencil reads the neighbours from it)
+    auto apply = [&](const V (&v)[2]) {
+        __syncwarp();
+        if (sv) {
+            op[2 * k] = v[0];
+            op[2 * k + 1] = v[1];
+        }
+        __syncwarp();
+        if (!sv) {
+            w[0] = w[1] = czero<V>();
+            return;
+        }
+        V a = czero<V>(), c = czero<V>(), e = czero<V>(), gg = czero<V>();
+        if (kt + 1 < et) a = cmul(u0, op[2 * (k + 1)] - op[2 * (k + 1) + 1]);          // +t: (1 - sigma_x)
+        if (kx + 1 < ex) c = cmul(u1, op[2 * (k + et)] + imul(op[2 * (k + et) + 1]));  // +x: (1 - sigma_y)
+        if (kt > 0) e = cmul(ul0, op[2 * (k - 1)] + op[2 * (k - 1) + 1]);              // -t: (1 + sigma_x)
+        if (kx > 0) gg = cmul(ul1, op[2 * (k - et)] - imul(op[2 * (k - et) + 1]));      // -x: (1 + sigma_y)
+        w[0] = mm * v[0] - half_ * (a + c + e + gg);
+        w[1] = mm * v[1] - half_ * (imul(gg) - imul(c) + e - a);
+    };
+    auto hsum = [](R s) {  // sum over the half-warp
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        return s;
+    };
+    auto nrm2 = [&](const V (&v)[2]) {
+        const R s = sv ? cnorm2(v[0]) + cnorm2(v[1]) : R(0);
+        return (double)hsum(s);
+    };
+    const int lead = lane & 16;  // the half's first lane
+
+    apply(x);
+#pragma unroll
+    for (int a = 0; a < 2; a++) w[a] = b[a] - w[a];
+    const double norm_b = sqrt(nrm2(b));
+    double err = sqrt(nrm2(w));
+    // a zero block right-hand side has the zero solution (the reference would divide by zero)
+    bool fin = !valid || norm_b == 0.0;
+    int maxIt = M;
+    for (int kr = 0; kr < p.restarts; kr++) {
+        const bool act = !fin;
+        if (!__any_sync(0xffffffffu, act)) break;
+        bool arn = act;
+        const R inv = R(act ? 1.0 / err : 0.0);
+#pragma unroll
+        for (int a = 0; a < 2; a++) Vb[0][a] = inv * w[a];
+        if (l16 == 0 && act) gm[0] = mkc(R(err), R(0));
+#pragma unroll
+        for (int j = 0; j < M; j++) {
+            if (!__any_sync(0xffffffffu, arn)) break;
+            apply(Vb[j]);
+            V h[M];
+#pragma unroll
+            for (int i = 0; i <= j; i++) {
+                V t = czero<V>();
+                if (sv)
+#pragma unroll
+                    for (int a = 0; a < 2; a++) t = cfmac(Vb[i][a], w[a], t);
+                h[i] = t;
+            }
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1)
+#pragma unroll
+                for (int i = 0; i <= j; i++) {
+                    h[i].x += __shfl_xor_sync(0xffffffffu, h[i].x, o);
+                    h[i].y += __shfl_xor_sync(0xffffffffu, h[i].y, o);
+                }
+#pragma unroll
+            for (int i = 0; i <= j; i++)
+#pragma unroll
+                for (int a = 0; a < 2; a++) w[a] = w[a] - cmul(h[i], Vb[i][a]);
+            const double hn = sqrt(nrm2(w));
+            if (arn && hn > 0) {
+                const R ih = R(1.0 / hn);
+#pragma unroll
+                for (int a = 0; a < 2; a++) Vb[j + 1][a] = ih * w[a];
+            }
+            int brk = 0;
+            if (l16 == 0 && arn) {
+#pragma unroll
+                for (int i = 0; i <= j; i++) H[i * M + j] = h[i];
+                H[(j + 1) * M + j] = mkc(R(hn), R(0));
+                for (int i = 0; i < j; i++) {  // FGMRES::rotation (src/fgmres.cpp:99-115)
+                    const V hij = H[i * M + j], hi1 = H[(i + 1) * M + j];
+                    const V tmp = cmulc(cn[i], hij) + cmulc(sn[i], hi1);
+                    H[(i + 1) * M + j] = cmul(cn[i], hi1) - cmul(sn[i], hij);
+                    H[i * M + j] = tmp;
+                }
+                const V hjj = H[j * M + j], hj1 = H[(j + 1) * M + j];
+                const R den = sqrt(cnorm2(hjj) + cnorm2(hj1));
+                sn[j] = mkc(hj1.x / den, hj1.y / den);
+                cn[j] = mkc(hjj.x / den, hjj.y / den);
+                H[j * M + j] = cmulc(cn[j], hjj) + cmulc(sn[j], hj1);
+                H[(j + 1) * M + j] = czero<V>();
+                gm[j + 1] = -cmul(sn[j], gm[j]);
+                gm[j] = cmulc(cn[j], gm[j]);
+                brk = (sqrt(cnorm2(gm[j + 1])) < p.tol * norm_b) ? 1 : 0;
+            }
+            brk = __shfl_sync(0xffffffffu, brk, lead);
+            if (arn && brk) {
+                maxIt = j + 1;  // not reset at the next restart (src/fgmres.cpp:14,56)
+                arn = false;
+            }
+        }
+        if (l16 == 0 && act) {  // solve_upper_triangular (src/fgmres.cpp:118-128)
+            for (int i = maxIt - 1; i >= 0; i--) {
+                V e = gm[i];
+                for (int jj = i + 1; jj < maxIt; jj++) e = e - cmul(H[i * M + jj], eta[jj]);
+                eta[i] = cdiv(e, H[i * M + i]);
+            }
+        }
+        __syncwarp();
+        if (act) {
+#pragma unroll
+            for (int jj = 0; jj < M; jj++) {
+                if (jj >= maxIt) break;
+                const V ej = eta[jj];
+#pragma unroll
+                for (int a = 0; a < 2; a++) x[a] = cfma(ej, Vb[jj][a], x[a]);
+            }
+        }
+        apply(x);
+#pragma unroll
+        for (int a = 0; a < 2; a++) w[a] = b[a] - w[a];
+        const double e2 = sqrt(nrm2(w));
+        if (act) {
+            err = e2;
+            if (err < p.tol * norm_b) fin = true;
+        }
+    }
+    // x_B += e  (src/sap.cpp:106-113)
+    if (sv && norm_b != 0.0)
+#pragma unroll
+        for (int a = 0; a < 2; a++) {
+            V* o = xg + ro + (long)nsite * 2 + a;
+            *o = *o + x[a];
+        }
+}
+
+template <typename V, int M>
+static void launch_fine_pair(cudaStream_t s, const Geom& g, const V* U, const V* r, V* x, SapKParams p) {
+    const int S = g.sel_x * g.sel_t;
+    const size_t tb = (sizeof(V) * ((M + 1) * M + (M + 1) + 3 * M) + sizeof(V) * 2 * S + 15) / 16 * 16;
+    const int tasks = p.nblocks * p.nrhs;
+    DDAMG_LAUNCH((sap_fine_pair_kernel<V, M>), ceil_div(tasks, 8), 128, tb * 8, s, g, U, r, x, p, tb);
+}
+
 template <typename V, int SPL, int M>
 static void launch_fine_reg(cudaStream_t s, const Geom& g, const V* U, const V* r, V* x, SapKParams p) {
     const int S = g.sel_x * g.sel_t;
@@ -1027,7 +1217,8 @@ void launch_sap_sweep_fine(cudaStream_t s, const Geom& g, const V* U, const V* r
     const int S = g.sel_x * g.sel_t;
     if (a.m > kSapMaxM) throw ParamFailure{"SAP block GMRES restart length above 8 is not supported"};
     SapKParams p{a.m, a.restarts, a.tol, a.m0, a.blocks, a.nblocks, a.done, nrhs, 1};
-    if (a.m == 5 && S <= 32) launch_fine_reg<V, 1, 5>(s, g, U, r, x, p);
+    if (a.m == 5 && S <= 16) launch_fine_pair<V, 5>(s, g, U, r, x, p);
+    else if (a.m == 5 && S <= 32) launch_fine_reg<V, 1, 5>(s, g, U, r, x, p);
     else if (a.m == 5 && S <= 64) launch_fine_reg<V, 2, 5>(s, g, U, r, x, p);
     else if (S <= 32) launch_fine_warp<V, 1>(s, g, U, r, x, p);
     else if (S <= 64) launch_fine_warp<V, 2>(s, g, U, r, x, p);

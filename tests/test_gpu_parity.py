@@ -306,3 +306,23 @@ def test_solve_batched_tensor_cores_vs_oracle(golden, cycle):
         worst = max(worst, rel(xr, xo))
     print(f"tensor-core batched mixed solve, cycle {int(cycle)}: max rel diff to the FP64 oracle {worst:.2e}")
     assert worst < 1e-9
+
+
+def test_sap_level0_small_blocks(golden):
+    """Level-0 SAP with 4 x 4-site blocks (configs[0]'s layout; the kernel that runs two block solves per
+    warp) against the oracle, and a 3-vector batch (an odd number of block tasks, so one half-warp has no
+    task) equal bit for bit to three single-vector sweeps."""
+    z = golden("solve_64x64_l2")
+    s, o = make_pair(z)
+    v = z["probe_0"]
+    xg, itg = s.SAP(0, v, nu=3)
+    xo, ito = o.sap(0, v, nu=3)
+    assert itg == ito
+    assert rel(xg, xo) < 1e-9
+    n = v.size
+    vs = [po.gaussian(n, 700 + r) for r in range(3)]
+    xb = s.SAP_batched(0, np.concatenate(vs), 3, nu=2, tol=0)
+    for r in range(3):
+        x1 = s.SAP_batched(0, vs[r], 1, nu=2, tol=0)
+        assert np.array_equal(xb[r * n:(r + 1) * n], x1), r
+    s.close()
