@@ -184,6 +184,9 @@ struct NanFailure {  // a NaN / Inf in an input or an iterate -> DDAMG_ERR_NAN
 struct NotConvergedFailure {  // an inner solve that a call depends on missed its tolerance -> DDAMG_NOT_CONVERGED
     std::string msg;
 };
+struct IoFailure {  // a file that cannot be opened or written -> DDAMG_ERR_IO
+    std::string msg;
+};
 
 // launch bookkeeping: every kernel launch in the library goes through this counter
 extern std::atomic<long long> g_launches;  // kernels launched by the library (all handles)

@@ -6,8 +6,10 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <ctime>
 #include <fstream>
 #include <functional>
+#include <iomanip>
 #include <map>
 #include <set>
 #include <memory>
@@ -15,6 +17,8 @@
 #include <string>
 #include <type_traits>
 #include <vector>
+
+#include <unistd.h>
 
 #include "internal.h"
 
@@ -131,6 +135,8 @@ struct ddamg_handle {
     long long prof_n[kProfKinds][DDAMG_MAX_LEVELS] = {};
     // fine-level Schwarz layouts by block counts (FGMRES_SAP, stand-alone fine SAP), made on first use
     std::map<std::pair<int, int>, ddamg::SapLayout> fine_sap;
+    // iterations of the last run of each method (ddamg_counter), -1 before the first
+    long long counts[DDAMG_COUNT_KINDS] = {-1, -1, -1, -1, -1, -1, -1};
 };
 
 namespace ddamg {
@@ -1044,6 +1050,7 @@ static ddamg_status solve_device(ddamg_handle* h, const double2* b, double2* x, 
     float ms = 0;
     DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     ddamg_status st = DDAMG_OK;
+    h->counts[p.cycle == DDAMG_CYCLE_K ? DDAMG_COUNT_KCYCLE : DDAMG_COUNT_VCYCLE] = *std::max_element(it.begin(), it.end());
     for (int r = 0; r < nrhs; r++) {
         const bool conv = rel[r] < p.fgmres_tolerance;
         if (!conv) st = DDAMG_NOT_CONVERGED;
@@ -1084,6 +1091,10 @@ using namespace ddamg;
     catch (const NotConvergedFailure& e) {                                                       \
         set_error(e.msg);                                                                        \
         return DDAMG_NOT_CONVERGED;                                                              \
+    }                                                                                            \
+    catch (const IoFailure& e) {                                                                 \
+        set_error(e.msg);                                                                        \
+        return DDAMG_ERR_IO;                                                                     \
     }                                                                                            \
     catch (const std::exception& e) {                                                            \
         set_error(e.what());                                                                     \
@@ -1656,6 +1667,7 @@ ddamg_status ddamg_gmres_plain(ddamg_t* h, const double* b, double* x, int m, in
         cudaFree(q);
         h->allocs.erase(std::find(h->allocs.begin(), h->allocs.end(), q));
     }
+    h->counts[DDAMG_COUNT_GMRES] = it;
     if (info) {
         info->iterations = it;
         info->converged = rel < tol;
@@ -1741,6 +1753,96 @@ ddamg_status ddamg_set_coarse_barrier_polls(ddamg_t* h, int polls) {
     for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second.exec);
     h->graphs.clear();
     h->graph_warm.clear();
+    API_END
+}
+
+// ------------------------------------------------------------------ run metadata
+namespace ddamg {
+// writeMetadata (src/io.cpp:72-145): the same lines, widths and number formats
+static void write_metadata(const ddamg_params& p, const long long* c, int cycle, double tol, const char* path) {
+    if (cycle != DDAMG_CYCLE_V && cycle != DDAMG_CYCLE_K) throw ParamFailure{"cycle must be 0 (V) or 1 (K)"};
+    if (p.levels < 2 || p.levels > DDAMG_MAX_LEVELS) throw ParamFailure{"levels out of range"};
+    std::string file;
+    if (path) {
+        file = path;
+    } else {
+        std::ostringstream fn;
+        fn << "metadata_" << p.Nx << "x" << p.Nt << "_Levels" << p.levels << (cycle == 0 ? "_Vcycle" : "_Kcycle")
+           << ".dat";
+        file = fn.str();
+    }
+    std::string host;
+    if (const char* e = std::getenv("HOSTNAME")) {
+        host = e;
+    } else {
+        char buf[256] = {};
+        if (gethostname(buf, sizeof(buf) - 1) == 0) host = buf;
+    }
+    const std::time_t now = std::time(nullptr);
+    std::tm tmv{};
+    localtime_r(&now, &tmv);
+    std::ostringstream o;
+    o << "Host: " << host << "\n";
+    o << "Date: " << std::put_time(&tmv, "%Y-%m-%d %H:%M:%S") << "\n";
+    o << "x ranks: " << 1 << "  t_ranks: " << 1 << "\n";
+    o << "m0: " << std::setprecision(7) << p.m0 << "\n";
+    o << "solvers tolerance: " << std::setprecision(4) << tol << "\n";
+    o << "#level, blocks_x (global), blocks_t (global), Ntest, SAP_blocks_x (local), SAP_blocks_t (local)\n";
+    for (int l = 0; l < p.levels - 1; l++) {
+        o << l;
+        for (int k = 1; k <= 5; k++) o << std::setw(5) << p.rows[l][k];
+        o << "\n";
+    }
+    auto triple = [&](int a, int b, double t) {
+        o << a << std::setw(5) << b << std::setw(15) << std::scientific << std::setprecision(7) << t << "\n";
+    };
+    o << "#SAP_test_vectors_iterations\n" << p.sap_test_vectors_iterations << "\n";
+    o << "#cycle (0 = V, 1 = K)\n" << cycle << "\n";
+    o << "#Pre-smoothing nu1, Post-smoothing nu2\n" << p.nu1 << std::setw(5) << p.nu2 << "\n";
+    o << "#sap gmres restart length, sap gmres restarts, sap gmres tolerance\n";
+    triple(p.sap_gmres_restart_length, p.sap_gmres_restarts, p.sap_gmres_tolerance);
+    o << "#GMRES restart length coarse level, GMRES restarts coarse level, GMRES tolerance coarse level\n";
+    triple(p.coarse_gmres_restart_length, p.coarse_gmres_restarts, p.coarse_gmres_tolerance);
+    o << "#FGMRES restart length, FGMRES restarts, FGMRES tolerance\n";
+    triple(p.fgmres_restart_length, p.fgmres_restarts, p.fgmres_tolerance);
+    const long long none = -1;  // FLOP counters are not kept
+    auto pair = [&](const char* head, long long it) { o << head << "\n" << it << std::setw(30) << none << "\n"; };
+    pair("#CG iterations,   FLOPS", c[DDAMG_COUNT_CG]);
+    pair("#BiCGStab iterations,   FLOPS", c[DDAMG_COUNT_BICG]);
+    pair("#GMRES iterations,   FLOPS", c[DDAMG_COUNT_GMRES]);
+    pair("#SAP iterations,   FLOPS", c[DDAMG_COUNT_SAP]);
+    pair("#FGMRES_SAP iterations,   FLOPS", c[DDAMG_COUNT_FGMRES_SAP]);
+    o << (cycle == 0 ? "#V cycle fgmres iterations,  Setup phase FLOPS, Total FLOPS\n"
+                     : "#K cycle fgmres iterations,  Setup phase FLOPS, Total FLOPS\n");
+    o << c[cycle == 0 ? DDAMG_COUNT_VCYCLE : DDAMG_COUNT_KCYCLE] << std::setw(30) << none << std::setw(30) << none
+      << "\n";
+    std::ofstream f(file);
+    if (!f) throw IoFailure{"cannot open " + file + " for writing"};
+    f << o.str();
+    if (!f) throw IoFailure{"write failed: " + file};
+}
+}  // namespace ddamg
+
+ddamg_status ddamg_get_counters(ddamg_t* h, long long counts[DDAMG_COUNT_KINDS]) {
+    if (!h || !counts) {
+        set_error("null argument");
+        return DDAMG_ERR_BAD_PARAM;
+    }
+    std::copy(h->counts, h->counts + DDAMG_COUNT_KINDS, counts);
+    return DDAMG_OK;
+}
+ddamg_status ddamg_write_metadata(ddamg_t* h, const char* path, int cycle, double tol) {
+    if (!h) {
+        set_error("null handle");
+        return DDAMG_ERR_BAD_PARAM;
+    }
+    return ddamg_write_metadata_params(&h->p, h->counts, cycle, tol, path);
+}
+ddamg_status ddamg_write_metadata_params(const ddamg_params* p, const long long counts[DDAMG_COUNT_KINDS], int cycle,
+                                         double tol, const char* path) {
+    API_BEGIN
+    if (!p || !counts) throw ParamFailure{"null argument"};
+    write_metadata(*p, counts, cycle, tol, path);
     API_END
 }
 
@@ -1837,6 +1939,7 @@ ddamg_status ddamg_fgmres_sap(ddamg_t* h, const double* b, double* x, int blocks
             cudaFree(q);
             h->allocs.erase(std::find(h->allocs.begin(), h->allocs.end(), q));
         }
+    h->counts[DDAMG_COUNT_FGMRES_SAP] = it;
     if (info) {
         info->iterations = it;
         info->converged = rel < tol;
@@ -1862,6 +1965,7 @@ ddamg_status ddamg_sap_fine(ddamg_t* h, const double* v, double* x, int blocks_x
     const int it = sap_t<double2>(h, 0, D.d.eta, D.d.psi, nu, tol, false, 1, true, &lay);
     DDAMG_CUDA_TRY(cudaMemcpyAsync(x, D.d.psi, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->s));
     sync(h);
+    h->counts[DDAMG_COUNT_SAP] = it;
     if (iters) *iters = it;
     API_END
 }
@@ -2042,6 +2146,7 @@ static ddamg_status krylov_run(ddamg_handle* h, int solver, const double* b, con
         float ms = 0;
         DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
         const double rel = nn[1] > 0 ? std::sqrt(nn[0] / nn[1]) : 0.0;
+        h->counts[solver == 0 ? DDAMG_COUNT_BICG : DDAMG_COUNT_CG] = st.iters;
         if (info) {
             info->iterations = st.iters;
             info->converged = st.done == 2;

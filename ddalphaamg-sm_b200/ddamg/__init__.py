@@ -89,6 +89,17 @@ def gaussian_field(n, seed):
     return out
 
 
+# iteration counters of the metadata file (src/variables.cpp:9-17), in ddamg_counter order
+COUNTER_NAMES = ("CG", "BiCG", "GMRES", "SAP", "FGMRES_SAP", "vCycle", "kCycle")
+
+
+def write_metadata(params, counts, cycle, tol, path=None):
+    """writeMetadata (src/io.cpp:72-145) from parameters and counters alone (host only, no device)."""
+    c = (ctypes.c_longlong * 7)(*[int(v) for v in counts])
+    check(_lib.load().ddamg_write_metadata_params(ctypes.byref(params), c, cycle, tol,
+                                                  path.encode() if path else None))
+
+
 class Solver:
     """One multigrid hierarchy on one GPU (AlgebraicMG + FGMRES_AMG of the reference)."""
 
@@ -257,6 +268,16 @@ class Solver:
         it = ctypes.c_int(0)
         check(self.L.ddamg_sap_fine(self.h, _dp(v), _dp(x), blocks_x, blocks_t, nu, tol, ctypes.byref(it)))
         return x, it.value
+
+    def counters(self):
+        """Iterations of the last run of each method (-1: not run), as a dict in the metadata file's order."""
+        c = (ctypes.c_longlong * 7)()
+        check(self.L.ddamg_get_counters(self.h, c))
+        return dict(zip(COUNTER_NAMES, list(c)))
+
+    def writeMetadata(self, cycle, tol, path=None):
+        """writeMetadata (src/io.cpp:72-145): the run metadata file; path None gives the reference's name."""
+        check(self.L.ddamg_write_metadata(self.h, path.encode() if path else None, cycle, tol))
 
     def set_coarse_barrier_polls(self, polls):
         """Polls after which a grid barrier of the coarsest-level GMRES gives up (DEVICE_TIMEOUT)."""

@@ -80,6 +80,10 @@ SIGNATURES = {
     "ddamg_coarse_gmres_noalloc": (_st, [_vp, _vp, _vp, _i, _i, _i, ctypes.c_double, _i, _i, ctypes.c_double, _vp,
                                          ctypes.POINTER(_i)]),
     "ddamg_set_coarse_barrier_polls": (_st, [_h, _i]),
+    "ddamg_get_counters": (_st, [_h, ctypes.POINTER(ctypes.c_longlong)]),
+    "ddamg_write_metadata": (_st, [_h, ctypes.c_char_p, _i, ctypes.c_double]),
+    "ddamg_write_metadata_params": (_st, [ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_longlong), _i,
+                                          ctypes.c_double, ctypes.c_char_p]),
     "ddamg_apply_multilevel": (_st, [_h, _dp, _dp, _i, ctypes.c_double, ctypes.POINTER(_i), _dp]),
     "ddamg_fgmres_sap": (_st, [_h, _dp, _dp, _i, _i, _i, _i, ctypes.c_double, ctypes.POINTER(SolveInfo)]),
     "ddamg_sap_fine": (_st, [_h, _dp, _dp, _i, _i, _i, ctypes.c_double, ctypes.POINTER(_i)]),

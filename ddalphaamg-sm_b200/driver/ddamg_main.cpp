@@ -2,11 +2,13 @@
 // ABI in include/ddamg.h only: it reads the same seven answers from standard input (ranks_x, ranks_t,
 // levels, m0, configuration file, right-hand-side file, parameters file), then runs Methods::CG,
 // FGMRES with the V-cycle and FGMRES with the K-cycle (src/methods.cpp:42-190) and checks both
-// multigrid solutions the way Methods::check_solution does.  The lattice size, a compile-time
+// multigrid solutions the way Methods::check_solution does, writing the two metadata files after the
+// checks as the reference does (writeMetadata).  The lattice size, a compile-time
 // constant of the reference (include/config.h), is the pair of command-line arguments.  There is one
 // GPU and no MPI: ranks_x and ranks_t are read and reported, not used.
 //
 //   ddamg_main Nx Nt [x_out.bin] < answers.txt
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -96,10 +98,21 @@ int main(int argc, char** argv) {
                 info.iterations);
     std::printf("time elapsed CG: %.4fs.\n\n", now() - t0);
 
+    // the run's iteration counters (the reference keeps them in globals, src/variables.cpp:9-17); each
+    // handle contributes the methods it ran before it is destroyed
+    long long counts[DDAMG_COUNT_KINDS], hc[DDAMG_COUNT_KINDS];
+    std::fill(counts, counts + DDAMG_COUNT_KINDS, -1LL);
+    auto collect = [&]() {
+        CHECK(ddamg_get_counters(h, hc));
+        for (int k = 0; k < DDAMG_COUNT_KINDS; k++)
+            if (hc[k] >= 0) counts[k] = hc[k];
+    };
+
     // FGMRES with the V-cycle, then with the K-cycle; each constructs (sets up) its hierarchy
     std::vector<double> xv(2 * n), xk(2 * n);
     for (int cycle = 0; cycle < 2; cycle++) {
         std::cout << "--------------FGMRES with AMG " << (cycle ? "K" : "V") << "-cycle--------------" << std::endl;
+        collect();
         ddamg_destroy(h);
         p.cycle = cycle ? DDAMG_CYCLE_K : DDAMG_CYCLE_V;
         CHECK(ddamg_create(&p, &h));
@@ -114,10 +127,14 @@ int main(int argc, char** argv) {
         std::printf("time elapsed FGMRES AMG %c-cycle: %.4fs (setup %.4fs).\n\n", cycle ? 'K' : 'V', now() - t0,
                     info.setup_seconds);
     }
+    collect();
+    // src/main.cpp:89-97: check each solution, then write its metadata file (writeMetadata, src/io.cpp:72-145)
     std::cout << "Checking solution of V-cycle" << std::endl;
     check_solution(h, xv, b, Nt);
+    CHECK(ddamg_write_metadata_params(&p, counts, 0, tol, nullptr));
     std::cout << "Checking solution of K-cycle" << std::endl;
     check_solution(h, xk, b, Nt);
+    CHECK(ddamg_write_metadata_params(&p, counts, 1, tol, nullptr));
     if (argc > 3) CHECK(ddamg_write_binary(argv[3], Nx, Nt, xv.data()));
     ddamg_destroy(h);
     return 0;

@@ -205,6 +205,30 @@ ddamg_status ddamg_coarse_gmres_noalloc(const void* links, const void* b, void* 
 /* changes coarse_barrier_polls of a live handle (launches made after the call use it; V-cycle graphs
  * captured earlier are dropped and captured again).  No reference counterpart. */
 ddamg_status ddamg_set_coarse_barrier_polls(ddamg_t* h, int polls);
+/* ------------------------------------------------------------------ run metadata */
+/* Iteration counters of the last run of each method, in the order the metadata file lists them;
+ * -1 for a method not run on the handle (src/variables.cpp:9-17). */
+typedef enum {
+    DDAMG_COUNT_CG = 0,         /* ddamg_cg_normal        (iter_counters::CGIt, Methods::CG) */
+    DDAMG_COUNT_BICG = 1,       /* ddamg_bicgstab         (iter_counters::BiCGIt) */
+    DDAMG_COUNT_GMRES = 2,      /* ddamg_gmres_plain      (iter_counters::GMRESIt) */
+    DDAMG_COUNT_SAP = 3,        /* ddamg_sap_fine         (iter_counters::SAPIt) */
+    DDAMG_COUNT_FGMRES_SAP = 4, /* ddamg_fgmres_sap       (iter_counters::FGMRES_SAPIt) */
+    DDAMG_COUNT_VCYCLE = 5,     /* ddamg_solve, V-cycle   (iter_counters::vCycleIt; most iterations over the batch) */
+    DDAMG_COUNT_KCYCLE = 6,     /* ddamg_solve, K-cycle   (iter_counters::kCycleIt) */
+    DDAMG_COUNT_KINDS = 7
+} ddamg_counter;
+ddamg_status ddamg_get_counters(ddamg_t* h, long long counts[DDAMG_COUNT_KINDS]);
+/* writeMetadata (src/io.cpp:72-145): the run metadata file, line for line in the reference's format
+ * (host, date, rank grid 1 x 1, m0, tolerance, one row per non-coarsest level, the solver constants and
+ * the iteration counters of the handle).  The reference's FLOP counters are not kept: every FLOPS
+ * column holds -1, the reference's value for a method that did not run.  path NULL: the reference's
+ * file name metadata_<Nx>x<Nt>_Levels<L>_{V,K}cycle.dat in the working directory.  The Host line is
+ * $HOSTNAME, else gethostname(). */
+ddamg_status ddamg_write_metadata(ddamg_t* h, const char* path, int cycle, double tol);
+/* the same from parameters and counters alone (no handle, no device) */
+ddamg_status ddamg_write_metadata_params(const ddamg_params* p, const long long counts[DDAMG_COUNT_KINDS], int cycle,
+                                         double tol, const char* path);
 /* one cycle from psi = 0: AlgebraicMG::v_cycle / k_cycle (src/amg.cpp:64-174) */
 ddamg_status ddamg_vcycle(ddamg_t* h, const double* eta, double* psi);
 ddamg_status ddamg_kcycle(ddamg_t* h, const double* eta, double* psi);

@@ -16,6 +16,9 @@
  *                     (AlgebraicMG::applyMultilevel after the injected setup; prints its cycle count)
  *   ref_harness fgmres_sap <levels> <m0> <params> <conf.bin> <rhs.bin> - <outdir> <m> <restarts> <tol>
  *   ref_harness sapfine <levels> <m0> <params> <conf.bin> <rhs.bin> - <outdir> <xblocks> <tblocks> <nu>
+ *   ref_harness metadata <levels> <m0> <params> <conf.bin> - - <outdir> <cycle> <tol>
+ *                     <CG> <BiCG> <GMRES> <SAP> <FGMRES_SAP> <Vcycle> <Kcycle>
+ *                     (writeMetadata with the iteration counters given; the file lands in outdir)
  *
  * conf.bin / rhs.bin use the reference binary record format (src/io.cpp:32-44).
  * probe.bin / tvec.bin / outputs are raw little-endian complex128 arrays
@@ -36,6 +39,7 @@
 #include <string>
 #include <vector>
 #include <utility>
+#include <unistd.h>
 
 #define private public
 #include "amg.h"
@@ -336,6 +340,27 @@ int main(int argc, char** argv) {
         const int it = sap.SAP(rhs, x, nu, 1e-10, false);
         dump("x.bin", interior(x, mpi::width_x, mpi::width_t, 2));
         std::ofstream(g_out + "/sapfine.txt") << "iterations " << it << "\n";
+        return 0;
+    }
+    if (mode == "metadata") {
+        /* writeMetadata (src/io.cpp:72-145) with the iteration counters set from the command line;
+         * the FLOP counters keep their initial -1 */
+        if (argc < 18) {
+            std::cerr << "metadata needs cycle tol and 7 counters\n";
+            return 2;
+        }
+        const int cycle = std::atoi(argv[9]);
+        const double tol = std::atof(argv[10]);
+        iter_counters::CGIt = std::atoll(argv[11]);
+        iter_counters::BiCGIt = std::atoll(argv[12]);
+        iter_counters::GMRESIt = std::atoll(argv[13]);
+        iter_counters::SAPIt = std::atoll(argv[14]);
+        iter_counters::FGMRES_SAPIt = std::atoll(argv[15]);
+        iter_counters::vCycleIt = std::atoll(argv[16]);
+        iter_counters::kCycleIt = std::atoll(argv[17]);
+        setenv("HOSTNAME", "golden-host", 1);
+        if (chdir(g_out.c_str()) != 0) return 3;
+        writeMetadata(cycle, tol);
         return 0;
     }
     if (mode == "krylov") {

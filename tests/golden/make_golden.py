@@ -58,6 +58,9 @@ CASES = [
          rows=[[0, 4, 8, 4, 2, 4], [1, 2, 4, 6, 2, 2]], beta=2.0, sweeps=20, seed=11, m=20, modes=("multilevel",)),
     dict(name="fgmres_sap_64x64", Nx=64, Nt=64, levels=2, m0=-0.18,
          rows=[[0, 16, 16, 10, 16, 16]], beta=2.0, sweeps=500, seed=2024, m=20, modes=("fgmres_sap",)),
+    # the run metadata file of writeMetadata (src/io.cpp:72-145), V and K, with set iteration counters
+    dict(name="metadata_16x32_l3", Nx=16, Nt=32, levels=3, m0=-0.10,
+         rows=[[0, 4, 8, 4, 2, 4], [1, 2, 4, 6, 2, 2]], beta=2.0, sweeps=20, seed=11, m=20, modes=("metadata",)),
     # the comparison solvers of src/conjugate_gradient.cpp (BiCGstab on D, CG on D^dagger D)
     dict(name="krylov_32x32", Nx=32, Nt=32, levels=2, m0=-0.15,
          rows=[[0, 8, 8, 6, 4, 4]], beta=2.0, sweeps=30, seed=12, m=20, modes=("krylov",)),
@@ -196,6 +199,20 @@ def make_case(c, work):
             del out["theta"], out["rhs"]
             for l in range(L):
                 del out[f"probe_{l}"]
+    if "metadata" in c["modes"]:
+        # counters CG, BiCGstab, GMRES, SAP, FGMRES_SAP, V-cycle, K-cycle; the V file leaves the K counter
+        # unset (-1) and the other way round, as after one Methods::Vcycle or Kcycle run
+        counts = {0: [1371, 411, -1, 3, 17, 9, -1], 1: [-1, -1, 250, -1, -1, -1, 5]}
+        for cyc, tol in ((0, 1e-10), (1, 1e-9)):
+            md = os.path.join(work, f"meta{cyc}")
+            os.makedirs(md)
+            run([harness, "metadata", str(L), repr(c["m0"]), pfile, conf, "-", "-", md, str(cyc), repr(tol)]
+                + [str(v) for v in counts[cyc]])
+            fname = f"metadata_{Nx}x{Nt}_Levels{L}_{'V' if cyc == 0 else 'K'}cycle.dat"
+            out[f"ref_metadata_{cyc}"] = np.frombuffer(open(os.path.join(md, fname), "rb").read(), dtype=np.uint8)
+            out[f"metadata_counts_{cyc}"] = np.array(counts[cyc], dtype=np.int64)
+            out[f"metadata_tol_{cyc}"] = tol
+        del out["theta"], out["rhs"]
     if "krylov" in c["modes"]:
         kd = os.path.join(work, "krylov")
         os.makedirs(kd)

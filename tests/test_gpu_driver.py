@@ -29,7 +29,8 @@ def test_driver_follows_the_reference_main(golden, tmp_path):
         for r in z["rows"]:
             f.write(" ".join(str(int(v)) for v in r) + "\n")
     answers = f"1 1 {int(z['levels'])} {float(z['m0'])!r} {conf} {rhs} {par}\n"
-    r = subprocess.run([DRIVER, str(Nx), str(Nt), xout], input=answers, capture_output=True, text=True, timeout=300)
+    r = subprocess.run([DRIVER, str(Nx), str(Nt), xout], input=answers, capture_output=True, text=True, timeout=300,
+                       cwd=str(tmp_path))
     assert r.returncode == 0, r.stderr
     out = r.stdout
     cg = int(re.search(r"CG for D\^\+D converged in (\d+) iterations", out).group(1))
@@ -42,5 +43,13 @@ def test_driver_follows_the_reference_main(golden, tmp_path):
     # the reference's own stock-setup V-cycle solve of this system
     assert abs(int(runs[0][0]) - int(zs["ref_iters_V_stock"])) <= 2
     assert out.count("Solution verified") == 2 and "Solution differs" not in out
+    # the two metadata files of src/main.cpp:92,97 (writeMetadata), in the working directory
+    L = int(z["levels"])
+    for tag, (it, _) in zip("VK", runs):
+        lines = open(tmp_path / f"metadata_{Nx}x{Nt}_Levels{L}_{tag}cycle.dat").read().splitlines()
+        i = lines.index(f"#{tag} cycle fgmres iterations,  Setup phase FLOPS, Total FLOPS")
+        assert int(lines[i + 1].split()[0]) == int(it)
+        i = lines.index("#CG iterations,   FLOPS")
+        assert int(lines[i + 1].split()[0]) == cg
     x = po.read_binary(xout, Nx, Nt)
     assert np.linalg.norm(x - zs["ref_x_V"]) / np.linalg.norm(zs["ref_x_V"]) < 1e-7

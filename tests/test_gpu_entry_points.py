@@ -117,6 +117,28 @@ def test_sap_fine_matches_reference(golden):
     s.close()
 
 
+def test_counters_and_metadata(golden, tmp_path):
+    """The handle's iteration counters follow each method's last run and land in the metadata file
+    (writeMetadata, src/io.cpp:72-145)."""
+    z = golden("multilevel_32x32_l2")
+    s, U = solver(z)
+    assert set(s.counters().values()) == {-1}
+    _, it_sap = s.SAP_fine(z["rhs"], 4, 8, nu=3)
+    _, info_f = s.fgmres_sap(z["rhs"], 4, 4, m=20, restarts=50, tol=1e-10)
+    _, info_v = s.solve(z["rhs"])
+    c = s.counters()
+    assert (c["SAP"], c["FGMRES_SAP"], c["vCycle"]) == (it_sap, info_f.iterations, info_v.iterations)
+    assert c["kCycle"] == -1 and c["CG"] == -1
+    path = str(tmp_path / "meta.dat")
+    s.writeMetadata(ddamg.CYCLE_V, 1e-10, path)
+    s.close()
+    lines = open(path).read().splitlines()
+    i = lines.index("#V cycle fgmres iterations,  Setup phase FLOPS, Total FLOPS")
+    assert int(lines[i + 1].split()[0]) == info_v.iterations
+    i = lines.index("#SAP iterations,   FLOPS")
+    assert int(lines[i + 1].split()[0]) == it_sap
+
+
 def test_coarse_barrier_timeout_then_recovers(golden):
     """A poll limit of 1 makes the coarsest GMRES kernel's first barrier that has to wait give up: every CTA
     leaves at its next barrier, the call reports DEVICE_TIMEOUT, and after the limit is restored the same
