@@ -168,6 +168,53 @@ void launch_gauge_force(cudaStream_t s, const double* th, double* F, int Nx, int
 void launch_hmc_momentum(cudaStream_t s, double* p, const double* Fg, const double* Ff, double eps, long nlinks);
 void launch_hmc_theta(cudaStream_t s, double* th, const double* p, double eps, long nlinks);
 
+// ------------------------------------------------------------ device-driven FGMRES (kernels_fgmres.cu)
+// Per-level state of one lockstep FGMRES (R right-hand sides, restart length m) whose Arnoldi
+// bookkeeping runs on the device; loops are CUDA graph conditional nodes.
+enum FgCtl {
+    kFgJ = 0,            // Arnoldi step of the current restart
+    kFgK = 1,            // restart
+    kFgNan = 2,          // a NaN or Inf was met (reported by the host after the solve)
+    kFgRunsOuter = 3,    // restart bodies run (cumulative)
+    kFgRunsInner = 4,    // Arnoldi-step bodies run (cumulative)
+    kFgRunsFirst = 5,    // K-cycle preconditioner bodies from zero (cumulative)
+    kFgRunsLater = 6,    // K-cycle preconditioner bodies from the previous Z_j (cumulative)
+    kFgCtlWords = 8
+};
+struct FgDev {
+    double2 *H = nullptr, *gm = nullptr, *cn = nullptr, *sn = nullptr;  // R x (m+1) x m, R x (m+1), R x m
+    double2* coef = nullptr;   // R x m back-substitution result
+    double2* alpha = nullptr;  // R scale factors of the next basis vector
+    double2* dots = nullptr;   // 2 x R x (m+1): the two Gram-Schmidt passes of the current step
+    double* nrm = nullptr;     // 2R squared norms
+    double *norm_b = nullptr, *err = nullptr;
+    int *maxIt = nullptr, *done = nullptr, *arn = nullptr, *ret = nullptr;
+    int* ctl = nullptr;  // kFgCtlWords
+};
+void launch_fg_start(cudaStream_t s, const FgDev& f, int R, int m, int restarts, cudaGraphConditionalHandle hc);
+void launch_fg_restart(cudaStream_t s, const FgDev& f, int R, int m, cudaGraphConditionalHandle hc);
+void launch_fg_arnoldi(cudaStream_t s, const FgDev& f, int R, int m, double tol, cudaGraphConditionalHandle hc);
+void launch_fg_backsub(cudaStream_t s, const FgDev& f, int R, int m);
+void launch_fg_restart_end(cudaStream_t s, const FgDev& f, int R, int m, int restarts, double tol,
+                           cudaGraphConditionalHandle hc);
+void launch_fg_select(cudaStream_t s, const FgDev& f, cudaGraphConditionalHandle first,
+                      cudaGraphConditionalHandle later);
+// multi-dot / multi-axpy over basis vectors 0..j with j = *jdev; results and coefficients at
+// [r*ldk + i]; kmax bounds k = j + 1
+template <typename V>
+void launch_multidot_dev(cudaStream_t s, const V* B, long ldb, long bstride, int kmax, const int* jdev, int ldk,
+                         const V* w, long wstride, long n, int nrhs, double2* partial, double2* out);
+template <typename V>
+void launch_multiaxpy_dev(cudaStream_t s, const V* B, long ldb, long bstride, const int* jdev, const double2* coef,
+                          int ldk, V* w, long wstride, long n, int nrhs);
+// Vb[j*slot + r*n + e] = alpha_r x[r*n + e]
+template <typename V>
+void launch_scale_slot(cudaStream_t s, const double2* alpha, const V* x, V* Vb, long slot, const int* jdev, long n,
+                       int nrhs);
+// to_slot = 0: dst[e] = src[j*slot + e]; 1: dst[j*slot + e] = src[e]
+template <typename A, typename B>
+void launch_slot_copy(cudaStream_t s, const A* src, B* dst, long slot, const int* jdev, int to_slot, long count);
+
 // ------------------------------------------------------------ coarsest GMRES (kernels_gmres.cu)
 struct CoarseGmresWork {
     double2* V = nullptr;      // (m+1) x n

@@ -3,6 +3,7 @@
 // All device work is issued on the handle's stream; data-dependent branches that would
 // otherwise need a host round trip (SAP early exit) are device-side flags.
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -42,7 +43,9 @@ template <typename V> struct LevelBufs {
     V* kZ = nullptr;
     V* kw = nullptr;
     V* kr = nullptr;
-    V* kx = nullptr;
+    // fixed copies of the current basis vector and preconditioned vector (device-driven FGMRES)
+    V* kin = nullptr;
+    V* kzf = nullptr;
 };
 
 struct LevelData {
@@ -60,6 +63,7 @@ struct LevelData {
     TcSapWork tcw;
     std::map<int, int> tc_shape;  // batch width -> tile shape chosen by the autotuner
     std::map<int, int> rb_choice; // 2 * batch width + fp32 -> right-hand sides per CTA (CUDA cores)
+    FgDev fg;                     // device-driven FGMRES state (level 0: the outer solve; >= 1: K-cycle)
 };
 constexpr int kTcMinRhs = 8;  // fewer right-hand sides leave too little link reuse for the tensor cores
 // A Schwarz-block layout of the fine level other than the parameters file's: the block counts of
@@ -137,6 +141,26 @@ struct ddamg_handle {
     std::map<std::pair<int, int>, ddamg::SapLayout> fine_sap;
     // iterations of the last run of each method (ddamg_counter), -1 before the first
     long long counts[DDAMG_COUNT_KINDS] = {-1, -1, -1, -1, -1, -1, -1};
+    // device-driven solves: one graph per batch width whose conditional nodes run the FGMRES loops
+    // (built on the second solve of a width; the first runs host driven and does the tuning)
+    struct CapBody {
+        int level, kind;  // kind: 0 the top graph, else the FgCtl run counter of the body
+        long long kernels;
+    };
+    struct SolveGraph {
+        cudaGraphExec_t exec;
+        std::vector<CapBody> bodies;
+    };
+    std::map<int, SolveGraph> solve_graphs;
+    std::set<int> solve_warm;
+    bool solve_graphs_off = false;
+    bool capturing = false;                 // h->s is recording a device-driven solve graph
+    cudaGraph_t cap_top = nullptr;          // its top-level graph (conditional handles live there)
+    std::vector<CapBody>* cap_bodies = nullptr;
+    int cap_cur = -1;                       // body the capture is recording into
+    long long cap_mark = 0;                 // g_launches when that segment began
+    double2* ovin = nullptr;                // fixed copies of V_j and Z_j of the outer FGMRES
+    double2* ozf = nullptr;
 };
 
 namespace ddamg {
@@ -299,12 +323,36 @@ static void allocate(ddamg_handle* h) {
                 D.f.kZ = dalloc_t<float2>(h, km * Rn);
                 D.f.kw = dalloc_t<float2>(h, Rn);
                 D.f.kr = dalloc_t<float2>(h, Rn);
+                D.f.kin = dalloc_t<float2>(h, Rn);
+                D.f.kzf = dalloc_t<float2>(h, Rn);
             } else {
                 D.d.kV = dalloc_t<double2>(h, (km + 1) * Rn);
                 D.d.kZ = dalloc_t<double2>(h, km * Rn);
                 D.d.kw = dalloc_t<double2>(h, Rn);
                 D.d.kr = dalloc_t<double2>(h, Rn);
+                D.d.kin = dalloc_t<double2>(h, Rn);
+                D.d.kzf = dalloc_t<double2>(h, Rn);
             }
+        }
+        if (l == 0 || p.cycle == DDAMG_CYCLE_K) {
+            const int fm = l == 0 ? p.fgmres_restart_length : p.kcycle_restart_length;
+            const size_t R = (size_t)p.max_rhs;
+            FgDev& f = D.fg;
+            f.H = dalloc_t<double2>(h, R * (fm + 1) * fm);
+            f.gm = dalloc_t<double2>(h, R * (fm + 1));
+            f.cn = dalloc_t<double2>(h, R * fm);
+            f.sn = dalloc_t<double2>(h, R * fm);
+            f.coef = dalloc_t<double2>(h, R * fm);
+            f.alpha = dalloc_t<double2>(h, R);
+            f.dots = dalloc_t<double2>(h, 2 * R * (fm + 1));
+            f.nrm = dalloc_t<double>(h, 2 * R);
+            f.norm_b = dalloc_t<double>(h, R);
+            f.err = dalloc_t<double>(h, R);
+            f.maxIt = dalloc_t<int>(h, R);
+            f.done = dalloc_t<int>(h, R);
+            f.arn = dalloc_t<int>(h, R);
+            f.ret = dalloc_t<int>(h, R);
+            f.ctl = dalloc_t<int>(h, kFgCtlWords);
         }
         D.done = dalloc_t<int>(h, W);
         D.vv = dalloc_t<double>(h, W);
@@ -364,6 +412,8 @@ static void allocate(ddamg_handle* h) {
     h->orr = dalloc_t<double2>(h, Rn0);
     h->ob = dalloc_t<double2>(h, Rn0);
     h->ox = dalloc_t<double2>(h, Rn0);
+    h->ovin = dalloc_t<double2>(h, Rn0);
+    h->ozf = dalloc_t<double2>(h, Rn0);
     const int mm = std::max(m, std::max(p.kcycle_restart_length, 1)) + 2;
     h->dpart = dalloc_t<double2>(h, (size_t)kRedBlocks * (2 * (size_t)W * mm + 2));
     h->dh = dalloc_t<double2>(h, 2 * (size_t)W * mm + 2);
@@ -718,6 +768,125 @@ static void fgmres_host(ddamg_handle* h, long n, int R, int m, int restarts, dou
     }
 }
 
+// ------------------------------------------------------------------ FGMRES (device driven)
+// While h->capturing, h->s records into a graph that replaces the host loop above: the loops become
+// conditional nodes whose conditions the control kernels of kernels_fgmres.cu set.  Recording is split
+// into segments: before a conditional node is added the capture is ended (its dependency set kept),
+// the node's body is recorded on the same stream, and the capture then resumes after the node.  Each
+// segment's kernels are counted against the body it belongs to, so the launches a solve ran follow
+// from the bodies' run counters.
+struct CapPoint {
+    std::vector<cudaGraphNode_t> deps;
+    cudaGraph_t graph;
+};
+static CapPoint cap_pause(ddamg_handle* h) {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    DDAMG_CUDA_TRY(cudaStreamGetCaptureInfo(h->s, &st, nullptr, &g, &deps, &nd));
+    if (st != cudaStreamCaptureStatusActive) throw CudaFailure{};
+    CapPoint p{std::vector<cudaGraphNode_t>(deps, deps + nd), g};
+    cudaGraph_t out = nullptr;
+    DDAMG_CUDA_TRY(cudaStreamEndCapture(h->s, &out));
+    (*h->cap_bodies)[h->cap_cur].kernels += g_launches - h->cap_mark;
+    return p;
+}
+static void cap_begin(ddamg_handle* h, cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps, int body) {
+    DDAMG_CUDA_TRY(cudaStreamBeginCaptureToGraph(h->s, g, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                                 cudaStreamCaptureModeRelaxed));
+    h->cap_cur = body;
+    h->cap_mark = g_launches;
+}
+static int cap_new_body(ddamg_handle* h, int level, int kind) {
+    h->cap_bodies->push_back({level, kind, 0});
+    return (int)h->cap_bodies->size() - 1;
+}
+static cudaGraphConditionalHandle cap_handle(ddamg_handle* h) {
+    cudaGraphConditionalHandle hc;
+    DDAMG_CUDA_TRY(cudaGraphConditionalHandleCreate(&hc, h->cap_top, 0, 0));
+    return hc;
+}
+// ends the current segment, adds a conditional node (while or if) after it and records `body` into the
+// node's graph as a new body of (level, kind); the capture resumes after the node
+static void cap_conditional(ddamg_handle* h, cudaGraphConditionalHandle hc, cudaGraphConditionalNodeType type,
+                            int level, int kind, const std::function<void()>& body) {
+    const int cur = h->cap_cur;
+    CapPoint p = cap_pause(h);
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = hc;
+    np.conditional.type = type;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    DDAMG_CUDA_TRY(cudaGraphAddNode(&node, p.graph, p.deps.empty() ? nullptr : p.deps.data(), p.deps.size(), &np));
+    cap_begin(h, np.conditional.phGraph_out[0], {}, cap_new_body(h, level, kind));
+    body();
+    cap_pause(h);
+    cap_begin(h, p.graph, {node}, cur);
+}
+
+// FGMRES::fgmres as fgmres_host computes it, recorded into the graph under construction.  M(in, out, R,
+// first): out = M in with in and out fixed buffers; first = restart 0 (the K-cycle starts from zero
+// there and from the previous Z_j after a restart), `select` says whether the two differ.
+template <typename V>
+static void fgmres_dev(ddamg_handle* h, int lvl, long n, int R, int m, int restarts, double tol,
+                       const std::function<void(const V*, V*, int)>& A,
+                       const std::function<void(const V*, V*, int, bool)>& M, bool select, const V* b, const V* x0,
+                       bool x0_zero, V* x, Krylov<V> K, V* vin, V* zf) {
+    cudaStream_t s = h->s;
+    const long Rn = (long)R * n;
+    const FgDev& f = h->lv[lvl].fg;
+    const int* jdev = f.ctl + kFgJ;
+    if (x0_zero) DDAMG_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(V) * Rn, s));
+    else if (x0 != x) DDAMG_CUDA_TRY(cudaMemcpyAsync(x, x0, sizeof(V) * Rn, cudaMemcpyDeviceToDevice, s));
+    DDAMG_CUDA_TRY(cudaMemsetAsync(K.Z, 0, sizeof(V) * Rn * m, s));
+    if (x0_zero) DDAMG_CUDA_TRY(cudaMemcpyAsync(K.r, b, sizeof(V) * Rn, cudaMemcpyDeviceToDevice, s));
+    else {
+        A(x, K.w, R);
+        launch_sub<V>(s, b, K.w, K.r, Rn);
+    }
+    launch_norm2<V>(s, b, n, n, R, h->dpart, f.nrm);
+    launch_norm2<V>(s, K.r, n, n, R, h->dpart, f.nrm + R);
+    const cudaGraphConditionalHandle hc_outer = cap_handle(h), hc_inner = cap_handle(h);
+    launch_fg_start(s, f, R, m, restarts, hc_outer);
+    cap_conditional(h, hc_outer, cudaGraphCondTypeWhile, lvl, kFgRunsOuter, [&]() {
+        launch_fg_restart(s, f, R, m, hc_inner);
+        launch_scale<V>(s, f.alpha, K.r, K.Vb, n, R);  // V_0 = r / beta
+        cap_conditional(h, hc_inner, cudaGraphCondTypeWhile, lvl, kFgRunsInner, [&]() {
+            launch_slot_copy<V, V>(s, K.Vb, vin, Rn, jdev, 0, Rn);
+            if (!select) {
+                M(vin, zf, R, false);
+            } else {
+                const cudaGraphConditionalHandle hf = cap_handle(h), hl = cap_handle(h);
+                launch_fg_select(s, f, hf, hl);
+                cap_conditional(h, hf, cudaGraphCondTypeIf, lvl, kFgRunsFirst, [&]() { M(vin, zf, R, true); });
+                cap_conditional(h, hl, cudaGraphCondTypeIf, lvl, kFgRunsLater, [&]() {
+                    launch_slot_copy<V, V>(s, K.Z, zf, Rn, jdev, 0, Rn);
+                    M(vin, zf, R, false);
+                });
+            }
+            launch_slot_copy<V, V>(s, zf, K.Z, Rn, jdev, 1, Rn);
+            A(zf, K.w, R);
+            double2* d1 = f.dots;
+            double2* d2 = f.dots + (long)R * (m + 1);
+            launch_multidot_dev<V>(s, K.Vb, Rn, n, m, jdev, m + 1, K.w, n, n, R, h->dpart, d1);
+            launch_multiaxpy_dev<V>(s, K.Vb, Rn, n, jdev, d1, m + 1, K.w, n, n, R);
+            launch_multidot_dev<V>(s, K.Vb, Rn, n, m, jdev, m + 1, K.w, n, n, R, h->dpart, d2);
+            launch_multiaxpy_dev<V>(s, K.Vb, Rn, n, jdev, d2, m + 1, K.w, n, n, R);
+            launch_norm2<V>(s, K.w, n, n, R, h->dpart, f.nrm);
+            launch_fg_arnoldi(s, f, R, m, tol, hc_inner);
+            launch_scale_slot<V>(s, f.alpha, K.w, K.Vb, Rn, jdev, n, R);  // V_{j+1}
+        });
+        launch_fg_backsub(s, f, R, m);
+        launch_multiaxpy<V>(s, K.Z, Rn, n, m, f.coef, x, n, n, R, +1.0);
+        A(x, K.w, R);
+        launch_sub<V>(s, b, K.w, K.r, Rn);
+        launch_norm2<V>(s, K.r, n, n, R, h->dpart, f.nrm);
+        launch_fg_restart_end(s, f, R, m, restarts, tol, hc_outer);
+    });
+}
+
 // ------------------------------------------------------------------ cycles
 static void cycle(ddamg_handle* h, int l, const void* eta, void* psi, bool psi_zero, int kind, int R);
 
@@ -793,6 +962,15 @@ static void cycle_t(ddamg_handle* h, int l, const V* eta, V* psi, bool psi_zero,
                 cycle(h, l + 1, in, out, restart == 0, DDAMG_CYCLE_K, RR);
             };
             Krylov<W> K{nb.kV, nb.kZ, nb.kw, nb.kr};
+            if (h->capturing) {
+                std::function<void(const W*, W*, int, bool)> Md = [h, l](const W* in, W* out, int RR, bool first) {
+                    cycle(h, l + 1, in, out, first, DDAMG_CYCLE_K, RR);
+                };
+                fgmres_dev<W>(h, l + 1, nn, R, p.kcycle_restart_length, p.kcycle_restarts, p.kcycle_tolerance, A, Md,
+                              true, static_cast<const W*>(en), static_cast<const W*>(en), false, static_cast<W*>(pn), K,
+                              nb.kin, nb.kzf);
+                return;
+            }
             fgmres_host<W>(h, nn, R, p.kcycle_restart_length, p.kcycle_restarts, p.kcycle_tolerance, A, &M,
                            static_cast<const W*>(en), static_cast<const W*>(en), false, static_cast<W*>(pn), K,
                            nullptr, nullptr);
@@ -820,7 +998,7 @@ static void level0_cycle(ddamg_handle* h, int R) {
         if (D.fp32) cycle(h, 0, D.f.eta, D.f.psi, true, h->p.cycle, R);
         else cycle(h, 0, D.d.eta, D.d.psi, true, h->p.cycle, R);
     };
-    if (!h->p.cuda_graphs || h->graphs_off || h->p.cycle != DDAMG_CYCLE_V || h->prof) {
+    if (!h->p.cuda_graphs || h->graphs_off || h->p.cycle != DDAMG_CYCLE_V || h->prof || h->capturing) {
         direct();
         return;
     }
@@ -1026,6 +1204,85 @@ static void setup(ddamg_handle* h, const double2* rnd_host, uint64_t seed) {
 }
 
 // ------------------------------------------------------------------ solve
+// The device-driven solve of R right-hand sides from h->ob into h->ox: built once per width (false if
+// this runtime cannot record or instantiate it; the host-driven loop is used from then on)
+static bool solve_graph(ddamg_handle* h, int R, const std::function<void(const double2*, double2*, int)>& A,
+                        const std::function<void(const double2*, double2*, int, bool)>& M, Krylov<double2> K) {
+    if (h->solve_graphs.count(R)) return true;
+    const ddamg_params& p = h->p;
+    const long n = h->lv[0].g.size();
+    const long long l0 = g_launches;
+    ddamg_handle::SolveGraph sg{nullptr, {}};
+    cudaGraph_t top = nullptr;
+    bool ok = cudaGraphCreate(&top, 0) == cudaSuccess;
+    if (ok) {
+        h->capturing = true;
+        h->cap_top = top;
+        h->cap_bodies = &sg.bodies;
+        try {
+            cap_begin(h, top, {}, cap_new_body(h, 0, 0));
+            for (int l = 0; l < h->L; l++)
+                if (h->lv[l].fg.ctl)
+                    DDAMG_CUDA_TRY(cudaMemsetAsync(h->lv[l].fg.ctl + kFgRunsOuter, 0, 4 * sizeof(int), h->s));
+            fgmres_dev<double2>(h, 0, n, R, p.fgmres_restart_length, p.fgmres_restarts, p.fgmres_tolerance, A, M,
+                                false, h->ob, nullptr, true, h->ox, K, h->ovin, h->ozf);
+            cap_pause(h);
+        } catch (...) {
+            ok = false;
+            cudaStreamCaptureStatus st;
+            if (cudaStreamIsCapturing(h->s, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+                cudaGraph_t junk = nullptr;
+                cudaStreamEndCapture(h->s, &junk);
+                if (junk && junk != top) cudaGraphDestroy(junk);
+            }
+        }
+        h->capturing = false;
+        h->cap_bodies = nullptr;
+        h->cap_top = nullptr;
+    }
+    if (ok && cudaGraphInstantiate(&sg.exec, top, 0) != cudaSuccess) ok = false;
+    if (top) cudaGraphDestroy(top);
+    g_launches = l0;  // recorded, not run
+    if (!ok) {
+        cudaGetLastError();
+        if (sg.exec) cudaGraphExecDestroy(sg.exec);
+        h->solve_graphs_off = true;
+        h->tune_log += "solve graph for rhs " + std::to_string(R) + ": not supported here, host-driven FGMRES\n";
+        return false;
+    }
+    long long kernels = 0;
+    for (const auto& bd : sg.bodies) kernels += bd.kernels;
+    h->tune_log += "solve graph rhs " + std::to_string(R) + ": " + std::to_string(sg.bodies.size()) + " bodies, " +
+                   std::to_string(kernels) + " kernels recorded (FGMRES loops on the device)\n";
+    h->solve_graphs[R] = sg;
+    return true;
+}
+static void run_solve_graph(ddamg_handle* h, int R, std::vector<int>& it, std::vector<double>& rel) {
+    const ddamg_handle::SolveGraph& sg = h->solve_graphs.at(R);
+    DDAMG_CUDA_TRY(cudaGraphLaunch(sg.exec, h->s));
+    std::vector<std::array<int, kFgCtlWords>> ctl(h->L);
+    for (int l = 0; l < h->L; l++)
+        if (h->lv[l].fg.ctl)
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(ctl[l].data(), h->lv[l].fg.ctl, sizeof(int) * kFgCtlWords,
+                                           cudaMemcpyDeviceToHost, h->s));
+    const FgDev& f = h->lv[0].fg;
+    std::vector<int> ret(R);
+    std::vector<double> err(R), nb(R);
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(ret.data(), f.ret, sizeof(int) * R, cudaMemcpyDeviceToHost, h->s));
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(err.data(), f.err, sizeof(double) * R, cudaMemcpyDeviceToHost, h->s));
+    DDAMG_CUDA_TRY(cudaMemcpyAsync(nb.data(), f.norm_b, sizeof(double) * R, cudaMemcpyDeviceToHost, h->s));
+    sync(h);
+    long long launched = 0;
+    for (const auto& bd : sg.bodies) launched += bd.kernels * (bd.kind == 0 ? 1 : ctl[bd.level][bd.kind]);
+    g_launches += launched;
+    for (int l = 0; l < h->L; l++)
+        if (h->lv[l].fg.ctl && ctl[l][kFgNan]) throw NanFailure{"NaN in the right-hand side or the Krylov basis"};
+    for (int r = 0; r < R; r++) {
+        it[r] = nb[r] == 0.0 ? 0 : ret[r];
+        rel[r] = nb[r] > 0 ? err[r] / nb[r] : 0.0;
+    }
+}
+
 static ddamg_status solve_device(ddamg_handle* h, const double2* b, double2* x, int nrhs, ddamg_solve_info* info) {
     if (!h->setup_done) throw ParamFailure{"run the setup before solving"};
     const ddamg_params& p = h->p;
@@ -1041,8 +1298,25 @@ static ddamg_status solve_device(ddamg_handle* h, const double2* b, double2* x, 
     Krylov<double2> K{h->oV, h->oZ, h->ow, h->orr};
     std::vector<int> it(nrhs);
     std::vector<double> rel(nrhs);
-    fgmres_host<double2>(h, n, nrhs, p.fgmres_restart_length, p.fgmres_restarts, p.fgmres_tolerance, A, &M, b,
-                         nullptr, true, x, K, it.data(), rel.data());
+    const bool graph = p.cuda_graphs && !h->prof && !h->solve_graphs_off;
+    if (graph && h->solve_warm.count(nrhs)) {
+        std::function<void(const double2*, double2*, int, bool)> Md = [h](const double2* in, double2* out, int R,
+                                                                          bool) { outer_prec(h, in, out, R); };
+        if (solve_graph(h, nrhs, A, Md, K)) {
+            if (b != h->ob)
+                DDAMG_CUDA_TRY(cudaMemcpyAsync(h->ob, b, sizeof(double2) * n * nrhs, cudaMemcpyDeviceToDevice, h->s));
+            run_solve_graph(h, nrhs, it, rel);
+            if (x != h->ox)
+                DDAMG_CUDA_TRY(cudaMemcpyAsync(x, h->ox, sizeof(double2) * n * nrhs, cudaMemcpyDeviceToDevice, h->s));
+        } else {
+            fgmres_host<double2>(h, n, nrhs, p.fgmres_restart_length, p.fgmres_restarts, p.fgmres_tolerance, A, &M, b,
+                                 nullptr, true, x, K, it.data(), rel.data());
+        }
+    } else {
+        fgmres_host<double2>(h, n, nrhs, p.fgmres_restart_length, p.fgmres_restarts, p.fgmres_tolerance, A, &M, b,
+                             nullptr, true, x, K, it.data(), rel.data());
+        if (graph) h->solve_warm.insert(nrhs);
+    }
     check_coarse_status(h, nullptr);
     check_tc_status(h);
     DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, h->s));
@@ -1207,6 +1481,7 @@ ddamg_status ddamg_destroy(ddamg_t* h) {
     cudaSetDevice(h->p.device);
     if (h->s) cudaStreamSynchronize(h->s);
     for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second.exec);
+    for (auto& kv : h->solve_graphs) cudaGraphExecDestroy(kv.second.exec);
     for (void* a : h->allocs) cudaFree(a);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : h->lane_ev) cudaEventDestroy(e);
@@ -1753,6 +2028,9 @@ ddamg_status ddamg_set_coarse_barrier_polls(ddamg_t* h, int polls) {
     for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second.exec);
     h->graphs.clear();
     h->graph_warm.clear();
+    for (auto& kv : h->solve_graphs) cudaGraphExecDestroy(kv.second.exec);
+    h->solve_graphs.clear();
+    h->solve_warm.clear();
     API_END
 }
 

@@ -127,14 +127,14 @@ def test_counters_and_metadata(golden, tmp_path):
     _, info_f = s.fgmres_sap(z["rhs"], 4, 4, m=20, restarts=50, tol=1e-10)
     _, info_v = s.solve(z["rhs"])
     c = s.counters()
-    assert (c["SAP"], c["FGMRES_SAP"], c["vCycle"]) == (it_sap, info_f.iterations, info_v.iterations)
+    assert (c["SAP"], c["FGMRES_SAP"], c["vCycle"]) == (it_sap, info_f.iterations, info_v[0].iterations)
     assert c["kCycle"] == -1 and c["CG"] == -1
     path = str(tmp_path / "meta.dat")
     s.writeMetadata(ddamg.CYCLE_V, 1e-10, path)
     s.close()
     lines = open(path).read().splitlines()
     i = lines.index("#V cycle fgmres iterations,  Setup phase FLOPS, Total FLOPS")
-    assert int(lines[i + 1].split()[0]) == info_v.iterations
+    assert int(lines[i + 1].split()[0]) == info_v[0].iterations
     i = lines.index("#SAP iterations,   FLOPS")
     assert int(lines[i + 1].split()[0]) == it_sap
 
