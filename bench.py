@@ -470,7 +470,7 @@ def run_ours(args, rank, world, local_rank):
                                                device=local_rank))
         sk.load_gauge(U)
         xk = torch.zeros_like(b_dev)
-        for _ in range(2):
+        for _ in range(3):  # the first solve of a width runs host driven, later ones as one device graph
             sk.setUpPhase(seed=w["setup_seed"])
             ik = sk.solve_device(b_dev.data_ptr(), xk.data_ptr())[0]
         sec["kcycle_same_workload"] = {
@@ -769,35 +769,49 @@ def krylov_256(ddamg, U, b, x_amg, dev):
     return out
 
 
+DW_N = 2048  # D_W bandwidth lattice: 384 MiB (FP64) / 192 MiB (FP32) of psi, U and output, above the 126 MB L2
+DW_ROWS = [[0, 256, 256, 4, 256, 256], [1, 32, 32, 4, 32, 32]]
+
+
 def dw_bandwidth(ddamg, torch, dev):
-    """D_W GB/s on a 1024x1024 lattice: 96 B/site FP64, 48 B/site FP32 (psi in, U, out; neighbour reuse perfect)."""
-    Nx = Nt = 1024
-    th, _ = ddamg.gauge_metropolis(Nx, Nt, 4.0, 10, 3, device=dev)
+    """D_W and D_W^dagger GB/s on a 2048x2048 lattice (inputs and output 1.5-3x the L2): 96 B/site FP64,
+    48 B/site FP32 (psi in, U, out; neighbour reuse perfect), one right-hand side per launch, 30 launches
+    timed with CUDA events on the library's stream.  Both kernel families: the register kernels (the
+    default) and the staged-tile kernel (bulk asynchronous copies of psi and link tiles into shared
+    memory)."""
+    N = DW_N
+    th, _ = ddamg.gauge_metropolis(N, N, 4.0, 2, 3, device=dev)
     U = np.exp(1j * th)
-    p = ddamg.default_params(Nx, Nt, 2, -0.07, [[0, 128, 128, 4, 128, 128]], device=dev, precision=ddamg.PREC_MIXED)
+    p = ddamg.default_params(N, N, 3, -0.07, DW_ROWS, device=dev, precision=ddamg.PREC_MIXED)
     s = ddamg.Solver(p)
     s.load_gauge(U)
     stream = torch.cuda.ExternalStream(s.stream())
-    out = {}
+    out = {"lattice": f"{N}x{N}", "rhs_per_launch": 1}
     for name, dt, bps in (("f64", torch.float64, 96), ("f32", torch.float32, 48)):
-        x = torch.randn(2 * 2 * Nx * Nt, dtype=dt, device=f"cuda:{dev}")
+        x = torch.randn(2 * 2 * N * N, dtype=dt, device=f"cuda:{dev}")
         y = torch.empty_like(x)
         fn = s.L.ddamg_apply_dirac_device if dt == torch.float64 else s.L.ddamg_apply_dirac_f32_device
-        for _ in range(3):
-            ddamg.check(fn(s.h, 0, x.data_ptr(), y.data_ptr(), 1))
-        reps = 50
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            e0.record(stream)
-            for _ in range(reps):
-                ddamg.check(fn(s.h, 0, x.data_ptr(), y.data_ptr(), 1))
-            e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / reps
-        out[name] = {"GB_s": bps * Nx * Nt / (ms * 1e-3) / 1e9, "us_per_apply": 1e3 * ms}
+        for kind, kname in ((1, "register"), (2, "staged")):
+            ddamg.set_stencil_kernel(kind)
+            for dag, dname in ((0, "D"), (1, "Ddag")):
+                for _ in range(3):
+                    ddamg.check(fn(s.h, dag, x.data_ptr(), y.data_ptr(), 1))
+                reps = 30
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                with torch.cuda.stream(stream):
+                    e0.record(stream)
+                    for _ in range(reps):
+                        ddamg.check(fn(s.h, dag, x.data_ptr(), y.data_ptr(), 1))
+                    e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / reps
+                key = f"{name}" if (kind == 1 and dag == 0) else f"{name}_{dname}_{kname}"
+                out[key] = {"GB_s": bps * N * N / (ms * 1e-3) / 1e9, "us_per_apply": 1e3 * ms}
+    ddamg.set_stencil_kernel(0)
     hbm, kind = peaks()
     for v in out.values():
-        v["frac_of_hbm"] = v["GB_s"] / hbm
+        if isinstance(v, dict):
+            v["frac_of_hbm"] = v["GB_s"] / hbm
     out["peak_kind"] = kind
     s.close()
     return out
@@ -810,24 +824,31 @@ def profile_case(name):
     tc-apply one batched FP32 level-1 SAP sweep pair on 512x512 with 64 right-hand sides
              (tc_block_apply_kernel, the tensor-core block operator);
     krylov   20 BiCGstab iterations on a 1024x1024 field (bicg_* kernels, 11 fields of 32 MiB);
-    dw       D_W and D_W^dagger on a 1024x1024 field, FP64 then FP32 (wilson_kernel, 32 + 32 MiB in/out)."""
+    dw       D_W and D_W^dagger on the 2048x2048 bandwidth lattice, FP64 then FP32, register kernels then
+             the staged-tile kernel (wilson_kernel, wilson_pair_kernel, wilson_stage_kernel; 128 MiB per
+             FP64 field)."""
     import ddamg
 
     if name == "dw":
         import torch
 
-        N = 1024
-        th, _ = ddamg.gauge_metropolis(N, N, 4.0, 10, 3)
-        s = ddamg.Solver(ddamg.default_params(N, N, 2, -0.07, [[0, 128, 128, 4, 128, 128]], precision=ddamg.PREC_MIXED))
+        N = DW_N
+        th, _ = ddamg.gauge_metropolis(N, N, 4.0, 2, 3)
+        s = ddamg.Solver(ddamg.default_params(N, N, 3, -0.07, DW_ROWS, precision=ddamg.PREC_MIXED))
         s.load_gauge(np.exp(1j * th))
-        for dt, fn in ((torch.float64, s.L.ddamg_apply_dirac_device), (torch.float32, s.L.ddamg_apply_dirac_f32_device)):
-            x = torch.randn(4 * N * N, dtype=dt, device="cuda")
-            y = torch.empty_like(x)
-            for dag in (0, 1):
-                for _ in range(2):
-                    ddamg.check(fn(s.h, dag, x.data_ptr(), y.data_ptr(), 1))
+        for kind in (1, 2):
+            ddamg.set_stencil_kernel(kind)
+            for dt, fn in ((torch.float64, s.L.ddamg_apply_dirac_device),
+                           (torch.float32, s.L.ddamg_apply_dirac_f32_device)):
+                x = torch.randn(4 * N * N, dtype=dt, device="cuda")
+                y = torch.empty_like(x)
+                for dag in (0, 1):
+                    for _ in range(2):
+                        ddamg.check(fn(s.h, dag, x.data_ptr(), y.data_ptr(), 1))
+        ddamg.set_stencil_kernel(0)
         torch.cuda.synchronize()
-        print("dw: 8 applications (FP64 D, D^dagger, FP32 D, D^dagger; 2 each) on 1024x1024")
+        print(f"dw: 16 applications (register then staged kernels; FP64 D, D^dagger, FP32 D, D^dagger; 2 each) on "
+              f"{N}x{N}")
         s.close()
         return 0
     if name == "krylov":

@@ -28,6 +28,11 @@ struct Geom {
 template <typename V>
 void launch_wilson(cudaStream_t s, const V* U, const V* in, V* out, const V* b, int Nx, int Nt, double m0,
                    int dagger, int nrhs);
+// D_W kernel choice (process-wide): 0 default, 1 register kernels, 2 staged tiles (bulk copies into
+// shared memory); the staged kernel's bounded-wait status word (1: a copy never arrived)
+void set_stencil_variant(int v);
+int stencil_variant();
+int stencil_status_read();
 void launch_link_derivative(cudaStream_t s, const double2* U, const double2* psi, const double2* lam, double* out,
                             int Nx, int Nt);
 void launch_metropolis_init(cudaStream_t s, double* th, int Nx, int Nt, uint64_t seed);
@@ -176,9 +181,10 @@ enum FgCtl {
     kFgK = 1,            // restart
     kFgNan = 2,          // a NaN or Inf was met (reported by the host after the solve)
     kFgRunsOuter = 3,    // restart bodies run (cumulative)
-    kFgRunsInner = 4,    // Arnoldi-step bodies run (cumulative)
-    kFgRunsFirst = 5,    // K-cycle preconditioner bodies from zero (cumulative)
-    kFgRunsLater = 6,    // K-cycle preconditioner bodies from the previous Z_j (cumulative)
+    kFgRunsInner = 4,    // Arnoldi-step bodies run (cumulative; for K-cycles those of restart 0)
+    kFgRunsFirst = 5,    // K-cycle restarts whose preconditioner starts from zero (restart 0)
+    kFgRunsLater = 6,    // K-cycle restarts whose preconditioner starts from the previous Z_j
+    kFgRunsInnerLater = 7,  // K-cycle Arnoldi-step bodies of restarts after the first
     kFgCtlWords = 8
 };
 struct FgDev {
@@ -192,13 +198,15 @@ struct FgDev {
     int* ctl = nullptr;  // kFgCtlWords
 };
 void launch_fg_start(cudaStream_t s, const FgDev& f, int R, int m, int restarts, cudaGraphConditionalHandle hc);
-void launch_fg_restart(cudaStream_t s, const FgDev& f, int R, int m, cudaGraphConditionalHandle hc);
-void launch_fg_arnoldi(cudaStream_t s, const FgDev& f, int R, int m, double tol, cudaGraphConditionalHandle hc);
+// hc_sel (if select): condition of the if/else node that picks the restart-0 loop (k == 0) or the later one
+void launch_fg_restart(cudaStream_t s, const FgDev& f, int R, int m, cudaGraphConditionalHandle hc0,
+                       cudaGraphConditionalHandle hc1, cudaGraphConditionalHandle hc_sel, int select);
+// counter: the FgCtl run counter of the body this step belongs to
+void launch_fg_arnoldi(cudaStream_t s, const FgDev& f, int R, int m, double tol, cudaGraphConditionalHandle hc,
+                       int counter);
 void launch_fg_backsub(cudaStream_t s, const FgDev& f, int R, int m);
 void launch_fg_restart_end(cudaStream_t s, const FgDev& f, int R, int m, int restarts, double tol,
                            cudaGraphConditionalHandle hc);
-void launch_fg_select(cudaStream_t s, const FgDev& f, cudaGraphConditionalHandle first,
-                      cudaGraphConditionalHandle later);
 // multi-dot / multi-axpy over basis vectors 0..j with j = *jdev; results and coefficients at
 // [r*ldk + i]; kmax bounds k = j + 1
 template <typename V>

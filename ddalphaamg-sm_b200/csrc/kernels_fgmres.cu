@@ -39,9 +39,12 @@ __global__ void __launch_bounds__(kFgThreads) fg_start_kernel(FgDev f, int R, in
     }
 }
 
-// top of a restart: V_0 = r / ||r|| for the right-hand sides still running (alpha), g = (||r||, 0, ...)
-__global__ void __launch_bounds__(kFgThreads) fg_restart_kernel(FgDev f, int R, int m,
-                                                                cudaGraphConditionalHandle hc_inner) {
+// top of a restart: V_0 = r / ||r|| for the right-hand sides still running (alpha), g = (||r||, 0, ...);
+// with select, the K-cycle's if/else node runs the loop of restart 0 (preconditioner from zero) or the
+// loop of later restarts (from the previous Z_j, src/amg.cpp:43-45)
+__global__ void __launch_bounds__(kFgThreads) fg_restart_kernel(FgDev f, int R, int m, cudaGraphConditionalHandle hc0,
+                                                                cudaGraphConditionalHandle hc1,
+                                                                cudaGraphConditionalHandle hc_sel, int select) {
     bool active = false;
     for (int r = threadIdx.x; r < R; r += blockDim.x) {
         const int run = !f.done[r];
@@ -54,7 +57,13 @@ __global__ void __launch_bounds__(kFgThreads) fg_restart_kernel(FgDev f, int R, 
     if (threadIdx.x == 0) {
         f.ctl[kFgJ] = 0;
         f.ctl[kFgRunsOuter]++;
-        cudaGraphSetConditional(hc_inner, any ? 1u : 0u);
+        cudaGraphSetConditional(hc0, any ? 1u : 0u);
+        if (select) {
+            const bool first = f.ctl[kFgK] == 0;
+            cudaGraphSetConditional(hc1, any ? 1u : 0u);
+            cudaGraphSetConditional(hc_sel, first ? 1u : 0u);
+            f.ctl[first ? kFgRunsFirst : kFgRunsLater]++;
+        }
     }
 }
 
@@ -62,7 +71,7 @@ __global__ void __launch_bounds__(kFgThreads) fg_restart_kernel(FgDev f, int R, 
 // ||w||, the previous rotations, a new rotation, the residual estimate |g_{j+1}| and the scale of
 // V_{j+1} (src/fgmres.cpp:35-70, FGMRES::rotation src/fgmres.cpp:99-115)
 __global__ void __launch_bounds__(kFgThreads) fg_arnoldi_kernel(FgDev f, int R, int m, double tol,
-                                                                cudaGraphConditionalHandle hc_inner) {
+                                                                cudaGraphConditionalHandle hc_inner, int counter) {
     const int j = f.ctl[kFgJ];
     bool active = false;
     for (int r = threadIdx.x; r < R; r += blockDim.x) {
@@ -108,7 +117,7 @@ __global__ void __launch_bounds__(kFgThreads) fg_arnoldi_kernel(FgDev f, int R, 
     const bool any = __syncthreads_or(active);
     if (threadIdx.x == 0) {
         f.ctl[kFgJ] = j + 1;
-        f.ctl[kFgRunsInner]++;
+        f.ctl[counter]++;
         cudaGraphSetConditional(hc_inner, (any && j + 1 < m) ? 1u : 0u);
     }
 }
@@ -155,15 +164,6 @@ __global__ void __launch_bounds__(kFgThreads) fg_restart_end_kernel(FgDev f, int
         f.ctl[kFgK] = k + 1;
         cudaGraphSetConditional(hc_outer, (any && k + 1 < restarts) ? 1u : 0u);
     }
-}
-
-// the K-cycle preconditioner of restart 0 starts from zero, later ones from the previous Z_j
-// (src/amg.cpp:43-45): selects one of the two captured variants
-__global__ void fg_select_kernel(FgDev f, cudaGraphConditionalHandle hc_first, cudaGraphConditionalHandle hc_later) {
-    const bool first = f.ctl[kFgK] == 0;
-    cudaGraphSetConditional(hc_first, first ? 1u : 0u);
-    cudaGraphSetConditional(hc_later, first ? 0u : 1u);
-    f.ctl[first ? kFgRunsFirst : kFgRunsLater]++;
 }
 
 // ---------------------------------------------------------------- basis kernels indexed on the device
@@ -285,11 +285,13 @@ void launch_slot_copy(cudaStream_t s, const A* src, B* dst, long slot, const int
 void launch_fg_start(cudaStream_t s, const FgDev& f, int R, int m, int restarts, cudaGraphConditionalHandle hc) {
     DDAMG_LAUNCH(fg_start_kernel, 1, kFgThreads, 0, s, f, R, m, restarts, hc);
 }
-void launch_fg_restart(cudaStream_t s, const FgDev& f, int R, int m, cudaGraphConditionalHandle hc) {
-    DDAMG_LAUNCH(fg_restart_kernel, 1, kFgThreads, 0, s, f, R, m, hc);
+void launch_fg_restart(cudaStream_t s, const FgDev& f, int R, int m, cudaGraphConditionalHandle hc0,
+                       cudaGraphConditionalHandle hc1, cudaGraphConditionalHandle hc_sel, int select) {
+    DDAMG_LAUNCH(fg_restart_kernel, 1, kFgThreads, 0, s, f, R, m, hc0, hc1, hc_sel, select);
 }
-void launch_fg_arnoldi(cudaStream_t s, const FgDev& f, int R, int m, double tol, cudaGraphConditionalHandle hc) {
-    DDAMG_LAUNCH(fg_arnoldi_kernel, 1, kFgThreads, 0, s, f, R, m, tol, hc);
+void launch_fg_arnoldi(cudaStream_t s, const FgDev& f, int R, int m, double tol, cudaGraphConditionalHandle hc,
+                       int counter) {
+    DDAMG_LAUNCH(fg_arnoldi_kernel, 1, kFgThreads, 0, s, f, R, m, tol, hc, counter);
 }
 void launch_fg_backsub(cudaStream_t s, const FgDev& f, int R, int m) {
     DDAMG_LAUNCH(fg_backsub_kernel, 1, kFgThreads, 0, s, f, R, m);
@@ -298,11 +300,6 @@ void launch_fg_restart_end(cudaStream_t s, const FgDev& f, int R, int m, int res
                            cudaGraphConditionalHandle hc) {
     DDAMG_LAUNCH(fg_restart_end_kernel, 1, kFgThreads, 0, s, f, R, m, restarts, tol, hc);
 }
-void launch_fg_select(cudaStream_t s, const FgDev& f, cudaGraphConditionalHandle first,
-                      cudaGraphConditionalHandle later) {
-    DDAMG_LAUNCH(fg_select_kernel, 1, 1, 0, s, f, first, later);
-}
-
 #define DDAMG_FG_INST(V)                                                                                      \
     template void launch_multidot_dev<V>(cudaStream_t, const V*, long, long, int, const int*, int, const V*,  \
                                          long, long, int, double2*, double2*);                                \

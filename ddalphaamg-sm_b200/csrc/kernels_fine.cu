@@ -1,6 +1,9 @@
 // Fine-level kernels: Wilson-Dirac stencil D_W / D_W^dagger on U(1) links, the link
 // derivative of L = Re(eta^dagger D^-1 b), the U(1) Metropolis generator and field fills.
+#include <atomic>
+
 #include "internal.h"
+#include "tc_sm100.cuh"
 
 namespace ddamg {
 
@@ -176,10 +179,213 @@ __global__ void __launch_bounds__(256) wilson_pair_kernel(const float2* __restri
     st8f(out + 2 * n0, oa0, oa1, ob0, ob1);
 }
 
+// D_W with staged tiles: a persistent CTA walks over tiles of TX x-rows by TT t-sites (and right-hand
+// sides), and for each tile one thread brings the tile's psi with its one-site halo and the links it
+// needs into shared memory with 1-D bulk asynchronous copies (TMA, cp.async.bulk; one copy per row
+// segment, the periodic wrap as separate one-site copies), two stages deep, completion counted on an
+// mbarrier.  The 256 threads then read every operand from shared memory: each psi value crosses L2
+// once per tile instead of five times.  Same arithmetic as wilson_kernel.
+constexpr int kStageThreads = 256;
+template <typename V> struct SiteStore;
+template <> struct SiteStore<double2> {
+    static __device__ __forceinline__ void ld(const double2* p, double2& a, double2& b) { ld2w(p, a, b); }
+    static __device__ __forceinline__ void st(double2* p, double2 a, double2 b) { st2w(p, a, b); }
+};
+template <> struct SiteStore<float2> {
+    static __device__ __forceinline__ void ld(const float2* p, float2& a, float2& b) { ld2(p, a, b); }
+    static __device__ __forceinline__ void st(float2* p, float2 a, float2 b) { st2(p, a, b); }
+};
+template <typename V, int TX, int TT>
+struct StageGeom {
+    static constexpr int S = 2 * sizeof(V);  // bytes per site: two complex numbers (psi spins, or U_0 U_1)
+    static constexpr int psi_bytes = (TX + 2) * (TT + 2) * S;
+    static constexpr int u_bytes = (TX + 1) * (TT + 1) * S;
+    static constexpr int stage_bytes = ((psi_bytes + u_bytes) + 127) / 128 * 128;
+    static constexpr int smem = 128 + 2 * stage_bytes;
+};
+// one thread: the copies of tile `tile` into the stage at `dst`, counted on *bar
+template <typename V, int TX, int TT>
+__device__ __forceinline__ void stage_issue(const V* U, const V* in, long stride, int Nx, int Nt, int R, int tile,
+                                            unsigned char* dst, uint64_t* bar) {
+    typedef StageGeom<V, TX, TT> G;
+    const int r = tile % R, tt = (tile / R) % (Nt / TT), tx = tile / R / (Nt / TT);
+    const int x0 = tx * TX, t0 = tt * TT;
+    tc::mbar_arrive_expect_tx(bar, G::psi_bytes + G::u_bytes);
+    const unsigned char* pin = reinterpret_cast<const unsigned char*>(in + r * stride);
+    const unsigned char* pu = reinterpret_cast<const unsigned char*>(U);
+    const long row = (long)Nt * G::S;
+    const int tl = t0 == 0 ? Nt - 1 : t0 - 1, tr = t0 + TT == Nt ? 0 : t0 + TT;
+    for (int i = 0; i < TX + 2; i++) {  // psi rows x0 - 1 .. x0 + TX, sites t0 - 1 .. t0 + TT
+        int x = x0 - 1 + i;
+        x = x < 0 ? x + Nx : (x >= Nx ? x - Nx : x);
+        const unsigned char* src = pin + x * row;
+        unsigned char* d = dst + i * (TT + 2) * G::S;
+        if (t0 > 0 && t0 + TT < Nt) {
+            tc::bulk_g2s(d, src + (long)(t0 - 1) * G::S, (TT + 2) * G::S, bar);
+        } else {
+            tc::bulk_g2s(d, src + (long)tl * G::S, G::S, bar);
+            tc::bulk_g2s(d + G::S, src + (long)t0 * G::S, TT * G::S, bar);
+            tc::bulk_g2s(d + (TT + 1) * G::S, src + (long)tr * G::S, G::S, bar);
+        }
+    }
+    unsigned char* du = dst + G::psi_bytes;
+    for (int i = 0; i < TX + 1; i++) {  // link rows x0 - 1 .. x0 + TX - 1, sites t0 - 1 .. t0 + TT - 1
+        int x = x0 - 1 + i;
+        x = x < 0 ? x + Nx : x;
+        const unsigned char* src = pu + x * row;
+        unsigned char* d = du + i * (TT + 1) * G::S;
+        if (t0 > 0) {
+            tc::bulk_g2s(d, src + (long)(t0 - 1) * G::S, (TT + 1) * G::S, bar);
+        } else {
+            tc::bulk_g2s(d, src + (long)tl * G::S, G::S, bar);
+            tc::bulk_g2s(d + G::S, src + (long)t0 * G::S, TT * G::S, bar);
+        }
+    }
+}
+template <typename V, bool DAG, bool RESID, int TX, int TT>
+__global__ void __launch_bounds__(kStageThreads) wilson_stage_kernel(const V* __restrict__ U, const V* __restrict__ in,
+                                                                     V* __restrict__ out, const V* __restrict__ b,
+                                                                     int Nx, int Nt, typename RealOf<V>::R m0,
+                                                                     long stride, int R, int* status) {
+    typedef typename RealOf<V>::R Rl;
+    typedef StageGeom<V, TX, TT> G;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+    unsigned char* stage = smem + 128;
+    const int ntiles = (Nx / TX) * (Nt / TT) * R;
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&full[0], 1);
+        tc::mbar_init(&full[1], 1);
+        tc::mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < 2; q++) {
+            const int tile = blockIdx.x + q * gridDim.x;
+            if (tile < ntiles)
+                stage_issue<V, TX, TT>(U, in, stride, Nx, Nt, R, tile, stage + q * G::stage_bytes, &full[q]);
+        }
+    }
+    const Rl mm = m0 + Rl(2), h = Rl(0.5);
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+        const int st = it & 1;
+        const bool ok = tc::mbar_wait(&full[st], (it >> 1) & 1, status);
+        if (__syncthreads_or(!ok)) break;  // a copy never arrived: the status word says so
+        const V* P = reinterpret_cast<const V*>(stage + st * G::stage_bytes);
+        const V* Us = reinterpret_cast<const V*>(stage + st * G::stage_bytes + G::psi_bytes);
+        const int r = tile % R, tt = (tile / R) % (Nt / TT), tx = tile / R / (Nt / TT);
+        const int x0 = tx * TX, t0 = tt * TT;
+        for (int q = threadIdx.x; q < TX * TT; q += kStageThreads) {
+            const int i = q / TT, t = q - i * TT;
+            const V* own = P + 2 * ((i + 1) * (TT + 2) + t + 1);
+            const V p0 = own[0], p1 = own[1];
+            const V a0 = own[2], a1 = own[3];                                     // +t
+            const V e0 = own[-2], e1 = own[-1];                                   // -t
+            const V c0 = own[2 * (TT + 2)], c1 = own[2 * (TT + 2) + 1];           // +x
+            const V g0 = own[-2 * (TT + 2)], g1 = own[-2 * (TT + 2) + 1];         // -x
+            const V* uo = Us + 2 * ((i + 1) * (TT + 1) + t + 1);
+            const V u0 = uo[0], u1 = uo[1];
+            const V ul0 = uo[-2];                                                 // U_0(x, t - 1)
+            const V ul1 = uo[-2 * (TT + 1) + 1];                                  // U_1(x - 1, t)
+            const int tg = t0 + t;
+            const Rl sr = (tg == Nt - 1) ? Rl(-1) : Rl(1), sl = (tg == 0) ? Rl(-1) : Rl(1);
+            V s0, s1;
+            if (!DAG) {
+                V a = sr * cmul(u0, a0 - a1);
+                V c = cmul(u1, c0 + imul(c1));
+                V e = sl * cmulc(ul0, e0 + e1);
+                V g = cmulc(ul1, g0 - imul(g1));
+                s0 = a + c + e + g;
+                s1 = -a - imul(c) + e + imul(g);
+            } else {
+                V a = sl * cmulc(ul0, e0 - e1);
+                V c = cmulc(ul1, g0 + imul(g1));
+                V e = sr * cmul(u0, a0 + a1);
+                V g = cmul(u1, c0 - imul(c1));
+                s0 = a + c + e + g;
+                s1 = -a - imul(c) + e + imul(g);
+            }
+            V o0 = mm * p0 - h * s0;
+            V o1 = mm * p1 - h * s1;
+            const long site = (long)(x0 + i) * Nt + tg;
+            if (RESID) {
+                V b0, b1;
+                SiteStore<V>::ld(b + r * stride + 2 * site, b0, b1);
+                o0 = b0 - o0;
+                o1 = b1 - o1;
+            }
+            SiteStore<V>::st(out + r * stride + 2 * site, o0, o1);
+        }
+        __syncthreads();  // every thread is done with this stage
+        if (threadIdx.x == 0 && tile + 2 * gridDim.x < ntiles)
+            stage_issue<V, TX, TT>(U, in, stride, Nx, Nt, R, tile + 2 * gridDim.x, stage + st * G::stage_bytes,
+                                   &full[st]);
+    }
+}
+
+// which D_W kernel launch_wilson uses: 0 the default, 1 the register kernels (wilson_kernel /
+// wilson_pair_kernel), 2 the staged-tile kernel where the lattice divides into its tiles
+static std::atomic<int> g_stencil_variant{0};
+static int* stencil_status();
+void set_stencil_variant(int v) {
+    stencil_status();  // allocated here, outside any stream capture
+    g_stencil_variant = v;
+}
+int stencil_variant() { return g_stencil_variant; }
+static int* stencil_status() {  // bounded-wait status word of the staged kernel, one per device
+    static int* p[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!p[dev]) {
+        DDAMG_CUDA_TRY(cudaMalloc(&p[dev], sizeof(int)));
+        DDAMG_CUDA_TRY(cudaMemset(p[dev], 0, sizeof(int)));
+    }
+    return p[dev];
+}
+int stencil_status_read() {
+    int v = 0;
+    DDAMG_CUDA_TRY(cudaMemcpy(&v, stencil_status(), sizeof(int), cudaMemcpyDeviceToHost));
+    return v;
+}
+template <typename V, int TX, int TT>
+static bool launch_wilson_staged(cudaStream_t s, const V* U, const V* in, V* out, const V* b, int Nx, int Nt,
+                                 double m0, int dagger, int nrhs) {
+    typedef typename RealOf<V>::R R;
+    typedef StageGeom<V, TX, TT> G;
+    auto a = [](const void* p, int al) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) % al) == 0; };
+    const int al = sizeof(V) == 16 ? 32 : 16;  // the site stores and loads of the epilogue
+    if (Nx % TX || Nt % TT || Nx < 2 || !a(U, al) || !a(in, al) || !a(out, al) || !a(b, al)) return false;
+    static int ctas_per_sm[2][2][2] = {};
+    static int sms = 0;
+    if (!sms) DDAMG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
+    const long stride = 2L * Nx * Nt;
+    const int ntiles = (Nx / TX) * (Nt / TT) * nrhs;
+    int* status = stencil_status();
+    auto go = [&](auto kern, int& cps) {
+        if (!cps) {
+            DDAMG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::smem));
+            DDAMG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cps, kern, kStageThreads, G::smem));
+            if (cps < 1) cps = 1;
+        }
+        const int grid = (int)std::min<long>(ntiles, (long)sms * cps);
+        DDAMG_LAUNCH(kern, grid, kStageThreads, G::smem, s, U, in, out, b, Nx, Nt, (R)m0, stride, nrhs, status);
+    };
+    if (dagger) {
+        if (b) go(wilson_stage_kernel<V, true, true, TX, TT>, ctas_per_sm[1][1][sizeof(V) == 16]);
+        else go(wilson_stage_kernel<V, true, false, TX, TT>, ctas_per_sm[1][0][sizeof(V) == 16]);
+    } else {
+        if (b) go(wilson_stage_kernel<V, false, true, TX, TT>, ctas_per_sm[0][1][sizeof(V) == 16]);
+        else go(wilson_stage_kernel<V, false, false, TX, TT>, ctas_per_sm[0][0][sizeof(V) == 16]);
+    }
+    return true;
+}
+
 template <typename V>
 void launch_wilson(cudaStream_t s, const V* U, const V* in, V* out, const V* b, int Nx, int Nt, double m0,
                    int dagger, int nrhs) {
     typedef typename RealOf<V>::R R;
+    if (g_stencil_variant == 2 && launch_wilson_staged<V, 8, 64>(s, U, in, out, b, Nx, Nt, m0, dagger, nrhs)) return;
     dim3 grid(ceil_div((long)Nx * Nt, 256), nrhs);
     long stride = 2L * Nx * Nt;
     // FP64 sites are 32 bytes: one 256-bit access per site when every field starts on a 32-byte

@@ -807,28 +807,34 @@ static cudaGraphConditionalHandle cap_handle(ddamg_handle* h) {
     DDAMG_CUDA_TRY(cudaGraphConditionalHandleCreate(&hc, h->cap_top, 0, 0));
     return hc;
 }
-// ends the current segment, adds a conditional node (while or if) after it and records `body` into the
-// node's graph as a new body of (level, kind); the capture resumes after the node
+// ends the current segment, adds a conditional node after it (a while node, an if node, or with two
+// bodies an if/else node) and records each body into its graph as a new body of (level, kind); the
+// capture resumes after the node
 static void cap_conditional(ddamg_handle* h, cudaGraphConditionalHandle hc, cudaGraphConditionalNodeType type,
-                            int level, int kind, const std::function<void()>& body) {
+                            int level, const std::vector<std::pair<int, std::function<void()>>>& bodies) {
     const int cur = h->cap_cur;
     CapPoint p = cap_pause(h);
     cudaGraphNodeParams np{};
     np.type = cudaGraphNodeTypeConditional;
     np.conditional.handle = hc;
     np.conditional.type = type;
-    np.conditional.size = 1;
+    np.conditional.size = (unsigned)bodies.size();
     cudaGraphNode_t node;
     DDAMG_CUDA_TRY(cudaGraphAddNode(&node, p.graph, p.deps.empty() ? nullptr : p.deps.data(), p.deps.size(), &np));
-    cap_begin(h, np.conditional.phGraph_out[0], {}, cap_new_body(h, level, kind));
-    body();
-    cap_pause(h);
+    for (size_t k = 0; k < bodies.size(); k++) {
+        cap_begin(h, np.conditional.phGraph_out[k], {}, cap_new_body(h, level, bodies[k].first));
+        bodies[k].second();
+        cap_pause(h);
+    }
     cap_begin(h, p.graph, {node}, cur);
 }
 
 // FGMRES::fgmres as fgmres_host computes it, recorded into the graph under construction.  M(in, out, R,
 // first): out = M in with in and out fixed buffers; first = restart 0 (the K-cycle starts from zero
-// there and from the previous Z_j after a restart), `select` says whether the two differ.
+// there and from the previous Z_j after a restart), `select` says whether the two differ.  With select
+// each restart picks one of two recorded Arnoldi loops through an if/else node (one conditional
+// evaluation per restart instead of one per step: an if node costs about 6.5 us on the device, a
+// while iteration about 3.5 us).
 template <typename V>
 static void fgmres_dev(ddamg_handle* h, int lvl, long n, int R, int m, int restarts, double tol,
                        const std::function<void(const V*, V*, int)>& A,
@@ -848,43 +854,58 @@ static void fgmres_dev(ddamg_handle* h, int lvl, long n, int R, int m, int resta
     }
     launch_norm2<V>(s, b, n, n, R, h->dpart, f.nrm);
     launch_norm2<V>(s, K.r, n, n, R, h->dpart, f.nrm + R);
-    const cudaGraphConditionalHandle hc_outer = cap_handle(h), hc_inner = cap_handle(h);
+    const cudaGraphConditionalHandle hc_outer = cap_handle(h), hc_in0 = cap_handle(h);
+    cudaGraphConditionalHandle hc_in1{}, hc_sel{};
+    if (select) {
+        hc_in1 = cap_handle(h);
+        hc_sel = cap_handle(h);
+    }
+    // one Arnoldi step; `later`: a K-cycle restart after the first, whose preconditioner starts from the
+    // previous restart's Z_j
+    auto step = [&](bool later, cudaGraphConditionalHandle hc, int counter) {
+        launch_slot_copy<V, V>(s, K.Vb, vin, Rn, jdev, 0, Rn);
+        if (later) launch_slot_copy<V, V>(s, K.Z, zf, Rn, jdev, 0, Rn);
+        M(vin, zf, R, !later);
+        launch_slot_copy<V, V>(s, zf, K.Z, Rn, jdev, 1, Rn);
+        A(zf, K.w, R);
+        double2* d1 = f.dots;
+        double2* d2 = f.dots + (long)R * (m + 1);
+        launch_multidot_dev<V>(s, K.Vb, Rn, n, m, jdev, m + 1, K.w, n, n, R, h->dpart, d1);
+        launch_multiaxpy_dev<V>(s, K.Vb, Rn, n, jdev, d1, m + 1, K.w, n, n, R);
+        launch_multidot_dev<V>(s, K.Vb, Rn, n, m, jdev, m + 1, K.w, n, n, R, h->dpart, d2);
+        launch_multiaxpy_dev<V>(s, K.Vb, Rn, n, jdev, d2, m + 1, K.w, n, n, R);
+        launch_norm2<V>(s, K.w, n, n, R, h->dpart, f.nrm);
+        launch_fg_arnoldi(s, f, R, m, tol, hc, counter);
+        launch_scale_slot<V>(s, f.alpha, K.w, K.Vb, Rn, jdev, n, R);  // V_{j+1}
+    };
     launch_fg_start(s, f, R, m, restarts, hc_outer);
-    cap_conditional(h, hc_outer, cudaGraphCondTypeWhile, lvl, kFgRunsOuter, [&]() {
-        launch_fg_restart(s, f, R, m, hc_inner);
+    cap_conditional(h, hc_outer, cudaGraphCondTypeWhile, lvl, {{kFgRunsOuter, [&]() {
+        launch_fg_restart(s, f, R, m, hc_in0, hc_in1, hc_sel, select ? 1 : 0);
         launch_scale<V>(s, f.alpha, K.r, K.Vb, n, R);  // V_0 = r / beta
-        cap_conditional(h, hc_inner, cudaGraphCondTypeWhile, lvl, kFgRunsInner, [&]() {
-            launch_slot_copy<V, V>(s, K.Vb, vin, Rn, jdev, 0, Rn);
-            if (!select) {
-                M(vin, zf, R, false);
-            } else {
-                const cudaGraphConditionalHandle hf = cap_handle(h), hl = cap_handle(h);
-                launch_fg_select(s, f, hf, hl);
-                cap_conditional(h, hf, cudaGraphCondTypeIf, lvl, kFgRunsFirst, [&]() { M(vin, zf, R, true); });
-                cap_conditional(h, hl, cudaGraphCondTypeIf, lvl, kFgRunsLater, [&]() {
-                    launch_slot_copy<V, V>(s, K.Z, zf, Rn, jdev, 0, Rn);
-                    M(vin, zf, R, false);
-                });
-            }
-            launch_slot_copy<V, V>(s, zf, K.Z, Rn, jdev, 1, Rn);
-            A(zf, K.w, R);
-            double2* d1 = f.dots;
-            double2* d2 = f.dots + (long)R * (m + 1);
-            launch_multidot_dev<V>(s, K.Vb, Rn, n, m, jdev, m + 1, K.w, n, n, R, h->dpart, d1);
-            launch_multiaxpy_dev<V>(s, K.Vb, Rn, n, jdev, d1, m + 1, K.w, n, n, R);
-            launch_multidot_dev<V>(s, K.Vb, Rn, n, m, jdev, m + 1, K.w, n, n, R, h->dpart, d2);
-            launch_multiaxpy_dev<V>(s, K.Vb, Rn, n, jdev, d2, m + 1, K.w, n, n, R);
-            launch_norm2<V>(s, K.w, n, n, R, h->dpart, f.nrm);
-            launch_fg_arnoldi(s, f, R, m, tol, hc_inner);
-            launch_scale_slot<V>(s, f.alpha, K.w, K.Vb, Rn, jdev, n, R);  // V_{j+1}
-        });
+        if (!select) {
+            cap_conditional(h, hc_in0, cudaGraphCondTypeWhile, lvl,
+                            {{kFgRunsInner, [&]() { step(false, hc_in0, kFgRunsInner); }}});
+        } else {
+            // the restart's loop is chosen once per restart, not per step: an if/else node over two loops
+            cap_conditional(h, hc_sel, cudaGraphCondTypeIf, lvl,
+                            {{kFgRunsFirst,
+                              [&]() {
+                                  cap_conditional(h, hc_in0, cudaGraphCondTypeWhile, lvl,
+                                                  {{kFgRunsInner, [&]() { step(false, hc_in0, kFgRunsInner); }}});
+                              }},
+                             {kFgRunsLater, [&]() {
+                                  cap_conditional(
+                                      h, hc_in1, cudaGraphCondTypeWhile, lvl,
+                                      {{kFgRunsInnerLater, [&]() { step(true, hc_in1, kFgRunsInnerLater); }}});
+                              }}});
+        }
         launch_fg_backsub(s, f, R, m);
         launch_multiaxpy<V>(s, K.Z, Rn, n, m, f.coef, x, n, n, R, +1.0);
         A(x, K.w, R);
         launch_sub<V>(s, b, K.w, K.r, Rn);
         launch_norm2<V>(s, K.r, n, n, R, h->dpart, f.nrm);
         launch_fg_restart_end(s, f, R, m, restarts, tol, hc_outer);
-    });
+    }}});
 }
 
 // ------------------------------------------------------------------ cycles
@@ -1223,7 +1244,8 @@ static bool solve_graph(ddamg_handle* h, int R, const std::function<void(const d
             cap_begin(h, top, {}, cap_new_body(h, 0, 0));
             for (int l = 0; l < h->L; l++)
                 if (h->lv[l].fg.ctl)
-                    DDAMG_CUDA_TRY(cudaMemsetAsync(h->lv[l].fg.ctl + kFgRunsOuter, 0, 4 * sizeof(int), h->s));
+                    DDAMG_CUDA_TRY(cudaMemsetAsync(h->lv[l].fg.ctl + kFgRunsOuter, 0,
+                                               (kFgCtlWords - kFgRunsOuter) * sizeof(int), h->s));
             fgmres_dev<double2>(h, 0, n, R, p.fgmres_restart_length, p.fgmres_restarts, p.fgmres_tolerance, A, M,
                                 false, h->ob, nullptr, true, h->ox, K, h->ovin, h->ozf);
             cap_pause(h);
@@ -1241,6 +1263,7 @@ static bool solve_graph(ddamg_handle* h, int R, const std::function<void(const d
         h->cap_top = nullptr;
     }
     if (ok && cudaGraphInstantiate(&sg.exec, top, 0) != cudaSuccess) ok = false;
+    if (ok && cudaGraphUpload(sg.exec, h->s) != cudaSuccess) ok = false;
     if (top) cudaGraphDestroy(top);
     g_launches = l0;  // recorded, not run
     if (!ok) {
@@ -1257,9 +1280,9 @@ static bool solve_graph(ddamg_handle* h, int R, const std::function<void(const d
     h->solve_graphs[R] = sg;
     return true;
 }
-static void run_solve_graph(ddamg_handle* h, int R, std::vector<int>& it, std::vector<double>& rel) {
+// after the solve graph's launch: its per-rhs results and the bodies' run counters (launch count)
+static void read_solve_graph(ddamg_handle* h, int R, std::vector<int>& it, std::vector<double>& rel) {
     const ddamg_handle::SolveGraph& sg = h->solve_graphs.at(R);
-    DDAMG_CUDA_TRY(cudaGraphLaunch(sg.exec, h->s));
     std::vector<std::array<int, kFgCtlWords>> ctl(h->L);
     for (int l = 0; l < h->L; l++)
         if (h->lv[l].fg.ctl)
@@ -1288,7 +1311,6 @@ static ddamg_status solve_device(ddamg_handle* h, const double2* b, double2* x, 
     const ddamg_params& p = h->p;
     const long n = h->lv[0].g.size();
     const Geom& g0 = h->lv[0].g;
-    DDAMG_CUDA_TRY(cudaEventRecord(h->ev0, h->s));
     std::function<void(const double2*, double2*, int)> A = [h, &g0](const double2* in, double2* out, int R) {
         launch_wilson<double2>(h->s, h->lv[0].d.U, in, out, nullptr, g0.Nx, g0.Nt, h->p.m0, 0, R);
     };
@@ -1299,27 +1321,29 @@ static ddamg_status solve_device(ddamg_handle* h, const double2* b, double2* x, 
     std::vector<int> it(nrhs);
     std::vector<double> rel(nrhs);
     const bool graph = p.cuda_graphs && !h->prof && !h->solve_graphs_off;
-    if (graph && h->solve_warm.count(nrhs)) {
+    bool use_graph = false;
+    if (graph && h->solve_warm.count(nrhs)) {  // built (host work, once per width) before the timed region
         std::function<void(const double2*, double2*, int, bool)> Md = [h](const double2* in, double2* out, int R,
                                                                           bool) { outer_prec(h, in, out, R); };
-        if (solve_graph(h, nrhs, A, Md, K)) {
-            if (b != h->ob)
-                DDAMG_CUDA_TRY(cudaMemcpyAsync(h->ob, b, sizeof(double2) * n * nrhs, cudaMemcpyDeviceToDevice, h->s));
-            run_solve_graph(h, nrhs, it, rel);
-            if (x != h->ox)
-                DDAMG_CUDA_TRY(cudaMemcpyAsync(x, h->ox, sizeof(double2) * n * nrhs, cudaMemcpyDeviceToDevice, h->s));
-        } else {
-            fgmres_host<double2>(h, n, nrhs, p.fgmres_restart_length, p.fgmres_restarts, p.fgmres_tolerance, A, &M, b,
-                                 nullptr, true, x, K, it.data(), rel.data());
-        }
+        use_graph = solve_graph(h, nrhs, A, Md, K);
+    }
+    DDAMG_CUDA_TRY(cudaEventRecord(h->ev0, h->s));
+    if (use_graph) {
+        if (b != h->ob)
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(h->ob, b, sizeof(double2) * n * nrhs, cudaMemcpyDeviceToDevice, h->s));
+        DDAMG_CUDA_TRY(cudaGraphLaunch(h->solve_graphs.at(nrhs).exec, h->s));
+        if (x != h->ox)
+            DDAMG_CUDA_TRY(cudaMemcpyAsync(x, h->ox, sizeof(double2) * n * nrhs, cudaMemcpyDeviceToDevice, h->s));
+        DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, h->s));
+        read_solve_graph(h, nrhs, it, rel);
     } else {
         fgmres_host<double2>(h, n, nrhs, p.fgmres_restart_length, p.fgmres_restarts, p.fgmres_tolerance, A, &M, b,
                              nullptr, true, x, K, it.data(), rel.data());
         if (graph) h->solve_warm.insert(nrhs);
+        DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, h->s));
     }
     check_coarse_status(h, nullptr);
     check_tc_status(h);
-    DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, h->s));
     sync(h);
     float ms = 0;
     DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
@@ -2100,6 +2124,21 @@ static void write_metadata(const ddamg_params& p, const long long* c, int cycle,
     if (!f) throw IoFailure{"write failed: " + file};
 }
 }  // namespace ddamg
+
+ddamg_status ddamg_set_stencil_kernel(int kind) {
+    API_BEGIN
+    if (kind < 0 || kind > 2) throw ParamFailure{"stencil kernel must be 0 (default), 1 (register) or 2 (staged)"};
+    set_stencil_variant(kind);
+    API_END
+}
+ddamg_status ddamg_get_stencil_kernel(int* kind) {
+    if (!kind) {
+        set_error("null argument");
+        return DDAMG_ERR_BAD_PARAM;
+    }
+    *kind = stencil_variant();
+    return DDAMG_OK;
+}
 
 ddamg_status ddamg_get_counters(ddamg_t* h, long long counts[DDAMG_COUNT_KINDS]) {
     if (!h || !counts) {

@@ -93,6 +93,18 @@ def gaussian_field(n, seed):
 COUNTER_NAMES = ("CG", "BiCG", "GMRES", "SAP", "FGMRES_SAP", "vCycle", "kCycle")
 
 
+def set_stencil_kernel(kind):
+    """D_W kernel choice, process-wide: 0 default, 1 register kernels, 2 staged tiles (bulk copies into
+    shared memory)."""
+    check(_lib.load().ddamg_set_stencil_kernel(int(kind)))
+
+
+def stencil_kernel():
+    k = ctypes.c_int(0)
+    check(_lib.load().ddamg_get_stencil_kernel(ctypes.byref(k)))
+    return k.value
+
+
 def write_metadata(params, counts, cycle, tol, path=None):
     """writeMetadata (src/io.cpp:72-145) from parameters and counters alone (host only, no device)."""
     c = (ctypes.c_longlong * 7)(*[int(v) for v in counts])

@@ -81,6 +81,8 @@ SIGNATURES = {
                                          ctypes.POINTER(_i)]),
     "ddamg_set_coarse_barrier_polls": (_st, [_h, _i]),
     "ddamg_get_counters": (_st, [_h, ctypes.POINTER(ctypes.c_longlong)]),
+    "ddamg_set_stencil_kernel": (_st, [_i]),
+    "ddamg_get_stencil_kernel": (_st, [ctypes.POINTER(_i)]),
     "ddamg_write_metadata": (_st, [_h, ctypes.c_char_p, _i, ctypes.c_double]),
     "ddamg_write_metadata_params": (_st, [ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_longlong), _i,
                                           ctypes.c_double, ctypes.c_char_p]),

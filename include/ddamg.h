@@ -76,10 +76,13 @@ typedef struct {
      * the block operator on tcgen05 tensor cores (TF32 inputs, FP32 accumulation); 0: CUDA
      * cores only.  No reference counterpart. */
     int tensor_cores;
-    /* 1 (default): each V-cycle preconditioner application (per batch width) is captured once into
-     * a CUDA graph and replayed; 0: kernels are launched one by one.  Off while per-kernel timing
-     * (ddamg_profile) is on and for the K-cycle, whose inner FGMRES is host driven.  No reference
-     * counterpart. */
+    /* 1 (default): solves run from CUDA graphs.  The first solve of a batch width runs host driven
+     * (it tunes the kernels and captures the V-cycle preconditioner into a graph that it replays);
+     * from the second on, the whole solve is one graph whose conditional nodes carry the FGMRES loops
+     * (the outer one and, for K-cycles, the inner FGMRES of every coarse level), with the Hessenberg
+     * and Givens work in device kernels, so no Arnoldi step waits for the host.  0: kernels are
+     * launched one by one from the host loop.  Off while per-kernel timing (ddamg_profile) is on.
+     * No reference counterpart. */
     int cuda_graphs;
     /* polls (64 ns sleeps apart) after which a grid barrier of the coarsest-level GMRES kernel gives up
      * and the solve returns DDAMG_ERR_DEVICE_TIMEOUT; default 2^24 (about 1-2 s); <= 0 also means the
@@ -205,6 +208,13 @@ ddamg_status ddamg_coarse_gmres_noalloc(const void* links, const void* b, void* 
 /* changes coarse_barrier_polls of a live handle (launches made after the call use it; V-cycle graphs
  * captured earlier are dropped and captured again).  No reference counterpart. */
 ddamg_status ddamg_set_coarse_barrier_polls(ddamg_t* h, int polls);
+/* Which D_W kernel the library uses, process-wide (no reference counterpart): 0 the default, 1 the
+ * register kernels (one or two sites per thread, neighbours through L1/L2), 2 the staged-tile kernel
+ * (persistent CTAs; bulk asynchronous copies bring 8 x 64-site tiles of psi with their halo and the
+ * links into shared memory, two stages deep), used where the lattice divides into its tiles. */
+ddamg_status ddamg_set_stencil_kernel(int kind);
+ddamg_status ddamg_get_stencil_kernel(int* kind);
+
 /* ------------------------------------------------------------------ run metadata */
 /* Iteration counters of the last run of each method, in the order the metadata file lists them;
  * -1 for a method not run on the handle (src/variables.cpp:9-17). */

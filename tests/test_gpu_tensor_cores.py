@@ -117,9 +117,11 @@ def test_solve_batched_tensor_cores(cycle):
 def test_cycle_graph_replay_matches_direct(R, precision):
     """The V-cycle captured into a CUDA graph (from the second preconditioner application of a
     batch width on) gives the same solves as launching the kernels one by one: bit-identical on
-    the CUDA-core paths; with the tensor-core smoother (R >= 8, mixed) each handle's autotuner may
-    pick another tile shape (another TF32 accumulation order), so there the iterations agree and
-    the solutions to 1e-9."""
+    the CUDA-core paths in the first solve (host-driven FGMRES around the replayed cycle); the second
+    solve runs as one device-driven graph whose Givens arithmetic is compiled for the device, so it
+    agrees to 1e-12 with the same iterations.  With the tensor-core smoother (R >= 8, mixed) each
+    handle's autotuner may pick another tile shape (another TF32 accumulation order), so there the
+    iterations agree and the solutions to 1e-9."""
     N = 128
     U, rows = synthetic(N, 16)
     n = 2 * N * N
@@ -137,9 +139,12 @@ def test_cycle_graph_replay_matches_direct(R, precision):
         out.append((res, report))
     (g_res, g_rep), (d_res, _) = out
     assert f"cycle graph rhs {R}:" in g_rep, g_rep
-    for (xg, ig), (xd, idd) in zip(g_res, d_res):
+    assert f"solve graph rhs {R}:" in g_rep, g_rep
+    for k, ((xg, ig), (xd, idd)) in enumerate(zip(g_res, d_res)):
         assert [i.iterations for i in ig] == [i.iterations for i in idd]
         if R >= 8 and precision == ddamg.PREC_MIXED:
             assert np.linalg.norm(xg - xd) / np.linalg.norm(xd) < 1e-9
-        else:
+        elif k == 0:
             assert np.array_equal(xg, xd)
+        else:
+            assert np.linalg.norm(xg - xd) / np.linalg.norm(xd) < 1e-12
