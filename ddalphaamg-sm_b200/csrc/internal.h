@@ -234,9 +234,24 @@ struct CoarseGmresWork {
     int* status = nullptr;     // [0] error flag, [1] iterations
     int grid = 0;
     int block = 0;             // threads per CTA (set by coarse_gmres_prepare)
+    int ncache = 0, nbs = 0;   // link matrices / basis slots of a CTA's sites in shared memory (coarse_gmres_prepare)
     long long spin_limit = 0;  // polls before a grid barrier gives up (<= 0: the default, 2^24)
 };
 void coarse_gmres_prepare(CoarseGmresWork& w, int n, int m, int dof, int device);
+// the same solve on one thread-block cluster per right-hand side (kernels_gmres.cu)
+struct CoarseClusterWork {
+    int C = 0;             // CTAs per cluster (16 or 8)
+    int clusters = 0;      // clusters of one launch (each loops over its share of the right-hand sides)
+    size_t smem = 0;
+    long wstride = 0;      // complex values of workspace per cluster: basis (m+1) n, w n, Hessenberg (m+1) m
+    double2* ws = nullptr;
+    int* status = nullptr;  // [1]: iterations
+};
+// false if the device cannot run the cluster kernel for this level (dof > 32, shared memory, cluster size)
+bool coarse_cluster_prepare(CoarseClusterWork& w, int n, int m, int dof, int max_rhs);
+void launch_coarse_gmres_cluster(cudaStream_t s, const CoarseClusterWork& w, const double2* links, const double2* b,
+                                 double2* x, int R, int Nx, int Nt, int dof, double m0, int m, int restarts,
+                                 double tol);
 // x = GMRES(m) x restarts solution of D x = b from x0 = b; returns on the stream
 void launch_coarse_gmres(cudaStream_t s, const CoarseGmresWork& w, const double2* links, const double2* b,
                          double2* x, int Nx, int Nt, int dof, double m0, int m, int restarts, double tol);

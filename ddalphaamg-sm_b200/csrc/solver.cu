@@ -107,6 +107,9 @@ struct ddamg_handle {
     double2* grad = nullptr;   // gradient work: psi, lambda, sigma_3 eta (3 fine vectors)
     ddamg::KrylovWork kry;                          // BiCGstab / CG comparison solvers (allocated on first use)
     ddamg::CoarseGmresWork cg;                      // lane 0: the handle's stream
+    ddamg::CoarseClusterWork ccl;                   // the cluster kernel's workspace (if the device runs it)
+    int coarse_kind = -1;                           // coarsest solver: -1 not chosen yet, 0 cooperative grid, 1 cluster
+    int coarse_kind_batch = -1;                     // the same for several right-hand sides at once
     std::vector<ddamg::CoarseGmresWork> cg_lane;    // lanes 1..: concurrent coarsest solves of a batch
     std::vector<cudaStream_t> lane_s;
     std::vector<cudaEvent_t> lane_ev;
@@ -283,6 +286,7 @@ static void build_geometry(ddamg_handle* h) {
     if (p.nu1 < 0 || p.nu2 < 0 || p.sap_test_vectors_iterations < 0) bad("smoothing counts must be >= 0");
     if (p.cycle != DDAMG_CYCLE_V && p.cycle != DDAMG_CYCLE_K) bad("cycle must be 0 (V) or 1 (K)");
     if (p.precision != DDAMG_PREC_DOUBLE && p.precision != DDAMG_PREC_MIXED) bad("precision must be 0 or 1");
+    if (p.coarse_kernel < 0 || p.coarse_kernel > 2) bad("coarse_kernel must be 0 (chosen), 1 (cooperative grid) or 2 (cluster)");
     int W = p.max_rhs;
     for (int l = 0; l < p.levels - 1; l++) W = std::max(W, h->lv[l].g.ntest);
     h->W = W;
@@ -434,6 +438,10 @@ static void allocate(ddamg_handle* h) {
     h->cg.bar = dalloc_t<unsigned>(h, 2);
     h->cg.status = dalloc_t<int>(h, 2);
     h->cg.spin_limit = p.coarse_barrier_polls;
+    if (coarse_cluster_prepare(h->ccl, (int)gc.size(), cm, gc.dof, p.max_rhs)) {
+        h->ccl.ws = dalloc_t<double2>(h, (size_t)h->ccl.clusters * h->ccl.wstride);
+        h->ccl.status = dalloc_t<int>(h, 2);
+    }
     // extra lanes so the coarsest solves of a batch run side by side (each a cooperative grid)
     const int lanes = std::min(p.max_rhs, 8);
     DDAMG_CUDA_TRY(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
@@ -560,12 +568,16 @@ static int coarse_solve(ddamg_handle* h, const double2* b, double2* x) {
     ProfScope ps(h, 1, h->L - 1);
     LevelData& D = h->lv[h->L - 1];
     const Geom& g = D.g;
-    launch_coarse_gmres(h->s, h->cg, D.d.links, b, x, g.Nx, g.Nt, g.dof, h->p.m0, h->p.coarse_gmres_restart_length,
-                        h->p.coarse_gmres_restarts, h->p.coarse_gmres_tolerance);
+    if (h->coarse_kind == 1)
+        launch_coarse_gmres_cluster(h->s, h->ccl, D.d.links, b, x, 1, g.Nx, g.Nt, g.dof, h->p.m0,
+                                    h->p.coarse_gmres_restart_length, h->p.coarse_gmres_restarts,
+                                    h->p.coarse_gmres_tolerance);
+    else
+        launch_coarse_gmres(h->s, h->cg, D.d.links, b, x, g.Nx, g.Nt, g.dof, h->p.m0,
+                            h->p.coarse_gmres_restart_length, h->p.coarse_gmres_restarts,
+                            h->p.coarse_gmres_tolerance);
     return 0;
 }
-// coarsest solves of R right-hand sides: right-hand side r runs on lane r mod K; lanes other than
-// 0 have their own stream, forked from and joined back into the handle's stream with events
 static void coarse_solve_batch(ddamg_handle* h, const double2* b, double2* x, int R) {
     if (R == 1) {
         coarse_solve(h, b, x);
@@ -574,6 +586,12 @@ static void coarse_solve_batch(ddamg_handle* h, const double2* b, double2* x, in
     ProfScope ps(h, 1, h->L - 1);
     LevelData& D = h->lv[h->L - 1];
     const Geom& g = D.g;
+    if (h->coarse_kind_batch == 1) {  // one launch: each cluster loops over its share of the right-hand sides
+        launch_coarse_gmres_cluster(h->s, h->ccl, D.d.links, b, x, R, g.Nx, g.Nt, g.dof, h->p.m0,
+                                    h->p.coarse_gmres_restart_length, h->p.coarse_gmres_restarts,
+                                    h->p.coarse_gmres_tolerance);
+        return;
+    }
     const long n = g.size();
     const int K = 1 + (int)h->cg_lane.size();
     DDAMG_CUDA_TRY(cudaEventRecord(h->fork_ev, h->s));
@@ -593,15 +611,76 @@ static void coarse_solve_batch(ddamg_handle* h, const double2* b, double2* x, in
 }
 static void check_coarse_status(ddamg_handle* h, int* iters) {
     const int K = 1 + (int)h->cg_lane.size();
-    std::vector<int> st(2 * K);
+    std::vector<int> st(2 * K + 2, 0);
     DDAMG_CUDA_TRY(cudaMemcpyAsync(st.data(), h->cg.status, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->s));
     for (int k = 1; k < K; k++)
         DDAMG_CUDA_TRY(cudaMemcpyAsync(st.data() + 2 * k, h->cg_lane[k - 1].status, 2 * sizeof(int),
                                        cudaMemcpyDeviceToHost, h->s));
+    if (h->ccl.status)
+        DDAMG_CUDA_TRY(
+            cudaMemcpyAsync(st.data() + 2 * K, h->ccl.status, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->s));
     sync(h);
     for (int k = 0; k < K; k++)
         if (st[2 * k] != 0) throw TimeoutFailure();
-    if (iters) *iters = st[1];
+    if (iters) *iters = h->coarse_kind == 1 ? st[2 * K + 1] : st[1];
+}
+// the coarsest solver, chosen once per handle at the end of its first setup: the cooperative-grid
+// kernel and the cluster kernel each solve random right-hand sides twice, one and (with max_rhs > 1) a
+// batch of max_rhs, and the faster second run wins for each (the cluster kernel only where the device
+// runs its clusters)
+static void tune_coarse(ddamg_handle* h) {
+    if (h->coarse_kind >= 0) return;
+    const int Rb = std::max(1, h->p.max_rhs);
+    if (!h->ccl.ws || h->p.coarse_kernel == 1) {
+        h->coarse_kind = h->coarse_kind_batch = 0;
+        h->tune_log += h->ccl.ws ? "coarsest solve: cooperative grid (requested)\n"
+                                 : "coarsest solve: cooperative grid (no cluster kernel for this level)\n";
+        return;
+    }
+    if (h->p.coarse_kernel == 2) {
+        h->coarse_kind = h->coarse_kind_batch = 1;
+        h->tune_log += "coarsest solve: cluster of " + std::to_string(h->ccl.C) + " CTAs (requested)\n";
+        return;
+    }
+    LevelData& D = h->lv[h->L - 1];
+    const Geom& g = D.g;
+    cudaStream_t s = h->s;
+    launch_fill_uniform(s, D.d.eta, g.size() * Rb, 0x5eedc0a25ull, 0);
+    auto time_it = [&](int kind, int R) {
+        float ms = 0;
+        h->coarse_kind = h->coarse_kind_batch = kind;
+        for (int rep = 0; rep < 2; rep++) {
+            DDAMG_CUDA_TRY(cudaEventRecord(h->ev0, s));
+            coarse_solve_batch(h, D.d.eta, D.d.psi, R);
+            DDAMG_CUDA_TRY(cudaEventRecord(h->ev1, s));
+            sync(h);
+            DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        }
+        check_coarse_status(h, nullptr);
+        return 1e3 * ms;
+    };
+    const double u0 = time_it(0, 1), u1 = time_it(1, 1);
+    const int k1 = u1 < u0 ? 1 : 0;
+    int kb = k1;
+    double b0 = 0, b1 = 0;
+    if (Rb > 1) {
+        b0 = time_it(0, Rb);
+        b1 = time_it(1, Rb);
+        kb = b1 < b0 ? 1 : 0;
+    }
+    h->coarse_kind = k1;
+    h->coarse_kind_batch = kb;
+    char buf[320];
+    snprintf(buf, sizeof(buf),
+             "coarsest solve, 1 rhs: cooperative grid %d CTAs %.1f us, cluster %d CTAs %.1f us -> %s\n", h->cg.grid, u0,
+             h->ccl.C, u1, k1 ? "cluster" : "cooperative grid");
+    h->tune_log += buf;
+    if (Rb > 1) {
+        snprintf(buf, sizeof(buf),
+                 "coarsest solve, %d rhs: cooperative grid on %d streams %.1f us, %d clusters %.1f us -> %s\n", Rb,
+                 1 + (int)h->cg_lane.size(), b0, std::min(Rb, h->ccl.clusters), b1, kb ? "cluster" : "cooperative grid");
+        h->tune_log += buf;
+    }
 }
 
 // the tensor-core sweeps record a bounded wait that gave up in a status word per level
@@ -1222,6 +1301,7 @@ static void setup(ddamg_handle* h, const double2* rnd_host, uint64_t seed) {
     DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     h->last_setup_s = ms * 1e-3;
     h->setup_done = true;
+    tune_coarse(h);  // once per handle, outside the setup's timed region
 }
 
 // ------------------------------------------------------------------ solve
@@ -1444,6 +1524,7 @@ ddamg_status ddamg_params_default(ddamg_params* p) {
     p->tensor_cores = 1;
     p->cuda_graphs = 1;
     p->coarse_barrier_polls = 1 << 24;
+    p->coarse_kernel = 0;
     return DDAMG_OK;
 }
 

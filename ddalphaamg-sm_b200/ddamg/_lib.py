@@ -27,6 +27,7 @@ class Params(ctypes.Structure):
         ("smoother_tolerance", ctypes.c_double), ("cycle", ctypes.c_int), ("precision", ctypes.c_int),
         ("max_rhs", ctypes.c_int), ("device", ctypes.c_int), ("tensor_cores", ctypes.c_int),
         ("cuda_graphs", ctypes.c_int), ("coarse_barrier_polls", ctypes.c_int),
+        ("coarse_kernel", ctypes.c_int),
     ]
 
 

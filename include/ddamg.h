@@ -84,10 +84,16 @@ typedef struct {
      * launched one by one from the host loop.  Off while per-kernel timing (ddamg_profile) is on.
      * No reference counterpart. */
     int cuda_graphs;
-    /* polls (64 ns sleeps apart) after which a grid barrier of the coarsest-level GMRES kernel gives up
-     * and the solve returns DDAMG_ERR_DEVICE_TIMEOUT; default 2^24 (about 1-2 s); <= 0 also means the
+    /* polls (each an L2 read and a 32 ns sleep) after which a grid barrier of the coarsest-level GMRES kernel gives up
+     * and the solve returns DDAMG_ERR_DEVICE_TIMEOUT; default 2^24 (a few seconds); <= 0 also means the
      * default.  The reference's MPI collectives wait without a bound. */
     int coarse_barrier_polls;
+    /* the coarsest-level GMRES kernel: 0 (default) chosen per handle at the end of its first setup by
+     * timing both on one right-hand side; 1 the cooperative-grid kernel (about two coarse sites per CTA,
+     * bounded grid barriers); 2 the thread-block-cluster kernel (one cluster of 16 CTAs per right-hand
+     * side, hardware cluster barriers, distributed shared memory; the cooperative kernel where the device
+     * or the level does not admit it).  No reference counterpart. */
+    int coarse_kernel;
 } ddamg_params;
 
 typedef struct {

@@ -24,11 +24,11 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-def solver(z, precision=ddamg.PREC_DOUBLE, cycle=ddamg.CYCLE_V, setup=True):
+def solver(z, precision=ddamg.PREC_DOUBLE, cycle=ddamg.CYCLE_V, setup=True, **kw):
     Nx, Nt, L = int(z["Nx"]), int(z["Nt"]), int(z["levels"])
     U = po.links_from_theta(z["theta"])
     s = ddamg.Solver(ddamg.default_params(Nx, Nt, L, float(z["m0"]), z["rows"], precision=precision, cycle=cycle,
-                                          fgmres_restart_length=int(z["fgmres_m"])))
+                                          fgmres_restart_length=int(z["fgmres_m"]), **kw))
     s.load_gauge(U)
     if setup:
         s.setUpPhase(vectors=po.uniform(int(z["rnd_count"]), int(z["seed"]) + 1))
@@ -144,7 +144,7 @@ def test_coarse_barrier_timeout_then_recovers(golden):
     leaves at its next barrier, the call reports DEVICE_TIMEOUT, and after the limit is restored the same
     handle's coarsest solve and full solve agree with the oracle (the status word is cleared per launch)."""
     z = golden("ops_16x32_l3")
-    s, U = solver(z)
+    s, U = solver(z, coarse_kernel=1)  # the cooperative-grid kernel, whose grid barriers poll
     o = po.Oracle(int(z["Nx"]), int(z["Nt"]), int(z["levels"]), float(z["m0"]), z["rows"], U)
     o.setup(po.uniform(int(z["rnd_count"]), int(z["seed"]) + 1))
     L = int(z["levels"])
