@@ -142,6 +142,14 @@ void launch_sap_sweep_tc(cudaStream_t s, const Geom& g, const TcSapWork& w, cons
 int tune_sap_tc(cudaStream_t s, const Geom& g, const TcSapWork& w, const float2* r, const SapArgs& a, int nrhs,
                 double* us);
 int tc_sweep_shapes();
+// the level operator out = D_c in (or b - D_c in) for nrhs right-hand sides on tcgen05 tensor cores
+// (TF32 inputs, FP32 accumulation), from the SAP sweeps' packed operator tiles; shape: 0..tc_op_shapes()-1
+// (64, 32 or 16 right-hand sides per CTA)
+bool tc_op_supported(const Geom& g);
+int tc_op_shapes();
+int tc_op_shape_rg(int shape);
+void launch_coarse_op_tc(cudaStream_t s, const Geom& g, const float* tiles, const float2* in, float2* out,
+                         const float2* b, double m0, int nrhs, int shape, int* status);
 void tc_sweep_shape(int idx, int* rg, int* stages, int* chains);
 
 // ------------------------------------------------------------ comparison solvers (kernels_krylov.cu)

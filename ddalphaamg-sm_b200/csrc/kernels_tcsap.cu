@@ -413,6 +413,225 @@ static void launch_apply(int shape, cudaStream_t s, const CUtensorMap& vmap, con
     }
 }
 
+// ---------------------------------------------------------------- the level operator on tensor cores
+// out = D_c v (or b - D_c v) on the whole level for R right-hand sides (Level::D_operator,
+// src/level.cpp:394-426, applied to a batch): per site and hop one M = 64, N = RG, K = 64 TF32 MMA
+// chain of the packed operator tile (-s_d M_d, the tiles of the SAP sweeps) with the neighbour's
+// vector tile, the five hops accumulating into one tensor-memory accumulator; the epilogue adds the
+// mass term (m0 + 2) v in FP32.  One CTA per run of consecutive sites and group of RG right-hand sides:
+// one thread streams (link tile, vector tile) pairs into an NA-deep ring (bulk copy + TMA, the periodic
+// neighbour computed on the fly), one thread issues the MMAs, the epilogue warps drain the two
+// accumulator buffers.  Every mbarrier wait is bounded as in tc_block_apply_kernel.
+struct OpArgs {
+    const float* tiles;
+    float2* dst;
+    const float2* src;   // v, for the mass term
+    const float2* bsub;  // non-null: dst = bsub - D_c v
+    int Nx, Nt, dof, ks, R, sites, spc;  // spc: sites per CTA
+    long n;                              // complex values per vector
+    float mm;
+    int* status;
+};
+template <int RG> __host__ __device__ constexpr uint32_t op_stage_bytes() { return kTileBytes + RG * 256; }
+template <int RG, int NA> inline size_t op_smem() { return 1024 + (size_t)NA * op_stage_bytes<RG>() + 8 * (2 * NA + 5); }
+
+template <int RG, int NA>
+__global__ void __launch_bounds__(apply_threads(RG), 1)
+    tc_coarse_op_kernel(const __grid_constant__ CUtensorMap vmap, OpArgs a) {
+    constexpr int EW = epi_warps(RG);
+    constexpr int CW = 4 * RG / EW;
+    constexpr uint32_t SB = op_stage_bytes<RG>();
+    extern __shared__ unsigned char smraw[];
+    __shared__ volatile int s_abort;
+    __shared__ uint32_t s_taddr;
+    unsigned char* sm =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
+    const int sb = blockIdx.x * a.spc, se = min(a.sites, sb + a.spc);
+    const int r0 = blockIdx.y * RG, nr = min(RG, a.R - r0);
+    const int ns = se - sb;
+    const int katoms = (a.ks + 3) >> 2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (ns <= 0) return;  // uniform over the CTA
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + (size_t)NA * SB);
+    uint64_t* fullS = bar;
+    uint64_t* emptyS = bar + NA;
+    uint64_t* accF = bar + 2 * NA;
+    uint64_t* accE = accF + 2;
+    uint64_t* drain = accE + 2;
+    if (threadIdx.x == 0) {
+        s_abort = 0;
+        for (int i = 0; i < NA; i++) {
+            mbar_init(&fullS[i], 1);
+            mbar_init(&emptyS[i], 1);
+        }
+        for (int i = 0; i < 2; i++) {
+            mbar_init(&accF[i], 1);
+            mbar_init(&accE[i], EW);
+        }
+        mbar_init(drain, 1);
+        mbar_fence_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(&s_taddr, 2 * RG);
+        tmem_relinquish();
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t taddr = s_taddr;
+    auto wait = [&](uint64_t* b, uint32_t parity) -> bool {
+        return mbar_try_wait(b, parity) || wait_slow(b, parity, a.status, &s_abort);
+    };
+    if (warp == EW) {
+        // ---------------- producer: for every (site, hop) the operator tile and the neighbour's vector tile
+        if (lane == 0) {
+            int issued = 0;
+            bool ok = true;
+            for (int s = sb; s < se && ok; s++) {
+                const int x = s / a.Nt, t = s - x * a.Nt;
+                for (int d = 0; d < 5; d++) {
+                    int nb;
+                    switch (d) {
+                        case 0: nb = s; break;
+                        case 1: nb = x * a.Nt + (t + 1 == a.Nt ? 0 : t + 1); break;
+                        case 2: nb = (x + 1 == a.Nx ? 0 : x + 1) * a.Nt + t; break;
+                        case 3: nb = x * a.Nt + (t == 0 ? a.Nt - 1 : t - 1); break;
+                        default: nb = (x == 0 ? a.Nx - 1 : x - 1) * a.Nt + t; break;
+                    }
+                    const int st = issued % NA;
+                    if (issued >= NA && !(ok = wait(&emptyS[st], (uint32_t)(issued / NA - 1) & 1u))) break;
+                    unsigned char* base = sm + (size_t)st * SB;
+                    mbar_arrive_expect_tx(&fullS[st], kTileBytes + (uint32_t)katoms * RG * 128);
+                    bulk_g2s(base, a.tiles + ((long)s * 5 + d) * kTcTileFloats, kTileBytes, &fullS[st]);
+                    for (int at = 0; at < katoms; at++)
+                        tma_load_3d(base + kTileBytes + at * RG * 128, &vmap, 32 * at, nb, r0, &fullS[st]);
+                    issued++;
+                }
+            }
+            for (int st = 0; st < NA; st++) {  // every copy issued has landed before the CTA may exit
+                const int cnt = issued > st ? (issued - 1 - st) / NA + 1 : 0;
+                if (cnt > 0) mbar_wait(&fullS[st], (uint32_t)(cnt - 1) & 1u, a.status);
+            }
+        }
+    } else if (warp == EW + 1) {
+        // ---------------- MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = idesc_tf32(64, RG);
+            const uint64_t sd0 = sdesc_k128(smem_u32(sm));
+            int consumed = 0;
+            bool ok = true;
+            for (int sl = 0; sl < ns && ok; sl++) {
+                const int b = sl & 1;
+                if (sl >= 2 && !wait(&accE[b], (uint32_t)((sl >> 1) - 1) & 1u)) break;
+                tc_fence_after();
+                const uint32_t dt = taddr + (uint32_t)(b * RG);
+                for (int d = 0; d < 5; d++) {
+                    const int st = consumed % NA;
+                    if (!(ok = wait(&fullS[st], (uint32_t)(consumed / NA) & 1u))) break;
+                    const uint64_t ad = sd0 + (uint64_t)(st * (SB >> 4));
+                    const uint64_t bd = ad + (uint64_t)(kTileBytes >> 4);
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        if (k >= a.ks) break;
+                        mma_tf32(dt, ad + (uint64_t)((k >> 2) * (8192 >> 4) + (k & 3) * 2),
+                                 bd + (uint64_t)((k >> 2) * (RG * 128 >> 4) + (k & 3) * 2), idesc,
+                                 (d == 0 && k == 0) ? 0u : 1u);
+                    }
+                    mma_commit(&emptyS[st]);
+                    consumed++;
+                }
+                if (!ok) break;
+                mma_commit(&accF[b]);
+            }
+            mma_commit(drain);  // every MMA of this CTA has finished before TMEM is released
+            mbar_wait(drain, 0, a.status);
+        }
+    } else {
+        // ---------------- epilogue (the accumulator layout of tc_block_apply_kernel)
+        const int q = warp & 3;
+        const int c0 = (warp >> 2) * CW;
+        const int m = 16 * q + (lane & 15);
+        const bool rowok = lane < 16 && m < 2 * a.dof;
+        const long ostride = a.n * 2;  // floats between right-hand sides
+        const int ncol = min(CW, nr - c0);
+        const float* __restrict__ v0 = reinterpret_cast<const float*>(a.src) + (long)(r0 + c0) * ostride + m;
+        float* __restrict__ d0 = reinterpret_cast<float*>(a.dst) + (long)(r0 + c0) * ostride + m;
+        const float* __restrict__ b0 =
+            a.bsub ? reinterpret_cast<const float*>(a.bsub) + (long)(r0 + c0) * ostride + m : nullptr;
+        for (int sl = 0; sl < ns; sl++) {
+            const int b = sl & 1;
+            if (!wait(&accF[b], (uint32_t)(sl >> 1) & 1u)) break;
+            tc_fence_after();
+            const uint32_t tb = taddr + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * RG + c0);
+            float acc[CW];
+            if constexpr (CW == 16) tmem_ld16(tb, acc);
+            else tmem_ld8(tb, acc);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&accE[b]);
+            if (rowok) {
+                const long so = (long)(sb + sl) * a.dof * 2;
+#pragma unroll
+                for (int c = 0; c < CW; c++) {
+                    if (c < ncol) {
+                        float w = a.mm * v0[so + c * ostride] + acc[c];
+                        if (b0) w = b0[so + c * ostride] - w;
+                        d0[so + c * ostride] = w;
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(taddr, 2 * RG);
+    }
+}
+
+template <int RG, int NA>
+static void launch_op_shape(cudaStream_t s, const Geom& g, const float* tiles, const float2* in, float2* out,
+                            const float2* b, double m0, int nrhs, int* status) {
+    const size_t smem = op_smem<RG, NA>();
+    DDAMG_CUDA_TRY(cudaFuncSetAttribute(tc_coarse_op_kernel<RG, NA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+    int sms = 0, dev = 0;
+    DDAMG_CUDA_TRY(cudaGetDevice(&dev));
+    DDAMG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int groups = (nrhs + RG - 1) / RG;
+    // one CTA per SM over all (site run, rhs group) pairs: runs of consecutive sites
+    const int runs = std::max(1, std::min(g.sites, sms / std::min(groups, sms)));
+    OpArgs a;
+    a.tiles = tiles;
+    a.dst = out;
+    a.src = in;
+    a.bsub = b;
+    a.Nx = g.Nx;
+    a.Nt = g.Nt;
+    a.dof = g.dof;
+    a.ks = (2 * g.dof + 7) / 8;
+    a.R = nrhs;
+    a.sites = g.sites;
+    a.spc = (g.sites + runs - 1) / runs;
+    a.n = g.size();
+    a.mm = (float)(m0 + 2.0);
+    a.status = status;
+    const CUtensorMap vmap = vector_map(in, g.dof, g.sites, nrhs, RG);
+    dim3 grid((g.sites + a.spc - 1) / a.spc, groups);
+    DDAMG_LAUNCH((tc_coarse_op_kernel<RG, NA>), grid, apply_threads(RG), smem, s, vmap, a);
+}
+// shapes: right-hand sides per CTA 64, 32, 16 (ring depths 6, 8, 10)
+int tc_op_shapes() { return 3; }
+int tc_op_shape_rg(int shape) { return shape == 0 ? 64 : shape == 1 ? 32 : 16; }
+bool tc_op_supported(const Geom& g) { return g.level >= 1 && g.dof <= 32 && g.dof % 2 == 0; }
+void launch_coarse_op_tc(cudaStream_t s, const Geom& g, const float* tiles, const float2* in, float2* out,
+                         const float2* b, double m0, int nrhs, int shape, int* status) {
+    switch (shape) {
+        case 0: launch_op_shape<64, 6>(s, g, tiles, in, out, b, m0, nrhs, status); break;
+        case 1: launch_op_shape<32, 8>(s, g, tiles, in, out, b, m0, nrhs, status); break;
+        default: launch_op_shape<16, 10>(s, g, tiles, in, out, b, m0, nrhs, status); break;
+    }
+}
+
 // ---------------------------------------------------------------- per (block, rhs) kernels
 // one warp per task = kb * R + r; lanes stride over the block's NE = S * dof unknowns
 struct TaskGeom {

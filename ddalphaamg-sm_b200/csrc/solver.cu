@@ -63,6 +63,7 @@ struct LevelData {
     TcSapWork tcw;
     std::map<int, int> tc_shape;  // batch width -> tile shape chosen by the autotuner
     std::map<int, int> rb_choice; // 2 * batch width + fp32 -> right-hand sides per CTA (CUDA cores)
+    std::map<int, int> tc_op;     // batch width -> level-operator kernel: -1 CUDA cores, else tensor-core shape
     FgDev fg;                     // device-driven FGMRES state (level 0: the outer solve; >= 1: K-cycle)
 };
 constexpr int kTcMinRhs = 8;  // fewer right-hand sides leave too little link reuse for the tensor cores
@@ -286,6 +287,7 @@ static void build_geometry(ddamg_handle* h) {
     if (p.nu1 < 0 || p.nu2 < 0 || p.sap_test_vectors_iterations < 0) bad("smoothing counts must be >= 0");
     if (p.cycle != DDAMG_CYCLE_V && p.cycle != DDAMG_CYCLE_K) bad("cycle must be 0 (V) or 1 (K)");
     if (p.precision != DDAMG_PREC_DOUBLE && p.precision != DDAMG_PREC_MIXED) bad("precision must be 0 or 1");
+    if (p.tensor_cores < 0 || p.tensor_cores > 2) bad("tensor_cores must be 0, 1 or 2");
     if (p.coarse_kernel < 0 || p.coarse_kernel > 2) bad("coarse_kernel must be 0 (chosen), 1 (cooperative grid) or 2 (cluster)");
     int W = p.max_rhs;
     for (int l = 0; l < p.levels - 1; l++) W = std::max(W, h->lv[l].g.ntest);
@@ -466,12 +468,77 @@ static void allocate(ddamg_handle* h) {
 }
 
 // ------------------------------------------------------------------ operators
-template <typename V> static void level_op(ddamg_handle* h, int l, const V* in, V* out, const V* b, int nrhs) {
+// The batched FP32 level operator of a level with tensor-core tiles: the first call per batch width
+// times the CUDA-core kernel and each tensor-core shape on the call's own operands (three runs each,
+// outside any graph capture: the first solve of a width runs directly) and keeps the fastest; the
+// last run of the chosen kernel leaves the result.
+static int tc_op_for(ddamg_handle* h, int l, const float2* in, float2* out, const float2* b, int nrhs) {
+    LevelData& D = h->lv[l];
+    auto it = D.tc_op.find(nrhs);
+    if (it != D.tc_op.end()) return it->second;
+    if (h->capturing) return -1;
+    const Geom& g = D.g;
+    cudaStream_t s = h->s;
+    cudaEvent_t e0, e1;
+    DDAMG_CUDA_TRY(cudaEventCreate(&e0));
+    DDAMG_CUDA_TRY(cudaEventCreate(&e1));
+    auto run = [&](int k) {
+        if (k < 0) launch_coarse_op<float2>(s, D.f.links, in, out, b, g.Nx, g.Nt, g.dof, h->p.m0, nrhs);
+        else launch_coarse_op_tc(s, g, D.tcw.tiles, in, out, b, h->p.m0, nrhs, k, D.tcw.status);
+    };
+    std::ostringstream o;
+    o << "level " << l << " rhs " << nrhs << " level operator:";
+    int best = -1;
+    double best_us = 0;
+    const bool forced = h->p.tensor_cores == 2;  // tensor cores whatever the timing
+    for (int k = forced ? 0 : -1; k < tc_op_shapes(); k++) {
+        if (k >= 0 && tc_op_shape_rg(k) / 2 >= nrhs * 2) continue;  // at most 4x padding
+        run(k);
+        DDAMG_CUDA_TRY(cudaEventRecord(e0, s));
+        for (int q = 0; q < 3; q++) run(k);
+        DDAMG_CUDA_TRY(cudaEventRecord(e1, s));
+        DDAMG_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0;
+        DDAMG_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        const double us = 1e3 * ms / 3;
+        if ((best == -1 && (k == -1 || forced)) || us < best_us) {
+            best = k;
+            best_us = us;
+        }
+        if (k < 0) o << " [CUDA cores: " << us << " us]";
+        else o << " [tensor cores, rhs/cta " << tc_op_shape_rg(k) << ": " << us << " us]";
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    run(best);
+    D.tc_op[nrhs] = best;
+    o << " -> " << (best < 0 ? std::string("CUDA cores") : "tensor cores rhs/cta " + std::to_string(tc_op_shape_rg(best)));
+    h->tune_log += o.str() + "\n";
+    return best;
+}
+// allow_tc = false keeps the CUDA-core kernel (the setup's smoothing: TF32 would coarsen the test vectors)
+template <typename V>
+static void level_op(ddamg_handle* h, int l, const V* in, V* out, const V* b, int nrhs, bool allow_tc = true) {
     ProfScope ps(h, 2, l);
     LevelData& D = h->lv[l];
     const Geom& g = D.g;
-    if (l == 0) launch_wilson<V>(h->s, B<V>(D).U, in, out, b, g.Nx, g.Nt, h->p.m0, 0, nrhs);
-    else launch_coarse_op<V>(h->s, B<V>(D).links, in, out, b, g.Nx, g.Nt, g.dof, h->p.m0, nrhs);
+    if (l == 0) {
+        launch_wilson<V>(h->s, B<V>(D).U, in, out, b, g.Nx, g.Nt, h->p.m0, 0, nrhs);
+        return;
+    }
+    if constexpr (std::is_same<V, float2>::value) {
+        if (allow_tc && D.tc && nrhs >= kTcMinRhs && h->p.tensor_cores && tc_op_supported(g)) {
+            auto it = D.tc_op.find(nrhs);
+            if (it == D.tc_op.end()) {  // tuned on this call, which it also completes
+                tc_op_for(h, l, in, out, b, nrhs);
+                if (D.tc_op.count(nrhs)) return;
+            } else if (it->second >= 0) {
+                launch_coarse_op_tc(h->s, g, D.tcw.tiles, in, out, b, h->p.m0, nrhs, it->second, D.tcw.status);
+                return;
+            }
+        }
+    }
+    launch_coarse_op<V>(h->s, B<V>(D).links, in, out, b, g.Nx, g.Nt, g.dof, h->p.m0, nrhs);
 }
 
 // tile shape of the tensor-core sweep for this batch width: tuned on first use (the tuner times the
@@ -532,7 +599,7 @@ static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, b
     const bool check = tol > 0.0;
     if (check) launch_norm2<V>(h->s, v, n, n, nrhs, h->dpart, D.vv);
     if (x_zero) DDAMG_CUDA_TRY(cudaMemcpyAsync(r, v, sizeof(V) * n * nrhs, cudaMemcpyDeviceToDevice, h->s));
-    else level_op<V>(h, l, x, r, v, nrhs);  // r = v - D x
+    else level_op<V>(h, l, x, r, v, nrhs, allow_tc);  // r = v - D x
     SapArgs a{h->p.sap_gmres_restart_length, h->p.sap_gmres_restarts, h->p.sap_gmres_tolerance, h->p.m0, nullptr, 0,
               D.done};
     for (int it = 0; it < nu; it++) {
@@ -550,7 +617,7 @@ static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, b
             }
             // the residual after the last black sweep only feeds the convergence test
             const bool last = (colour == 1 && it == nu - 1);
-            if (!last || (check && want_iters)) level_op<V>(h, l, x, r, v, nrhs);
+            if (!last || (check && want_iters)) level_op<V>(h, l, x, r, v, nrhs, allow_tc);
         }
         if (check && (it < nu - 1 || want_iters)) {
             launch_norm2<V>(h->s, r, n, n, nrhs, h->dpart, D.rr);
@@ -1190,7 +1257,7 @@ static bool sap_setup_split(ddamg_handle* h, int l, const V* v, V* x, int nu, in
     SapArgs a{h->p.sap_gmres_restart_length, h->p.sap_gmres_restarts, h->p.sap_gmres_tolerance, h->p.m0, D.red,
               D.nred, D.done};
     DDAMG_CUDA_TRY(cudaMemsetAsync(D.done, 0, sizeof(int) * nrhs, h->s));
-    level_op<V>(h, l, x, r, v, nrhs);  // r = v - D x for every vector
+    level_op<V>(h, l, x, r, v, nrhs, false);  // r = v - D x for every vector (CUDA cores: test-vector quality)
     const int var = rb_for<V>(h, l, r, a, nrhs);  // tuned on first use on red sweeps (times into scratch, syncs)
     const int rb = var / 4;
     const int G = nrhs / rb;
@@ -1204,7 +1271,7 @@ static bool sap_setup_split(ddamg_handle* h, int l, const V* v, V* x, int nu, in
                 a.blocks = colour == 0 ? D.red : D.black;
                 a.nblocks = colour == 0 ? D.nred : D.nblack;
                 launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs, var);
-                if (!(colour == 1 && it == nu - 1)) level_op<V>(h, l, x, r, v, nrhs);
+                if (!(colour == 1 && it == nu - 1)) level_op<V>(h, l, x, r, v, nrhs, false);
             }
         return true;
     }
@@ -1772,6 +1839,23 @@ ddamg_status ddamg_apply_dirac_f32_device(ddamg_t* h, int dagger, const void* in
     API_END
 }
 
+ddamg_status ddamg_apply_level_op_device(ddamg_t* h, int level, int fp32, const void* in, void* out, int nrhs) {
+    CHECK_HANDLE(h);
+    API_BEGIN
+    need_level(h, level, true);
+    if (level == 0 && !h->gauge) throw ParamFailure{"no gauge field loaded"};
+    if (level > 0) need_setup(h);
+    if (!in || !out || nrhs < 1) throw ParamFailure{"ddamg_apply_level_op_device: bad argument"};
+    LevelData& D = h->lv[level];
+    if (fp32) {
+        if (!D.fp32) throw ParamFailure{"this level has no FP32 operator (a mixed-precision handle has one below the coarsest level)"};
+        level_op<float2>(h, level, static_cast<const float2*>(in), static_cast<float2*>(out), nullptr, nrhs);
+    } else {
+        level_op<double2>(h, level, static_cast<const double2*>(in), static_cast<double2*>(out), nullptr, nrhs);
+    }
+    check_tc_status(h);
+    API_END
+}
 ddamg_status ddamg_apply_level_op(ddamg_t* h, int level, const double* in, double* out) {
     CHECK_HANDLE(h);
     API_BEGIN

@@ -65,6 +65,7 @@ SIGNATURES = {
     "ddamg_apply_dirac_device": (_st, [_h, _i, _vp, _vp, _i]),
     "ddamg_apply_dirac_f32_device": (_st, [_h, _i, _vp, _vp, _i]),
     "ddamg_apply_level_op": (_st, [_h, _i, _dp, _dp]),
+    "ddamg_apply_level_op_device": (_st, [_h, _i, _i, _vp, _vp, _i]),
     "ddamg_restrict": (_st, [_h, _i, _dp, _dp]),
     "ddamg_prolong": (_st, [_h, _i, _dp, _dp]),
     "ddamg_sap": (_st, [_h, _i, _dp, _dp, _i, ctypes.c_double, ctypes.POINTER(_i)]),

@@ -73,8 +73,10 @@ typedef struct {
     int max_rhs;                      /* right-hand sides one ddamg_solve call may carry (>= 1) */
     int device;                       /* CUDA device ordinal */
     /* 1 (default): in mixed precision, coarse-level SAP sweeps over >= 8 right-hand sides run
-     * the block operator on tcgen05 tensor cores (TF32 inputs, FP32 accumulation); 0: CUDA
-     * cores only.  No reference counterpart. */
+     * the block operator on tcgen05 tensor cores (TF32 inputs, FP32 accumulation), and the batched
+     * level operator D_c (the residuals of the cycles, the K-cycle's inner FGMRES) runs on them where the
+     * autotuner measures them faster than the CUDA-core kernel; 2: the level operator always on tensor
+     * cores where the level admits them; 0: CUDA cores only.  No reference counterpart. */
     int tensor_cores;
     /* 1 (default): solves run from CUDA graphs.  The first solve of a batch width runs host driven
      * (it tunes the kernels and captures the V-cycle preconditioner into a graph that it replays);
@@ -156,6 +158,12 @@ ddamg_status ddamg_apply_dirac_device(ddamg_t* h, int dagger, const void* in, vo
 ddamg_status ddamg_apply_dirac_f32_device(ddamg_t* h, int dagger, const void* in, void* out, int nrhs);
 /* Level::D_operator (src/level.cpp:394-426) at level l >= 0, FP64 */
 ddamg_status ddamg_apply_level_op(ddamg_t* h, int level, const double* in, double* out);
+/* the same on nrhs right-hand sides in device memory ([rhs][site][dof], complex), on the handle's
+ * stream: fp32 = 0 the FP64 operator (double2 data), fp32 = 1 the working-precision FP32 operator of a
+ * mixed-precision handle (float2 data; with tensor_cores and nrhs >= 8 the batched tensor-core kernel
+ * where the autotuner measured it faster, TF32 inputs with FP32 accumulation).  Level::D_operator
+ * (src/level.cpp:394-426) for a batch. */
+ddamg_status ddamg_apply_level_op_device(ddamg_t* h, int level, int fp32, const void* in, void* out, int nrhs);
 /* Level::Pdagg_v (src/level.cpp:145-189): level l -> l+1 */
 ddamg_status ddamg_restrict(ddamg_t* h, int level, const double* in, double* out);
 /* Level::P_vc (src/level.cpp:92-141): level l+1 -> l */
