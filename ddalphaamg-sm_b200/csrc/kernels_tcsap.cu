@@ -420,7 +420,7 @@ static void launch_apply(int shape, cudaStream_t s, const CUtensorMap& vmap, con
 // vector tile, the five hops accumulating into one tensor-memory accumulator; the epilogue adds the
 // mass term (m0 + 2) v in FP32.  One CTA per run of consecutive sites and group of RG right-hand sides:
 // one thread streams (link tile, vector tile) pairs into an NA-deep ring (bulk copy + TMA, the periodic
-// neighbour computed on the fly), one thread issues the MMAs, the epilogue warps drain the two
+// neighbour computed on the fly), one thread issues the MMAs, the epilogue warps drain kOpAcc
 // accumulator buffers.  Every mbarrier wait is bounded as in tc_block_apply_kernel.
 struct OpArgs {
     const float* tiles;
@@ -433,7 +433,10 @@ struct OpArgs {
     int* status;
 };
 template <int RG> __host__ __device__ constexpr uint32_t op_stage_bytes() { return kTileBytes + RG * 256; }
-template <int RG, int NA> inline size_t op_smem() { return 1024 + (size_t)NA * op_stage_bytes<RG>() + 8 * (2 * NA + 5); }
+constexpr int kOpAcc = 4;  // accumulator buffers in tensor memory: the epilogue of site s overlaps the MMAs of s + 1 .. s + 3
+template <int RG, int NA> inline size_t op_smem() {
+    return 1024 + (size_t)NA * op_stage_bytes<RG>() + 8 * (2 * NA + 2 * kOpAcc + 1);
+}
 
 template <int RG, int NA>
 __global__ void __launch_bounds__(apply_threads(RG), 1)
@@ -456,15 +459,15 @@ __global__ void __launch_bounds__(apply_threads(RG), 1)
     uint64_t* fullS = bar;
     uint64_t* emptyS = bar + NA;
     uint64_t* accF = bar + 2 * NA;
-    uint64_t* accE = accF + 2;
-    uint64_t* drain = accE + 2;
+    uint64_t* accE = accF + kOpAcc;
+    uint64_t* drain = accE + kOpAcc;
     if (threadIdx.x == 0) {
         s_abort = 0;
         for (int i = 0; i < NA; i++) {
             mbar_init(&fullS[i], 1);
             mbar_init(&emptyS[i], 1);
         }
-        for (int i = 0; i < 2; i++) {
+        for (int i = 0; i < kOpAcc; i++) {
             mbar_init(&accF[i], 1);
             mbar_init(&accE[i], EW);
         }
@@ -472,7 +475,7 @@ __global__ void __launch_bounds__(apply_threads(RG), 1)
         mbar_fence_init();
     }
     if (warp == 0) {
-        tmem_alloc(&s_taddr, 2 * RG);
+        tmem_alloc(&s_taddr, kOpAcc * RG);
         tmem_relinquish();
     }
     __syncthreads();
@@ -520,8 +523,8 @@ __global__ void __launch_bounds__(apply_threads(RG), 1)
             int consumed = 0;
             bool ok = true;
             for (int sl = 0; sl < ns && ok; sl++) {
-                const int b = sl & 1;
-                if (sl >= 2 && !wait(&accE[b], (uint32_t)((sl >> 1) - 1) & 1u)) break;
+                const int b = sl % kOpAcc;
+                if (sl >= kOpAcc && !wait(&accE[b], (uint32_t)(sl / kOpAcc - 1) & 1u)) break;
                 tc_fence_after();
                 const uint32_t dt = taddr + (uint32_t)(b * RG);
                 for (int d = 0; d < 5; d++) {
@@ -558,8 +561,17 @@ __global__ void __launch_bounds__(apply_threads(RG), 1)
         const float* __restrict__ b0 =
             a.bsub ? reinterpret_cast<const float*>(a.bsub) + (long)(r0 + c0) * ostride + m : nullptr;
         for (int sl = 0; sl < ns; sl++) {
-            const int b = sl & 1;
-            if (!wait(&accF[b], (uint32_t)(sl >> 1) & 1u)) break;
+            const int b = sl % kOpAcc;
+            // the site's own vector (mass term) and b are loaded before the accumulator is waited for
+            const long so = (long)(sb + sl) * a.dof * 2;
+            float vv[CW], bv[CW];
+#pragma unroll
+            for (int c = 0; c < CW; c++) {
+                const bool ok = rowok && c < ncol;
+                vv[c] = ok ? v0[so + c * ostride] : 0.f;
+                bv[c] = (ok && b0) ? b0[so + c * ostride] : 0.f;
+            }
+            if (!wait(&accF[b], (uint32_t)(sl / kOpAcc) & 1u)) break;
             tc_fence_after();
             const uint32_t tb = taddr + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * RG + c0);
             float acc[CW];
@@ -569,12 +581,11 @@ __global__ void __launch_bounds__(apply_threads(RG), 1)
             __syncwarp();
             if (lane == 0) mbar_arrive(&accE[b]);
             if (rowok) {
-                const long so = (long)(sb + sl) * a.dof * 2;
 #pragma unroll
                 for (int c = 0; c < CW; c++) {
                     if (c < ncol) {
-                        float w = a.mm * v0[so + c * ostride] + acc[c];
-                        if (b0) w = b0[so + c * ostride] - w;
+                        float w = a.mm * vv[c] + acc[c];
+                        if (b0) w = bv[c] - w;
                         d0[so + c * ostride] = w;
                     }
                 }
@@ -584,7 +595,7 @@ __global__ void __launch_bounds__(apply_threads(RG), 1)
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        tmem_dealloc(taddr, 2 * RG);
+        tmem_dealloc(taddr, kOpAcc * RG);
     }
 }
 
