@@ -324,6 +324,13 @@ __global__ void __launch_bounds__(apply_threads(RG), 1)
         const int ncol = min(CW, nr - c0);  // valid columns of this warp (may be <= 0)
         for (int s = 0; s < S; s++) {
             const int b = s & 1;
+            // b of this site is loaded before the accumulator is waited for, and the accumulator is
+            // released as soon as it is in registers, so no global-memory latency sits between the
+            // MMAs of consecutive sites
+            const long so = (long)s * a.dof * 2;
+            float bv[CW];
+#pragma unroll
+            for (int c = 0; c < CW; c++) bv[c] = (rowok && b0 && c < ncol) ? b0[so + c * ostride] : 0.f;
             if (!wait(&accF[b], (uint32_t)(s >> 1) & 1u)) break;
             tc_fence_after();
             const uint32_t tb = taddr + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * NCH * RG + c0);
@@ -339,25 +346,28 @@ __global__ void __launch_bounds__(apply_threads(RG), 1)
 #pragma unroll
                 for (int c = 0; c < CW; c++) acc[c] += part[c];
             }
-            if (rowok) {
+            // the site's own vector from the window before the release: once the accumulator is
+            // released the MMA thread may let the producer refill this window slot
+            float vv[CW];
+            {
                 const unsigned char* self = Bbuf + (size_t)s_slot[s] * kBBytes + (size_t)c0 * 128;
-                const long so = (long)s * a.dof * 2;
-                float bv[CW];
 #pragma unroll
-                for (int c = 0; c < CW; c++) bv[c] = (b0 && c < ncol) ? b0[so + c * ostride] : 0.f;
+                for (int c = 0; c < CW; c++)
+                    vv[c] = (rowok && c < ncol) ? *reinterpret_cast<const float*>(self + c * 128 + soff[c & 7]) : 0.f;
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&accE[b]);
+            if (rowok) {
 #pragma unroll
                 for (int c = 0; c < CW; c++) {
                     if (c < ncol) {
-                        const float v = *reinterpret_cast<const float*>(self + c * 128 + soff[c & 7]);
-                        float w = mm * v + acc[c];
+                        float w = mm * vv[c] + acc[c];
                         if (b0) w = bv[c] - w;
                         dst0[so + c * ostride] = w;
                     }
                 }
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&accE[b]);
         }
     }
     __syncthreads();
