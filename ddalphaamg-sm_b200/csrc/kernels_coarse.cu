@@ -274,8 +274,58 @@ __global__ void __launch_bounds__(256) orthonormalize_kernel(Geom g, double2* __
         tv[(long)cc * g.size() + gidx(e)] = sm[q];
     }
 }
+// The same for aggregates of at most 32 unknowns per spin (level 0: 16 sites of one colour): one warp per
+// (aggregate, spin), one unknown per lane, the warp's vectors in its own slice of shared memory and warp
+// sums instead of CTA barriers.  With one unknown per lane the CTA version's block_sum reduces to the same
+// warp butterfly (the other warps add exact zeros), so the results are bit for bit those of
+// orthonormalize_kernel.
+constexpr int kOrthWarps = 8;
+__global__ void __launch_bounds__(32 * kOrthWarps) orthonormalize_warp_kernel(Geom g, double2* __restrict__ tv) {
+    extern __shared__ double2 sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int task = blockIdx.x * kOrthWarps + warp;
+    if (task >= 2 * g.agg_x * g.agg_t) return;  // whole warps; no CTA barrier follows
+    const int b = task >> 1, s = task & 1;
+    const int bx = b / g.agg_t, bt = b - bx * g.agg_t;
+    const int C = g.colors, E = g.el_x * g.el_t * C, Nv = g.ntest;
+    const bool own = lane < E;
+    long gi = 0;
+    if (own) {
+        const int k = lane / C, c = lane - k * C;
+        const int kx = k / g.el_t, kt = k - kx * g.el_t;
+        gi = ((long)(bx * g.el_x + kx) * g.Nt + bt * g.el_t + kt) * g.dof + c * 2 + s;
+    }
+    double2* v = sm + (size_t)warp * Nv * 32;  // v[cc * 32 + lane]: only this lane's column is touched
+    for (int cc = 0; cc < Nv; cc++) v[cc * 32 + lane] = own ? tv[(long)cc * g.size() + gi] : make_double2(0.0, 0.0);
+    for (int nt = 0; nt < Nv; nt++) {
+        double2 w = v[nt * 32 + lane];
+        for (int ntt = 0; ntt < nt; ntt++) {
+            const double2 u = v[ntt * 32 + lane];
+            double2 p = make_double2(0.0, 0.0);
+            if (own) p = cfmac(u, w, p);  // w * conj(u)
+            p = warp_sum(p);
+            if (own) w = w - cmul(p, u);
+        }
+        double nr = 0.0;
+        if (own) nr += cnorm2(w);
+        const double nrm = sqrt(warp_sum(make_double2(nr, 0.0)).x);
+        if (nrm > 1e-8 && own) w = make_double2(w.x / nrm, w.y / nrm);
+        v[nt * 32 + lane] = w;
+    }
+    if (own)
+        for (int cc = 0; cc < Nv; cc++) tv[(long)cc * g.size() + gi] = v[cc * 32 + lane];
+}
+
 void launch_orthonormalize(cudaStream_t s, const Geom& g, double2* tv) {
     const int E = g.el_x * g.el_t * g.colors;
+    if (E <= 32) {
+        const size_t smem = sizeof(double2) * (size_t)kOrthWarps * g.ntest * 32;
+        DDAMG_CUDA_TRY(cudaFuncSetAttribute(orthonormalize_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+        const int tasks = 2 * g.agg_x * g.agg_t;
+        DDAMG_LAUNCH(orthonormalize_warp_kernel, (tasks + kOrthWarps - 1) / kOrthWarps, 32 * kOrthWarps, smem, s, g, tv);
+        return;
+    }
     size_t smem = sizeof(double2) * (size_t)g.ntest * E;
     DDAMG_CUDA_TRY(cudaFuncSetAttribute(orthonormalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     DDAMG_LAUNCH(orthonormalize_kernel, 2 * g.agg_x * g.agg_t, 256, smem, s, g, tv);
@@ -315,6 +365,7 @@ __global__ void __launch_bounds__(256) build_links_kernel(Geom g, const double2*
     double2* Wn = acc + 5 * dc * dc;       // [df][Nv]
     double2* Wm = Wn + df * Nv;            // [df][Nv]
     double2* T = Wm + df * Nv;             // [df][dc]
+    double2* Fs = T + df * dc;             // [df][df]: the hop's link matrix (levels >= 1)
     const int b = blockIdx.x;
     const int bx = b / g.agg_t, bt = b - bx * g.agg_t;
     for (int q = threadIdx.x; q < 5 * dc * dc; q += blockDim.x) acc[q] = make_double2(0.0, 0.0);
@@ -341,6 +392,10 @@ __global__ void __launch_bounds__(256) build_links_kernel(Geom g, const double2*
                 const int rr = q / Nv, s = q - rr * Nv;
                 Wm[q] = tv[(long)s * g.size() + (long)m * df + rr];
             }
+            if (g.level > 0) {  // every T entry reads C values of the link: stage it once
+                const double2* F = links + ((long)n * 5 + h) * df * df;
+                for (int q = threadIdx.x; q < df * df; q += blockDim.x) Fs[q] = F[q];
+            }
             __syncthreads();
             // T[(c,alf)][(s,bet)] = sum_b' F_h(n)[(c,alf)][(b',bet)] w_s(m)[b'][bet]
             for (int q = threadIdx.x; q < df * dc; q += blockDim.x) {
@@ -350,10 +405,9 @@ __global__ void __launch_bounds__(256) build_links_kernel(Geom g, const double2*
                 if (g.level == 0) {
                     a = cmul(level0_link(U, g.Nx, g.Nt, n, h, rr, bet), Wm[bet * Nv + s]);
                 } else {
-                    const double2* F = links + ((long)n * 5 + h) * df * df;
                     for (int bb = 0; bb < C; bb++) {
                         const int jj = bb * 2 + bet;
-                        a = cfma(F[(long)jj * df + rr], Wm[jj * Nv + s], a);
+                        a = cfma(Fs[jj * df + rr], Wm[jj * Nv + s], a);
                     }
                 }
                 T[q] = a;
@@ -377,10 +431,76 @@ __global__ void __launch_bounds__(256) build_links_kernel(Geom g, const double2*
         next[(long)b * 5 * dc * dc + q] = acc[d * dc * dc + i * dc + j];
     }
 }
+// Level 0 (dof 2, one colour): the same sums with all operands staged once per aggregate.  The
+// per-hop loop above is latency bound there (four tiny hops per fine site, three barriers and a global
+// round trip each); here the aggregate's test vectors with a one-site halo and its hop matrices come
+// into shared memory together, and every thread then forms whole entries of the coarse links, each
+// summing its (site, hop) terms in the order of the loop above, so the result is bit for bit the same.
+__global__ void __launch_bounds__(256) build_links_l0_kernel(Geom g, const double2* __restrict__ U,
+                                                             const double2* __restrict__ tv,
+                                                             double2* __restrict__ next) {
+    extern __shared__ double2 sm[];
+    const int Nv = g.ntest, dc = 2 * Nv, ex = g.el_x, et = g.el_t, K = ex * et;
+    const int hx = ex + 2, ht = et + 2;  // halo box of the aggregate
+    double2* Wh = sm;                    // [hx * ht][2][Nv]: w_p(site)[alf]
+    double2* F = Wh + (size_t)hx * ht * 2 * Nv;  // [K][5][2][2]: F_h(n_k)[alf][bet]
+    const int b = blockIdx.x;
+    const int bx = b / g.agg_t, bt = b - bx * g.agg_t;
+    for (int q = threadIdx.x; q < hx * ht * 2 * Nv; q += blockDim.x) {
+        const int site = q / (2 * Nv), r = q - site * 2 * Nv, alf = r / Nv, p = r - alf * Nv;
+        const int lx = site / ht - 1, lt = site % ht - 1;
+        int x = bx * ex + lx, t = bt * et + lt;
+        x = x < 0 ? x + g.Nx : (x >= g.Nx ? x - g.Nx : x);
+        t = t < 0 ? t + g.Nt : (t >= g.Nt ? t - g.Nt : t);
+        Wh[q] = tv[(long)p * g.size() + ((long)x * g.Nt + t) * 2 + alf];
+    }
+    for (int q = threadIdx.x; q < K * 16; q += blockDim.x) {
+        const int k = q / 16, h = 1 + (q / 4) % 4, alf = (q / 2) % 2, bet = q % 2;
+        const int kx = k / et, kt = k - kx * et;
+        const int n = (bx * ex + kx) * g.Nt + bt * et + kt;
+        F[((size_t)k * 5 + h) * 4 + alf * 2 + bet] = level0_link(U, g.Nx, g.Nt, n, h, alf, bet);
+    }
+    __syncthreads();
+    const int dd = dc * dc;
+    for (int q = threadIdx.x; q < 5 * dd; q += blockDim.x) {
+        const int D = q / dd, rem = q - D * dd, i = rem / dc, j = rem - i * dc;  // entry (i, j) of D
+        const int p = i >> 1, alf = i & 1, s = j >> 1, bet = j & 1;
+        double2 a = make_double2(0.0, 0.0);
+        // the (site, hop) pairs whose hop lands in D, in the loop order above (sites, then hops 1-4);
+        // a hop leaves the aggregate only from its edge, so D > 0 visits one row or column of sites
+        for (int kx = 0; kx < ex; kx++) {
+            if ((D == 2 && kx != ex - 1) || (D == 4 && kx != 0)) continue;
+            for (int kt = 0; kt < et; kt++) {
+                if ((D == 1 && kt != et - 1) || (D == 3 && kt != 0)) continue;
+                const int k = kx * et + kt;
+                const double2 wn = Wh[((size_t)(kx + 1) * ht + (kt + 1)) * 2 * Nv + alf * Nv + p];
+#pragma unroll
+                for (int h = 1; h < 5; h++) {
+                    const bool inside = h == 1 ? kt + 1 < et : h == 2 ? kx + 1 < ex : h == 3 ? kt > 0 : kx > 0;
+                    if ((inside ? 0 : h) != D) continue;
+                    const int mx = kx + (h == 2) - (h == 4), mt = kt + (h == 1) - (h == 3);
+                    const double2 wm = Wh[((size_t)(mx + 1) * ht + (mt + 1)) * 2 * Nv + bet * Nv + s];
+                    const double2 t = cmul(F[((size_t)k * 5 + h) * 4 + alf * 2 + bet], wm);
+                    a = cfmac(wn, t, a);
+                }
+            }
+        }
+        next[(long)b * 5 * dd + D * dd + j * dc + i] = a;  // [site][d][j][i]
+    }
+}
+
 void launch_build_coarse_links(cudaStream_t s, const Geom& g, const double2* U, const double2* links,
                                const double2* tv, double2* next_links) {
     const int df = g.dof, dc = 2 * g.ntest;
-    size_t smem = sizeof(double2) * ((size_t)5 * dc * dc + 2 * (size_t)df * g.ntest + (size_t)df * dc);
+    if (g.level == 0 && g.dof == 2) {
+        const int K = g.el_x * g.el_t;
+        const size_t smem = sizeof(double2) * ((size_t)(g.el_x + 2) * (g.el_t + 2) * 2 * g.ntest + (size_t)K * 20);
+        DDAMG_CUDA_TRY(
+            cudaFuncSetAttribute(build_links_l0_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        DDAMG_LAUNCH(build_links_l0_kernel, g.agg_x * g.agg_t, 256, smem, s, g, U, tv, next_links);
+        return;
+    }
+    size_t smem = sizeof(double2) * ((size_t)5 * dc * dc + 2 * (size_t)df * g.ntest + (size_t)df * dc + (size_t)df * df);
     DDAMG_CUDA_TRY(cudaFuncSetAttribute(build_links_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     DDAMG_LAUNCH(build_links_kernel, g.agg_x * g.agg_t, 256, smem, s, g, U, links, tv, next_links);
 }
