@@ -824,6 +824,8 @@ def profile_case(name):
     tc-apply one batched FP32 level-1 SAP sweep pair on 512x512 with 64 right-hand sides
              (tc_block_apply_kernel, the tensor-core block operator);
     krylov   20 BiCGstab iterations on a 1024x1024 field (bicg_* kernels, 11 fields of 32 MiB);
+    tc-op    the batched FP32 level-1 operator on 512x512 with 64 right-hand sides on tensor cores
+             (tc_coarse_op_kernel: 328 MB of operator tiles, 67 MB of vectors in and out);
     dw       D_W and D_W^dagger on the 2048x2048 bandwidth lattice, FP64 then FP32, register kernels then
              the staged-tile kernel (wilson_kernel, wilson_pair_kernel, wilson_stage_kernel; 128 MiB per
              FP64 field)."""
@@ -849,6 +851,25 @@ def profile_case(name):
         torch.cuda.synchronize()
         print(f"dw: 16 applications (register then staged kernels; FP64 D, D^dagger, FP32 D, D^dagger; 2 each) on "
               f"{N}x{N}")
+        s.close()
+        return 0
+    if name == "tc-op":
+        import torch
+
+        N, R = 512, 64
+        th, _ = ddamg.gauge_metropolis(N, N, 3.0, 200, 512)
+        p = ddamg.default_params(N, N, 3, -0.10, [[0, 64, 64, 16, 64, 64], [1, 16, 16, 16, 16, 16]],
+                                 precision=ddamg.PREC_MIXED, max_rhs=R, tensor_cores=2)
+        s = ddamg.Solver(p)
+        s.load_gauge(np.exp(1j * th))
+        s.setUpPhase(seed=3)
+        n1 = s.size(1)
+        x = torch.randn(R * n1 * 2, dtype=torch.float32, device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(2):  # the first call tunes the tile shape
+            ddamg.check(s.L.ddamg_apply_level_op_device(s.h, 1, 1, x.data_ptr(), y.data_ptr(), R))
+        torch.cuda.synchronize()
+        print("tc-op:", [l for l in s.autotune_report().splitlines() if "level operator" in l])
         s.close()
         return 0
     if name == "krylov":
@@ -908,7 +929,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the 1024x1024 and 512x512 batched lines")
-    ap.add_argument("--profile-case", choices=["sap-l1", "tc-apply", "krylov", "dw"],
+    ap.add_argument("--profile-case", choices=["sap-l1", "tc-apply", "krylov", "dw", "tc-op"],
                     help="run one small case of a hot kernel for an ncu capture and exit")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
