@@ -97,6 +97,7 @@ struct SapArgs {
     const int* blocks;  // block indices of this colour
     int nblocks;
     const int* done;    // per-rhs skip flags (may be null)
+    const void* vres = nullptr;  // coarse sweeps of sap_block2_kernel: form r_B = v_B - (D x)_B from this v
 };
 template <typename V>
 void launch_sap_sweep_fine(cudaStream_t s, const Geom& g, const V* U, const V* r, V* x, const SapArgs& a,

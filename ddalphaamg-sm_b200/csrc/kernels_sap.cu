@@ -1171,6 +1171,7 @@ static void launch_sap(cudaStream_t s, const Geom& g, const V* L, const V* r, V*
     const int threads = std::min(1024, ((NE + 31) / 32) * 32);
     const int ept = (NE + threads - 1) / threads;
     SapKParams p{a.m, a.restarts, a.tol, a.m0, a.blocks, a.nblocks, a.done, nrhs, 1};
+    p.vres = a.vres;
     // level 0 keeps one vector per CTA: its links are 32 B per site, so there is nothing to share,
     // and a wider CTA would only cost shared memory and occupancy
     int rb = DENSE ? pick_rb(nrhs, ept, a.m, NE, threads, sizeof(V)) : 1, kern = 0;
@@ -1178,6 +1179,8 @@ static void launch_sap(cudaStream_t s, const Geom& g, const V* L, const V* r, V*
         rb = variant / 4;
         kern = variant % 4;
     }
+    if (a.vres && !(DENSE && kern == 1))
+        throw ParamFailure{"internal: a fused-residual sweep needs the sap_block2_kernel variant"};
     if (DENSE && kern == 1) {
         if (rb == 4) launch_sap2<V, 4>(s, g, L, r, x, p);
         else if (rb == 2) launch_sap2<V, 2>(s, g, L, r, x, p);
@@ -1216,6 +1219,7 @@ template <typename V>
 void launch_sap_sweep_fine(cudaStream_t s, const Geom& g, const V* U, const V* r, V* x, const SapArgs& a, int nrhs) {
     const int S = g.sel_x * g.sel_t;
     if (a.m > kSapMaxM) throw ParamFailure{"SAP block GMRES restart length above 8 is not supported"};
+    if (a.vres) throw ParamFailure{"internal: the level-0 sweeps read the residual"};
     SapKParams p{a.m, a.restarts, a.tol, a.m0, a.blocks, a.nblocks, a.done, nrhs, 1};
     if (a.m == 5 && S <= 16) launch_fine_pair<V, 5>(s, g, U, r, x, p);
     else if (a.m == 5 && S <= 32) launch_fine_reg<V, 1, 5>(s, g, U, r, x, p);

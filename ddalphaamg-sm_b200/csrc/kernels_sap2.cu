@@ -184,11 +184,60 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
     }
     const int dd2 = dof * dof;
     V b[RB], x[RB], w[RB];
+    const V* __restrict__ vres = static_cast<const V*>(p.vres);
+    if (!vres) {
 #pragma unroll
-    for (int r = 0; r < RB; r++) {
-        b[r] = (ev && act[r]) ? rg[(long)(r0 + r) * g.size() + (long)n * dof + i] : czero<V>();
-        x[r] = b[r];
+        for (int r = 0; r < RB; r++) b[r] = (ev && act[r]) ? rg[(long)(r0 + r) * g.size() + (long)n * dof + i] : czero<V>();
+    } else {
+        // r_B = v - D x on this block's sites, all five hops, each link element loaded once for the CTA's
+        // right-hand sides (the iterate of the other colour's blocks is final: the previous sweep has
+        // finished); Level::D_operator (src/level.cpp:394-426) restricted to the block's sites
+        V acc[RB];
+#pragma unroll
+        for (int r = 0; r < RB; r++) acc[r] = czero<V>();
+        if (ev) {
+            const int gx = bx * ex + kx, gt = bt * et + kt;
+#pragma unroll 1
+            for (int d = 0; d < 5; d++) {
+                int nb = n;
+                R sg = R(1);
+                if (d == 1) {
+                    nb = gx * g.Nt + (gt + 1 == g.Nt ? 0 : gt + 1);
+                    if (gt == g.Nt - 1) sg = R(-1);
+                } else if (d == 2) {
+                    nb = (gx + 1 == g.Nx ? 0 : gx + 1) * g.Nt + gt;
+                } else if (d == 3) {
+                    nb = gx * g.Nt + (gt == 0 ? g.Nt - 1 : gt - 1);
+                    if (gt == 0) sg = R(-1);
+                } else if (d == 4) {
+                    nb = (gx == 0 ? g.Nx - 1 : gx - 1) * g.Nt + gt;
+                }
+                const V* Mt = L + ((long)n * 5 + d) * dd2 + i;
+                const V* xn = xg + (long)r0 * g.size() + (long)nb * dof;
+                V ae[RB], ao[RB];  // even and odd columns: two independent chains per right-hand side
+#pragma unroll
+                for (int r = 0; r < RB; r++) ae[r] = ao[r] = czero<V>();
+                for (int j = 0; j < dof; j += 2) {  // dof is even
+                    const V m0 = __ldg(Mt + (long)j * dof), m1 = __ldg(Mt + (long)(j + 1) * dof);
+#pragma unroll
+                    for (int r = 0; r < RB; r++) {
+                        if (r0 + r >= p.nrhs) break;  // the CTA's last group may be partial
+                        ae[r] = cfma(m0, xn[(long)r * g.size() + j], ae[r]);
+                        ao[r] = cfma(m1, xn[(long)r * g.size() + j + 1], ao[r]);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < RB; r++) acc[r] = acc[r] + sg * (ae[r] + ao[r]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RB; r++) {
+            const long o = (long)(r0 + r) * g.size() + (long)n * dof + i;
+            b[r] = (ev && act[r]) ? vres[o] - (mm * xg[o] - acc[r]) : czero<V>();
+        }
     }
+#pragma unroll
+    for (int r = 0; r < RB; r++) x[r] = b[r];
 
     // w = D_B op for the RB vectors op[r * NE + .]; fill: keep the cached matrices while loading them
     auto apply = [&](const V* op, bool fill) {

@@ -24,6 +24,9 @@ struct SapKParams {
     const int* done;
     int nrhs;     // vectors in the sweep
     int ngroups;  // CTAs per Schwarz block: ceil(nrhs / RB)
+    // non-null: the sweep forms each block's residual r_B = v_B - (D x)_B itself from the SAP right-hand
+    // side v (this pointer, the sweep's vector type) and the iterate, instead of reading r
+    const void* vres = nullptr;
 };
 
 // the latency-trimmed coarse sweep (kernels_sap2.cu): blocks of at most 512 unknowns at restart length 5

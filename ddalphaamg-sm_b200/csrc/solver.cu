@@ -588,6 +588,12 @@ template <typename V> static int rb_for(ddamg_handle* h, int l, const V* r, cons
 // SAP_C::SAP (src/sap.cpp:81-165) on nrhs independent vectors; returns the reference's value
 // for rhs 0 when want_iters (one host sync), else nu.  lay: a fine-level block layout other than the
 // level's; allow_tc: batched FP32 coarse sweeps may use the tensor-core block operator.
+// A black sweep may form its blocks' residuals from the iterate only if no two blocks of one colour
+// touch: every block count is even (checkerboard across the periodic wrap) or 1 (the block is its own
+// neighbour across the wrap, and reads the iterate before it updates it)
+static bool fusable_residual(const Geom& g) {
+    return (g.sap_x == 1 || g.sap_x % 2 == 0) && (g.sap_t == 1 || g.sap_t % 2 == 0);
+}
 template <typename V>
 static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, bool x_zero, int nrhs, bool want_iters,
                  const SapLayout* lay = nullptr, bool allow_tc = true) {
@@ -602,21 +608,34 @@ static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, b
     else level_op<V>(h, l, x, r, v, nrhs, allow_tc);  // r = v - D x
     SapArgs a{h->p.sap_gmres_restart_length, h->p.sap_gmres_restarts, h->p.sap_gmres_tolerance, h->p.m0, nullptr, 0,
               D.done};
+    const bool tc = std::is_same<V, float2>::value && D.tc && allow_tc && nrhs >= kTcMinRhs;
     for (int it = 0; it < nu; it++) {
+        bool fused = false;  // this iteration's black sweep forms its blocks' residuals itself
         for (int colour = 0; colour < 2; colour++) {
             a.blocks = colour == 0 ? (lay ? lay->red : D.red) : (lay ? lay->black : D.black);
             a.nblocks = colour == 0 ? (lay ? lay->nred : D.nred) : (lay ? lay->nblack : D.nblack);
+            a.vres = (colour == 1 && fused) ? static_cast<const void*>(v) : nullptr;
+            int var = 0;
             {
                 ProfScope ps(h, 0, l);
                 if (l == 0) launch_sap_sweep_fine<V>(h->s, g, B<V>(D).U, r, x, a, nrhs);
-                else if (std::is_same<V, float2>::value && D.tc && allow_tc && nrhs >= kTcMinRhs)
+                else if (tc)
                     launch_sap_sweep_tc(h->s, g, D.tcw, reinterpret_cast<const float2*>(r),
                                         reinterpret_cast<float2*>(x), a, nrhs,
                                         tc_shape_for(h, l, reinterpret_cast<const float2*>(r), a, nrhs));
-                else launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs, rb_for<V>(h, l, r, a, nrhs));
+                else {
+                    var = rb_for<V>(h, l, r, a, nrhs);
+                    launch_sap_sweep_coarse<V>(h->s, g, B<V>(D).links, r, x, a, nrhs, var);
+                }
             }
-            // the residual after the last black sweep only feeds the convergence test
+            // the residual after the last black sweep only feeds the convergence test; the one after a
+            // red sweep is left to the black sweep where sap_block2_kernel runs it (each block forms its
+            // own r_B = v_B - (D x)_B, so the global operator application is saved)
             const bool last = (colour == 1 && it == nu - 1);
+            if (colour == 0 && l > 0 && !lay && var % 4 == 1 && fusable_residual(g)) {
+                fused = true;
+                continue;
+            }
             if (!last || (check && want_iters)) level_op<V>(h, l, x, r, v, nrhs, allow_tc);
         }
         if (check && (it < nu - 1 || want_iters)) {
@@ -1290,11 +1309,14 @@ static bool sap_setup_split(ddamg_handle* h, int l, const V* v, V* x, int nu, in
         const long off = (long)k * rb * n;
         SapArgs ak = a;
         ak.done = D.done + k * rb;
+        const bool fuse = var % 4 == 1 && fusable_residual(g);
         for (int it = 0; it < nu; it++)
             for (int colour = 0; colour < 2; colour++) {
                 ak.blocks = colour == 0 ? D.red : D.black;
                 ak.nblocks = colour == 0 ? D.nred : D.nblack;
+                ak.vres = (colour == 1 && fuse) ? static_cast<const void*>(v + off) : nullptr;
                 launch_sap_sweep_coarse<V>(st, g, B<V>(D).links, r + off, x + off, ak, rb, var);
+                if (colour == 0 && fuse) continue;  // the black sweep forms its blocks' residuals
                 if (!(colour == 1 && it == nu - 1))
                     launch_coarse_op<V>(st, B<V>(D).links, x + off, r + off, v + off, g.Nx, g.Nt, g.dof, h->p.m0, rb);
             }
