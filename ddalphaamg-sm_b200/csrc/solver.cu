@@ -604,17 +604,25 @@ static int sap_t(ddamg_handle* h, int l, const V* v, V* x, int nu, double tol, b
     DDAMG_CUDA_TRY(cudaMemsetAsync(D.done, 0, sizeof(int) * nrhs, h->s));
     const bool check = tol > 0.0;
     if (check) launch_norm2<V>(h->s, v, n, n, nrhs, h->dpart, D.vv);
+    const bool tc = std::is_same<V, float2>::value && D.tc && allow_tc && nrhs >= kTcMinRhs;
+    // with the sweep variant already tuned, the first red sweep also forms its blocks' residuals itself
+    // (r = v - D x is read only there); the first use tunes on the global residual
+    bool fuse0 = false;
+    if (!x_zero && l > 0 && !lay && !tc && fusable_residual(g)) {
+        auto itv = D.rb_choice.find(nrhs * 2 + (std::is_same<V, float2>::value ? 1 : 0));
+        fuse0 = itv != D.rb_choice.end() && itv->second % 4 == 1;
+    }
     if (x_zero) DDAMG_CUDA_TRY(cudaMemcpyAsync(r, v, sizeof(V) * n * nrhs, cudaMemcpyDeviceToDevice, h->s));
-    else level_op<V>(h, l, x, r, v, nrhs, allow_tc);  // r = v - D x
+    else if (!fuse0) level_op<V>(h, l, x, r, v, nrhs, allow_tc);  // r = v - D x
     SapArgs a{h->p.sap_gmres_restart_length, h->p.sap_gmres_restarts, h->p.sap_gmres_tolerance, h->p.m0, nullptr, 0,
               D.done};
-    const bool tc = std::is_same<V, float2>::value && D.tc && allow_tc && nrhs >= kTcMinRhs;
     for (int it = 0; it < nu; it++) {
         bool fused = false;  // this iteration's black sweep forms its blocks' residuals itself
         for (int colour = 0; colour < 2; colour++) {
             a.blocks = colour == 0 ? (lay ? lay->red : D.red) : (lay ? lay->black : D.black);
             a.nblocks = colour == 0 ? (lay ? lay->nred : D.nred) : (lay ? lay->nblack : D.nblack);
-            a.vres = (colour == 1 && fused) ? static_cast<const void*>(v) : nullptr;
+            a.vres = ((colour == 1 && fused) || (colour == 0 && it == 0 && fuse0)) ? static_cast<const void*>(v)
+                                                                                 : nullptr;
             int var = 0;
             {
                 ProfScope ps(h, 0, l);
@@ -1276,7 +1284,11 @@ static bool sap_setup_split(ddamg_handle* h, int l, const V* v, V* x, int nu, in
     SapArgs a{h->p.sap_gmres_restart_length, h->p.sap_gmres_restarts, h->p.sap_gmres_tolerance, h->p.m0, D.red,
               D.nred, D.done};
     DDAMG_CUDA_TRY(cudaMemsetAsync(D.done, 0, sizeof(int) * nrhs, h->s));
-    level_op<V>(h, l, x, r, v, nrhs, false);  // r = v - D x for every vector (CUDA cores: test-vector quality)
+    // r = v - D x for every vector (CUDA cores: test-vector quality); once the sweep variant is tuned, the
+    // groups' first red sweeps form it themselves where the residual can be fused
+    const int rkey = nrhs * 2 + (std::is_same<V, float2>::value ? 1 : 0);
+    const bool pre_fuse = D.rb_choice.count(rkey) != 0 && D.rb_choice[rkey] % 4 == 1 && fusable_residual(g);
+    if (!pre_fuse) level_op<V>(h, l, x, r, v, nrhs, false);
     const int var = rb_for<V>(h, l, r, a, nrhs);  // tuned on first use on red sweeps (times into scratch, syncs)
     const int rb = var / 4;
     const int G = nrhs / rb;
@@ -1285,6 +1297,7 @@ static bool sap_setup_split(ddamg_handle* h, int l, const V* v, V* x, int nu, in
     // one colour's links fit in L2 (128x128 sites at dof 32, 671 MB per colour, lost 38 % of its setup)
     const double colour_link_bytes = 0.5 * (double)g.sites * 5 * g.dof * g.dof * sizeof(V);
     if (G < 2 || G * rb != nrhs || colour_link_bytes > 100e6) {  // one stream: the plain sweep loop
+        if (pre_fuse) level_op<V>(h, l, x, r, v, nrhs, false);
         for (int it = 0; it < nu; it++)
             for (int colour = 0; colour < 2; colour++) {
                 a.blocks = colour == 0 ? D.red : D.black;
@@ -1314,7 +1327,9 @@ static bool sap_setup_split(ddamg_handle* h, int l, const V* v, V* x, int nu, in
             for (int colour = 0; colour < 2; colour++) {
                 ak.blocks = colour == 0 ? D.red : D.black;
                 ak.nblocks = colour == 0 ? D.nred : D.nblack;
-                ak.vres = (colour == 1 && fuse) ? static_cast<const void*>(v + off) : nullptr;
+                ak.vres = ((colour == 1 && fuse) || (colour == 0 && it == 0 && pre_fuse))
+                              ? static_cast<const void*>(v + off)
+                              : nullptr;
                 launch_sap_sweep_coarse<V>(st, g, B<V>(D).links, r + off, x + off, ak, rb, var);
                 if (colour == 0 && fuse) continue;  // the black sweep forms its blocks' residuals
                 if (!(colour == 1 && it == nu - 1))
