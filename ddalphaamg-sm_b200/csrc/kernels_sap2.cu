@@ -191,39 +191,75 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
     } else {
         // r_B = v - D x on this block's sites, all five hops, each link element loaded once for the CTA's
         // right-hand sides (the iterate of the other colour's blocks is final: the previous sweep has
-        // finished); Level::D_operator (src/level.cpp:394-426) restricted to the block's sites
+        // finished); Level::D_operator (src/level.cpp:394-426) restricted to the block's sites.
+        // The iterate at the five neighbours of every block site is staged first in the Krylov basis's
+        // space (unused until the first restart; 5 <= M + 1 vectors per rhs), with independent coalesced
+        // loads, so the link chains below wait on link loads only (several in flight), not on one operand
+        // round trip per column pair.
+        V* const stg = sm.basis;  // [d][r][NE]: x_{r0+r} at site nbr_d(k), entry j, at (d * RB + r) * NE + k * dof + j
+        for (int q = threadIdx.x; q < 5 * RB * NE; q += blockDim.x) {
+            const int d = q / (RB * NE), rem = q - d * RB * NE, r = rem / NE, el = rem - r * NE;
+            const int kq = el / dof, jq = el - kq * dof, qkx = kq / et;
+            const int qx = bx * ex + qkx, qt = bt * et + (kq - qkx * et);
+            int nb = qx * g.Nt + qt;
+            if (d == 1) nb = qx * g.Nt + (qt + 1 == g.Nt ? 0 : qt + 1);
+            else if (d == 2) nb = (qx + 1 == g.Nx ? 0 : qx + 1) * g.Nt + qt;
+            else if (d == 3) nb = qx * g.Nt + (qt == 0 ? g.Nt - 1 : qt - 1);
+            else if (d == 4) nb = (qx == 0 ? g.Nx - 1 : qx - 1) * g.Nt + qt;
+            stg[q] = (r0 + r < p.nrhs) ? xg[(long)(r0 + r) * g.size() + (long)nb * dof + jq] : czero<V>();
+        }
+        __syncthreads();
         V acc[RB];
 #pragma unroll
         for (int r = 0; r < RB; r++) acc[r] = czero<V>();
         if (ev) {
-            const int gx = bx * ex + kx, gt = bt * et + kt;
+            const int gt = bt * et + kt;
 #pragma unroll 1
             for (int d = 0; d < 5; d++) {
-                int nb = n;
-                R sg = R(1);
-                if (d == 1) {
-                    nb = gx * g.Nt + (gt + 1 == g.Nt ? 0 : gt + 1);
-                    if (gt == g.Nt - 1) sg = R(-1);
-                } else if (d == 2) {
-                    nb = (gx + 1 == g.Nx ? 0 : gx + 1) * g.Nt + gt;
-                } else if (d == 3) {
-                    nb = gx * g.Nt + (gt == 0 ? g.Nt - 1 : gt - 1);
-                    if (gt == 0) sg = R(-1);
-                } else if (d == 4) {
-                    nb = (gx == 0 ? g.Nx - 1 : gx - 1) * g.Nt + gt;
-                }
+                const R sg = ((d == 1 && gt == g.Nt - 1) || (d == 3 && gt == 0)) ? R(-1) : R(1);
                 const V* Mt = L + ((long)n * 5 + d) * dd2 + i;
-                const V* xn = xg + (long)r0 * g.size() + (long)nb * dof;
+                const V* xs = stg + (size_t)d * RB * NE + (size_t)k * dof;
+                // an in-block hop with a cache slot is kept on the way, so the first application reads it
+                // from shared memory
+                int nbd = nbk[0], csd = cslot[0];  // selects, not a dynamic index (which would put the
+#pragma unroll                                     // arrays in local memory)
+                for (int h = 1; h < 5; h++)
+                    if (h == d) {
+                        nbd = nbk[h];
+                        csd = cslot[h];
+                    }
+                const bool keep = nbd >= 0 && csd < ncache;
+                V* Mc = sm.cache + (size_t)csd * dd2 + i;
                 V ae[RB], ao[RB];  // even and odd columns: two independent chains per right-hand side
 #pragma unroll
                 for (int r = 0; r < RB; r++) ae[r] = ao[r] = czero<V>();
-                for (int j = 0; j < dof; j += 2) {  // dof is even
+                constexpr int RCH = CH;  // link loads in flight (even)
+                int j = 0;
+                for (; j + RCH <= dof; j += RCH) {
+                    V mv[RCH];
+#pragma unroll
+                    for (int u = 0; u < RCH; u++) mv[u] = __ldg(Mt + (long)(j + u) * dof);
+                    if (keep)
+#pragma unroll
+                        for (int u = 0; u < RCH; u++) Mc[(size_t)(j + u) * dof] = mv[u];
+#pragma unroll
+                    for (int u = 0; u < RCH; u += 2)
+#pragma unroll
+                        for (int r = 0; r < RB; r++) {
+                            ae[r] = cfma(mv[u], xs[(size_t)r * NE + j + u], ae[r]);
+                            ao[r] = cfma(mv[u + 1], xs[(size_t)r * NE + j + u + 1], ao[r]);
+                        }
+                }
+                for (; j < dof; j += 2) {  // dof is even
                     const V m0 = __ldg(Mt + (long)j * dof), m1 = __ldg(Mt + (long)(j + 1) * dof);
+                    if (keep) {
+                        Mc[(size_t)j * dof] = m0;
+                        Mc[(size_t)(j + 1) * dof] = m1;
+                    }
 #pragma unroll
                     for (int r = 0; r < RB; r++) {
-                        if (r0 + r >= p.nrhs) break;  // the CTA's last group may be partial
-                        ae[r] = cfma(m0, xn[(long)r * g.size() + j], ae[r]);
-                        ao[r] = cfma(m1, xn[(long)r * g.size() + j + 1], ao[r]);
+                        ae[r] = cfma(m0, xs[(size_t)r * NE + j], ae[r]);
+                        ao[r] = cfma(m1, xs[(size_t)r * NE + j + 1], ao[r]);
                     }
                 }
 #pragma unroll
@@ -300,12 +336,12 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
 #define SAP2_TOT(r, q) twp[(r) * KS + (q)]
     double2* const twp = sm.tw + (size_t)wid * SL;  // this warp's copy of the totals
 
-    // x = x0 = b; r = b - D_B x (this application fills the link cache)
+    // x = x0 = b; r = b - D_B x (this application fills the link cache, unless the fused residual did)
 #pragma unroll
     for (int r = 0; r < RB; r++)
         if (ev) sm.op[(size_t)r * NE + e] = x[r];
     __syncthreads();
-    apply(sm.op, true);
+    apply(sm.op, vres == nullptr);
     double norm_b[RB], err[RB];
     bool fin[RB];  // converged, inactive, or a zero right-hand side
     int maxIt[RB];
