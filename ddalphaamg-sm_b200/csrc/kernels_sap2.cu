@@ -328,8 +328,9 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
         for (int r = 0; r < RB; r++) w[r] = mm * op[(size_t)r * NE + e] - (acc[r][0] + acc[r][1]);
     };
     constexpr int NV = M + 1;  // values per rhs in a reduction: the dots and the new norm
-    // this warp's partial sums of all right-hand sides (sv[r][q]) into buffer rbuf
-#define SAP2_PARTIAL(val) warp_partials<RB, NV, KS>(val, sm.red + ((size_t)rbuf * nwe + wid) * SL)
+    // this warp's partial sums of values 0..nv-1 of all right-hand sides into buffer rbuf (the slots from
+    // nv on keep older sums, which the totals below never read)
+#define SAP2_PARTIAL(nv, val) warp_partials<RB, nv, KS>(val, sm.red + ((size_t)rbuf * nwe + wid) * SL)
     // CTA totals of slots 0..cnt of every rhs in buffer buf (every warp forms them itself); then
     // SAP2_TOT(r, q) is total q of rhs r
 #define SAP2_TOTALS(buf, cnt) cta_totals<RB, KS>(sm.red + (size_t)(buf) * nwe * SL, SL, nwe, cnt, twp)
@@ -347,8 +348,8 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
     int maxIt[RB];
 #pragma unroll
     for (int r = 0; r < RB; r++) w[r] = b[r] - w[r];
-    SAP2_PARTIAL([&](int r, int q) {  // ||b||^2, ||r||^2
-        return make_double2(ev && q < 2 ? (double)cnorm2(q == 0 ? b[r] : w[r]) : 0.0, 0.0);
+    SAP2_PARTIAL(2, [&](int r, int q) {  // ||b||^2, ||r||^2
+        return make_double2(ev ? (double)cnorm2(q == 0 ? b[r] : w[r]) : 0.0, 0.0);
     });
     __syncthreads();
     SAP2_TOTALS(rbuf, 2);
@@ -393,14 +394,24 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
             apply(sm.basis + (size_t)j * NE * RB, false);  // w = D_B V_j
             // classical Gram-Schmidt coefficients <w, V_i>, i <= j, and ||w||^2 (slot j + 1)
             // (selects on j, not a store at index j + 1, which would put the values in local memory)
-            SAP2_PARTIAL([&](int r, int q) {
-                double2 v = make_double2(0.0, 0.0);
-                if (arn[r] && ev) {
-                    if (q <= j) v = cfmac(to_d(sm.basis[((size_t)q * RB + r) * NE + e]), to_d(w[r]), v);
-                    v.x += (q == j + 1) ? (double)cnorm2(w[r]) : 0.0;
-                }
-                return v;
-            });
+            {
+                auto gs = [&](int r, int q) {
+                    double2 v = make_double2(0.0, 0.0);
+                    if (arn[r] && ev) {
+                        if (q <= j) v = cfmac(to_d(sm.basis[((size_t)q * RB + r) * NE + e]), to_d(w[r]), v);
+                        v.x += (q == j + 1) ? (double)cnorm2(w[r]) : 0.0;
+                    }
+                    return v;
+                };
+                // the j + 2 live values of each rhs packed densely: fewer warp-sum groups for early j (the
+                // sum of a value does not depend on its place in the group)
+                static_assert(M == 5, "the restart length of this kernel is 5");
+                if (j == 0) SAP2_PARTIAL(2, gs);
+                else if (j == 1) SAP2_PARTIAL(3, gs);
+                else if (j == 2) SAP2_PARTIAL(4, gs);
+                else if (j == 3) SAP2_PARTIAL(5, gs);
+                else SAP2_PARTIAL(6, gs);
+            }
             __syncthreads();  // partial sums visible
             const int dbuf = rbuf;
             rbuf ^= 1;
@@ -443,8 +454,8 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
                         if (q <= j) sm.ct[r * KS + q] = t[q];
             }
             if (reduce_norm) {
-                SAP2_PARTIAL([&](int r, int q) {
-                    return make_double2(arn[r] && ev && q == 0 ? (double)cnorm2(w[r]) : 0.0, 0.0);
+                SAP2_PARTIAL(1, [&](int r, int q) {
+                    return make_double2(arn[r] && ev ? (double)cnorm2(w[r]) : 0.0, 0.0);
                 });
                 __syncthreads();
                 SAP2_TOTALS(rbuf, 1);
@@ -553,7 +564,7 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
         apply(sm.op, false);
 #pragma unroll
         for (int r = 0; r < RB; r++) w[r] = b[r] - w[r];
-        SAP2_PARTIAL([&](int r, int q) { return make_double2(ev && q == 0 ? (double)cnorm2(w[r]) : 0.0, 0.0); });
+        SAP2_PARTIAL(1, [&](int r, int q) { return make_double2(ev ? (double)cnorm2(w[r]) : 0.0, 0.0); });
         __syncthreads();
         SAP2_TOTALS(rbuf, 1);
 #pragma unroll
