@@ -905,12 +905,15 @@ __global__ void __launch_bounds__(128, (sizeof(V) == 8 || SPL == 1) ? 4 : 1) sap
 // half-warp, so that no lane idles (one task per warp would leave lanes 16-31 without a site).  The
 // halves run the block GMRES in lockstep: each keeps its own Arnoldi / restart state, and the loops
 // continue while either half is still working; a half that has finished computes values it never uses.
-// Every reduction is a butterfly over the half (xor 8, 4, 2, 1).  The Arnoldi control is trimmed for
-// latency: ||w||^2 rides in the Gram-Schmidt butterfly and the new norm follows from
+// Every reduction is a butterfly over the half (xor 8, 4, 2, 1).  In FP64 the Arnoldi control is trimmed
+// for latency: ||w||^2 rides in the Gram-Schmidt butterfly and the new norm follows from
 // ||w - V h||^2 = ||w||^2 - sum |h_i|^2 (w is reduced again only where that cancels), the norm and the
 // Givens rotation use reciprocal square roots, the Hessenberg column is rotated in the lead lane's
 // registers, and the restart's triangular solve multiplies by reciprocal diagonal entries formed with the
-// rotation; the results agree with sap_fine_reg_kernel's to rounding.
+// rotation; the results agree with sap_fine_reg_kernel's to rounding.  FP32 blocks keep that kernel's
+// control (FP32 half-warp sums, square roots and divisions): with the trimmed control the smoothed test
+// vectors of a mixed-precision setup drifted from the FP64 ones (coarse operator 5.5e-3 apart instead of
+// about 1e-4).
 template <typename V, int M>
 __global__ void __launch_bounds__(128, 4) sap_fine_pair_kernel(Geom g, const V* __restrict__ U, const V* __restrict__ rg,
                                                               V* __restrict__ xg, SapKParams p, size_t tbytes) {
@@ -978,137 +981,231 @@ __global__ void __launch_bounds__(128, 4) sap_fine_pair_kernel(Geom g, const V* 
     };
     const int lead = lane & 16;  // the half's first lane
     V* const dinv = H + M * M;  // 1 / H[q][q] once column q is rotated (row M of H is not kept)
-    // ||w - V h||^2 = ||w||^2 - sum |h_i|^2 for an orthonormal V: ||w||^2 joins the Gram-Schmidt butterfly,
-    // and w is reduced again only where the difference cancels below this share of ||w||^2
-    constexpr double kCancel = sizeof(R) == 8 ? 1e-4 : 1e-2;
+    // FP64: ||w - V h||^2 = ||w||^2 - sum |h_i|^2 for an orthonormal V, so ||w||^2 joins the Gram-Schmidt
+    // butterfly and w is reduced again only where the difference cancels below this share of ||w||^2
+    constexpr double kCancel = 1e-4;
 
     apply(x);
 #pragma unroll
     for (int a = 0; a < 2; a++) w[a] = b[a] - w[a];
     const double norm_b = sqrt(nrm2(b));
     double err = sqrt(nrm2(w));
-    const double thr = p.tol * norm_b, thr2 = thr * thr;
     // a zero block right-hand side has the zero solution (the reference would divide by zero)
     bool fin = !valid || norm_b == 0.0;
     int maxIt = M;
-    for (int kr = 0; kr < p.restarts; kr++) {
-        const bool act = !fin;
-        if (!__any_sync(0xffffffffu, act)) break;
-        bool arn = act;
-        const R inv = R(act ? 1.0 / err : 0.0);
-#pragma unroll
-        for (int a = 0; a < 2; a++) Vb[0][a] = inv * w[a];
-        if (l16 == 0 && act) gm[0] = mkc(R(err), R(0));
-#pragma unroll
-        for (int j = 0; j < M; j++) {
-            if (!__any_sync(0xffffffffu, arn)) break;
-            apply(Vb[j]);
-            V h[M];
-#pragma unroll
-            for (int i = 0; i <= j; i++) {
-                V t = czero<V>();
-                if (sv)
-#pragma unroll
-                    for (int a = 0; a < 2; a++) t = cfmac(Vb[i][a], w[a], t);
-                h[i] = t;
-            }
-            R s2 = sv ? cnorm2(w[0]) + cnorm2(w[1]) : R(0);
-#pragma unroll
-            for (int o = 8; o > 0; o >>= 1) {
-#pragma unroll
+    if constexpr (sizeof(R) == 8) {
+        const double thr = p.tol * norm_b, thr2 = thr * thr;
+        for (int kr = 0; kr < p.restarts; kr++) {
+            const bool act = !fin;
+            if (!__any_sync(0xffffffffu, act)) break;
+            bool arn = act;
+            const R inv = R(act ? 1.0 / err : 0.0);
+    #pragma unroll
+            for (int a = 0; a < 2; a++) Vb[0][a] = inv * w[a];
+            if (l16 == 0 && act) gm[0] = mkc(R(err), R(0));
+    #pragma unroll
+            for (int j = 0; j < M; j++) {
+                if (!__any_sync(0xffffffffu, arn)) break;
+                apply(Vb[j]);
+                V h[M];
+    #pragma unroll
                 for (int i = 0; i <= j; i++) {
-                    h[i].x += __shfl_xor_sync(0xffffffffu, h[i].x, o);
-                    h[i].y += __shfl_xor_sync(0xffffffffu, h[i].y, o);
+                    V t = czero<V>();
+                    if (sv)
+    #pragma unroll
+                        for (int a = 0; a < 2; a++) t = cfmac(Vb[i][a], w[a], t);
+                    h[i] = t;
                 }
-                s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-            }
-#pragma unroll
-            for (int i = 0; i <= j; i++)
-#pragma unroll
-                for (int a = 0; a < 2; a++) w[a] = w[a] - cmul(h[i], Vb[i][a]);
-            double hh = 0.0;
-#pragma unroll
-            for (int i = 0; i <= j; i++) hh += (double)cnorm2(h[i]);
-            double hn2 = (double)s2 - hh;
-            const bool redo = !(hn2 > kCancel * (double)s2);
-            if (__any_sync(0xffffffffu, redo)) {  // warp-uniform: both halves take part in the butterfly
-                const double t = nrm2(w);
-                if (redo) hn2 = t;
-            }
-            double ih = 0.0, hn = 0.0;
-            if (hn2 > 0.0) {
-                ih = rsqrt(hn2);
-                hn = hn2 * ih;
-            }
-            if (arn && hn > 0) {
-#pragma unroll
-                for (int a = 0; a < 2; a++) Vb[j + 1][a] = R(ih) * w[a];
-            }
-            int brk = 0;
-            if (l16 == 0 && arn) {  // column j of the Hessenberg matrix, FGMRES::rotation (src/fgmres.cpp:99-115)
-                V hc[M + 1];
-#pragma unroll
-                for (int i = 0; i <= j; i++) hc[i] = h[i];
-                hc[j + 1] = mkc(R(hn), R(0));
-#pragma unroll
-                for (int i = 0; i < j; i++) {
-                    const V ci = cn[i], si = sn[i];
-                    const V tmp = cmulc(ci, hc[i]) + cmulc(si, hc[i + 1]);
-                    hc[i + 1] = cmul(ci, hc[i + 1]) - cmul(si, hc[i]);
-                    hc[i] = tmp;
+                R s2 = sv ? cnorm2(w[0]) + cnorm2(w[1]) : R(0);
+    #pragma unroll
+                for (int o = 8; o > 0; o >>= 1) {
+    #pragma unroll
+                    for (int i = 0; i <= j; i++) {
+                        h[i].x += __shfl_xor_sync(0xffffffffu, h[i].x, o);
+                        h[i].y += __shfl_xor_sync(0xffffffffu, h[i].y, o);
+                    }
+                    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
                 }
-                const R iden = R(rsqrt((double)cnorm2(hc[j]) + (double)cnorm2(hc[j + 1])));
-                const V s_j = mkc(hc[j + 1].x * iden, hc[j + 1].y * iden);
-                const V c_j = mkc(hc[j].x * iden, hc[j].y * iden);
-                sn[j] = s_j;
-                cn[j] = c_j;
-                const V hd = cmulc(c_j, hc[j]) + cmulc(s_j, hc[j + 1]);
-#pragma unroll
-                for (int i = 0; i < j; i++) H[i * M + j] = hc[i];
-                const R id2 = R(1.0 / (double)cnorm2(hd));
-                dinv[j] = mkc(hd.x * id2, -hd.y * id2);
-                const V gj = gm[j], g1 = -cmul(s_j, gj);
-                gm[j + 1] = g1;
-                gm[j] = cmulc(c_j, gj);
-                brk = ((double)cnorm2(g1) < thr2) ? 1 : 0;
+    #pragma unroll
+                for (int i = 0; i <= j; i++)
+    #pragma unroll
+                    for (int a = 0; a < 2; a++) w[a] = w[a] - cmul(h[i], Vb[i][a]);
+                double hh = 0.0;
+    #pragma unroll
+                for (int i = 0; i <= j; i++) hh += (double)cnorm2(h[i]);
+                double hn2 = (double)s2 - hh;
+                const bool redo = !(hn2 > kCancel * (double)s2);
+                if (__any_sync(0xffffffffu, redo)) {  // warp-uniform: both halves take part in the butterfly
+                    const double t = nrm2(w);
+                    if (redo) hn2 = t;
+                }
+                double ih = 0.0, hn = 0.0;
+                if (hn2 > 0.0) {
+                    ih = rsqrt(hn2);
+                    hn = hn2 * ih;
+                }
+                if (arn && hn > 0) {
+    #pragma unroll
+                    for (int a = 0; a < 2; a++) Vb[j + 1][a] = R(ih) * w[a];
+                }
+                int brk = 0;
+                if (l16 == 0 && arn) {  // column j of the Hessenberg matrix, FGMRES::rotation (src/fgmres.cpp:99-115)
+                    V hc[M + 1];
+    #pragma unroll
+                    for (int i = 0; i <= j; i++) hc[i] = h[i];
+                    hc[j + 1] = mkc(R(hn), R(0));
+    #pragma unroll
+                    for (int i = 0; i < j; i++) {
+                        const V ci = cn[i], si = sn[i];
+                        const V tmp = cmulc(ci, hc[i]) + cmulc(si, hc[i + 1]);
+                        hc[i + 1] = cmul(ci, hc[i + 1]) - cmul(si, hc[i]);
+                        hc[i] = tmp;
+                    }
+                    const R iden = R(rsqrt((double)cnorm2(hc[j]) + (double)cnorm2(hc[j + 1])));
+                    const V s_j = mkc(hc[j + 1].x * iden, hc[j + 1].y * iden);
+                    const V c_j = mkc(hc[j].x * iden, hc[j].y * iden);
+                    sn[j] = s_j;
+                    cn[j] = c_j;
+                    const V hd = cmulc(c_j, hc[j]) + cmulc(s_j, hc[j + 1]);
+    #pragma unroll
+                    for (int i = 0; i < j; i++) H[i * M + j] = hc[i];
+                    const R id2 = R(1.0 / (double)cnorm2(hd));
+                    dinv[j] = mkc(hd.x * id2, -hd.y * id2);
+                    const V gj = gm[j], g1 = -cmul(s_j, gj);
+                    gm[j + 1] = g1;
+                    gm[j] = cmulc(c_j, gj);
+                    brk = ((double)cnorm2(g1) < thr2) ? 1 : 0;
+                }
+                brk = __shfl_sync(0xffffffffu, brk, lead);
+                if (arn && brk) {
+                    maxIt = j + 1;  // not reset at the next restart (src/fgmres.cpp:14,56)
+                    arn = false;
+                }
             }
-            brk = __shfl_sync(0xffffffffu, brk, lead);
-            if (arn && brk) {
-                maxIt = j + 1;  // not reset at the next restart (src/fgmres.cpp:14,56)
-                arn = false;
+            if (l16 == 0 && act) {  // solve_upper_triangular (src/fgmres.cpp:118-128) with the reciprocal diagonal
+                V et[M];
+    #pragma unroll
+                for (int q = M - 1; q >= 0; q--) {
+                    et[q] = czero<V>();
+                    if (q >= maxIt) continue;
+                    V e = gm[q];
+    #pragma unroll
+                    for (int jj = q + 1; jj < M; jj++)
+                        if (jj < maxIt) e = e - cmul(H[q * M + jj], et[jj]);
+                    et[q] = cmul(e, dinv[q]);
+                    eta[q] = et[q];
+                }
+            }
+            __syncwarp();
+            if (act) {
+    #pragma unroll
+                for (int jj = 0; jj < M; jj++) {
+                    if (jj >= maxIt) break;
+                    const V ej = eta[jj];
+    #pragma unroll
+                    for (int a = 0; a < 2; a++) x[a] = cfma(ej, Vb[jj][a], x[a]);
+                }
+            }
+            apply(x);
+    #pragma unroll
+            for (int a = 0; a < 2; a++) w[a] = b[a] - w[a];
+            const double e2 = sqrt(nrm2(w));
+            if (act) {
+                err = e2;
+                if (err < p.tol * norm_b) fin = true;
             }
         }
-        if (l16 == 0 && act) {  // solve_upper_triangular (src/fgmres.cpp:118-128) with the reciprocal diagonal
-            V et[M];
-#pragma unroll
-            for (int q = M - 1; q >= 0; q--) {
-                et[q] = czero<V>();
-                if (q >= maxIt) continue;
-                V e = gm[q];
-#pragma unroll
-                for (int jj = q + 1; jj < M; jj++)
-                    if (jj < maxIt) e = e - cmul(H[q * M + jj], et[jj]);
-                et[q] = cmul(e, dinv[q]);
-                eta[q] = et[q];
+    } else {  // FP32: the control of the reg kernel (FP32 sums, sqrt norms, divisions)
+        for (int kr = 0; kr < p.restarts; kr++) {
+            const bool act = !fin;
+            if (!__any_sync(0xffffffffu, act)) break;
+            bool arn = act;
+            const R inv = R(act ? 1.0 / err : 0.0);
+    #pragma unroll
+            for (int a = 0; a < 2; a++) Vb[0][a] = inv * w[a];
+            if (l16 == 0 && act) gm[0] = mkc(R(err), R(0));
+    #pragma unroll
+            for (int j = 0; j < M; j++) {
+                if (!__any_sync(0xffffffffu, arn)) break;
+                apply(Vb[j]);
+                V h[M];
+    #pragma unroll
+                for (int i = 0; i <= j; i++) {
+                    V t = czero<V>();
+                    if (sv)
+    #pragma unroll
+                        for (int a = 0; a < 2; a++) t = cfmac(Vb[i][a], w[a], t);
+                    h[i] = t;
+                }
+    #pragma unroll
+                for (int o = 8; o > 0; o >>= 1)
+    #pragma unroll
+                    for (int i = 0; i <= j; i++) {
+                        h[i].x += __shfl_xor_sync(0xffffffffu, h[i].x, o);
+                        h[i].y += __shfl_xor_sync(0xffffffffu, h[i].y, o);
+                    }
+    #pragma unroll
+                for (int i = 0; i <= j; i++)
+    #pragma unroll
+                    for (int a = 0; a < 2; a++) w[a] = w[a] - cmul(h[i], Vb[i][a]);
+                const double hn = sqrt(nrm2(w));
+                if (arn && hn > 0) {
+                    const R ih = R(1.0 / hn);
+    #pragma unroll
+                    for (int a = 0; a < 2; a++) Vb[j + 1][a] = ih * w[a];
+                }
+                int brk = 0;
+                if (l16 == 0 && arn) {
+    #pragma unroll
+                    for (int i = 0; i <= j; i++) H[i * M + j] = h[i];
+                    H[(j + 1) * M + j] = mkc(R(hn), R(0));
+                    for (int i = 0; i < j; i++) {  // FGMRES::rotation (src/fgmres.cpp:99-115)
+                        const V hij = H[i * M + j], hi1 = H[(i + 1) * M + j];
+                        const V tmp = cmulc(cn[i], hij) + cmulc(sn[i], hi1);
+                        H[(i + 1) * M + j] = cmul(cn[i], hi1) - cmul(sn[i], hij);
+                        H[i * M + j] = tmp;
+                    }
+                    const V hjj = H[j * M + j], hj1 = H[(j + 1) * M + j];
+                    const R den = sqrt(cnorm2(hjj) + cnorm2(hj1));
+                    sn[j] = mkc(hj1.x / den, hj1.y / den);
+                    cn[j] = mkc(hjj.x / den, hjj.y / den);
+                    H[j * M + j] = cmulc(cn[j], hjj) + cmulc(sn[j], hj1);
+                    H[(j + 1) * M + j] = czero<V>();
+                    gm[j + 1] = -cmul(sn[j], gm[j]);
+                    gm[j] = cmulc(cn[j], gm[j]);
+                    brk = (sqrt(cnorm2(gm[j + 1])) < p.tol * norm_b) ? 1 : 0;
+                }
+                brk = __shfl_sync(0xffffffffu, brk, lead);
+                if (arn && brk) {
+                    maxIt = j + 1;  // not reset at the next restart (src/fgmres.cpp:14,56)
+                    arn = false;
+                }
             }
-        }
-        __syncwarp();
-        if (act) {
-#pragma unroll
-            for (int jj = 0; jj < M; jj++) {
-                if (jj >= maxIt) break;
-                const V ej = eta[jj];
-#pragma unroll
-                for (int a = 0; a < 2; a++) x[a] = cfma(ej, Vb[jj][a], x[a]);
+            if (l16 == 0 && act) {  // solve_upper_triangular (src/fgmres.cpp:118-128)
+                for (int i = maxIt - 1; i >= 0; i--) {
+                    V e = gm[i];
+                    for (int jj = i + 1; jj < maxIt; jj++) e = e - cmul(H[i * M + jj], eta[jj]);
+                    eta[i] = cdiv(e, H[i * M + i]);
+                }
             }
-        }
-        apply(x);
-#pragma unroll
-        for (int a = 0; a < 2; a++) w[a] = b[a] - w[a];
-        const double e2 = sqrt(nrm2(w));
-        if (act) {
-            err = e2;
-            if (err < p.tol * norm_b) fin = true;
+            __syncwarp();
+            if (act) {
+    #pragma unroll
+                for (int jj = 0; jj < M; jj++) {
+                    if (jj >= maxIt) break;
+                    const V ej = eta[jj];
+    #pragma unroll
+                    for (int a = 0; a < 2; a++) x[a] = cfma(ej, Vb[jj][a], x[a]);
+                }
+            }
+            apply(x);
+    #pragma unroll
+            for (int a = 0; a < 2; a++) w[a] = b[a] - w[a];
+            const double e2 = sqrt(nrm2(w));
+            if (act) {
+                err = e2;
+                if (err < p.tol * norm_b) fin = true;
+            }
         }
     }
     // x_B += e  (src/sap.cpp:106-113)
