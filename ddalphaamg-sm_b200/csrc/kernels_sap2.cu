@@ -377,21 +377,72 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
             if (ev) sm.basis[(size_t)r * NE + e] = inv * w[r];
             if (wid == 0 && lane == 0) sm.gm[r * (M + 1)] = make_double2(err[r], 0.0);
         }
-        for (int j = 0; j < M; j++) {
-            __syncthreads();  // v_j complete; warp 0's step j-1 (flags, Hessenberg) visible
-            if (j > 0) {
-                anyarn = false;
+        // warp 0: column jr of every active rhs's Hessenberg matrix, its Givens rotation and break flag
+        // (FGMRES::rotation, src/fgmres.cpp:99-115), from the totals of step jr in ct
+        auto rotate = [&](int jr) {
+            __syncwarp();
+            bool a = false;
+            double nbr = 0.0;
 #pragma unroll
-                for (int r = 0; r < RB; r++) {
-                    if (arn[r] && sm.flag[r * M + j - 1]) {
-                        maxIt[r] = j;  // not reset at the next restart (src/fgmres.cpp:14,56)
-                        arn[r] = false;
-                    }
-                    anyarn |= arn[r];
+            for (int r = 0; r < RB; r++)
+                if (r == lane) {
+                    a = arn[r];
+                    nbr = norm_b[r];
                 }
-                if (!anyarn) break;
+            if (lane < RB && a) {  // lane r: Hessenberg column jr of rhs r
+                const int r = lane;
+                double2* H = sm.H + r * (M + 1) * M;
+                double2* cn = sm.cn + r * M;
+                double2* sn = sm.sn + r * M;
+                double2* gm = sm.gm + r * (M + 1);
+                const double2* ct = sm.ct + r * KS;
+                double2 hc[M + 1];
+#pragma unroll
+                for (int q = 0; q <= M; q++) hc[q] = (q <= jr + 1) ? ct[q] : make_double2(0.0, 0.0);
+#pragma unroll
+                for (int q = 0; q < M; q++) {  // FGMRES::rotation (src/fgmres.cpp:99-115)
+                    if (q >= jr) break;
+                    const double2 tmp = cmulc(cn[q], hc[q]) + cmulc(sn[q], hc[q + 1]);
+                    hc[q + 1] = cmul(cn[q], hc[q + 1]) - cmul(sn[q], hc[q]);
+                    hc[q] = tmp;
+                }
+                double2 hjj = make_double2(0.0, 0.0), hj1 = hjj;
+#pragma unroll
+                for (int q = 0; q < M; q++)
+                    if (q == jr) {
+                        hjj = hc[q];
+                        hj1 = hc[q + 1];
+                    }
+                const double iden = rsqrt(cnorm2(hjj) + cnorm2(hj1));
+                const double2 s_j = make_double2(hj1.x * iden, hj1.y * iden);
+                const double2 c_j = make_double2(hjj.x * iden, hjj.y * iden);
+                sn[jr] = s_j;
+                cn[jr] = c_j;
+                const double2 hd = cmulc(c_j, hjj) + cmulc(s_j, hj1);
+#pragma unroll
+                for (int q = 0; q < M; q++) {
+                    if (q > jr) break;
+                    H[q * M + jr] = (q == jr) ? hd : hc[q];
+                }
+                const double id2 = 1.0 / cnorm2(hd);
+                sm.dinv[r * M + jr] = make_double2(hd.x * id2, -hd.y * id2);
+                const double2 gj = gm[jr];
+                const double2 g1 = -cmul(s_j, gj);
+                gm[jr + 1] = g1;
+                gm[jr] = cmulc(c_j, gj);
+                const double thr = p.tol * nbr;
+                sm.flag[r * M + jr] = (cnorm2(g1) < thr * thr) ? 1 : 0;
             }
+        };
+        // The rotation of step j - 1 runs on warp 0 after its share of step j's application (warp 0's sites
+        // have fewer in-block hops than the busiest warps'), and its break flags are read after step j's
+        // partial-sum barrier: a rhs that met the tolerance at step j - 1 drops out there, its step-j values
+        // unused: the arithmetic of the step-by-step order.
+        int jdone = 0;
+        for (int j = 0; j < M; j++) {
+            __syncthreads();  // v_j complete
             apply(sm.basis + (size_t)j * NE * RB, false);  // w = D_B V_j
+            if (j > 0 && wid == 0) rotate(j - 1);
             // classical Gram-Schmidt coefficients <w, V_i>, i <= j, and ||w||^2 (slot j + 1)
             // (selects on j, not a store at index j + 1, which would put the values in local memory)
             {
@@ -412,7 +463,19 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
                 else if (j == 3) SAP2_PARTIAL(5, gs);
                 else SAP2_PARTIAL(6, gs);
             }
-            __syncthreads();  // partial sums visible
+            __syncthreads();  // partial sums visible; warp 0's step j - 1 (flags, Hessenberg) visible
+            if (j > 0) {
+                anyarn = false;
+#pragma unroll
+                for (int r = 0; r < RB; r++) {
+                    if (arn[r] && sm.flag[r * M + j - 1]) {
+                        maxIt[r] = j;  // not reset at the next restart (src/fgmres.cpp:14,56)
+                        arn[r] = false;
+                    }
+                    anyarn |= arn[r];
+                }
+                if (!anyarn) break;
+            }
             const int dbuf = rbuf;
             rbuf ^= 1;
             // ||w - V h||^2 = ||w||^2 - sum |h_i|^2 for orthonormal V: no second reduction, unless the
@@ -474,62 +537,9 @@ __global__ void __launch_bounds__(MAXT, 1) sap_block2_kernel(Geom g, const V* __
                 if (arn[r] && hn[r] > 0 && ev) sm.basis[((size_t)(j + 1) * RB + r) * NE + e] = R(ihn[r]) * w[r];
                 if (wid == 0 && lane == 0) sm.ct[r * KS + j + 1] = make_double2(hn[r], 0.0);
             }
-            if (wid == 0) {
-                __syncwarp();
-                bool a = false;
-                double nbr = 0.0;
-#pragma unroll
-                for (int r = 0; r < RB; r++)
-                    if (r == lane) {
-                        a = arn[r];
-                        nbr = norm_b[r];
-                    }
-                if (lane < RB && a) {  // lane r: Hessenberg column j of rhs r
-                    const int r = lane;
-                    double2* H = sm.H + r * (M + 1) * M;
-                    double2* cn = sm.cn + r * M;
-                    double2* sn = sm.sn + r * M;
-                    double2* gm = sm.gm + r * (M + 1);
-                    const double2* ct = sm.ct + r * KS;
-                    double2 hc[M + 1];
-#pragma unroll
-                    for (int q = 0; q <= M; q++) hc[q] = (q <= j + 1) ? ct[q] : make_double2(0.0, 0.0);
-#pragma unroll
-                    for (int q = 0; q < M; q++) {  // FGMRES::rotation (src/fgmres.cpp:99-115)
-                        if (q >= j) break;
-                        const double2 tmp = cmulc(cn[q], hc[q]) + cmulc(sn[q], hc[q + 1]);
-                        hc[q + 1] = cmul(cn[q], hc[q + 1]) - cmul(sn[q], hc[q]);
-                        hc[q] = tmp;
-                    }
-                    double2 hjj = make_double2(0.0, 0.0), hj1 = hjj;
-#pragma unroll
-                    for (int q = 0; q < M; q++)
-                        if (q == j) {
-                            hjj = hc[q];
-                            hj1 = hc[q + 1];
-                        }
-                    const double iden = rsqrt(cnorm2(hjj) + cnorm2(hj1));
-                    const double2 s_j = make_double2(hj1.x * iden, hj1.y * iden);
-                    const double2 c_j = make_double2(hjj.x * iden, hjj.y * iden);
-                    sn[j] = s_j;
-                    cn[j] = c_j;
-                    const double2 hd = cmulc(c_j, hjj) + cmulc(s_j, hj1);
-#pragma unroll
-                    for (int q = 0; q < M; q++) {
-                        if (q > j) break;
-                        H[q * M + j] = (q == j) ? hd : hc[q];
-                    }
-                    const double id2 = 1.0 / cnorm2(hd);
-                    sm.dinv[r * M + j] = make_double2(hd.x * id2, -hd.y * id2);
-                    const double2 gj = gm[j];
-                    const double2 g1 = -cmul(s_j, gj);
-                    gm[j + 1] = g1;
-                    gm[j] = cmulc(c_j, gj);
-                    const double thr = p.tol * nbr;
-                    sm.flag[r * M + j] = (cnorm2(g1) < thr * thr) ? 1 : 0;
-                }
-            }
+            jdone = j + 1;
         }
+        if (jdone == M && wid == 0) rotate(M - 1);  // the last step's column
         __syncthreads();  // the last step's Hessenberg column and rotations visible
         // solve_upper_triangular (src/fgmres.cpp:118-128), repeated by every thread; x += sum eta_j V_j
 #pragma unroll
